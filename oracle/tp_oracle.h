@@ -1,0 +1,130 @@
+/*
+ * CPU oracle for the Toothpaste blind-rotation hot path (TEST INFRASTRUCTURE).
+ *
+ * This is a plain-C restatement of the reference library's algorithms over the
+ * Goldilocks prime p = 2^64 - 2^32 + 1. It exists only to check the CUDA path:
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+ * it, and never as the thing that is measured or shipped.
+ *
+ * Parity pins: every routine is checked against the reference itself, compiled
+ * from its own sources by oracle/Makefile into oracle/_ref/, through the golden
+ * fixtures under tests/golden/ (generated by tests/golden/make_golden.py).
+ *
+ * Each function cites the reference file:line it restates (paths relative to
+ * the reference project root).
+ */
+#ifndef TP_ORACLE_H
+#define TP_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TPO_P 0xFFFFFFFF00000001ULL
+
+/* ---- seeded sampler (project-defined stand-in for the OpenFHE samplers) ----
+ * Stream: splitmix64. uniform(q): rejection sampling on the smallest all-ones
+ * mask >= q-1. gaussian(std, q): Box-Muller (first output only), rounded to the
+ * nearest integer (ties away from zero), returned mod q; std == 0 gives 0 and
+ * draws nothing. The oracle/shim/openfhe.h shim draws in exactly the same way,
+ * so a reference build seeded identically produces identical keys. */
+typedef struct { uint64_t s; } tpo_rng;
+void tpo_rng_seed(tpo_rng* r, uint64_t seed);
+uint64_t tpo_next64(tpo_rng* r);
+uint64_t tpo_uniform(tpo_rng* r, uint64_t q);
+uint64_t tpo_gaussian(tpo_rng* r, double std_dev, uint64_t q);
+
+/* ---- Goldilocks scalar arithmetic (lib/include/backend/solinas_internal.h:39-113) */
+uint64_t tpo_add(uint64_t a, uint64_t b);
+uint64_t tpo_sub(uint64_t a, uint64_t b);
+uint64_t tpo_mul(uint64_t a, uint64_t b);
+uint64_t tpo_pow(uint64_t b, uint64_t e);
+uint64_t tpo_inv(uint64_t a);
+
+/* ---- negacyclic NTT (lib/src/backend/solinas.cpp:168-313) ----
+ * Forward: natural-order coefficients -> evaluations in bit-reversed order,
+ * out[k] = a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N). Backward includes 1/N.
+ * In-place allowed. Returns 0, or -1 for an unsupported N. */
+int tpo_ntt_forward(uint64_t N, uint64_t* out, const uint64_t* in);
+int tpo_ntt_backward(uint64_t N, uint64_t* out, const uint64_t* in);
+uint64_t tpo_psi(uint64_t N);
+
+/* ---- gadget decomposition, coefficient domain (lib/include/static/gadget_decomp.h) ----
+ * out is digits x N, digit-major. Signed: :16-28 + :156-205. Unsigned (the
+ * binary-CGGI rule of lib/src/operators/mux_operator.cpp:24-26,46-69). */
+void tpo_signed_digits(uint64_t* out, const uint64_t* in, uint64_t N, uint64_t digits, uint64_t basis_log2);
+void tpo_unsigned_digits(uint64_t* out, const uint64_t* in, uint64_t N, uint64_t digits, uint64_t basis_log2);
+
+/* ---- encryption / key generation (lib/src/base_crypto.cpp:27-97,137-155) ---- */
+void tpo_make_rlwe(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const uint64_t* msg,
+                   const uint64_t* sk_ntt, int msg_is_ntt);
+void tpo_make_rgsw(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const uint64_t* msg,
+                   const uint64_t* sk_ntt, uint64_t basis, uint64_t digits, int msg_is_ntt);
+void tpo_phase_rlwe(uint64_t N, uint64_t* out, const uint64_t* rlwe, const uint64_t* sk_ntt);
+
+enum { TPO_CGGI_BINARY = 0, TPO_CGGI_TERNARY = 1, TPO_BMMP_BINARY = 2 };
+
+/* Words of the blind-rotation key in the reference layout (m_brk). */
+uint64_t tpo_brk_words(int variant, uint64_t N, uint64_t n, uint64_t digits);
+
+/* CGGI KeyGenBinary / KeyGenTernary (lib/src/operators/cggi_blind_rotation.cpp:264-311)
+ * and BMMP KeyGenBinary (lib/src/operators/bmmp_blind_rotation.cpp:229-262). */
+void tpo_br_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                   double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk);
+
+/* BlindRotate: CGGI (cggi_blind_rotation.cpp:236-262, 313-472) and BMMP
+ * (bmmp_blind_rotation.cpp:325-335, 280-323, 354-419; MultiMux mux_operator.cpp:204-294).
+ * result may equal acc. Returns 0, or -1 on bad parameters. */
+int tpo_blind_rotate(int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                     const uint64_t* brk, uint64_t* result, const uint64_t* lwe, const uint64_t* acc,
+                     int out_coef);
+
+/* Same, for `count` independent rotations on `threads` POSIX threads
+ * (lwe stride n+1, acc/result stride 2N). Used as the CPU baseline. */
+int tpo_blind_rotate_many(int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                          const uint64_t* brk, uint64_t* results, const uint64_t* lwes,
+                          const uint64_t* accs, uint64_t count, int out_coef, int threads);
+
+/* ---- key switching (lib/src/operators/rlwe_conversion.cpp:187-249,
+ *      lib/src/operators/lwe_conversion.cpp:174-239) ---- */
+void tpo_rlwe_ks_keygen(tpo_rng* r, uint64_t N, uint64_t basis_log2, uint64_t digits, double std_dev,
+                        const uint64_t* source_key, const uint64_t* target_key, uint64_t* ksk);
+/* out -= sum_j NTT(d_j(in.A)) * ksk_j ; out.B += in.B. in = [A coef | B ntt]. */
+void tpo_rlwe_ks(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* ksk,
+                 uint64_t* out, const uint64_t* in);
+void tpo_lwe_ks_keygen(tpo_rng* r, uint64_t q, uint64_t n_in, uint64_t n_out, uint64_t basis_log2,
+                       uint64_t digits, double std_dev, const uint64_t* source_key,
+                       const uint64_t* target_key, uint64_t* ksk);
+void tpo_lwe_ks(uint64_t q, uint64_t n_in, uint64_t n_out, uint64_t basis_log2, uint64_t digits,
+                const uint64_t* ksk, uint64_t* out, const uint64_t* in);
+void tpo_make_lwe(tpo_rng* r, uint64_t q, uint64_t n, double std_dev, uint64_t* out, uint64_t msg,
+                  const uint64_t* secret);
+
+/* ---- automorphisms and packing (lib/src/utils/math_utils.cpp:70-85,
+ *      lib/src/operators/automorphism_evaluation.cpp:43-63,150-206,
+ *      lib/src/operators/lwe_to_rlwe_packing.cpp:46-58,129-251) ---- */
+void tpo_negacyclic_automorphism(uint64_t* out, const uint64_t* in, uint64_t index, uint64_t N);
+void tpo_auto_keygen(tpo_rng* r, uint64_t N, uint64_t basis_log2, uint64_t digits, double std_dev,
+                     uint64_t index, const uint64_t* rlwe_key, uint64_t* ksk);
+/* out (NTT domain) = KS(aut_index(in)); in is [A coef | B coef]. out must be pre-zeroed. */
+void tpo_auto_eval(uint64_t N, uint64_t basis_log2, uint64_t digits, uint64_t index,
+                   const uint64_t* ksk, uint64_t* out, const uint64_t* in);
+/* Keys for indices 2^j+1, j = 1..logN, each 2*N*digits words, concatenated. */
+void tpo_pack_keygen(tpo_rng* r, uint64_t N, uint64_t basis_log2, uint64_t digits, double std_dev,
+                     const uint64_t* rlwe_key, uint64_t* keys);
+/* Pack len LWEs (each N+1 words) into one RLWE [A|B] coefficient domain. */
+int tpo_pack(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* keys,
+             uint64_t* out, const uint64_t* in, uint64_t len);
+
+/* SampleExtract (lib/include/static/sample_extraction.h:20-36): writes nothing
+ * where the source coefficient is zero (the caller pre-zeroes). */
+void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index, uint64_t N);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
