@@ -1,0 +1,114 @@
+"""Python mirror of the reference's blind-rotation operator API over the C ABI.
+
+Mirrors CGGIBlindRotationContext / BMMPBlindRotationContext and
+BlindRotator::BlindRotate (lib/include/interfaces/blindrotation_operator.h:183-212
+of the reference) for tests, the benchmark and the serving loop. Key
+generation stays with the caller (the C++ adapters in fhetoothpaste_b200/host/
+run it on the host); this class takes the generated key words.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as nat
+
+BINARY, TERNARY = "binary", "ternary"
+
+
+class BlindRotationContext:
+    """Parameters of one blind-rotation operator (CGGI binary/ternary or BMMP)."""
+
+    def __init__(self, variant: int, ring_dim: int, lwe_dim: int, basis: int, digits: int,
+                 modulus: int = nat.GOLDILOCKS, std: float = 0.0):
+        self.variant = int(variant)
+        self.modulus = int(modulus)
+        self.N = int(ring_dim)
+        self.n = int(lwe_dim)
+        self.basis = int(basis)
+        self.basis_log2 = self.basis.bit_length() - 1
+        self.digits = int(digits)
+        self.std = float(std)
+
+    def params(self) -> nat.BrParams:
+        return nat.BrParams(self.variant, self.modulus, self.N, self.n, self.basis, self.digits)
+
+    def key_words(self) -> int:
+        g = {nat.TP_BR_CGGI_BINARY: 1, nat.TP_BR_CGGI_TERNARY: 2, nat.TP_BR_BMMP_BINARY: 3}[self.variant]
+        groups = self.n // 2 if self.variant == nat.TP_BR_BMMP_BINARY else self.n
+        return groups * g * 4 * self.N * self.digits
+
+
+class GpuBlindRotator:
+    """A blind-rotation key resident on one GPU plus its launch context."""
+
+    def __init__(self, ctx: BlindRotationContext, brk: np.ndarray, device: int = 0):
+        L = nat.lib()
+        self.ctx = ctx
+        self.device = device
+        h = ctypes.c_void_p()
+        prm = ctx.params()
+        nat.check(L.tp_br_create(ctypes.byref(prm), device, ctypes.byref(h)))
+        self._h = h
+        brk = np.ascontiguousarray(brk, dtype=np.uint64)
+        nat.check(L.tp_br_upload_key(self._h, nat.ptr(brk), brk.size))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            nat.lib().tp_br_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    # BlindRotator::BlindRotate(result, lwe, accumulator, output_as_coefficients)
+    def BlindRotate(self, result: np.ndarray, lwe: np.ndarray, acc: np.ndarray,
+                    output_as_coefficients: bool = False) -> None:
+        for a, w in ((result, 2 * self.ctx.N), (lwe, self.ctx.n + 1), (acc, 2 * self.ctx.N)):
+            if a.dtype != np.uint64 or not a.flags.c_contiguous or a.size < w:
+                raise ValueError("buffers must be contiguous uint64 arrays of the operator's sizes")
+        nat.check(nat.lib().tp_br_blind_rotate(self._h, nat.ptr(result), nat.ptr(lwe), nat.ptr(acc),
+                                               int(bool(output_as_coefficients))))
+
+    def blind_rotate_batch_host(self, lwes: np.ndarray, accs: np.ndarray, out_coef: bool = False,
+                                stream: int | None = None) -> np.ndarray:
+        """Rotates every row of `lwes` (batch x (n+1)); `accs` is batch x 2N or one 2N row."""
+        lwes = np.ascontiguousarray(lwes, dtype=np.uint64)
+        accs = np.ascontiguousarray(accs, dtype=np.uint64)
+        batch = lwes.shape[0]
+        shared = accs.ndim == 1
+        out = np.empty((batch, 2 * self.ctx.N), dtype=np.uint64)
+        nat.check(nat.lib().tp_br_blind_rotate_batch_host(
+            self._h, batch, nat.ptr(out), nat.ptr(lwes), lwes.shape[1], nat.ptr(accs),
+            0 if shared else accs.shape[1], int(bool(out_coef)), stream))
+        nat.check(nat.lib().tp_br_check(self._h, stream))
+        return out
+
+    def blind_rotate_batch(self, results_ptr: int, lwes_ptr: int, lwe_stride: int, accs_ptr: int,
+                           acc_stride: int, batch: int, out_coef: bool = False, stream: int | None = None) -> None:
+        """Device-pointer batch launch (asynchronous on `stream`)."""
+        nat.check(nat.lib().tp_br_blind_rotate_batch(self._h, batch, results_ptr, lwes_ptr, lwe_stride, accs_ptr,
+                                                     acc_stride, int(bool(out_coef)), stream))
+
+    def check(self, stream: int | None = None) -> None:
+        nat.check(nat.lib().tp_br_check(self._h, stream))
+
+
+def ntt_forward(ring_dim: int, count: int, out_ptr: int, in_ptr: int, stream: int | None = None) -> None:
+    nat.check(nat.lib().tp_ntt_forward(ring_dim, count, out_ptr, in_ptr, stream))
+
+
+def ntt_backward(ring_dim: int, count: int, out_ptr: int, in_ptr: int, stream: int | None = None) -> None:
+    nat.check(nat.lib().tp_ntt_backward(ring_dim, count, out_ptr, in_ptr, stream))
+
+
+def sample_extract_batch(ring_dim: int, batch: int, out_ptr: int, rlwe_ptr: int, stream: int | None = None) -> None:
+    nat.check(nat.lib().tp_sample_extract_batch(ring_dim, batch, out_ptr, rlwe_ptr, stream))

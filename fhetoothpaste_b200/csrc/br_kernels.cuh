@@ -1,0 +1,262 @@
+// Batched blind rotation (CGGI binary / CGGI ternary / BMMP) for sm_100a.
+//
+// One thread block rotates one ciphertext at a time with T = N/8 threads and
+// loops over the batch (persistent grid, a few blocks per SM). The RLWE
+// accumulator [A | B] lives in shared memory, in the NTT domain, for all n
+// CMux iterations. Per iteration the block runs the reference's CMux with the
+// same residues (cggi_blind_rotation.cpp:313-472, bmmp_blind_rotation.cpp:354-419,
+// mux_operator.cpp:30-294):
+//   backward NTT of A and B -> gadget digits -> forward NTT of each digit ->
+//   multiply-accumulate against the iteration's key rows -> monomial weights ->
+//   accumulator update.
+// Keys are streamed from HBM through L2: all blocks walk the iterations in the
+// same order at about the same pace, so each key row is fetched from HBM about
+// once per wave of blocks and served from L2 to the rest of the batch.
+//
+// Key layout on the device (built by key_relayout_kernel from the reference's
+// m_brk): per iteration group `it` (an LWE index for CGGI, a pair for BMMP),
+// per gadget row r (0..2l-1; rows < l multiply digits of A, rows >= l digits
+// of B), the C = 2*G components (G RGSWs x {A, B} halves) of slot k = 8t + 2jp
+// + e sit at  ((c*4 + jp)*T + t)*2 + e,  so each thread's 16-byte loads are
+// contiguous across the warp.
+#pragma once
+
+#include "gl_arith.cuh"
+#include "ntt_block.cuh"
+
+namespace tp {
+
+enum BrVariant : int { kCggiBinary = 0, kCggiTernary = 1, kBmmpBinary = 2 };
+
+// RGSWs consumed per iteration group.
+__host__ __device__ constexpr int br_rgsw_per_group(int variant) {
+    return variant == kCggiBinary ? 1 : (variant == kCggiTernary ? 2 : 3);
+}
+
+struct BrKernelParams {
+    const uint64_t* key;      // device layout, see above
+    const uint64_t* tw_fwd;   // N: psi^brv(k)
+    const uint64_t* tw_inv;   // N: psi^-brv(k)
+    const uint64_t* psi_pow;  // 2N: psi^k
+    const uint64_t* lwes;
+    uint64_t lwe_stride;
+    const uint64_t* accs;
+    uint64_t acc_stride;
+    uint64_t* out;
+    uint64_t batch;
+    uint32_t n;
+    uint32_t digits;
+    uint32_t out_coef;
+    uint64_t n_inv;           // N^-1 mod p
+    uint64_t corr;            // signed-decomposition corrector (canonical)
+    uint32_t dshift[8];       // per-digit shift
+    uint64_t dmask[8];        // per-digit mask
+    uint64_t ddelta[8];       // per-digit offset subtracted (signed) or 0 (unsigned)
+    unsigned int* err;        // bit 0: an LWE word was outside [0, 2N)
+};
+
+// Shared memory of one block, in words: twiddles (2N), two exchange buffers
+// (2N), accumulator (2N), LWE vector (n+1, rounded up to an even count).
+__host__ __device__ constexpr size_t br_smem_words(int N, uint32_t n) { return 6 * (size_t)N + ((n + 2) & ~1u); }
+
+// Exponent e_k = 2 brv(k) + 1 of slot k: NTT(X^a)[k] = psi^(e_k a mod 2N).
+template <int LOGN>
+__device__ __forceinline__ uint32_t slot_exponent(int k) {
+    return 2u * (__brev((uint32_t)k) >> (32 - LOGN)) + 1u;
+}
+
+template <int LOGN>
+__device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, uint32_t ek, uint32_t a) {
+    return __ldg(psi_pow + ((ek * a) & (2u * (1u << LOGN) - 1u)));
+}
+
+// Resident blocks per SM the kernel is compiled for (register budget
+// 65536 / (T * blocks)); N = 4096 needs 200 KB of shared memory, so one block.
+__host__ __device__ constexpr int br_min_blocks(int logn, int variant) {
+    return (logn >= 12 || variant == kBmmpBinary) ? 1 : 2;
+}
+
+template <int LOGN, int VARIANT>
+__global__ void __launch_bounds__((1 << LOGN) / 8, br_min_blocks(LOGN, VARIANT))
+br_kernel(const BrKernelParams prm) {
+    using SH = NttShape<LOGN>;
+    constexpr int N = SH::N;
+    constexpr int T = SH::T;
+    constexpr int G = br_rgsw_per_group(VARIANT);
+    constexpr int C = 2 * G;                 // key components per slot
+    constexpr uint32_t MASK2N = 2u * N - 1u;
+    constexpr bool SIGNED = VARIANT != kCggiBinary;
+
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* tw_f = smem;
+    uint64_t* tw_i = smem + N;
+    uint64_t* xbuf0 = smem + 2 * N;
+    uint64_t* xbuf1 = smem + 3 * N;
+    uint64_t* acc = smem + 4 * N;            // [(h*8 + j)*T + t]
+    uint64_t* lwe_s = smem + 6 * N;
+
+    const int t = threadIdx.x;
+    const uint32_t n = prm.n;
+    const uint32_t L = prm.digits;
+
+    for (int i = t; i < N; i += T) {
+        tw_f[i] = prm.tw_fwd[i];
+        tw_i[i] = prm.tw_inv[i];
+    }
+
+    uint32_t ek[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ek[j] = slot_exponent<LOGN>(8 * t + j);
+
+    int sel = 0;
+    auto xb = [&]() -> uint64_t* {
+        uint64_t* b = sel ? xbuf1 : xbuf0;
+        sel ^= 1;
+        return b;
+    };
+
+    for (uint64_t b = blockIdx.x; b < prm.batch; b += gridDim.x) {
+        __syncthreads();  // previous ciphertext done with lwe_s / acc
+        const uint64_t* lwe = prm.lwes + b * prm.lwe_stride;
+        bool bad = false;
+        for (uint32_t i = t; i <= n; i += T) {
+            uint64_t v = lwe[i];
+            bad |= v > MASK2N;
+            lwe_s[i] = v & MASK2N;
+        }
+        if (bad) atomicOr(prm.err, 1u);
+        __syncthreads();
+
+        // Prologue: acc = NTT(acc_in) * X^b   (cggi_blind_rotation.cpp:242,333-358)
+        {
+            const uint64_t* ain = prm.accs + b * prm.acc_stride;
+            const uint32_t bb = (uint32_t)lwe_s[n];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t x[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) x[j] = ain[h * N + t + j * T];
+                ntt_forward<LOGN>(x, t, xb(), tw_f);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[(h * 8 + j) * T + t] = gl_mul(x[j], mono<LOGN>(prm.psi_pow, ek[j], bb));
+            }
+        }
+
+        const uint32_t step = VARIANT == kBmmpBinary ? 2 : 1;
+        for (uint32_t i = 0; i < n; i += step) {
+            uint32_t a0 = (uint32_t)lwe_s[i];
+            uint32_t a1 = 0;
+            if constexpr (VARIANT == kBmmpBinary) {
+                a0 = (2u * N - a0) & MASK2N;                         // X^{-a} (bmmp_blind_rotation.cpp:403-404)
+                a1 = (2u * N - (uint32_t)lwe_s[i + 1]) & MASK2N;
+            } else {
+                if (a0 == 0) continue;                               // cggi_blind_rotation.cpp:369-370
+            }
+            const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
+
+            uint64_t o[C][8];
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) o[c][j] = 0;
+
+            // Binary CGGI decomposes (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the
+            // other variants decompose acc itself (mux_operator.cpp:174-177, 219-224).
+            uint64_t mpos[8];
+            if constexpr (VARIANT == kCggiBinary) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) mpos[j] = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], 2u * N - a0), 1);
+            }
+
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint64_t cx[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    cx[j] = acc[(h * 8 + j) * T + t];
+                    if constexpr (VARIANT == kCggiBinary) cx[j] = gl_mul(cx[j], mpos[j]);
+                }
+                ntt_backward_unscaled<LOGN>(cx, t, xb(), tw_i);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    cx[j] = gl_mul(cx[j], prm.n_inv);
+                    if constexpr (SIGNED) cx[j] = gl_add(cx[j], prm.corr);
+                }
+                for (uint32_t d = 0; d < L; ++d) {
+                    const uint32_t sh = prm.dshift[d];
+                    const uint64_t mk = prm.dmask[d];
+                    const uint64_t dl = prm.ddelta[d];
+                    uint64_t x[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint64_t raw = (cx[j] >> sh) & mk;
+                        x[j] = SIGNED ? gl_sub(raw, dl) : raw;
+                    }
+                    ntt_forward<LOGN>(x, t, xb(), tw_f);
+                    const uint64_t* kr = kit + (uint64_t)(h * L + d) * (N * C);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+#pragma unroll
+                        for (int jp = 0; jp < 4; ++jp) {
+                            const ulonglong2 kv =
+                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
+                            o[c][2 * jp] = gl_add(o[c][2 * jp], gl_mul(x[2 * jp], kv.x));
+                            o[c][2 * jp + 1] = gl_add(o[c][2 * jp + 1], gl_mul(x[2 * jp + 1], kv.y));
+                        }
+                    }
+                }
+            }
+
+            // Accumulator update.
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                uint64_t ua = acc[j * T + t];
+                uint64_t ub = acc[(8 + j) * T + t];
+                if constexpr (VARIANT == kCggiBinary) {
+                    // acc += ExtProd (mux_operator.cpp:151)
+                    ua = gl_add(ua, o[0][j]);
+                    ub = gl_add(ub, o[1][j]);
+                } else if constexpr (VARIANT == kCggiTernary) {
+                    // acc += (X^{-a}-1) ExtProd(lo) + (X^{a}-1) ExtProd(hi) (mux_operator.cpp:188-200)
+                    const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], 2u * N - a0), 1);
+                    const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], a0), 1);
+                    ua = gl_add(ua, gl_add(gl_mul(o[0][j], mp), gl_mul(o[2][j], mn)));
+                    ub = gl_add(ub, gl_add(gl_mul(o[1][j], mp), gl_mul(o[3][j], mn)));
+                } else {
+                    // weights X^{a0}-1, X^{a1}-1, X^{a0+a1}-X^{a0}-X^{a1}+1
+                    // (bmmp_blind_rotation.cpp:280-323; MultiMux mux_operator.cpp:274-291)
+                    const uint64_t m0 = mono<LOGN>(prm.psi_pow, ek[j], a0);
+                    const uint64_t m1 = mono<LOGN>(prm.psi_pow, ek[j], a1);
+                    const uint64_t m2 = mono<LOGN>(prm.psi_pow, ek[j], (a0 + a1) & MASK2N);
+                    const uint64_t w0 = gl_sub(m0, 1);
+                    const uint64_t w1 = gl_sub(m1, 1);
+                    const uint64_t w2 = gl_add(gl_sub(gl_sub(m2, m0), m1), 1);
+                    ua = gl_add(ua, gl_add(gl_add(gl_mul(o[0][j], w0), gl_mul(o[2][j], w1)), gl_mul(o[4][j], w2)));
+                    ub = gl_add(ub, gl_add(gl_add(gl_mul(o[1][j], w0), gl_mul(o[3][j], w1)), gl_mul(o[5][j], w2)));
+                }
+                acc[j * T + t] = ua;
+                acc[(8 + j) * T + t] = ub;
+            }
+        }
+
+        // Epilogue (cggi_blind_rotation.cpp:258-261).
+        uint64_t* res = prm.out + b * (2ull * N);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint64_t x[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) x[j] = acc[(h * 8 + j) * T + t];
+            if (prm.out_coef) {
+                ntt_backward_unscaled<LOGN>(x, t, xb(), tw_i);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) res[h * N + t + j * T] = gl_mul(x[j], prm.n_inv);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    *reinterpret_cast<ulonglong2*>(res + h * N + 8 * t + 2 * c) = make_ulonglong2(x[2 * c], x[2 * c + 1]);
+            }
+        }
+    }
+}
+
+}  // namespace tp

@@ -1,0 +1,449 @@
+// C ABI of the blind-rotation engine (include/toothpaste_gpu.h): contexts,
+// key upload, launches, error reporting.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/toothpaste_gpu.h"
+#include "br_kernels.cuh"
+#include "dispatch.h"
+#include "misc_kernels.cuh"
+#include "util_kernels.cuh"
+
+namespace {
+
+using u128 = unsigned __int128;
+constexpr uint64_t kP = 0xFFFFFFFF00000001ull;
+
+thread_local std::string g_err;
+
+tp_status fail(tp_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define TP_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(e_ == cudaErrorMemoryAllocation ? TP_ERR_OOM : TP_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                   \
+    } while (0)
+
+// ---- host Goldilocks arithmetic (tables only) ----
+uint64_t hmul(uint64_t a, uint64_t b) { return (uint64_t)(((u128)a * b) % kP); }
+uint64_t hpow(uint64_t b, uint64_t e) {
+    uint64_t r = 1;
+    b %= kP;
+    while (e) {
+        if (e & 1) r = hmul(r, b);
+        b = hmul(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+uint64_t hinv(uint64_t a) { return hpow(a, kP - 2); }
+uint32_t brv(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int i = 0; i < bits; ++i) {
+        r = (r << 1) | (x & 1);
+        x >>= 1;
+    }
+    return r;
+}
+int ilog2(uint64_t x) {
+    int r = 0;
+    while ((1ull << r) < x) ++r;
+    return r;
+}
+
+// Per-(device, N) tables: forward/inverse twiddles psi^(+-brv(k)) and psi^k, k < 2N.
+struct Tables {
+    int device = -1;
+    int logn = 0;
+    uint64_t* tw_fwd = nullptr;
+    uint64_t* tw_inv = nullptr;
+    uint64_t* psi_pow = nullptr;
+    uint64_t n_inv = 0;
+};
+
+std::mutex g_tab_mu;
+std::vector<Tables*> g_tables;
+
+tp_status get_tables(int device, int logn, const Tables** out) {
+    std::lock_guard<std::mutex> lk(g_tab_mu);
+    for (auto* t : g_tables)
+        if (t->device == device && t->logn == logn) {
+            *out = t;
+            return TP_OK;
+        }
+    const uint64_t N = 1ull << logn;
+    // psi = 7^((p-1)/2N) (lib/src/backend/solinas.cpp:176)
+    const uint64_t psi = hpow(7, (kP - 1) >> (logn + 1));
+    const uint64_t psi_inv = hinv(psi);
+    std::vector<uint64_t> pw(2 * N), pwi(N), tf(N), ti(N);
+    pw[0] = 1;
+    for (uint64_t i = 1; i < 2 * N; ++i) pw[i] = hmul(pw[i - 1], psi);
+    pwi[0] = 1;
+    for (uint64_t i = 1; i < N; ++i) pwi[i] = hmul(pwi[i - 1], psi_inv);
+    for (uint64_t k = 0; k < N; ++k) {
+        tf[k] = pw[brv((uint32_t)k, logn)];
+        ti[k] = pwi[brv((uint32_t)k, logn)];
+    }
+    auto* t = new Tables();
+    t->device = device;
+    t->logn = logn;
+    t->n_inv = hinv(N);
+    cudaError_t e = cudaMalloc(&t->tw_fwd, N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&t->tw_inv, N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&t->psi_pow, 2 * N * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(t->tw_fwd, tf.data(), N * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->tw_inv, ti.data(), N * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->psi_pow, pw.data(), 2 * N * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(t->tw_fwd);
+        cudaFree(t->tw_inv);
+        cudaFree(t->psi_pow);
+        delete t;
+        return fail(e == cudaErrorMemoryAllocation ? TP_ERR_OOM : TP_ERR_CUDA, "table upload: %s",
+                    cudaGetErrorString(e));
+    }
+    g_tables.push_back(t);
+    *out = t;
+    return TP_OK;
+}
+
+int sm_count(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    return v > 0 ? v : 1;
+}
+
+}  // namespace
+
+struct tp_br_ctx {
+    tp_br_params prm{};
+    int device = 0;
+    int logn = 0;
+    int G = 1;                    // RGSWs per iteration group
+    uint64_t groups = 0;          // iteration groups (n, or n/2 for BMMP)
+    uint64_t key_words = 0;
+    const Tables* tab = nullptr;
+    uint64_t* key = nullptr;      // device layout
+    bool key_ready = false;
+    unsigned int* err = nullptr;  // device error word
+    tp::BrKernelParams kp{};
+    const void* kernel = nullptr;
+    size_t smem_bytes = 0;
+    int grid_cap = 1;             // resident blocks on the device
+    // workspace for host-pointer calls
+    uint64_t* ws = nullptr;
+    uint64_t ws_words = 0;
+    std::mutex mu;                // serializes host-pointer calls on one context
+};
+
+extern "C" {
+
+const char* tp_last_error(void) { return g_err.c_str(); }
+
+const char* tp_version(void) { return "toothpaste-b200 0.1 (sm_100a)"; }
+
+tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
+    if (!p || !out) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    if (p->modulus != kP) return fail(TP_ERR_PARAM, "modulus must be the Goldilocks prime 2^64-2^32+1");
+    if (p->variant < 0 || p->variant > 2) return fail(TP_ERR_PARAM, "unknown variant %d", p->variant);
+    const uint64_t N = p->ring_dim;
+    if (N < 128 || N > 4096 || (N & (N - 1))) return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (p->lwe_dim == 0) return fail(TP_ERR_PARAM, "lwe_dim must be positive");
+    if (p->variant == TP_BR_BMMP_BINARY && (p->lwe_dim % 2)) return fail(TP_ERR_PARAM, "BMMP needs an even lwe_dim");
+    if (p->basis < 2 || (p->basis & (p->basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
+    const int beta = ilog2(p->basis);
+    if (beta > 30) return fail(TP_ERR_PARAM, "basis above 2^30 is not supported");
+    const int max_digits = (64 + beta - 1) / beta;
+    if (p->digits < 1 || p->digits > 8 || (int)p->digits > max_digits)
+        return fail(TP_ERR_PARAM, "digits must be in [1, min(8, ceil(64/beta))]");
+
+    auto* c = new tp_br_ctx();
+    c->prm = *p;
+    c->device = device;
+    c->logn = ilog2(N);
+    c->G = tp::br_rgsw_per_group(p->variant);
+    c->groups = p->variant == TP_BR_BMMP_BINARY ? p->lwe_dim / 2 : p->lwe_dim;
+    c->key_words = c->groups * (uint64_t)c->G * 4 * N * p->digits;
+
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(TP_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    }
+    tp_status s = get_tables(device, c->logn, &c->tab);
+    if (s != TP_OK) {
+        delete c;
+        return s;
+    }
+    e = cudaMalloc(&c->err, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(c->err, 0, sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(TP_ERR_CUDA, "error word: %s", cudaGetErrorString(e));
+    }
+
+    // Decomposition constants.
+    tp::BrKernelParams& kp = c->kp;
+    kp.tw_fwd = c->tab->tw_fwd;
+    kp.tw_inv = c->tab->tw_inv;
+    kp.psi_pow = c->tab->psi_pow;
+    kp.n = p->lwe_dim;
+    kp.digits = p->digits;
+    kp.n_inv = c->tab->n_inv;
+    kp.err = c->err;
+    if (p->variant == TP_BR_CGGI_BINARY) {
+        // unsigned digits, first shift beta*(ceil(64/beta)-1) (mux_operator.cpp:23-26,46-69)
+        const int first = beta * (max_digits - 1);
+        for (uint32_t d = 0; d < p->digits; ++d) {
+            kp.dshift[d] = (uint32_t)(first - (int)d * beta);
+            kp.dmask[d] = (1ull << beta) - 1;
+            kp.ddelta[d] = 0;
+        }
+        kp.corr = 0;
+    } else {
+        // signed digits (gadget_decomp.h:16-28,156-205)
+        uint64_t corr = 0;
+        int64_t shift = 64 - beta;
+        while (shift > 0) {
+            corr += 1ull << (shift + beta - 1);
+            shift -= beta;
+        }
+        const uint64_t least = 1ull << (shift + beta - 1);
+        corr += least;
+        kp.corr = corr % kP;
+        int64_t sh = 64 - beta;
+        uint64_t mask = (1ull << beta) - 1;
+        for (uint32_t d = 0; d < p->digits; ++d) {
+            uint64_t delta = 1ull << (beta - 1);
+            if ((int)d == max_digits - 1) {
+                delta = least;
+                sh = 0;
+                mask = (delta << 1) - 1;
+            }
+            kp.dshift[d] = (uint32_t)sh;
+            kp.dmask[d] = mask;
+            kp.ddelta[d] = delta;
+            sh -= beta;
+        }
+    }
+
+    c->kernel = tp::br_kernel_lookup(c->logn, p->variant);
+    c->smem_bytes = tp::br_smem_words((int)N, p->lwe_dim) * 8;
+    e = cudaFuncSetAttribute((const void*)c->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes);
+    int per_sm = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)c->kernel, (int)(N / 8), c->smem_bytes);
+    if (e != cudaSuccess || per_sm < 1) {
+        cudaFree(c->err);
+        delete c;
+        return fail(TP_ERR_PARAM, "blind-rotation kernel does not fit (N=%llu, n=%u, smem=%zu): %s",
+                    (unsigned long long)N, p->lwe_dim, (size_t)c->smem_bytes,
+                    e == cudaSuccess ? "no resident block" : cudaGetErrorString(e));
+    }
+    c->grid_cap = per_sm * sm_count(device);
+    *out = c;
+    return TP_OK;
+}
+
+tp_status tp_br_destroy(tp_br_ctx* c) {
+    if (!c) return TP_OK;
+    cudaSetDevice(c->device);
+    cudaFree(c->key);
+    cudaFree(c->err);
+    cudaFree(c->ws);
+    delete c;
+    return TP_OK;
+}
+
+uint64_t tp_br_key_words(const tp_br_ctx* c) { return c ? c->key_words : 0; }
+
+tp_status tp_br_upload_key(tp_br_ctx* c, const uint64_t* brk, uint64_t words) {
+    if (!c || !brk) return fail(TP_ERR_PARAM, "null argument");
+    if (words != c->key_words)
+        return fail(TP_ERR_LAYOUT, "key has %llu words, context expects %llu", (unsigned long long)words,
+                    (unsigned long long)c->key_words);
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    if (!c->key) TP_CUDA(cudaMalloc(&c->key, c->key_words * 8));
+    const uint64_t N = c->prm.ring_dim;
+    const uint64_t per_group = (uint64_t)c->G * 4 * N * c->prm.digits;
+    // stage at most ~128 MB of the reference layout at a time
+    uint64_t chunk = (128ull << 20) / (per_group * 8);
+    if (chunk < 1) chunk = 1;
+    if (chunk > c->groups) chunk = c->groups;
+    uint64_t* stage = nullptr;
+    TP_CUDA(cudaMalloc(&stage, chunk * per_group * 8));
+    tp_status st = TP_OK;
+    for (uint64_t g0 = 0; g0 < c->groups && st == TP_OK; g0 += chunk) {
+        const uint64_t ng = std::min(chunk, c->groups - g0);
+        cudaError_t e = cudaMemcpy(stage, brk + g0 * per_group, ng * per_group * 8, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            const uint64_t total = ng * per_group;
+            const int threads = 256;
+            const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
+            tp::key_relayout_kernel<<<(unsigned)blocks, threads>>>(c->key + g0 * per_group, stage, ng, c->G,
+                                                                    2 * c->prm.digits, c->logn);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) st = fail(TP_ERR_CUDA, "key upload: %s", cudaGetErrorString(e));
+    }
+    cudaFree(stage);
+    if (st == TP_OK) c->key_ready = true;
+    return st;
+}
+
+tp_status tp_br_blind_rotate_batch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                   uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
+                                   void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return TP_OK;
+    if (!results || !lwes || !accs) return fail(TP_ERR_PARAM, "null buffer");
+    if (lwe_stride < (uint64_t)c->prm.lwe_dim + 1) return fail(TP_ERR_PARAM, "lwe_stride below n+1");
+    if (acc_stride != 0 && acc_stride < 2ull * c->prm.ring_dim) return fail(TP_ERR_PARAM, "acc_stride below 2N");
+    if (((uintptr_t)results & 15) || ((uintptr_t)accs & 7) || ((uintptr_t)lwes & 7))
+        return fail(TP_ERR_PARAM, "results must be 16-byte aligned, lwes/accs 8-byte aligned");
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::BrKernelParams kp = c->kp;
+    kp.key = c->key;
+    kp.lwes = lwes;
+    kp.lwe_stride = lwe_stride;
+    kp.accs = accs;
+    kp.acc_stride = acc_stride;
+    kp.out = results;
+    kp.batch = batch;
+    kp.out_coef = out_coef ? 1u : 0u;
+    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_cap);
+    void* args[] = {&kp};
+    TP_CUDA(cudaLaunchKernel(c->kernel, dim3(grid), dim3(c->prm.ring_dim / 8), args, c->smem_bytes,
+                             (cudaStream_t)stream));
+    return TP_OK;
+}
+
+tp_status tp_br_check(tp_br_ctx* c, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    TP_CUDA(cudaSetDevice(c->device));
+    TP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    unsigned int flags = 0;
+    TP_CUDA(cudaMemcpy(&flags, c->err, sizeof flags, cudaMemcpyDeviceToHost));
+    TP_CUDA(cudaMemset(c->err, 0, sizeof flags));
+    if (flags & 1u) return fail(TP_ERR_PARAM, "an LWE word was outside [0, 2N); it was reduced mod 2N");
+    return TP_OK;
+}
+
+static tp_status ensure_ws(tp_br_ctx* c, uint64_t words) {
+    if (c->ws_words >= words) return TP_OK;
+    cudaFree(c->ws);
+    c->ws = nullptr;
+    c->ws_words = 0;
+    TP_CUDA(cudaMalloc(&c->ws, words * 8));
+    c->ws_words = words;
+    return TP_OK;
+}
+
+tp_status tp_br_blind_rotate_batch_host(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                        uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
+                                        void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (batch == 0) return TP_OK;
+    if (!results || !lwes || !accs) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->prm.ring_dim, n = c->prm.lwe_dim;
+    if (lwe_stride < n + 1) return fail(TP_ERR_PARAM, "lwe_stride below n+1");
+    if (acc_stride != 0 && acc_stride < 2 * N) return fail(TP_ERR_PARAM, "acc_stride below 2N");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    const uint64_t lw = (batch * (n + 1) + 1) & ~1ull;
+    const uint64_t aw = acc_stride ? batch * 2 * N : 2 * N;
+    const uint64_t rw = batch * 2 * N;
+    tp_status s = ensure_ws(c, lw + aw + rw);
+    if (s != TP_OK) return s;
+    uint64_t* d_res = c->ws;
+    uint64_t* d_acc = c->ws + rw;
+    uint64_t* d_lwe = c->ws + rw + aw;
+    cudaStream_t st = (cudaStream_t)stream;
+    TP_CUDA(cudaMemcpy2DAsync(d_lwe, (n + 1) * 8, lwes, lwe_stride * 8, (n + 1) * 8, batch, cudaMemcpyHostToDevice, st));
+    if (acc_stride)
+        TP_CUDA(cudaMemcpy2DAsync(d_acc, 2 * N * 8, accs, acc_stride * 8, 2 * N * 8, batch, cudaMemcpyHostToDevice, st));
+    else
+        TP_CUDA(cudaMemcpyAsync(d_acc, accs, 2 * N * 8, cudaMemcpyHostToDevice, st));
+    s = tp_br_blind_rotate_batch(c, batch, d_res, d_lwe, n + 1, d_acc, acc_stride ? 2 * N : 0, out_coef, stream);
+    if (s != TP_OK) return s;
+    TP_CUDA(cudaMemcpyAsync(results, d_res, rw * 8, cudaMemcpyDeviceToHost, st));
+    TP_CUDA(cudaStreamSynchronize(st));
+    return TP_OK;
+}
+
+tp_status tp_br_blind_rotate(tp_br_ctx* c, uint64_t* result, const uint64_t* lwe, const uint64_t* acc, int out_coef) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    tp_status s = tp_br_blind_rotate_batch_host(c, 1, result, lwe, (uint64_t)c->prm.lwe_dim + 1, acc,
+                                                2ull * c->prm.ring_dim, out_coef, nullptr);
+    if (s != TP_OK) return s;
+    return tp_br_check(c, nullptr);
+}
+
+tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* out, const uint64_t* rlwe,
+                                  void* stream) {
+    if (ring_dim < 2 || (ring_dim & (ring_dim - 1))) return fail(TP_ERR_PARAM, "ring_dim must be a power of two");
+    if (batch == 0) return TP_OK;
+    if (!out || !rlwe) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t total = batch * ((uint64_t)ring_dim + 1);
+    const int threads = 256;
+    const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
+    tp::sample_extract0_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(out, rlwe, batch, ring_dim);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
+static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
+                            bool fwd) {
+    if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (count == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    if (((uintptr_t)out & 15) || ((uintptr_t)in & 15)) return fail(TP_ERR_PARAM, "buffers must be 16-byte aligned");
+    int device = 0;
+    TP_CUDA(cudaGetDevice(&device));
+    const int logn = ilog2(ring_dim);
+    const Tables* tab = nullptr;
+    tp_status s = get_tables(device, logn, &tab);
+    if (s != TP_OK) return s;
+    const void* k = tp::ntt_kernel_lookup(logn, fwd);
+    const size_t smem = 3ull * ring_dim * 8;
+    TP_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    TP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k, ring_dim / 8, smem));
+    const uint64_t grid = std::min<uint64_t>(count, (uint64_t)std::max(1, per_sm) * sm_count(device));
+    const uint64_t* tw = fwd ? tab->tw_fwd : tab->tw_inv;
+    uint64_t n_inv = tab->n_inv;
+    void* args[] = {&out, &in, &count, &tw, &n_inv};
+    TP_CUDA(cudaLaunchKernel(k, dim3((unsigned)grid), dim3(ring_dim / 8), args, smem, (cudaStream_t)stream));
+    return TP_OK;
+}
+
+tp_status tp_ntt_forward(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream) {
+    return ntt_launch(ring_dim, count, out, in, stream, true);
+}
+
+tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream) {
+    return ntt_launch(ring_dim, count, out, in, stream, false);
+}
+
+}  // extern "C"

@@ -1,0 +1,43 @@
+// Kernel lookup across the per-ring-size compilation units.
+#pragma once
+
+namespace tp {
+
+const void* br_kernel_ptr_7(int variant);
+const void* ntt_kernel_ptr_7(bool forward);
+const void* br_kernel_ptr_8(int variant);
+const void* ntt_kernel_ptr_8(bool forward);
+const void* br_kernel_ptr_9(int variant);
+const void* ntt_kernel_ptr_9(bool forward);
+const void* br_kernel_ptr_10(int variant);
+const void* ntt_kernel_ptr_10(bool forward);
+const void* br_kernel_ptr_11(int variant);
+const void* ntt_kernel_ptr_11(bool forward);
+const void* br_kernel_ptr_12(int variant);
+const void* ntt_kernel_ptr_12(bool forward);
+
+inline const void* br_kernel_lookup(int logn, int variant) {
+    switch (logn) {
+        case 7: return br_kernel_ptr_7(variant);
+        case 8: return br_kernel_ptr_8(variant);
+        case 9: return br_kernel_ptr_9(variant);
+        case 10: return br_kernel_ptr_10(variant);
+        case 11: return br_kernel_ptr_11(variant);
+        case 12: return br_kernel_ptr_12(variant);
+        default: return nullptr;
+    }
+}
+
+inline const void* ntt_kernel_lookup(int logn, bool forward) {
+    switch (logn) {
+        case 7: return ntt_kernel_ptr_7(forward);
+        case 8: return ntt_kernel_ptr_8(forward);
+        case 9: return ntt_kernel_ptr_9(forward);
+        case 10: return ntt_kernel_ptr_10(forward);
+        case 11: return ntt_kernel_ptr_11(forward);
+        case 12: return ntt_kernel_ptr_12(forward);
+        default: return nullptr;
+    }
+}
+
+}  // namespace tp

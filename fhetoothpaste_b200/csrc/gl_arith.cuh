@@ -1,0 +1,123 @@
+// Goldilocks (p = 2^64 - 2^32 + 1) arithmetic for sm_100a.
+//
+// All functions take and return canonical residues in [0, p). The 64x64-bit
+// product is built from 32-bit IMAD chains (Blackwell has no 64-bit integer
+// multiplier); the 128-bit result x = r0 + r1 2^32 + r2 2^64 + r3 2^96 is reduced
+// with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p):  x = (r1:r0) - r3 + r2 (2^32 - 1).
+#pragma once
+
+#include <cstdint>
+
+namespace tp {
+
+constexpr uint64_t kP = 0xFFFFFFFF00000001ull;
+constexpr uint64_t kEps = 0x00000000FFFFFFFFull;  // 2^64 mod p
+
+__device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
+__device__ __forceinline__ uint64_t pack64(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
+
+// a + b mod p.  a + (b + eps) carries out iff a + b >= p; without the carry the
+// eps is taken back.
+__device__ __forceinline__ uint64_t gl_add(uint64_t a, uint64_t b) {
+    uint32_t sl, sh;
+    asm("{\n\t"
+        ".reg .u32 bl, bh, c, m;\n\t"
+        "add.cc.u32 bl, %2, 0xFFFFFFFF;\n\t"
+        "addc.u32 bh, %3, 0;\n\t"
+        "add.cc.u32 %0, %4, bl;\n\t"
+        "addc.cc.u32 %1, %5, bh;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "sub.u32 m, c, 1;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(sl), "=r"(sh)
+        : "r"(lo32(b)), "r"(hi32(b)), "r"(lo32(a)), "r"(hi32(a)));
+    return pack64(sl, sh);
+}
+
+// a - b mod p: on borrow add p, i.e. subtract eps modulo 2^64.
+__device__ __forceinline__ uint64_t gl_sub(uint64_t a, uint64_t b) {
+    uint32_t dl, dh;
+    asm("{\n\t"
+        ".reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(dl), "=r"(dh)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    return pack64(dl, dh);
+}
+
+// -a mod p.
+__device__ __forceinline__ uint64_t gl_neg(uint64_t a) { return a == 0 ? 0 : kP - a; }
+
+// 128-bit product a*b as four 32-bit words.
+__device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                         uint32_t& r3) {
+    asm("{\n\t"
+        "mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+}
+
+// Reduces x = r0 + r1 2^32 + r2 2^64 + r3 2^96 (any 128-bit value) to [0, p).
+__device__ __forceinline__ uint64_t gl_reduce128(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+    uint32_t s0, s1;
+    asm("{\n\t"
+        ".reg .u32 t0, t1, m, m1, u0, u1, c, x0, x1;\n\t"
+        ".reg .pred pc;\n\t"
+        // t = (r1:r0) - r3; on borrow add p (t stays below 2^64)
+        "sub.cc.u32 t0, %2, %5;\n\t"
+        "subc.cc.u32 t1, %3, 0;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "and.b32 m1, m, 1;\n\t"
+        "add.cc.u32 t0, t0, m1;\n\t"
+        "addc.u32 t1, t1, m;\n\t"
+        // u = r2 * (2^32 - 1) = (r2 : 0) - (0 : r2)
+        "sub.cc.u32 u0, 0, %4;\n\t"
+        "subc.u32 u1, %4, 0;\n\t"
+        // s = t + u; on carry add eps (cannot carry again)
+        "add.cc.u32 %0, t0, u0;\n\t"
+        "addc.cc.u32 %1, t1, u1;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "neg.s32 c, c;\n\t"
+        "add.cc.u32 %0, %0, c;\n\t"
+        "addc.u32 %1, %1, 0;\n\t"
+        // canonical: s >= p  <=>  s + eps carries; then s - p = s + eps (mod 2^64)
+        "add.cc.u32 x0, %0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 x1, %1, 0;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "setp.ne.u32 pc, c, 0;\n\t"
+        "selp.b32 %0, x0, %0, pc;\n\t"
+        "selp.b32 %1, x1, %1, pc;\n\t"
+        "}"
+        : "=r"(s0), "=r"(s1)
+        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
+    return pack64(s0, s1);
+}
+
+// a * b mod p.
+__device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
+    uint32_t r0, r1, r2, r3;
+    mul_wide(a, b, r0, r1, r2, r3);
+    return gl_reduce128(r0, r1, r2, r3);
+}
+
+// Canonical residue of any 64-bit value.
+__device__ __forceinline__ uint64_t gl_canon(uint64_t x) { return x >= kP ? x - kP : x; }
+
+}  // namespace tp

@@ -1,0 +1,21 @@
+// Kernel instantiations for N = 1024 (compiled as a separate unit so the
+// ring sizes build in parallel).
+#include "br_kernels.cuh"
+#include "dispatch.h"
+#include "misc_kernels.cuh"
+
+namespace tp {
+
+const void* br_kernel_ptr_10(int variant) {
+    switch (variant) {
+        case kCggiBinary: return (const void*)br_kernel<10, kCggiBinary>;
+        case kCggiTernary: return (const void*)br_kernel<10, kCggiTernary>;
+        default: return (const void*)br_kernel<10, kBmmpBinary>;
+    }
+}
+
+const void* ntt_kernel_ptr_10(bool forward) {
+    return forward ? (const void*)ntt_batch_kernel<10, true> : (const void*)ntt_batch_kernel<10, false>;
+}
+
+}  // namespace tp

@@ -1,0 +1,21 @@
+// Kernel instantiations for N = 4096 (compiled as a separate unit so the
+// ring sizes build in parallel).
+#include "br_kernels.cuh"
+#include "dispatch.h"
+#include "misc_kernels.cuh"
+
+namespace tp {
+
+const void* br_kernel_ptr_12(int variant) {
+    switch (variant) {
+        case kCggiBinary: return (const void*)br_kernel<12, kCggiBinary>;
+        case kCggiTernary: return (const void*)br_kernel<12, kCggiTernary>;
+        default: return (const void*)br_kernel<12, kBmmpBinary>;
+    }
+}
+
+const void* ntt_kernel_ptr_12(bool forward) {
+    return forward ? (const void*)ntt_batch_kernel<12, true> : (const void*)ntt_batch_kernel<12, false>;
+}
+
+}  // namespace tp

@@ -1,0 +1,203 @@
+// Thread-block negacyclic NTT over Goldilocks for one polynomial of N = 2^LOGN
+// coefficients held 8 per thread by T = N/8 threads.
+//
+// The transform is the reference's (lib/src/backend/solinas.cpp:228-313):
+// forward = Cooley-Tukey, natural-order coefficients in, evaluations out in
+// bit-reversed order (slot k = a(psi^(2 brv(k) + 1))), block i of the level
+// with m blocks using psi^brv(m+i); backward = Gentleman-Sande with
+// psi^-brv(m+i), natural order out, scaled by 1/N. Since every value is an
+// exact residue, any evaluation order of the same butterflies gives the same
+// words as the reference.
+//
+// Levels are processed in passes of up to three (radix-8 groups in registers).
+// Between passes the data goes through a shared-memory exchange buffer of N
+// words. Passes whose blocks span at most 256 coefficients touch only their
+// own warp's 256-word region, so those exchanges need only __syncwarp; the
+// others use __syncthreads.
+//
+// Register layouts ("where thread t holds what"):
+//   coefficient layout: x[j] = coefficient t + j*T            (pass 0 groups)
+//   slot layout:        x[j] = slot 8t + j                     (last pass groups)
+// forward: coefficient layout -> slot layout; backward: slot -> coefficient.
+//
+// Exchange-buffer hazards: a transform's first shared-memory write may race
+// with another warp still reading the previous transform's last exchange, so
+// callers alternate between two buffers; every transform of N >= 512 contains
+// a block-wide barrier, which orders transform k's reads before transform
+// k+2's writes to the same buffer.
+#pragma once
+
+#include "gl_arith.cuh"
+
+namespace tp {
+
+template <int LOGN>
+struct NttShape {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int T = N / 8;
+    static constexpr int NPASS = (LOGN + 2) / 3;
+    __host__ __device__ static constexpr int L0(int p) { return 3 * p; }
+    __host__ __device__ static constexpr int S(int p) { return 3 * p + 3 <= LOGN ? 3 : LOGN - 3 * p; }
+    // A pass whose level-L0 blocks have at most 256 coefficients stays inside
+    // the 256-word region of its warp.
+    __host__ __device__ static constexpr bool WarpLocal(int p) { return LOGN - L0(p) <= 8; }
+    static constexpr bool SingleWarp = (T <= 32);
+};
+
+// Swizzled position of coefficient/slot `idx` in an exchange buffer: 16-byte
+// chunk c = idx/2 is stored at chunk c ^ ((c >> 3) & 7). Keeps every pass's
+// 8-byte accesses (per half-warp) and 16-byte accesses (per quarter-warp)
+// free of bank conflicts.
+__device__ __forceinline__ int xpos(int idx) {
+    const int c = idx >> 1;
+    return ((c ^ ((c >> 3) & 7)) << 1) | (idx & 1);
+}
+
+// Index of the e-th register (0..7) of thread t in pass P.
+template <int LOGN, int P>
+__device__ __forceinline__ int pass_index(int t, int e) {
+    using SH = NttShape<LOGN>;
+    constexpr int S = SH::S(P);
+    constexpr int G = 1 << S;
+    constexpr int PER = 8 / G;
+    constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+    const int q = e / G, j = e % G;
+    const int g = PER * t + q;
+    const int blk = g / TMIN, off = g % TMIN;
+    return blk * G * TMIN + off + j * TMIN;
+}
+
+template <int LOGN>
+__device__ __forceinline__ void ntt_sync(bool block_wide) {
+    using SH = NttShape<LOGN>;
+    if (SH::T < 32 || block_wide) __syncthreads();
+    else __syncwarp();
+}
+
+// Forward butterflies of pass P on the thread's registers.
+template <int LOGN, int P>
+__device__ __forceinline__ void fwd_pass_math(uint64_t x[8], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN>;
+    constexpr int S = SH::S(P);
+    constexpr int G = 1 << S;
+    constexpr int PER = 8 / G;
+    constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+    constexpr int L0 = SH::L0(P);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int blk = (PER * t + q) / TMIN;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            const int half = G >> (k + 1);
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                if (j & half) continue;
+                const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
+                const uint64_t u = x[q * G + j];
+                const uint64_t v = gl_mul(x[q * G + j + half], w);
+                x[q * G + j] = gl_add(u, v);
+                x[q * G + j + half] = gl_sub(u, v);
+            }
+        }
+    }
+}
+
+// Inverse butterflies of pass P (levels in reverse order).
+template <int LOGN, int P>
+__device__ __forceinline__ void inv_pass_math(uint64_t x[8], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN>;
+    constexpr int S = SH::S(P);
+    constexpr int G = 1 << S;
+    constexpr int PER = 8 / G;
+    constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+    constexpr int L0 = SH::L0(P);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int blk = (PER * t + q) / TMIN;
+#pragma unroll
+        for (int k = S - 1; k >= 0; --k) {
+            const int half = G >> (k + 1);
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                if (j & half) continue;
+                const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
+                const uint64_t u = x[q * G + j];
+                const uint64_t v = x[q * G + j + half];
+                x[q * G + j] = gl_add(u, v);
+                x[q * G + j + half] = gl_mul(gl_sub(u, v), w);
+            }
+        }
+    }
+}
+
+template <int LOGN, int P>
+__device__ __forceinline__ void xstore(uint64_t* buf, const uint64_t x[8], int t) {
+    using SH = NttShape<LOGN>;
+    if constexpr (P == SH::NPASS - 1) {
+        // slot layout: 8 contiguous words, written as four 16-byte chunks
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int idx = 8 * t + 2 * c;
+            *reinterpret_cast<ulonglong2*>(buf + xpos(idx)) = make_ulonglong2(x[2 * c], x[2 * c + 1]);
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) buf[xpos(pass_index<LOGN, P>(t, e))] = x[e];
+    }
+}
+
+template <int LOGN, int P>
+__device__ __forceinline__ void xload(const uint64_t* buf, uint64_t x[8], int t) {
+    using SH = NttShape<LOGN>;
+    if constexpr (P == SH::NPASS - 1) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int idx = 8 * t + 2 * c;
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(buf + xpos(idx));
+            x[2 * c] = v.x;
+            x[2 * c + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) x[e] = buf[xpos(pass_index<LOGN, P>(t, e))];
+    }
+}
+
+template <int LOGN, int P>
+__device__ __forceinline__ void fwd_passes_from(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw) {
+    using SH = NttShape<LOGN>;
+    fwd_pass_math<LOGN, P>(x, t, tw);
+    if constexpr (P + 1 < SH::NPASS) {
+        xstore<LOGN, P>(buf, x, t);
+        ntt_sync<LOGN>(!SH::WarpLocal(P));
+        xload<LOGN, P + 1>(buf, x, t);
+        fwd_passes_from<LOGN, P + 1>(x, t, buf, tw);
+    }
+}
+
+template <int LOGN, int P>
+__device__ __forceinline__ void inv_passes_from(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw) {
+    using SH = NttShape<LOGN>;
+    inv_pass_math<LOGN, P>(x, t, tw);
+    if constexpr (P > 0) {
+        xstore<LOGN, P>(buf, x, t);
+        ntt_sync<LOGN>(!SH::WarpLocal(P - 1));
+        xload<LOGN, P - 1>(buf, x, t);
+        inv_passes_from<LOGN, P - 1>(x, t, buf, tw);
+    }
+}
+
+// Forward NTT: x in coefficient layout -> x in slot layout.
+template <int LOGN>
+__device__ __forceinline__ void ntt_forward(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
+    fwd_passes_from<LOGN, 0>(x, t, buf, tw_fwd);
+}
+
+// Backward NTT without the 1/N factor: x in slot layout -> coefficient layout.
+template <int LOGN>
+__device__ __forceinline__ void ntt_backward_unscaled(uint64_t x[8], int t, uint64_t* buf,
+                                                      const uint64_t* tw_inv) {
+    inv_passes_from<LOGN, NttShape<LOGN>::NPASS - 1>(x, t, buf, tw_inv);
+}
+
+}  // namespace tp

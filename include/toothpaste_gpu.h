@@ -1,0 +1,132 @@
+/*
+ * toothpaste_gpu.h — C ABI of the B200 (sm_100a) blind-rotation engine.
+ *
+ * Plain C types only: device and host buffers are uint64_t pointers, streams are
+ * passed as `void*` (a cudaStream_t, NULL = the legacy default stream). Every
+ * entry point returns a tp_status; tp_last_error() gives a message for the
+ * calling thread. No exception crosses this boundary.
+ *
+ * Arithmetic is over the Goldilocks prime p = 2^64 - 2^32 + 1. All ciphertext
+ * words are canonical residues in [0, p); polynomials have N coefficients with
+ * N a power of two in [128, 4096]. "NTT domain" means the reference's
+ * evaluation order: slot k holds a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N)
+ * (lib/src/backend/solinas.cpp:168-313 of the reference).
+ *
+ * Each declaration names the reference interface it replaces (file:line in the
+ * reference project).
+ */
+#ifndef TOOTHPASTE_GPU_H
+#define TOOTHPASTE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TP_OK = 0,
+    TP_ERR_PARAM = 1,   /* invalid argument or unsupported parameter set */
+    TP_ERR_OOM = 2,     /* device allocation failed */
+    TP_ERR_CUDA = 3,    /* a CUDA call failed (message in tp_last_error) */
+    TP_ERR_TIMEOUT = 4, /* a bounded device-side wait ran out */
+    TP_ERR_LAYOUT = 5,  /* key size or layout does not match the context */
+    TP_ERR_STATE = 6    /* call order: e.g. rotate before a key was uploaded */
+} tp_status;
+
+/* Blind-rotation variants (reference: KeyDistribution BINARY/TERNARY for
+ * CGGIBlindRotationContext, lib/include/operators/cggi_blind_rotation.h:24;
+ * BMMPBlindRotationContext with step_size 2, lib/include/operators/bmmp_blind_rotation.h:23). */
+typedef enum {
+    TP_BR_CGGI_BINARY = 0,
+    TP_BR_CGGI_TERNARY = 1,
+    TP_BR_BMMP_BINARY = 2
+} tp_br_variant;
+
+/* Parameters of CGGIBlindRotationContext(distr, modulus, ring_dim, lwe_dim,
+ * basis, digits, std) (lib/src/operators/cggi_blind_rotation.cpp:14-25). `std`
+ * only matters for key generation, which stays on the host. */
+typedef struct {
+    int32_t variant;     /* tp_br_variant */
+    uint64_t modulus;    /* must be 0xFFFFFFFF00000001 */
+    uint32_t ring_dim;   /* N */
+    uint32_t lwe_dim;    /* n (even for BMMP) */
+    uint64_t basis;      /* gadget base, a power of two 2^beta, beta in [2, 32] */
+    uint32_t digits;     /* l, 1..8 */
+} tp_br_params;
+
+typedef struct tp_br_ctx tp_br_ctx;
+
+/* Creates a context on `device` (its tables are built there). Replaces the
+ * operator construction of CGGIBlindRotationContext::ConstructOperator
+ * (lib/src/operators/cggi_blind_rotation.cpp:184-199) minus key generation. */
+tp_status tp_br_create(const tp_br_params* params, int device, tp_br_ctx** out);
+tp_status tp_br_destroy(tp_br_ctx* ctx);
+
+/* Number of uint64 words of the blind-rotation key in the reference layout
+ * (the m_brk of KeyGenBinary/KeyGenTernary, cggi_blind_rotation.cpp:264-311,
+ * or BMMP KeyGenBinary, bmmp_blind_rotation.cpp:229-262). */
+uint64_t tp_br_key_words(const tp_br_ctx* ctx);
+
+/* Uploads a key in that reference layout from host memory (`words` must equal
+ * tp_br_key_words) and re-lays it out on the device. Synchronous. */
+tp_status tp_br_upload_key(tp_br_ctx* ctx, const uint64_t* brk_host, uint64_t words);
+
+/* Drop-in for BlindRotator::BlindRotate(result, lwe, acc, output_as_coefficients)
+ * (lib/include/interfaces/blindrotation_operator.h:202-203; CGGI body
+ * cggi_blind_rotation.cpp:236-262, BMMP body bmmp_blind_rotation.cpp:325-335).
+ * Host pointers: lwe has n+1 words [a_0..a_{n-1}, b], each in [0, 2N); acc is
+ * 2N words [A | B] in the coefficient domain; result receives 2N words in the
+ * NTT domain, or coefficients when out_coef != 0. result may equal acc.
+ * Synchronous; one rotation per launch (the plain form). */
+tp_status tp_br_blind_rotate(tp_br_ctx* ctx, uint64_t* result, const uint64_t* lwe, const uint64_t* acc,
+                             int out_coef);
+
+/* Batched form of the same call on device buffers: rotation b reads
+ * lwes + b*lwe_stride and accs + b*acc_stride (acc_stride 0 = one accumulator
+ * shared by the whole batch) and writes results + b*2N. Asynchronous on
+ * `stream`; runs as one persistent launch whose accumulators stay on chip for
+ * all n iterations. Inputs outside [0, 2N) are reduced mod 2N and flagged;
+ * tp_br_check flags them. No reference counterpart (the reference rotates
+ * one ciphertext per call). */
+tp_status tp_br_blind_rotate_batch(tp_br_ctx* ctx, uint64_t batch, uint64_t* results_dev,
+                                   const uint64_t* lwes_dev, uint64_t lwe_stride, const uint64_t* accs_dev,
+                                   uint64_t acc_stride, int out_coef, void* stream);
+
+/* The batched call on host buffers: copies in, rotates, copies out, waits. */
+tp_status tp_br_blind_rotate_batch_host(tp_br_ctx* ctx, uint64_t batch, uint64_t* results,
+                                        const uint64_t* lwes, uint64_t lwe_stride, const uint64_t* accs,
+                                        uint64_t acc_stride, int out_coef, void* stream);
+
+/* Waits for the context's work on `stream` and reports device-side input
+ * errors seen since the last check (TP_ERR_PARAM for out-of-range LWE words). */
+tp_status tp_br_check(tp_br_ctx* ctx, void* stream);
+
+/* SampleExtract at index 0 of a batch of RLWE ciphertexts in the coefficient
+ * domain (lib/include/static/sample_extraction.h:20-36), device buffers: out
+ * b gets N+1 words at out + b*(N+1). The reference leaves a word untouched
+ * where the source coefficient is 0; this kernel writes 0 there, which equals
+ * the reference's result on a pre-zeroed buffer. */
+tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* out_dev, const uint64_t* rlwe_dev,
+                                  void* stream);
+
+/* Batched negacyclic NTT on device buffers, `count` polynomials of N words,
+ * in-place allowed. Replaces SolinasWorker::ForwardNTT / BackwardNTT
+ * (lib/src/backend/solinas.cpp:228-313); backward includes 1/N. */
+tp_status tp_ntt_forward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, const uint64_t* in_dev,
+                         void* stream);
+tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, const uint64_t* in_dev,
+                          void* stream);
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* tp_last_error(void);
+
+/* Library version string. */
+const char* tp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

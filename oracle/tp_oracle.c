@@ -65,7 +65,20 @@ uint64_t tpo_add(uint64_t a, uint64_t b) {
 
 uint64_t tpo_sub(uint64_t a, uint64_t b) { return a >= b ? a - b : a + (P - b); }
 
-uint64_t tpo_mul(uint64_t a, uint64_t b) { return (uint64_t)(((u128)a * b) % P); }
+/* 128-bit value -> canonical, with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p)
+ * (elemops::reduce128, lib/include/backend/solinas_internal.h:62-73). */
+static uint64_t reduce128(u128 x) {
+    const uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64);
+    const uint64_t hh = hi >> 32, hl = hi & EPS;
+    uint64_t t = lo - hh;
+    if (lo < hh) t -= EPS;
+    const uint64_t u = (hl << 32) - hl;
+    uint64_t r = t + u;
+    if (r < u) r += EPS;
+    return r >= P ? r - P : r;
+}
+
+uint64_t tpo_mul(uint64_t a, uint64_t b) { return reduce128((u128)a * b); }
 
 uint64_t tpo_pow(uint64_t b, uint64_t e) {
     uint64_t r = 1;

@@ -1,0 +1,115 @@
+"""Blind-rotation parity on the GPU through the C ABI.
+
+Bit-exact against the golden vectors recorded from the reference library and
+against the C oracle on fresh seeded inputs.
+"""
+import numpy as np
+import pytest
+
+from brcases import case_inputs, case_key
+from oracle.oracle import lwe_inputs, random_acc
+
+pytestmark = pytest.mark.gpu
+
+ALL_CASES = ["small_binary_n256", "small_ternary_n128", "small_bmmp_n512", "cfg1_binary_n1024",
+             "cfg5a_ternary_n1024", "cfg2_ternary_n2048", "cfg3_bmmp_n2048", "cfg5c_ternary_n4096"]
+SMALL = ["small_binary_n256", "small_ternary_n128", "small_bmmp_n512"]
+
+
+def rotator(oracle, golden, name):
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    manifest, _ = golden
+    case = manifest["br"][name]
+    _, _, brk = case_key(oracle, name, case)
+    ctx = BlindRotationContext(case["variant"], case["N"], case["n"], 1 << case["basis_log2"], case["digits"])
+    return case, GpuBlindRotator(ctx, brk)
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_plain_blind_rotate_matches_reference(native, oracle, golden, name):
+    case, rot = rotator(oracle, golden, name)
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for i, oc in enumerate(coefs):
+        res = np.zeros(2 * case["N"], np.uint64)
+        rot.BlindRotate(res, np.ascontiguousarray(lwes[i]), np.ascontiguousarray(accs[i]), bool(oc))
+        np.testing.assert_array_equal(res, expect[i])
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_batched_blind_rotate_matches_reference(native, oracle, golden, name):
+    case, rot = rotator(oracle, golden, name)
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for oc in (0, 1):
+        idx = [i for i, c in enumerate(coefs) if c == oc]
+        got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+        np.testing.assert_array_equal(got, expect[idx])
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_batch_against_oracle_fresh_inputs(native, oracle, golden, name):
+    """A batch larger than the resident grid, so blocks loop over ciphertexts."""
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    batch = 2 * 148 * 8 + 5
+    lwes = lwe_inputs(N, n, batch, 777)
+    accs = random_acc(N, batch, 778)
+    for oc in (0, 1):
+        got = rot.blind_rotate_batch_host(lwes, accs, out_coef=bool(oc))
+        for b in (0, 1, 148, batch // 2, batch - 1):
+            exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b],
+                                      accs[b], oc)
+            np.testing.assert_array_equal(got[b], exp, err_msg=f"ciphertext {b}")
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_shared_accumulator_and_edge_words(native, oracle, golden, name):
+    """acc_stride 0 (one test polynomial for the whole batch); a_i in {0, N, 2N-1}, b >= N."""
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    lwes = lwe_inputs(N, n, 6, 91)
+    lwes[0, :] = 0                      # every a_i = 0 and b = 0: the accumulator only goes through the NTTs
+    lwes[1, :] = N                      # X^N = -1 everywhere
+    lwes[2, :] = 2 * N - 1
+    lwes[3, n] = N + 1
+    acc = random_acc(N, 1, 92)[0]
+    got = rot.blind_rotate_batch_host(lwes, acc, out_coef=True)
+    for b in range(6):
+        exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], acc, 1)
+        np.testing.assert_array_equal(got[b], exp, err_msg=f"ciphertext {b}")
+
+
+def test_out_of_range_lwe_is_reported(native, oracle, golden):
+    from fhetoothpaste_b200 import TpError
+    case, rot = rotator(oracle, golden, "small_ternary_n128")
+    N, n = case["N"], case["n"]
+    lwes = lwe_inputs(N, n, 2, 5)
+    lwes[1, 3] = 2 * N + 3
+    acc = random_acc(N, 1, 6)[0]
+    with pytest.raises(TpError) as ei:
+        rot.blind_rotate_batch_host(lwes, acc)
+    assert ei.value.status == 1
+    # the flag is cleared once reported
+    rot.blind_rotate_batch_host(lwes[:1], acc)
+
+
+def test_result_may_alias_accumulator(native, oracle, golden, cuda):
+    """SAP passes result == accumulator (sap_decomposer.cpp:369); the batch kernel reads every
+    accumulator word of a ciphertext before writing its result."""
+    torch = cuda
+    case, rot = rotator(oracle, golden, "small_binary_n256")
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, "small_binary_n256", case)
+    lwes = lwe_inputs(N, n, 3, 21)
+    accs = random_acc(N, 3, 22)
+    d_lwe = torch.from_numpy(lwes.view(np.int64)).cuda()
+    d_acc = torch.from_numpy(accs.view(np.int64)).cuda()
+    rot.blind_rotate_batch(d_acc.data_ptr(), d_lwe.data_ptr(), n + 1, d_acc.data_ptr(), 2 * N, 3, out_coef=True)
+    rot.check()
+    got = d_acc.cpu().numpy().view(np.uint64)
+    for b in range(3):
+        exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], accs[b], 1)
+        np.testing.assert_array_equal(got[b], exp)
