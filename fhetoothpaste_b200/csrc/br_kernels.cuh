@@ -92,7 +92,7 @@ br_kernel(const BrKernelParams prm) {
     uint64_t* tw_i = smem + N;
     uint64_t* xbuf0 = smem + 2 * N;
     uint64_t* xbuf1 = smem + 3 * N;
-    uint64_t* acc = smem + 4 * N;            // [(h*8 + j)*T + t]
+    uint64_t* acc = smem + 4 * N;            // [(h*8 + j)*T + t], canonical, NTT domain
     uint64_t* lwe_s = smem + 6 * N;
 
     const int t = threadIdx.x;
@@ -103,10 +103,6 @@ br_kernel(const BrKernelParams prm) {
         tw_f[i] = prm.tw_fwd[i];
         tw_i[i] = prm.tw_inv[i];
     }
-
-    uint32_t ek[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) ek[j] = slot_exponent<LOGN>(8 * t + j);
 
     int sel = 0;
     auto xb = [&]() -> uint64_t* {
@@ -131,18 +127,20 @@ br_kernel(const BrKernelParams prm) {
         {
             const uint64_t* ain = prm.accs + b * prm.acc_stride;
             const uint32_t bb = (uint32_t)lwe_s[n];
-#pragma unroll
+#pragma unroll 1
             for (int h = 0; h < 2; ++h) {
                 uint64_t x[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) x[j] = ain[h * N + t + j * T];
                 ntt_forward<LOGN>(x, t, xb(), tw_f);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[(h * 8 + j) * T + t] = gl_mul(x[j], mono<LOGN>(prm.psi_pow, ek[j], bb));
+                for (int j = 0; j < 8; ++j)
+                    acc[(h * 8 + j) * T + t] = gl_mul(x[j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j), bb));
             }
         }
 
         const uint32_t step = VARIANT == kBmmpBinary ? 2 : 1;
+#pragma unroll 1
         for (uint32_t i = 0; i < n; i += step) {
             uint32_t a0 = (uint32_t)lwe_s[i];
             uint32_t a1 = 0;
@@ -154,55 +152,53 @@ br_kernel(const BrKernelParams prm) {
             }
             const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
 
+            // MAC accumulators (lazy residues, any 64-bit value)
             uint64_t o[C][8];
 #pragma unroll
             for (int c = 0; c < C; ++c)
 #pragma unroll
                 for (int j = 0; j < 8; ++j) o[c][j] = 0;
 
-            // Binary CGGI decomposes (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the
-            // other variants decompose acc itself (mux_operator.cpp:174-177, 219-224).
-            uint64_t mpos[8];
-            if constexpr (VARIANT == kCggiBinary) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) mpos[j] = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], 2u * N - a0), 1);
-            }
-
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                uint64_t cx[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    cx[j] = acc[(h * 8 + j) * T + t];
-                    if constexpr (VARIANT == kCggiBinary) cx[j] = gl_mul(cx[j], mpos[j]);
-                }
-                ntt_backward_unscaled<LOGN>(cx, t, xb(), tw_i);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    cx[j] = gl_mul(cx[j], prm.n_inv);
-                    if constexpr (SIGNED) cx[j] = gl_add(cx[j], prm.corr);
-                }
-                for (uint32_t d = 0; d < L; ++d) {
-                    const uint32_t sh = prm.dshift[d];
-                    const uint64_t mk = prm.dmask[d];
-                    const uint64_t dl = prm.ddelta[d];
-                    uint64_t x[8];
+            uint64_t cx[8];  // corrected coefficients of the half being decomposed
+#pragma unroll 1
+            for (uint32_t r = 0; r < 2 * L; ++r) {
+                if (r == 0 || r == L) {
+                    // Backward NTT of one accumulator half. Binary CGGI decomposes
+                    // (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the other variants
+                    // decompose acc itself (mux_operator.cpp:174-177, 219-224).
+                    const int h = r == 0 ? 0 : 1;
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
-                        const uint64_t raw = (cx[j] >> sh) & mk;
-                        x[j] = SIGNED ? gl_sub(raw, dl) : raw;
+                        cx[j] = acc[(h * 8 + j) * T + t];
+                        if constexpr (VARIANT == kCggiBinary)
+                            cx[j] = gl_mul(cx[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j),
+                                                                    2u * N - a0), 1));
                     }
-                    ntt_forward<LOGN>(x, t, xb(), tw_f);
-                    const uint64_t* kr = kit + (uint64_t)(h * L + d) * (N * C);
+                    ntt_backward_unscaled<LOGN>(cx, t, xb(), tw_i);
+                    // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
 #pragma unroll
-                    for (int c = 0; c < C; ++c) {
+                    for (int j = 0; j < 8; ++j) cx[j] = gl_canon(gl_fma_lazy(prm.corr, cx[j], prm.n_inv));
+                }
+                const uint32_t d = r < L ? r : r - L;
+                const uint32_t sh = prm.dshift[d];
+                const uint64_t mk = prm.dmask[d];
+                const uint64_t dl = prm.ddelta[d];
+                uint64_t x[8];
 #pragma unroll
-                        for (int jp = 0; jp < 4; ++jp) {
-                            const ulonglong2 kv =
-                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
-                            o[c][2 * jp] = gl_add(o[c][2 * jp], gl_mul(x[2 * jp], kv.x));
-                            o[c][2 * jp + 1] = gl_add(o[c][2 * jp + 1], gl_mul(x[2 * jp + 1], kv.y));
-                        }
+                for (int j = 0; j < 8; ++j) {
+                    const uint64_t raw = (cx[j] >> sh) & mk;
+                    x[j] = SIGNED ? gl_sub(raw, dl) : raw;
+                }
+                ntt_forward<LOGN>(x, t, xb(), tw_f);
+                const uint64_t* kr = kit + (uint64_t)r * (N * C);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+#pragma unroll
+                    for (int jp = 0; jp < 4; ++jp) {
+                        const ulonglong2 kv =
+                            __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
+                        o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[2 * jp], kv.x);
+                        o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[2 * jp + 1], kv.y);
                     }
                 }
             }
@@ -210,29 +206,30 @@ br_kernel(const BrKernelParams prm) {
             // Accumulator update.
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
+                const uint32_t ek = slot_exponent<LOGN>(8 * t + j);
                 uint64_t ua = acc[j * T + t];
                 uint64_t ub = acc[(8 + j) * T + t];
                 if constexpr (VARIANT == kCggiBinary) {
                     // acc += ExtProd (mux_operator.cpp:151)
-                    ua = gl_add(ua, o[0][j]);
-                    ub = gl_add(ub, o[1][j]);
+                    ua = gl_add(ua, gl_canon(o[0][j]));
+                    ub = gl_add(ub, gl_canon(o[1][j]));
                 } else if constexpr (VARIANT == kCggiTernary) {
                     // acc += (X^{-a}-1) ExtProd(lo) + (X^{a}-1) ExtProd(hi) (mux_operator.cpp:188-200)
-                    const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], 2u * N - a0), 1);
-                    const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek[j], a0), 1);
-                    ua = gl_add(ua, gl_add(gl_mul(o[0][j], mp), gl_mul(o[2][j], mn)));
-                    ub = gl_add(ub, gl_add(gl_mul(o[1][j], mp), gl_mul(o[3][j], mn)));
+                    const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek, 2u * N - a0), 1);
+                    const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek, a0), 1);
+                    ua = gl_canon(gl_fma_lazy(gl_fma_lazy(ua, o[0][j], mp), o[2][j], mn));
+                    ub = gl_canon(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], mp), o[3][j], mn));
                 } else {
                     // weights X^{a0}-1, X^{a1}-1, X^{a0+a1}-X^{a0}-X^{a1}+1
                     // (bmmp_blind_rotation.cpp:280-323; MultiMux mux_operator.cpp:274-291)
-                    const uint64_t m0 = mono<LOGN>(prm.psi_pow, ek[j], a0);
-                    const uint64_t m1 = mono<LOGN>(prm.psi_pow, ek[j], a1);
-                    const uint64_t m2 = mono<LOGN>(prm.psi_pow, ek[j], (a0 + a1) & MASK2N);
+                    const uint64_t m0 = mono<LOGN>(prm.psi_pow, ek, a0);
+                    const uint64_t m1 = mono<LOGN>(prm.psi_pow, ek, a1);
+                    const uint64_t m2 = mono<LOGN>(prm.psi_pow, ek, (a0 + a1) & MASK2N);
                     const uint64_t w0 = gl_sub(m0, 1);
                     const uint64_t w1 = gl_sub(m1, 1);
                     const uint64_t w2 = gl_add(gl_sub(gl_sub(m2, m0), m1), 1);
-                    ua = gl_add(ua, gl_add(gl_add(gl_mul(o[0][j], w0), gl_mul(o[2][j], w1)), gl_mul(o[4][j], w2)));
-                    ub = gl_add(ub, gl_add(gl_add(gl_mul(o[1][j], w0), gl_mul(o[3][j], w1)), gl_mul(o[5][j], w2)));
+                    ua = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ua, o[0][j], w0), o[2][j], w1), o[4][j], w2));
+                    ub = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2));
                 }
                 acc[j * T + t] = ua;
                 acc[(8 + j) * T + t] = ub;
@@ -241,7 +238,7 @@ br_kernel(const BrKernelParams prm) {
 
         // Epilogue (cggi_blind_rotation.cpp:258-261).
         uint64_t* res = prm.out + b * (2ull * N);
-#pragma unroll
+#pragma unroll 1
         for (int h = 0; h < 2; ++h) {
             uint64_t x[8];
 #pragma unroll

@@ -412,6 +412,18 @@ tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* o
     return TP_OK;
 }
 
+tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out, const uint64_t* a, const uint64_t* b,
+                         const uint64_t* c, void* stream) {
+    if (op < 0 || op > 5) return fail(TP_ERR_PARAM, "unknown op %d", op);
+    if (count == 0) return TP_OK;
+    if (!out || !a || !b || !c) return fail(TP_ERR_PARAM, "null buffer");
+    const int threads = 256;
+    const uint64_t blocks = std::min<uint64_t>((count + threads - 1) / threads, 65535);
+    tp::debug_arith_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(op, count, out, a, b, c);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd) {
     if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))

@@ -51,4 +51,21 @@ __global__ void sample_extract0_kernel(uint64_t* __restrict__ out, const uint64_
     }
 }
 
+// Element-wise arithmetic check (tp_debug_arith).
+__global__ void debug_arith_kernel(int op, uint64_t count, uint64_t* __restrict__ out, const uint64_t* __restrict__ a,
+                                   const uint64_t* __restrict__ b, const uint64_t* __restrict__ c) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = 0;
+        switch (op) {
+            case 0: r = gl_add(a[i], b[i]); break;
+            case 1: r = gl_sub(a[i], b[i]); break;
+            case 2: r = gl_mul(a[i], b[i]); break;
+            case 3: r = gl_canon(gl_fma_lazy(c[i], a[i], b[i])); break;
+            case 4: r = gl_canon(gl_reduce128_lazy(lo32(a[i]), hi32(a[i]), lo32(b[i]), hi32(b[i]))); break;
+            default: r = gl_canon(a[i]); break;
+        }
+        out[i] = r;
+    }
+}
+
 }  // namespace tp

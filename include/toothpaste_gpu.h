@@ -52,7 +52,7 @@ typedef struct {
     uint64_t modulus;    /* must be 0xFFFFFFFF00000001 */
     uint32_t ring_dim;   /* N */
     uint32_t lwe_dim;    /* n (even for BMMP) */
-    uint64_t basis;      /* gadget base, a power of two 2^beta, beta in [2, 32] */
+    uint64_t basis;      /* gadget base, a power of two 2^beta, beta in [1, 30] */
     uint32_t digits;     /* l, 1..8 */
 } tp_br_params;
 
@@ -118,6 +118,14 @@ tp_status tp_ntt_forward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, c
                          void* stream);
 tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, const uint64_t* in_dev,
                           void* stream);
+
+/* Diagnostic: element-wise Goldilocks primitives of the kernels on device
+ * buffers, for testing them against exact integer arithmetic. op: 0 a+b,
+ * 1 a-b, 2 a*b (a, b canonical); 3 c + a*b (any 64-bit a, b, c); 4 reduction
+ * of the 128-bit value a + 2^64 b; 5 canonical form of a. Results canonical.
+ * No reference counterpart (internal arithmetic check). */
+tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out_dev, const uint64_t* a_dev, const uint64_t* b_dev,
+                         const uint64_t* c_dev, void* stream);
 
 /* Message for the last failing call on this thread ("" if none). */
 const char* tp_last_error(void);
