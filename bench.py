@@ -1,0 +1,391 @@
+"""Benchmark of the batched blind rotation on B200 (one JSON line on rank 0).
+
+Workload (default): batched CGGI blind rotation with a ternary LWE secret,
+n = 630, N = 2048, Goldilocks, signed gadget base 2^12 with l = 3; 4096
+independent LWE ciphertexts per step, each with its own seeded 16-entry LUT
+test polynomial (trivial RLWE, coefficient domain), NTT-domain output. One
+step = one persistent launch over the whole batch.
+
+  value  blind rotations/s with inputs resident in HBM (kernel time, CUDA events)
+  e2e    the same through the host-buffer C-ABI call (tp_br_blind_rotate_batch_host):
+         host->device copy of the step's LWEs and test polynomials, the launch,
+         device->host copy of the results, all inside the timed region
+  plain  the one-rotation-per-launch form (batch 1) for the batched/plain ratio
+
+`--impl reference` times the reference library's own CPU blind rotation (built
+from its sources into oracle/_ref/, one rotator per host thread) on a bounded
+sample of the same workload. Multi-GPU runs (torchrun) shard the batch: every
+rank rotates its own 4096 ciphertexts, no collective on the data path
+(weak scaling); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+P = 0xFFFFFFFF00000001
+
+WORKLOADS = {
+    # name: variant, N, n, basis_log2, digits, batch
+    "cggi_ternary_n2048": (1, 2048, 630, 12, 3, 4096),
+    "cggi_binary_n1024": (0, 1024, 500, 16, 4, 4096),
+    "bmmp_binary_n2048": (2, 2048, 768, 16, 4, 2048),
+    "cggi_ternary_n4096": (1, 4096, 900, 12, 3, 1024),
+}
+DESCR = {
+    "cggi_ternary_n2048": "batched CGGI blind rotation, ternary n=630, N=2048, Goldilocks, base 2^12 l=3",
+    "cggi_binary_n1024": "CGGI blind rotation, binary n=500, N=1024, Goldilocks, base 2^16 l=4",
+    "bmmp_binary_n2048": "BMMP blind rotation, binary n=768 (384 pairs), N=2048, base 2^16 l=4",
+    "cggi_ternary_n4096": "CGGI blind rotation, ternary n=900, N=4096, base 2^12 l=3",
+}
+
+
+def ntt_mm(N: int) -> int:
+    return N // 2 * (N.bit_length() - 1)
+
+
+def modmul_per_iteration(variant: int, N: int, l: int) -> int:
+    """Algorithmic modmul count of one CMux iteration (NTT counted as N/2 log2 N)."""
+    if variant == 0:
+        return 2 * N + (2 + 2 * l) * ntt_mm(N) + 4 * l * N
+    if variant == 1:
+        return (2 + 2 * l) * ntt_mm(N) + 8 * l * N + 4 * N
+    return (2 + 2 * l) * ntt_mm(N) + 12 * l * N + 6 * N
+
+
+def workload_modmuls(variant: int, N: int, n: int, l: int, lwes: np.ndarray) -> int:
+    """Modmuls of one launch over `lwes` (CGGI skips a_i = 0, BMMP does not)."""
+    if variant == 2:
+        iters = lwes.shape[0] * (n // 2)
+    else:
+        iters = int(np.count_nonzero(lwes[:, :n]))
+    edge = lwes.shape[0] * (2 * ntt_mm(N) + 2 * N)  # prologue NTTs and X^b
+    return iters * modmul_per_iteration(variant, N, l) + edge
+
+
+def lut_polys(N: int, count: int, seed: int) -> np.ndarray:
+    """count x 2N trivial RLWEs (A = 0) of random 16-entry negacyclic LUT test polynomials."""
+    from oracle.oracle import sm64
+    delta = P // 16
+    tables = (sm64(seed, count * 16) % np.uint64(16)).reshape(count, 16)
+    vals = np.array([(int(v) * delta) % P for v in range(16)], dtype=np.uint64)
+    B = np.repeat(vals[tables.astype(np.int64)], N // 16, axis=1)
+    return np.concatenate([np.zeros((count, N), np.uint64), B], axis=1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profiles(workload: str):
+    """DRAM bytes per launch from the committed ncu summary of this workload, if any."""
+    f = ROOT / "profiles" / "traffic.json"
+    if not f.exists():
+        return None, None
+    d = json.loads(f.read_text()).get(workload)
+    if not d:
+        return None, None
+    return d.get("dram_bytes_per_launch"), d.get("source")
+
+
+def cpu_reference_sample(variant, N, n, bl, l, lwes, accs, seconds_target=15.0):
+    """Times the reference library's CPU blind rotation on a bounded sample,
+    one rotator per host thread. Returns (BR/s, threads, rotations, seconds)."""
+    import ctypes
+
+    from oracle.oracle import Reference, lwe_secret, ptr, rlwe_secret
+    ref = Reference()
+    L = ref.L
+    cores = os.cpu_count() or 1
+    key_bytes = (n if variant < 2 else n // 2) * (1 if variant == 0 else (2 if variant == 1 else 3)) * 4 * N * l * 8
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        avail = 16 << 30
+    threads = max(1, min(cores, int(avail * 0.5 // max(key_bytes, 1))))
+    lk = lwe_secret(variant, n, N, 1)
+    rk = rlwe_secret(N, 2)
+    L.ref_seed(3)
+    h = L.ref_br_create(variant, N, n, bl, l, 0.0, ptr(lk), ptr(rk))
+    # one warm rotation to size the sample
+    one = np.empty(2 * N, np.uint64)
+    t0 = time.perf_counter()
+    L.ref_br_rotate(h, ptr(one), ptr(np.ascontiguousarray(lwes[0])), ptr(np.ascontiguousarray(accs[0])), 0)
+    t1 = time.perf_counter() - t0
+    per_thread = max(1, int(seconds_target / max(t1, 1e-3) / 4))
+    count = min(threads * per_thread, lwes.shape[0])
+    res = np.empty((count, 2 * N), np.uint64)
+    secs = L.ref_br_rotate_many(h, ptr(res), ptr(np.ascontiguousarray(lwes[:count])),
+                                ptr(np.ascontiguousarray(accs[:count])), count, 0, threads)
+    L.ref_br_destroy(h)
+    return count / secs, threads, count, secs
+
+
+def run_reference(args, wl):
+    variant, N, n, bl, l, batch = WORKLOADS[wl]
+    from oracle.oracle import lwe_inputs
+    lwes = lwe_inputs(N, n, batch, 7)
+    accs = lut_polys(N, batch, 8)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, threads, count, secs = cpu_reference_sample(variant, N, n, bl, l, lwes, accs,
+                                                       seconds_target=args.ref_seconds)
+        if s >= args.warmup:
+            vals.append((v, threads, count, secs))
+    v = statistics.median([x[0] for x in vals])
+    threads, count = vals[-1][1], vals[-1][2]
+    cfg = {"workload": DESCR[wl], "batch": batch, "ring_dim": N, "lwe_dim": n, "gadget": f"2^{bl} l={l}",
+           "inputs": "seeded synthetic LWEs + per-ciphertext LUT test polynomials"}
+    line = {"impl": "reference", "metric": "blind rotations/sec", "value": round(v, 3), "unit": "BR/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(statistics.median([x[3] for x in vals]) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": round(v, 3), "unit": "BR/s", "cores": threads, "kind": "reference",
+                             "sample": f"{count} rotations per step on {threads} threads (one rotator each), "
+                                       "reference library built from its own sources (oracle/_ref)"},
+            "e2e": {"value": round(v, 3), "unit": "BR/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cggi_ternary_n2048", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=0, help="override the per-GPU batch")
+    ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = args.workload
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, wl)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator, _native
+    from oracle.oracle import lwe_inputs
+
+    variant, N, n, bl, l, batch = WORKLOADS[wl]
+    if args.batch:
+        batch = args.batch
+    ctx = BlindRotationContext(variant, N, n, 1 << bl, l)
+    # Key words are uniform residues: timing does not depend on their values
+    # (parity with real keys is covered by the test suite).
+    kw = ctx.key_words()
+    rng = np.random.default_rng(1234 + rank)
+    brk = rng.integers(0, 2**63, kw, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, kw, dtype=np.uint64)
+    brk = np.where(brk >= np.uint64(P), brk - np.uint64(P), brk)
+    rot = GpuBlindRotator(ctx, brk, device=local)
+    del brk
+
+    lwes_h = lwe_inputs(N, n, batch, 7 + 1000 * rank)
+    accs_h = lut_polys(N, batch, 8 + 1000 * rank)
+    lw = torch.from_numpy(lwes_h.view(np.int64)).cuda()
+    ac = torch.from_numpy(accs_h.view(np.int64)).cuda()
+    out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        rot.blind_rotate_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch, stream=stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        barrier()
+    rot.check(stream)
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = batch * world / (ms * 1e-3)
+    launches = args.steps
+
+    # end-to-end through the host-buffer call: pinned host inputs, copies inside
+    lw_p = torch.from_numpy(lwes_h.view(np.int64)).pin_memory()
+    ac_p = torch.from_numpy(accs_h.view(np.int64)).pin_memory()
+    res_p = torch.empty((batch, 2 * N), dtype=torch.int64).pin_memory()
+    L = _native.lib()
+
+    def e2e_step():
+        _native.check(L.tp_br_blind_rotate_batch_host(
+            rot.handle, batch, _native.ctypes.cast(res_p.data_ptr(), _native.U64P),
+            _native.ctypes.cast(lw_p.data_ptr(), _native.U64P), n + 1,
+            _native.ctypes.cast(ac_p.data_ptr(), _native.U64P), 2 * N, 0, stream))
+
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(1):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = batch * world / e2e_s
+    launches += e2e_steps + 1
+    h2d = lwes_h.nbytes + accs_h.nbytes
+    d2h = batch * 2 * N * 8
+
+    # plain form: one rotation per launch
+    one_out = torch.empty((1, 2 * N), dtype=torch.int64, device="cuda")
+    plain_reps = 3
+    rot.blind_rotate_batch(one_out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, 1, stream=stream)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(plain_reps):
+        rot.blind_rotate_batch(one_out.data_ptr(), lw[i:].data_ptr(), n + 1, ac[i:].data_ptr(), 2 * N, 1,
+                               stream=stream)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / plain_reps
+    launches += plain_reps + 1
+
+    # roofline: algorithmic modmuls per launch over the kernel's launch time,
+    # against the measured 64x64->128 product rate of this GPU
+    import ctypes
+    prod, imad = ctypes.c_double(), ctypes.c_double()
+    _native.check(L.tp_measure_int_peak(local, ctypes.byref(prod), ctypes.byref(imad)))
+    mm = workload_modmuls(variant, N, n, l, lwes_h)
+    achieved = mm / (ms * 1e-3)
+    traffic, tsrc = traffic_from_profiles(wl)
+    key_bytes = kw * 8
+
+    line = {
+        "metric": "blind rotations/sec", "value": round(value, 2), "unit": "BR/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)", "data": "synthetic",
+        "config": {"workload": DESCR[wl], "batch_per_gpu": batch, "ring_dim": N, "lwe_dim": n,
+                   "gadget": f"2^{bl} l={l}", "output": "NTT domain",
+                   "l2": f"inputs larger than L2: {key_bytes / 2**20:.0f} MiB key streamed per launch",
+                   "key": "uniform random key words (timing does not depend on key values)"},
+        "e2e": {"value": round(e2e_val, 2), "unit": "BR/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "plain": {"value": round(1e3 / plain_ms, 3), "unit": "BR/s", "ms_per_rotation": round(plain_ms, 3),
+                  "batched_over_plain": round(value / world / (1e3 / plain_ms), 1)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "int32", "achieved": round(achieved / 1e9, 1), "peak": round(prod.value / 1e9, 1),
+                     "unit": "Gmodmul/s", "frac": round(achieved / prod.value, 4), "traffic": traffic,
+                     "traffic_source": tsrc,
+                     "peak_source": "measured 64x64->128 IMAD-chain product rate of this GPU (tp_measure_int_peak)",
+                     "imad_per_s": round(imad.value / 1e12, 2),
+                     "algorithmic_modmul_per_launch": mm,
+                     "key_hbm": {"bytes_per_launch": key_bytes,
+                                 "achieved_gbs": round(key_bytes / (ms * 1e-3) / 1e9, 1)}},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, threads, count, secs = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
+                                                           seconds_target=args.ref_seconds)
+            line["cpu_baseline"] = {"value": round(v, 3), "unit": "BR/s", "cores": threads, "kind": "reference",
+                                    "sample": f"{count} rotations on {threads} threads in {secs:.1f}s "
+                                              "(reference library, one rotator per thread)"}
+        except Exception as exc:  # the baseline is reported, not required
+            line["cpu_baseline"] = {"value": None, "unit": "BR/s", "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {exc}"}
+    rot.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -60,6 +60,8 @@ def lib() -> ctypes.CDLL:
         "tp_ntt_forward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_ntt_backward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_debug_arith": (ctypes.c_int, [ctypes.c_int, U64, VP, VP, VP, VP, VP]),
+        "tp_measure_int_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                ctypes.POINTER(ctypes.c_double)]),
         "tp_last_error": (ctypes.c_char_p, []),
         "tp_version": (ctypes.c_char_p, []),
     }

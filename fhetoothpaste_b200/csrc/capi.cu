@@ -424,6 +424,38 @@ tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out, const uint64_t* 
     return TP_OK;
 }
 
+tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_per_s) {
+    if (!products_per_s || !imad_per_s) return fail(TP_ERR_PARAM, "null argument");
+    TP_CUDA(cudaSetDevice(device));
+    const int threads = 256, per_sm = 8, iters = 2048;
+    const int blocks = sm_count(device) * per_sm;
+    uint64_t* out = nullptr;
+    TP_CUDA(cudaMalloc(&out, (size_t)blocks * threads * 8));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float ms[2] = {0, 0};
+    for (int mode = 0; mode < 2; ++mode) {
+        for (int rep = 0; rep < 3; ++rep) {  // last repetition is timed
+            cudaEventRecord(e0);
+            if (mode == 0) tp::int_peak_kernel<0><<<blocks, threads>>>(out, 12345, iters);
+            else tp::int_peak_kernel<1><<<blocks, threads>>>(out, 12345, iters);
+            cudaEventRecord(e1);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms[mode], e0, e1);
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "peak probe: %s", cudaGetErrorString(e));
+    const double ops = (double)blocks * threads * iters * 8;
+    *products_per_s = ops / (ms[0] * 1e-3);
+    *imad_per_s = 4 * ops / (ms[1] * 1e-3);
+    return TP_OK;
+}
+
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd) {
     if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))

@@ -68,4 +68,37 @@ __global__ void debug_arith_kernel(int op, uint64_t count, uint64_t* __restrict_
     }
 }
 
+// INT32 peak probes: independent chains of 64x64->128 products (mul_wide,
+// exactly as the kernels issue them) or of 32-bit mad.lo.
+template <int MODE>
+__global__ void int_peak_kernel(uint64_t* out, uint64_t seed, int iters) {
+    uint64_t a[8], b[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        a[j] = (seed * (threadIdx.x + 1 + j) + j) % kP;
+        b[j] = (a[j] ^ 0x9E3779B97F4A7C15ull) % kP;
+    }
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (MODE == 0) {
+                uint32_t r0, r1, r2, r3;
+                mul_wide(a[j], b[j], r0, r1, r2, r3);
+                a[j] = pack64(r0 ^ r2, r1 ^ r3);
+            } else {
+                uint32_t x = lo32(a[j]), y = lo32(b[j]), z = hi32(a[j]);
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x) : "r"(y), "r"(z));
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(z) : "r"(y), "r"(x));
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x) : "r"(y), "r"(z));
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(z) : "r"(y), "r"(x));
+                a[j] = pack64(x, z);
+            }
+        }
+    }
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s ^= a[j] ^ b[j];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace tp

@@ -127,6 +127,13 @@ tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, 
 tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out_dev, const uint64_t* a_dev, const uint64_t* b_dev,
                          const uint64_t* c_dev, void* stream);
 
+/* Measures, on `device`, the throughput of the 64x64 -> 128-bit integer
+ * product every Goldilocks modmul needs (32-bit IMAD chains, as in the
+ * kernels) and of plain 32-bit mad.lo, in operations per second. The
+ * benchmark uses the product rate as the INT32 roof. No reference
+ * counterpart. */
+tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_per_s);
+
 /* Message for the last failing call on this thread ("" if none). */
 const char* tp_last_error(void);
 
