@@ -71,9 +71,11 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
 }
 
 // Resident blocks per SM the kernel is compiled for (register budget
-// 65536 / (T * blocks)); N = 4096 needs 200 KB of shared memory, so one block.
+// 65536 / (T * blocks)). From N = 2048 up one block per SM with the full
+// register file measured faster than two blocks that spill (ternary N = 2048:
+// 6.0k vs 5.3k rotations/s); N = 4096 needs 200 KB of shared memory anyway.
 __host__ __device__ constexpr int br_min_blocks(int logn, int variant) {
-    return (logn >= 12 || variant == kBmmpBinary) ? 1 : 2;
+    return (logn >= 12 || (logn == 11 && variant != kCggiBinary) || variant == kBmmpBinary) ? 1 : 2;
 }
 
 template <int LOGN, int VARIANT>

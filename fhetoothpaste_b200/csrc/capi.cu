@@ -9,7 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/toothpaste_gpu.h"
+#include "toothpaste_gpu.h"
 #include "br_kernels.cuh"
 #include "dispatch.h"
 #include "misc_kernels.cuh"
