@@ -222,6 +222,9 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="override the per-GPU batch")
     ap.add_argument("--ref-seconds", type=float, default=15.0, help="CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="full", choices=["full", "kernel"],
+                    help="kernel: only warm-up + timed batch launches (for profiler captures)")
+    ap.add_argument("--lwe-dim", type=int, default=0, help="override n (smaller profiler captures)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +252,8 @@ def main():
     variant, N, n, bl, l, batch = WORKLOADS[wl]
     if args.batch:
         batch = args.batch
+    if args.lwe_dim:
+        n = args.lwe_dim
     ctx = BlindRotationContext(variant, N, n, 1 << bl, l)
     # Key words are uniform residues: timing does not depend on their values
     # (parity with real keys is covered by the test suite).
@@ -286,6 +291,14 @@ def main():
         barrier()
     rot.check(stream)
     ms = e0.elapsed_time(e1) / args.steps
+    if args.mode == "kernel":
+        if rank == 0:
+            print(json.dumps({"mode": "kernel", "workload": wl, "batch": batch, "lwe_dim": n,
+                              "ms_per_launch": round(ms, 3), "rotations_per_s": round(batch / (ms * 1e-3), 1)}))
+        rot.close()
+        if dist:
+            dist.destroy_process_group()
+        return
     if dist:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -59,6 +59,22 @@ def lib() -> ctypes.CDLL:
         "tp_sample_extract_batch": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_ntt_forward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_ntt_backward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
+        "tp_rlwe_ks_create": (ctypes.c_int, [ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(VP)]),
+        "tp_auto_create": (ctypes.c_int, [ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                          ctypes.POINTER(VP)]),
+        "tp_pack_create": (ctypes.c_int, [ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(VP)]),
+        "tp_ks_destroy": (ctypes.c_int, [VP]),
+        "tp_ks_key_words": (U64, [VP]),
+        "tp_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
+        "tp_rlwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_auto_eval_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_pack_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
+        "tp_lwe_ks_create": (ctypes.c_int, [U64, ctypes.c_uint32, ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_int,
+                                            ctypes.POINTER(VP)]),
+        "tp_lwe_ks_destroy": (ctypes.c_int, [VP]),
+        "tp_lwe_ks_key_words": (U64, [VP]),
+        "tp_lwe_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
+        "tp_lwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
         "tp_debug_arith": (ctypes.c_int, [ctypes.c_int, U64, VP, VP, VP, VP, VP]),
         "tp_measure_int_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]),

@@ -14,6 +14,8 @@
 #include "dispatch.h"
 #include "misc_kernels.cuh"
 #include "util_kernels.cuh"
+#include "ks_kernels.cuh"
+#include "ks_util_kernels.cuh"
 
 namespace {
 
@@ -127,6 +129,42 @@ int sm_count(int device) {
     int v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
     return v > 0 ? v : 1;
+}
+
+// Signed-digit constants of SignedGadgetDecomposeRepNTT on a 64-bit modulus
+// (lib/include/static/gadget_decomp.h:16-28,156-205).
+void signed_digit_consts(int beta, uint32_t digits, uint64_t& corr, uint32_t* dshift, uint64_t* dmask,
+                         uint64_t* ddelta) {
+    const int max_digits = (64 + beta - 1) / beta;
+    uint64_t c = 0;
+    int64_t shift = 64 - beta;
+    while (shift > 0) {
+        c += 1ull << (shift + beta - 1);
+        shift -= beta;
+    }
+    const uint64_t least = 1ull << (shift + beta - 1);
+    c += least;
+    corr = c % kP;
+    int64_t sh = 64 - beta;
+    uint64_t mask = (1ull << beta) - 1;
+    for (uint32_t d = 0; d < digits; ++d) {
+        uint64_t delta = 1ull << (beta - 1);
+        if ((int)d == max_digits - 1) {
+            delta = least;
+            sh = 0;
+            mask = (delta << 1) - 1;
+        }
+        dshift[d] = (uint32_t)sh;
+        dmask[d] = mask;
+        ddelta[d] = delta;
+        sh -= beta;
+    }
+}
+
+uint32_t inv_mod_2n(uint32_t t, uint32_t two_n) {
+    for (uint32_t x = 1; x < two_n; x += 2)
+        if ((uint64_t)x * t % two_n == 1) return x;
+    return 0;
 }
 
 }  // namespace
@@ -453,6 +491,329 @@ tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_p
     const double ops = (double)blocks * threads * iters * 8;
     *products_per_s = ops / (ms[0] * 1e-3);
     *imad_per_s = 4 * ops / (ms[1] * 1e-3);
+    return TP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Key switching contexts: RLWE -> RLWE, automorphism, packing
+// ---------------------------------------------------------------------------
+struct tp_ks_ctx {
+    int kind = 0;                 // 0 RLWE KS, 1 automorphism, 2 packing
+    int device = 0;
+    int logn = 0;
+    uint32_t N = 0;
+    uint32_t digits = 0;
+    uint32_t index = 0;           // automorphism index (kind 1)
+    int nkeys = 1;                // packing: logN keys, index 2^j + 1, j = 1..logN
+    uint64_t key_words = 0;
+    const Tables* tab = nullptr;
+    uint64_t* key = nullptr;
+    bool key_ready = false;
+    tp::KsKernelParams kp{};
+    size_t smem = 0;
+    int per_sm[4] = {0, 0, 0, 0};
+    uint64_t* work = nullptr;     // packing tree nodes
+    uint64_t work_words = 0;
+    std::mutex mu;
+};
+
+static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t digits, uint32_t index, int device,
+                           tp_ks_ctx** out) {
+    if (!out) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (basis < 2 || (basis & (basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
+    const int beta = ilog2(basis);
+    if (beta > 30) return fail(TP_ERR_PARAM, "basis above 2^30 is not supported");
+    const int max_digits = (64 + beta - 1) / beta;
+    if (digits < 1 || digits > 8 || (int)digits > max_digits)
+        return fail(TP_ERR_PARAM, "digits must be in [1, min(8, ceil(64/beta))]");
+    if (kind == 1 && (index % 2 == 0 || index >= 2 * ring_dim))
+        return fail(TP_ERR_PARAM, "automorphism index must be odd and below 2N");
+    auto* c = new tp_ks_ctx();
+    c->kind = kind;
+    c->device = device;
+    c->N = ring_dim;
+    c->logn = ilog2(ring_dim);
+    c->digits = digits;
+    c->index = index;
+    c->nkeys = kind == 2 ? c->logn : 1;
+    c->key_words = (uint64_t)c->nkeys * digits * 2 * ring_dim;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(TP_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    }
+    tp_status s = get_tables(device, c->logn, &c->tab);
+    if (s != TP_OK) {
+        delete c;
+        return s;
+    }
+    tp::KsKernelParams& kp = c->kp;
+    kp.tw_fwd = c->tab->tw_fwd;
+    kp.tw_inv = c->tab->tw_inv;
+    kp.digits = digits;
+    kp.n_inv = c->tab->n_inv;
+    signed_digit_consts(beta, digits, kp.corr, kp.dshift, kp.dmask, kp.ddelta);
+    c->smem = tp::ks_smem_words(ring_dim) * 8;
+    for (int mode = 0; mode < 4; ++mode) {
+        const void* k = tp::ks_kernel_lookup(c->logn, mode);
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->per_sm[mode], k, ring_dim / 8, c->smem);
+        if (e != cudaSuccess || c->per_sm[mode] < 1) {
+            delete c;
+            return fail(TP_ERR_CUDA, "key-switch kernel set-up: %s", cudaGetErrorString(e));
+        }
+    }
+    *out = c;
+    return TP_OK;
+}
+
+tp_status tp_rlwe_ks_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, int device, tp_ks_ctx** out) {
+    return ks_create(0, ring_dim, basis, digits, 0, device, out);
+}
+
+tp_status tp_auto_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, uint32_t index, int device,
+                         tp_ks_ctx** out) {
+    return ks_create(1, ring_dim, basis, digits, index, device, out);
+}
+
+tp_status tp_pack_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, int device, tp_ks_ctx** out) {
+    return ks_create(2, ring_dim, basis, digits, 0, device, out);
+}
+
+tp_status tp_ks_destroy(tp_ks_ctx* c) {
+    if (!c) return TP_OK;
+    cudaSetDevice(c->device);
+    cudaFree(c->key);
+    cudaFree(c->work);
+    delete c;
+    return TP_OK;
+}
+
+uint64_t tp_ks_key_words(const tp_ks_ctx* c) { return c ? c->key_words : 0; }
+
+tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
+    if (!c || !ksk) return fail(TP_ERR_PARAM, "null argument");
+    if (words != c->key_words)
+        return fail(TP_ERR_LAYOUT, "key has %llu words, context expects %llu", (unsigned long long)words,
+                    (unsigned long long)c->key_words);
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    if (!c->key) TP_CUDA(cudaMalloc(&c->key, c->key_words * 8));
+    uint64_t* stage = nullptr;
+    TP_CUDA(cudaMalloc(&stage, c->key_words * 8));
+    cudaError_t e = cudaMemcpy(stage, ksk, c->key_words * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        // each key: l rows of [A | B] (the reference's m_ksk) -> [row][c][jp][t][2]
+        const uint64_t total = c->key_words;
+        const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 65535);
+        tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(stage);
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "key upload: %s", cudaGetErrorString(e));
+    c->key_ready = true;
+    return TP_OK;
+}
+
+static tp_status ks_launch(tp_ks_ctx* c, int mode, const tp::KsKernelParams& kp, cudaStream_t st) {
+    const uint64_t grid = std::min<uint64_t>(kp.items, (uint64_t)c->per_sm[mode] * sm_count(c->device));
+    tp::KsKernelParams p = kp;
+    void* args[] = {&p};
+    TP_CUDA(cudaLaunchKernel(tp::ks_kernel_lookup(c->logn, mode), dim3((unsigned)grid), dim3(c->N / 8), args, c->smem,
+                             st));
+    return TP_OK;
+}
+
+tp_status tp_rlwe_ks_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
+    if (!c || c->kind != 0) return fail(TP_ERR_PARAM, "not an RLWE key-switching context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::KsKernelParams kp = c->kp;
+    kp.key = c->key;
+    kp.in = in;
+    kp.out = out;
+    kp.items = batch;
+    kp.in_stride = kp.out_stride = 2ull * c->N;
+    return ks_launch(c, tp::kKsRlwe, kp, (cudaStream_t)stream);
+}
+
+tp_status tp_auto_eval_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
+    if (!c || c->kind != 1) return fail(TP_ERR_PARAM, "not an automorphism context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    if (out == in) return fail(TP_ERR_PARAM, "automorphism output must not alias its input");
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::KsKernelParams kp = c->kp;
+    kp.key = c->key;
+    kp.in = in;
+    kp.out = out;
+    kp.items = batch;
+    kp.in_stride = kp.out_stride = 2ull * c->N;
+    kp.auto_index = c->index;
+    kp.auto_index_inv = inv_mod_2n(c->index, 2 * c->N);
+    return ks_launch(c, tp::kKsAuto, kp, (cudaStream_t)stream);
+}
+
+tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out, const uint64_t* in, void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (packs == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->N;
+    if (len < 2 || len > N || (len & (len - 1))) return fail(TP_ERR_PARAM, "len must be a power of two in [2, N]");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    const uint64_t need = packs * len * 2 * N;
+    if (c->work_words < need) {
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_words = 0;
+        TP_CUDA(cudaMalloc(&c->work, need * 8));
+        c->work_words = need;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int log_len = ilog2(len);
+    {
+        const uint64_t blocks = std::min<uint64_t>((need + 255) / 256, 65535 * 4ull);
+        tp::pack_l0_kernel<<<(unsigned)std::min<uint64_t>(blocks, 65535), 256, 0, st>>>(
+            c->work, in, packs, (uint32_t)len, (uint32_t)log_len, (uint32_t)c->logn, c->tab->n_inv);
+        TP_CUDA(cudaGetLastError());
+    }
+    const uint64_t kw = (uint64_t)c->digits * 2 * N;
+    tp::KsKernelParams kp = c->kp;
+    // tree merges, level by level (lwe_to_rlwe_packing.cpp:170-224)
+    for (int L = 1; L <= log_len; ++L) {
+        kp.key = c->key + (uint64_t)(L - 1) * kw;
+        kp.in = c->work;
+        kp.out = c->work;
+        kp.items = packs * (len >> L);
+        kp.in_stride = kp.out_stride = (1ull << L) * 2 * N;
+        kp.right_offset = (1ull << (L - 1)) * 2 * N;
+        kp.auto_index = (1u << L) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = (uint32_t)(N >> L);
+        tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
+        if (s != TP_OK) return s;
+    }
+    // trailing traces when len < N (lwe_to_rlwe_packing.cpp:228-234)
+    for (int i = 0; i < c->logn - log_len; ++i) {
+        const int j = c->logn - i;
+        kp.key = c->key + (uint64_t)(j - 1) * kw;
+        kp.in = c->work;
+        kp.out = c->work;
+        kp.items = packs;
+        kp.in_stride = kp.out_stride = len * 2 * N;
+        kp.right_offset = 0;
+        kp.auto_index = (1u << j) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = 0;
+        tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+        if (s != TP_OK) return s;
+    }
+    TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, c->work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
+    return TP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// LWE -> LWE key switching
+// ---------------------------------------------------------------------------
+struct tp_lwe_ks_ctx {
+    int device = 0;
+    uint32_t n_in = 0, n_out = 0, digits = 0;
+    uint64_t key_words = 0;
+    uint64_t* key = nullptr;
+    bool key_ready = false;
+    tp::LweKsParams kp{};
+};
+
+tp_status tp_lwe_ks_create(uint64_t modulus, uint32_t n_in, uint32_t n_out, uint64_t basis, uint32_t digits,
+                           int device, tp_lwe_ks_ctx** out) {
+    if (!out) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    if (modulus != kP) return fail(TP_ERR_PARAM, "the GPU LWE key switch runs on the Goldilocks modulus only");
+    if (n_in == 0 || n_out == 0) return fail(TP_ERR_PARAM, "dimensions must be positive");
+    if (basis < 2 || (basis & (basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
+    const int beta = ilog2(basis);
+    if (beta > 30) return fail(TP_ERR_PARAM, "basis above 2^30 is not supported");
+    // LWEtoLWEConverter::Convert shifts by 64 - beta - j*beta for every digit j
+    // (lwe_conversion.cpp:226-236); every shift must stay non-negative.
+    if (digits < 1 || digits > 8 || (uint64_t)digits * beta > 64)
+        return fail(TP_ERR_PARAM, "digits * log2(basis) must be at most 64 (and digits at most 8)");
+    auto* c = new tp_lwe_ks_ctx();
+    c->device = device;
+    c->n_in = n_in;
+    c->n_out = n_out;
+    c->digits = digits;
+    c->key_words = (uint64_t)n_in * digits * (n_out + 1);
+    tp::LweKsParams& kp = c->kp;
+    kp.n_in = n_in;
+    kp.n_out = n_out;
+    kp.digits = digits;
+    const int max_digits = (64 + beta - 1) / beta;
+    uint64_t corr = 0;
+    int64_t shift = 64 - beta;
+    while (shift > 0) {
+        corr += 1ull << (shift + beta - 1);
+        shift -= beta;
+    }
+    const uint64_t least = 1ull << (shift + beta - 1);
+    corr += least;
+    kp.corr = corr % kP;
+    for (uint32_t j = 0; j < digits; ++j) {
+        kp.dshift[j] = (uint32_t)(64 - beta - (int)j * beta);
+        kp.dmask[j] = (1ull << beta) - 1;
+        kp.ddelta[j] = (int)j != max_digits - 1 ? 1ull << (beta - 1) : least;
+    }
+    *out = c;
+    return TP_OK;
+}
+
+tp_status tp_lwe_ks_destroy(tp_lwe_ks_ctx* c) {
+    if (!c) return TP_OK;
+    cudaSetDevice(c->device);
+    cudaFree(c->key);
+    delete c;
+    return TP_OK;
+}
+
+uint64_t tp_lwe_ks_key_words(const tp_lwe_ks_ctx* c) { return c ? c->key_words : 0; }
+
+tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
+    if (!c || !ksk) return fail(TP_ERR_PARAM, "null argument");
+    if (words != c->key_words)
+        return fail(TP_ERR_LAYOUT, "key has %llu words, context expects %llu", (unsigned long long)words,
+                    (unsigned long long)c->key_words);
+    TP_CUDA(cudaSetDevice(c->device));
+    if (!c->key) TP_CUDA(cudaMalloc(&c->key, c->key_words * 8));
+    TP_CUDA(cudaMemcpy(c->key, ksk, c->key_words * 8, cudaMemcpyHostToDevice));
+    c->key_ready = true;
+    return TP_OK;
+}
+
+tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    if (batch > 65535ull * tp::kLweKsRows) return fail(TP_ERR_PARAM, "batch too large for one launch");
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::LweKsParams kp = c->kp;
+    kp.ksk = c->key;
+    kp.in = in;
+    kp.out = out;
+    kp.batch = batch;
+    dim3 grid((c->n_out + 1 + tp::kLweKsCols - 1) / tp::kLweKsCols,
+              (unsigned)((batch + tp::kLweKsRows - 1) / tp::kLweKsRows));
+    tp::lwe_ks_kernel<<<grid, tp::kLweKsCols, 0, (cudaStream_t)stream>>>(kp);
+    TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
 

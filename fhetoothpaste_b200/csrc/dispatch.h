@@ -15,6 +15,12 @@ const void* br_kernel_ptr_11(int variant);
 const void* ntt_kernel_ptr_11(bool forward);
 const void* br_kernel_ptr_12(int variant);
 const void* ntt_kernel_ptr_12(bool forward);
+const void* ks_kernel_ptr_7(int mode);
+const void* ks_kernel_ptr_8(int mode);
+const void* ks_kernel_ptr_9(int mode);
+const void* ks_kernel_ptr_10(int mode);
+const void* ks_kernel_ptr_11(int mode);
+const void* ks_kernel_ptr_12(int mode);
 
 inline const void* br_kernel_lookup(int logn, int variant) {
     switch (logn) {
@@ -36,6 +42,18 @@ inline const void* ntt_kernel_lookup(int logn, bool forward) {
         case 10: return ntt_kernel_ptr_10(forward);
         case 11: return ntt_kernel_ptr_11(forward);
         case 12: return ntt_kernel_ptr_12(forward);
+        default: return nullptr;
+    }
+}
+
+inline const void* ks_kernel_lookup(int logn, int mode) {
+    switch (logn) {
+        case 7: return ks_kernel_ptr_7(mode);
+        case 8: return ks_kernel_ptr_8(mode);
+        case 9: return ks_kernel_ptr_9(mode);
+        case 10: return ks_kernel_ptr_10(mode);
+        case 11: return ks_kernel_ptr_11(mode);
+        case 12: return ks_kernel_ptr_12(mode);
         default: return nullptr;
     }
 }

@@ -2,6 +2,7 @@
 // ring sizes build in parallel).
 #include "br_kernels.cuh"
 #include "dispatch.h"
+#include "ks_kernels.cuh"
 #include "misc_kernels.cuh"
 
 namespace tp {
@@ -16,6 +17,15 @@ const void* br_kernel_ptr_8(int variant) {
 
 const void* ntt_kernel_ptr_8(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<8, true> : (const void*)ntt_batch_kernel<8, false>;
+}
+
+const void* ks_kernel_ptr_8(int mode) {
+    switch (mode) {
+        case kKsRlwe: return (const void*)ks_kernel<8, kKsRlwe>;
+        case kKsAuto: return (const void*)ks_kernel<8, kKsAuto>;
+        case kKsMerge: return (const void*)ks_kernel<8, kKsMerge>;
+        default: return (const void*)ks_kernel<8, kKsTrace>;
+    }
 }
 
 }  // namespace tp

@@ -1,0 +1,200 @@
+// Key switching on the GPU: RLWE -> RLWE key switch, automorphism evaluation,
+// the merge/trace steps of n-LWE -> RLWE packing, and LWE -> LWE key switch.
+//
+// The RLWE kernels share one core with the blind rotation: a block of
+// T = N/8 threads takes the coefficient-domain A part of one ciphertext, forms
+// its signed gadget digits (lib/include/static/gadget_decomp.h:156-205), runs a
+// forward NTT per digit and multiply-accumulates against the key rows
+// (lib/src/operators/rlwe_conversion.cpp:224-249). Key rows are laid out like
+// the blind-rotation key (C = 2 components, A and B, per slot).
+#pragma once
+
+#include "gl_arith.cuh"
+#include "ntt_block.cuh"
+
+namespace tp {
+
+enum KsMode : int {
+    kKsRlwe = 0,   // out -= KS(in.A coef); out.B += in.B (NTT)
+    kKsAuto = 1,   // out -= KS(aut_t(in.A)); out.B += NTT(aut_t(in.B)); in coefficient domain
+    kKsMerge = 2,  // packing merge: left <- (right + X^s left) + INTT(AutoKS(right - X^s left))
+    kKsTrace = 3   // trace step:    x <- x + INTT(AutoKS(x))
+};
+
+struct KsKernelParams {
+    const uint64_t* key;      // device layout: [digit][c][jp][t][2], C = 2
+    const uint64_t* tw_fwd;
+    const uint64_t* tw_inv;
+    const uint64_t* in;       // per item: 2N words (kKsRlwe/kKsAuto), node pairs (kKsMerge), node (kKsTrace)
+    uint64_t* out;
+    uint64_t items;           // ciphertexts (or merges)
+    uint64_t in_stride;       // words between items' inputs
+    uint64_t out_stride;      // words between items' outputs
+    uint64_t right_offset;    // kKsMerge: words from left node to right node
+    uint32_t digits;
+    uint32_t auto_index;      // t (odd)
+    uint32_t auto_index_inv;  // t^-1 mod 2N
+    uint32_t shift;           // kKsMerge: X^shift rotation of the left node
+    uint64_t n_inv;
+    uint64_t corr;
+    uint32_t dshift[8];
+    uint64_t dmask[8];
+    uint64_t ddelta[8];
+};
+
+// Shared memory of a key-switching block, in words: twiddles (2N) + two exchange buffers (2N).
+__host__ __device__ constexpr size_t ks_smem_words(int N) { return 4 * (size_t)N; }
+
+// Coefficient m of aut_t(x) for x in the coefficient domain: x_i moves to
+// i*t mod 2N with a sign flip past N (automorphism_evaluation.cpp:183-206), so
+// m comes from i = m * t^-1 mod 2N.
+template <int LOGN>
+__device__ __forceinline__ uint64_t aut_coeff(const uint64_t* x, uint32_t m, uint32_t tinv) {
+    constexpr uint32_t N = 1u << LOGN;
+    const uint32_t i = (m * tinv) & (2 * N - 1);
+    const uint64_t v = x[i & (N - 1)];
+    return i >= N ? gl_neg(v) : v;
+}
+
+// Coefficient m of X^s * x (negacyclic shift; lwe_to_rlwe_packing.cpp:192-196).
+template <int LOGN>
+__device__ __forceinline__ uint64_t rot_coeff(const uint64_t* x, uint32_t m, uint32_t s) {
+    constexpr uint32_t N = 1u << LOGN;
+    return m >= s ? x[m - s] : gl_neg(x[N + m - s]);
+}
+
+// sum_d NTT(digit_d(a)) * key_d for both components (lazy residues), a in the
+// coefficient layout and canonical.
+template <int LOGN>
+__device__ __forceinline__ void ks_mac(uint64_t a[8], const KsKernelParams& prm, int t, uint64_t* buf0,
+                                       uint64_t* buf1, int& sel, const uint64_t* tw_f, uint64_t o[2][8]) {
+    constexpr int N = 1 << LOGN;
+    constexpr int T = N / 8;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        a[j] = gl_add(a[j], prm.corr);
+        o[0][j] = 0;
+        o[1][j] = 0;
+    }
+#pragma unroll 1
+    for (uint32_t d = 0; d < prm.digits; ++d) {
+        const uint32_t sh = prm.dshift[d];
+        const uint64_t mk = prm.dmask[d];
+        const uint64_t dl = prm.ddelta[d];
+        uint64_t x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = gl_sub((a[j] >> sh) & mk, dl);
+        ntt_forward<LOGN>(x, t, sel ? buf1 : buf0, tw_f);
+        sel ^= 1;
+        const uint64_t* kr = prm.key + (uint64_t)d * (2 * N);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+#pragma unroll
+            for (int jp = 0; jp < 4; ++jp) {
+                const ulonglong2 kv = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
+                o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[2 * jp], kv.x);
+                o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[2 * jp + 1], kv.y);
+            }
+        }
+    }
+}
+
+template <int LOGN, int MODE>
+__global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelParams prm) {
+    constexpr int N = 1 << LOGN;
+    constexpr int T = N / 8;
+    extern __shared__ __align__(16) uint64_t smem[];
+    uint64_t* tw_f = smem;
+    uint64_t* tw_i = smem + N;
+    uint64_t* buf0 = smem + 2 * N;
+    uint64_t* buf1 = smem + 3 * N;
+    const int t = threadIdx.x;
+    for (int i = t; i < N; i += T) {
+        tw_f[i] = prm.tw_fwd[i];
+        tw_i[i] = prm.tw_inv[i];
+    }
+    int sel = 0;
+    for (uint64_t it = blockIdx.x; it < prm.items; it += gridDim.x) {
+        __syncthreads();
+        const uint64_t* in = prm.in + it * prm.in_stride;
+        uint64_t* out = prm.out + it * prm.out_stride;
+        uint64_t a[8], bb[8], base[2][8];
+        // ---- gather inputs (every global read precedes the first barrier below,
+        //      so kKsMerge/kKsTrace may write their result in place) ----
+        if constexpr (MODE == kKsRlwe) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a[j] = in[t + j * T];
+        } else if constexpr (MODE == kKsAuto) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                a[j] = aut_coeff<LOGN>(in, t + j * T, prm.auto_index_inv);
+                bb[j] = aut_coeff<LOGN>(in + N, t + j * T, prm.auto_index_inv);
+            }
+        } else {
+            const uint64_t* left = in;
+            const uint64_t* right = in + (MODE == kKsMerge ? prm.right_offset : 0);
+            const uint32_t s = prm.shift;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t m = t + j * T;
+                    // diff = right - X^s left at the automorphism's source index
+                    const uint32_t i = (m * prm.auto_index_inv) & (2 * N - 1);
+                    const uint32_t src = i & (N - 1);
+                    uint64_t dv = right[h * N + src];
+                    uint64_t sv = right[h * N + m];
+                    if constexpr (MODE == kKsMerge) {
+                        dv = gl_sub(dv, rot_coeff<LOGN>(left + h * N, src, s));
+                        sv = gl_add(sv, rot_coeff<LOGN>(left + h * N, m, s));
+                    }
+                    if (i >= N) dv = gl_neg(dv);
+                    if (h == 0) a[j] = dv;
+                    else bb[j] = dv;
+                    base[h][j] = sv;
+                }
+            }
+        }
+        // ---- key switch of the A part ----
+        uint64_t o[2][8];
+        ks_mac<LOGN>(a, prm, t, buf0, buf1, sel, tw_f, o);
+        if constexpr (MODE == kKsRlwe) {
+            // out -= KS; out.B += in.B (rlwe_conversion.cpp:243-248); slots 8t..8t+7
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int k = 8 * t + j;
+                out[k] = gl_sub(out[k], gl_canon(o[0][j]));
+                out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), in[N + k]);
+            }
+        } else {
+            // NTT of the automorphism's B part (automorphism_evaluation.cpp:156)
+            ntt_forward<LOGN>(bb, t, sel ? buf1 : buf0, tw_f);
+            sel ^= 1;
+            if constexpr (MODE == kKsAuto) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int k = 8 * t + j;
+                    out[k] = gl_sub(out[k], gl_canon(o[0][j]));
+                    out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), bb[j]);
+                }
+            } else {
+                // Auto eval output (NTT) -> coefficients, added to the sum half
+                // (lwe_to_rlwe_packing.cpp:205-210, 228-233)
+                uint64_t r[8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) r[j] = h == 0 ? gl_neg(gl_canon(o[0][j]))
+                                                              : gl_sub(bb[j], gl_canon(o[1][j]));
+                    ntt_backward_unscaled<LOGN>(r, t, sel ? buf1 : buf0, tw_i);
+                    sel ^= 1;
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[j], prm.n_inv));
+                }
+            }
+        }
+    }
+}
+
+}  // namespace tp

@@ -1,0 +1,127 @@
+"""Python mirrors of the reference's key-switching operators over the C ABI.
+
+  GpuRLWEtoRLWEConverter  RLWEtoRLWEConverter::Convert  (lib/src/operators/rlwe_conversion.cpp:224-249)
+  GpuAutomorphismEvaluator AutomorphismEvaluator::Eval  (lib/src/operators/automorphism_evaluation.cpp:150-159)
+  GpuLWEtoRLWEPacker      LWEtoRLWEPacker::Pack          (lib/src/operators/lwe_to_rlwe_packing.cpp:129-236)
+  GpuLWEtoLWEConverter    LWEtoLWEConverter::Convert     (lib/src/operators/lwe_conversion.cpp:205-239)
+
+Each takes its key in the reference layout (the operator's m_ksk; for the
+packer the automorphism keys for indices 2^j + 1, j = 1..log2 N, concatenated).
+The batch methods take device pointers and run asynchronously on `stream`;
+the numpy methods copy in and out and wait.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as nat
+
+
+def _dev(torch, a: np.ndarray):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int64)).cuda()
+
+
+class _KsBase:
+    def __init__(self, handle: ctypes.c_void_p, key: np.ndarray):
+        self._h = handle
+        key = np.ascontiguousarray(key, dtype=np.uint64)
+        nat.check(nat.lib().tp_ks_upload_key(self._h, nat.ptr(key), key.size))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            nat.lib().tp_ks_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuRLWEtoRLWEConverter(_KsBase):
+    def __init__(self, ring_dim: int, basis: int, digits: int, ksk: np.ndarray, device: int = 0):
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().tp_rlwe_ks_create(ring_dim, basis, digits, device, ctypes.byref(h)))
+        self.N = ring_dim
+        super().__init__(h, ksk)
+
+    def convert_batch(self, batch: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_rlwe_ks_batch(self._h, batch, out_ptr, in_ptr, stream))
+
+    def Convert(self, out: np.ndarray, inp: np.ndarray) -> None:
+        """out -= KS(inp.A); out.B += inp.B, rows of 2N words (numpy, in place)."""
+        import torch
+        d_in, d_out = _dev(torch, inp), _dev(torch, out)
+        self.convert_batch(d_in.numel() // (2 * self.N), d_out.data_ptr(), d_in.data_ptr())
+        out[...] = d_out.cpu().numpy().view(np.uint64).reshape(out.shape)
+
+
+class GpuAutomorphismEvaluator(_KsBase):
+    def __init__(self, ring_dim: int, basis: int, digits: int, index: int, ksk: np.ndarray, device: int = 0):
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().tp_auto_create(ring_dim, basis, digits, index, device, ctypes.byref(h)))
+        self.N = ring_dim
+        super().__init__(h, ksk)
+
+    def eval_batch(self, batch: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_auto_eval_batch(self._h, batch, out_ptr, in_ptr, stream))
+
+    def Eval(self, out: np.ndarray, inp: np.ndarray) -> None:
+        import torch
+        d_in, d_out = _dev(torch, inp), _dev(torch, out)
+        self.eval_batch(d_in.numel() // (2 * self.N), d_out.data_ptr(), d_in.data_ptr())
+        out[...] = d_out.cpu().numpy().view(np.uint64).reshape(out.shape)
+
+
+class GpuLWEtoRLWEPacker(_KsBase):
+    def __init__(self, ring_dim: int, basis: int, digits: int, keys: np.ndarray, device: int = 0):
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().tp_pack_create(ring_dim, basis, digits, device, ctypes.byref(h)))
+        self.N = ring_dim
+        super().__init__(h, keys)
+
+    def pack_batch(self, packs: int, length: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_pack_batch(self._h, packs, length, out_ptr, in_ptr, stream))
+
+    def Pack(self, lwes: np.ndarray, length: int) -> np.ndarray:
+        """Packs `lwes` (packs*length rows of N+1 words); returns packs x 2N coefficients."""
+        import torch
+        d_in = _dev(torch, lwes)
+        packs = d_in.numel() // (length * (self.N + 1))
+        d_out = torch.empty((packs, 2 * self.N), dtype=torch.int64, device="cuda")
+        self.pack_batch(packs, length, d_out.data_ptr(), d_in.data_ptr())
+        return d_out.cpu().numpy().view(np.uint64)
+
+
+class GpuLWEtoLWEConverter:
+    def __init__(self, n_in: int, n_out: int, basis: int, digits: int, ksk: np.ndarray, device: int = 0,
+                 modulus: int = nat.GOLDILOCKS):
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().tp_lwe_ks_create(modulus, n_in, n_out, basis, digits, device, ctypes.byref(h)))
+        self._h = h
+        self.n_in, self.n_out = n_in, n_out
+        ksk = np.ascontiguousarray(ksk, dtype=np.uint64)
+        nat.check(nat.lib().tp_lwe_ks_upload_key(self._h, nat.ptr(ksk), ksk.size))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            nat.lib().tp_lwe_ks_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def convert_batch(self, batch: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_lwe_ks_batch(self._h, batch, out_ptr, in_ptr, stream))
+
+    def Convert(self, out: np.ndarray, inp: np.ndarray) -> None:
+        import torch
+        d_in, d_out = _dev(torch, inp), _dev(torch, out)
+        self.convert_batch(d_in.numel() // (self.n_in + 1), d_out.data_ptr(), d_in.data_ptr())
+        out[...] = d_out.cpu().numpy().view(np.uint64).reshape(out.shape)

@@ -119,6 +119,72 @@ tp_status tp_ntt_forward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, c
 tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out_dev, const uint64_t* in_dev,
                           void* stream);
 
+/* ---- Key switching, automorphisms, packing ------------------------------ */
+
+typedef struct tp_ks_ctx tp_ks_ctx;
+
+/* RLWE -> RLWE key switching context, RLWEConversionContext(distr, modulus, N,
+ * basis, digits, std) (lib/include/operators/endo_glwe_conversion.h:256).
+ * Key: the converter's m_ksk, l rows of [A | B] in the NTT domain (KeyGen,
+ * lib/src/operators/rlwe_conversion.cpp:187-218). */
+tp_status tp_rlwe_ks_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, int device, tp_ks_ctx** out);
+
+/* Automorphism X -> X^index followed by the key switch s(X^index) -> s(X),
+ * AutomorphismContext(..., automorphism_index) (lib/include/operators/automorphism_evaluation.h:25);
+ * index odd and below 2N. Key: the inner converter's m_ksk. */
+tp_status tp_auto_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, uint32_t index, int device,
+                         tp_ks_ctx** out);
+
+/* n-LWE -> RLWE packing, LWEtoRLWEPackingContext(distr, modulus, N, basis,
+ * digits, std) (lib/include/operators/lwe_to_rlwe_packing.h:18). Keys: the
+ * automorphism keys for indices 2^j + 1, j = 1..log2 N, each l x 2N words,
+ * concatenated in that order (the evaluators of ConstructOperator,
+ * lib/src/operators/lwe_to_rlwe_packing.cpp:46-58). */
+tp_status tp_pack_create(uint32_t ring_dim, uint64_t basis, uint32_t digits, int device, tp_ks_ctx** out);
+
+tp_status tp_ks_destroy(tp_ks_ctx* ctx);
+uint64_t tp_ks_key_words(const tp_ks_ctx* ctx);
+/* Host key in the reference layout above; re-laid out on the device. Synchronous. */
+tp_status tp_ks_upload_key(tp_ks_ctx* ctx, const uint64_t* key_host, uint64_t words);
+
+/* Batched RLWEtoRLWEConverter::Convert(out, in) (rlwe_conversion.cpp:224-249),
+ * device buffers of 2N words per ciphertext: in = [A coefficients | B NTT];
+ * out -= KS(in.A) and out.B += in.B, like the reference (which expects a
+ * pre-zeroed out). out may equal in. Asynchronous. */
+tp_status tp_rlwe_ks_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev, void* stream);
+
+/* Batched AutomorphismEvaluator::Eval(out, in) (automorphism_evaluation.cpp:150-159):
+ * in = [A | B] coefficients, out (NTT domain) -= KS(aut(A)), out.B += NTT(aut(B)).
+ * out must not alias in. Asynchronous. */
+tp_status tp_auto_eval_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev,
+                             void* stream);
+
+/* Batched LWEtoRLWEPacker::Pack(out, in, len) (lwe_to_rlwe_packing.cpp:129-236):
+ * `packs` packings of `len` LWEs each (len a power of two in [2, N]; LWE e of
+ * pack p at in + (p*len + e)*(N+1)), out + p*2N gets the packed RLWE in the
+ * coefficient domain. The tree runs level by level over all packs, one launch
+ * per level, in a context-owned work area of packs*len*2N words. Asynchronous. */
+tp_status tp_pack_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev, const uint64_t* in_dev,
+                        void* stream);
+
+typedef struct tp_lwe_ks_ctx tp_lwe_ks_ctx;
+
+/* LWE -> LWE key switching, LWEConversionContext(distr, modulus, n_in, n_out,
+ * basis, digits, std) (lib/include/operators/endo_glwe_conversion.h:28), on the
+ * Goldilocks modulus. Key: the converter's m_ksk, n_in x digits x (n_out+1)
+ * (KeyGen, lib/src/operators/lwe_conversion.cpp:174-203), used as laid out. */
+tp_status tp_lwe_ks_create(uint64_t modulus, uint32_t n_in, uint32_t n_out, uint64_t basis, uint32_t digits,
+                           int device, tp_lwe_ks_ctx** out);
+tp_status tp_lwe_ks_destroy(tp_lwe_ks_ctx* ctx);
+uint64_t tp_lwe_ks_key_words(const tp_lwe_ks_ctx* ctx);
+tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* ctx, const uint64_t* key_host, uint64_t words);
+
+/* Batched LWEtoLWEConverter::Convert(out, in) (lwe_conversion.cpp:205-239):
+ * in b has n_in+1 words, out b has n_out+1 words; out[n_out] = in[n_in] and
+ * out -= sum of signed digits times key rows (the reference expects out[0..n_out)
+ * pre-zeroed). Asynchronous. */
+tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev, void* stream);
+
 /* Diagnostic: element-wise Goldilocks primitives of the kernels on device
  * buffers, for testing them against exact integer arithmetic. op: 0 a+b,
  * 1 a-b, 2 a*b (a, b canonical); 3 c + a*b (any 64-bit a, b, c); 4 reduction

@@ -196,6 +196,57 @@ class Oracle:
         assert rc == 0
         return res
 
+    # key switching
+    def rlwe_ks_keygen(self, N, bl, dg, std, src, tgt, seed):
+        r = Rng(seed)
+        k = np.empty(dg * 2 * N, np.uint64)
+        self.L.tpo_rlwe_ks_keygen(ctypes.byref(r), N, bl, dg, std, ptr(np.ascontiguousarray(src, np.uint64)),
+                                  ptr(np.ascontiguousarray(tgt, np.uint64)), ptr(k))
+        return k
+
+    def rlwe_ks(self, N, bl, dg, ksk, inp, out=None):
+        out = np.zeros(2 * N, np.uint64) if out is None else np.array(out, dtype=np.uint64)
+        self.L.tpo_rlwe_ks(N, bl, dg, ptr(ksk), ptr(out), ptr(np.ascontiguousarray(inp, np.uint64)))
+        return out
+
+    def auto_keygen(self, N, bl, dg, std, index, key, seed):
+        r = Rng(seed)
+        k = np.empty(dg * 2 * N, np.uint64)
+        self.L.tpo_auto_keygen(ctypes.byref(r), N, bl, dg, std, index, ptr(np.ascontiguousarray(key, np.uint64)),
+                               ptr(k))
+        return k
+
+    def auto_eval(self, N, bl, dg, index, ksk, inp):
+        out = np.zeros(2 * N, np.uint64)
+        self.L.tpo_auto_eval(N, bl, dg, index, ptr(ksk), ptr(out), ptr(np.ascontiguousarray(inp, np.uint64)))
+        return out
+
+    def pack_keygen(self, N, bl, dg, std, key, seed):
+        r = Rng(seed)
+        logn = N.bit_length() - 1
+        k = np.empty(logn * dg * 2 * N, np.uint64)
+        self.L.tpo_pack_keygen(ctypes.byref(r), N, bl, dg, std, ptr(np.ascontiguousarray(key, np.uint64)), ptr(k))
+        return k
+
+    def pack(self, N, bl, dg, keys, lwes, length):
+        out = np.empty(2 * N, np.uint64)
+        assert self.L.tpo_pack(N, bl, dg, ptr(keys), ptr(out), ptr(np.ascontiguousarray(lwes, np.uint64)),
+                               length) == 0
+        return out
+
+    def lwe_ks_keygen(self, q, n_in, n_out, bl, dg, std, src, tgt, seed):
+        r = Rng(seed)
+        k = np.empty(n_in * dg * (n_out + 1), np.uint64)
+        self.L.tpo_lwe_ks_keygen(ctypes.byref(r), q, n_in, n_out, bl, dg, std,
+                                 ptr(np.ascontiguousarray(src, np.uint64)), ptr(np.ascontiguousarray(tgt, np.uint64)),
+                                 ptr(k))
+        return k
+
+    def lwe_ks(self, q, n_in, n_out, bl, dg, ksk, inp):
+        out = np.zeros(n_out + 1, np.uint64)
+        self.L.tpo_lwe_ks(q, n_in, n_out, bl, dg, ptr(ksk), ptr(out), ptr(np.ascontiguousarray(inp, np.uint64)))
+        return out
+
     def phase_rlwe(self, rlwe_ntt: np.ndarray, sk: np.ndarray) -> np.ndarray:
         N = sk.size
         sk_ntt = self.ntt_forward(sk)
@@ -240,9 +291,11 @@ class Reference:
             "ref_lwe_ks_destroy": (None, [VP]),
             "ref_auto_create": (VP, [U64, U64, U64, D, ctypes.c_uint32, U64P]),
             "ref_auto_eval": (None, [VP, U64P, U64P]),
+            "ref_auto_key_copy": (None, [VP, U64P]),
             "ref_auto_destroy": (None, [VP]),
             "ref_pack_create": (VP, [U64, U64, U64, D, U64P]),
             "ref_pack": (None, [VP, U64P, U64P, U64]),
+            "ref_pack_key_copy": (None, [VP, U64P]),
             "ref_pack_destroy": (None, [VP]),
             "ref_sample_extract": (None, [U64P, U64P, U64, U64]),
         }

@@ -193,6 +193,11 @@ void* ref_auto_create(uint64_t N, uint64_t basis_log2, uint64_t digits, double s
 
 void ref_auto_eval(void* hp, uint64_t* out, const uint64_t* in) { ((AutomorphismEvaluator*)hp)->Eval(out, in); }
 
+void ref_auto_key_copy(void* hp, uint64_t* out) {
+    const auto& k = ((AutomorphismEvaluator*)hp)->m_converter->m_ksk;
+    std::copy(k.begin(), k.end(), out);
+}
+
 void ref_auto_destroy(void* hp) { delete (AutomorphismEvaluator*)hp; }
 
 // n-LWE -> RLWE packing.
@@ -205,6 +210,14 @@ void* ref_pack_create(uint64_t N, uint64_t basis_log2, uint64_t digits, double s
 }
 
 void ref_pack(void* hp, uint64_t* out, const uint64_t* in, uint64_t len) { ((LWEtoRLWEPacker*)hp)->Pack(out, in, len); }
+
+// The packer's automorphism keys (index 2^j + 1, j = 1..logN), concatenated.
+void ref_pack_key_copy(void* hp, uint64_t* out) {
+    for (auto& ev : ((LWEtoRLWEPacker*)hp)->m_auto_evaluators) {
+        const auto& k = ev->m_converter->m_ksk;
+        out = std::copy(k.begin(), k.end(), out);
+    }
+}
 
 void ref_pack_destroy(void* hp) { delete (LWEtoRLWEPacker*)hp; }
 

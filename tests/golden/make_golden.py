@@ -37,6 +37,21 @@ BR_CASES = [
 ]
 
 
+# (name, kind, N, basis_log2, digits, extra): extra = automorphism index, pack length or (n_in, n_out)
+KS_CASES = [
+    ("rlwe_ks_n2048", "rlwe_ks", 2048, 16, 4, None),
+    ("rlwe_ks_n256_b12", "rlwe_ks", 256, 12, 3, None),
+    ("auto5_n2048", "auto", 2048, 16, 4, 5),
+    ("auto2049_n2048", "auto", 2048, 16, 4, 2049),
+    ("auto33_n128", "auto", 128, 16, 4, 33),
+    ("pack2_n128", "pack", 128, 16, 4, 2),
+    ("pack32_n256", "pack", 256, 16, 4, 32),
+    ("pack2048_n2048", "pack", 2048, 16, 4, 2048),
+    ("lwe_ks_2048_630", "lwe_ks", 0, 16, 4, (2048, 630)),
+    ("lwe_ks_64_16_b8", "lwe_ks", 0, 8, 3, (64, 16)),
+]
+
+
 def br_inputs(name: str, N: int, n: int, seed: int):
     """Two rotations per case: edge-valued LWE words with a random acc (NTT-domain
     output), then uniform words with another random acc (coefficient output)."""
@@ -47,6 +62,14 @@ def br_inputs(name: str, N: int, n: int, seed: int):
     lwes[0, n] = N + 5
     accs = random_acc(N, 2, seed + 2)
     return lwes, accs, [0, 1]
+
+
+def lwe_ks_secrets(n_in: int, n_out: int, seed: int):
+    """Ternary LWE secrets mod p (-1 as p-1) for the LWE key-switching cases."""
+    def tern(n, sd):
+        x = sm64(sd, n) % np.uint64(3)
+        return np.array([0, 1, P - 1], dtype=np.uint64)[x.astype(np.int64)]
+    return tern(n_in, seed + 10), tern(n_out, seed + 11)
 
 
 def case_seed(name: str) -> int:
@@ -97,6 +120,75 @@ def main() -> None:
             "key_seed": key_seed, "key_words": int(kw), "key_sha256": sha256(brk),
             "lwe_sha256": sha256(lwes), "acc_sha256": sha256(accs), "out_coef": coefs,
         }
+        print(f"{name}: {time.time() - t0:.1f}s", flush=True)
+
+    # Key switching, automorphisms, packing, LWE key switching
+    manifest["ks"] = {}
+    for name, kind, N, bl, dg, extra in KS_CASES:
+        t0 = time.time()
+        seed = case_seed(name)
+        key = rlwe_secret(N, seed + 10)
+        key2 = rlwe_secret(N, seed + 11)
+        L.ref_seed(seed + 12)
+        meta = {"kind": kind, "N": N, "basis_log2": bl, "digits": dg, "std": 3.2, "seed": seed, "key_seed": seed + 12}
+        if kind == "rlwe_ks":
+            h = L.ref_rlwe_ks_create(N, bl, dg, 3.2, ptr(key), ptr(key2))
+            ksk = np.empty(dg * 2 * N, np.uint64)
+            L.ref_rlwe_ks_key_copy(h, ptr(ksk))
+            ins = random_acc(N, 2, seed + 1)
+            outs = []
+            for i in range(2):
+                o = np.zeros(2 * N, np.uint64)
+                L.ref_rlwe_ks_convert(h, ptr(o), ptr(np.ascontiguousarray(ins[i])))
+                outs.append(o)
+            L.ref_rlwe_ks_destroy(h)
+            meta.update(key_sha256=sha256(ksk), input_sha256=sha256(ins))
+        elif kind == "auto":
+            h = L.ref_auto_create(N, bl, dg, 3.2, extra, ptr(key))
+            ksk = np.empty(dg * 2 * N, np.uint64)
+            L.ref_auto_key_copy(h, ptr(ksk))
+            ins = random_acc(N, 2, seed + 1)
+            outs = []
+            for i in range(2):
+                o = np.zeros(2 * N, np.uint64)
+                L.ref_auto_eval(h, ptr(o), ptr(np.ascontiguousarray(ins[i])))
+                outs.append(o)
+            L.ref_auto_destroy(h)
+            meta.update(index=extra, key_sha256=sha256(ksk), input_sha256=sha256(ins))
+        elif kind == "pack":
+            h = L.ref_pack_create(N, bl, dg, 3.2, ptr(key))
+            logn = N.bit_length() - 1
+            keys = np.empty(logn * dg * 2 * N, np.uint64)
+            L.ref_pack_key_copy(h, ptr(keys))
+            length = extra
+            lwes = uniform_mod(seed + 1, length * (N + 1), P).reshape(length, N + 1)
+            o = np.empty(2 * N, np.uint64)
+            L.ref_pack(h, ptr(o), ptr(lwes), length)
+            outs = [o]
+            L.ref_pack_destroy(h)
+            meta.update(len=length, key_sha256=sha256(keys), input_sha256=sha256(lwes))
+        else:  # lwe_ks: extra = (n_in, n_out)
+            n_in, n_out = extra
+            src, tgt = lwe_ks_secrets(n_in, n_out, seed)
+            ins = uniform_mod(seed + 1, 2 * (n_in + 1), P).reshape(2, n_in + 1)
+            outs = []
+            # One fresh converter per input: LWEtoLWEConverter::Convert clears only
+            # the first (n_out + 8) / 8 accumulator words between calls
+            # (ZERO_UINT64_ARR(m_acc.data(), n_out + 1) at lwe_conversion.cpp:217
+            # expands to memset(.., n_out + 1 * sizeof(uint64_t))), so only a
+            # converter's first call gives the intended result.
+            for i in range(2):
+                L.ref_seed(seed + 12)
+                h = L.ref_lwe_ks_create(P, n_in, n_out, bl, dg, 3.2, ptr(src), ptr(tgt))
+                ksk = np.empty(n_in * dg * (n_out + 1), np.uint64)
+                L.ref_lwe_ks_key_copy(h, ptr(ksk))
+                o = np.zeros(n_out + 1, np.uint64)
+                L.ref_lwe_ks_convert(h, ptr(o), ptr(np.ascontiguousarray(ins[i])))
+                outs.append(o)
+                L.ref_lwe_ks_destroy(h)
+            meta.update(n_in=n_in, n_out=n_out, key_sha256=sha256(ksk), input_sha256=sha256(ins))
+        arrays[f"ks_{name}"] = np.stack(outs)
+        manifest["ks"][name] = meta
         print(f"{name}: {time.time() - t0:.1f}s", flush=True)
 
     np.savez(OUT / "golden.npz", **arrays)
