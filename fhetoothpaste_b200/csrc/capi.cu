@@ -852,3 +852,100 @@ tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out, cons
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Packing without any device allocation
+// ---------------------------------------------------------------------------
+// Callers that cannot allocate device memory at call time use this: a serving
+// process whose device memory is owned by another allocator (for example a
+// framework pool that has reserved nearly all of HBM up front), or a latency
+// loop that must not pay for cudaMalloc/cudaFree, which can block and
+// synchronise the device. tp_pack_batch grows a work area with cudaMalloc;
+// this variant keeps its packing-tree nodes in the fixed array below instead.
+//
+// The array is a file-scope device variable: every GPU that loads this
+// library reserves its kPackScratchWords * 8 bytes (16 MiB) until the process
+// exits. In host code the name `g_pack_scratch` only stands in for the
+// variable, it is not a device address; the device address is fetched once
+// per device with cudaGetSymbolAddress and cached.
+
+namespace {
+constexpr uint64_t kPackScratchWords = 2ull << 20;  // 16 MiB of packing-tree nodes
+constexpr int kMaxDevices = 64;
+std::mutex g_pack_scratch_mu;
+uint64_t* g_pack_scratch_addr[kMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) uint64_t g_pack_scratch[kPackScratchWords];
+
+extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out,
+                                           const uint64_t* in, void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (packs == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->N;
+    if (len < 2 || len > N || (len & (len - 1))) return fail(TP_ERR_PARAM, "len must be a power of two in [2, N]");
+    const uint64_t need = packs * len * 2 * N;
+    if (need > kPackScratchWords)
+        return fail(TP_ERR_PARAM,
+                    "packs * len * 2N = %llu words exceeds the fixed scratch of %llu words (16 MiB); "
+                    "use fewer packs per call or tp_pack_batch",
+                    (unsigned long long)need, (unsigned long long)kPackScratchWords);
+    if (c->device < 0 || c->device >= kMaxDevices) return fail(TP_ERR_PARAM, "device index out of range");
+    TP_CUDA(cudaSetDevice(c->device));
+    uint64_t* work = nullptr;
+    {
+        // First call on this device (now current): look up the array's device address.
+        std::lock_guard<std::mutex> lk(g_pack_scratch_mu);
+        if (!g_pack_scratch_addr[c->device]) {
+            void* addr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&addr, g_pack_scratch);
+            if (e != cudaSuccess || !addr)
+                return fail(TP_ERR_CUDA, "cudaGetSymbolAddress(g_pack_scratch): %s", cudaGetErrorString(e));
+            g_pack_scratch_addr[c->device] = static_cast<uint64_t*>(addr);
+        }
+        work = g_pack_scratch_addr[c->device];
+    }
+    // Every word of the nodes in use is written by the set-up kernel below
+    // before any merge reads it, so nothing left by an earlier call is read.
+    cudaStream_t st = (cudaStream_t)stream;
+    const int log_len = ilog2(len);
+    {
+        const uint64_t blocks = std::min<uint64_t>((need + 255) / 256, 65535);
+        tp::pack_l0_kernel<<<(unsigned)blocks, 256, 0, st>>>(work, in, packs, (uint32_t)len, (uint32_t)log_len,
+                                                            (uint32_t)c->logn, c->tab->n_inv);
+        TP_CUDA(cudaGetLastError());
+    }
+    const uint64_t kw = (uint64_t)c->digits * 2 * N;
+    tp::KsKernelParams kp = c->kp;
+    for (int L = 1; L <= log_len; ++L) {
+        kp.key = c->key + (uint64_t)(L - 1) * kw;
+        kp.in = work;
+        kp.out = work;
+        kp.items = packs * (len >> L);
+        kp.in_stride = kp.out_stride = (1ull << L) * 2 * N;
+        kp.right_offset = (1ull << (L - 1)) * 2 * N;
+        kp.auto_index = (1u << L) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = (uint32_t)(N >> L);
+        tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
+        if (s != TP_OK) return s;
+    }
+    for (int i = 0; i < c->logn - log_len; ++i) {
+        const int j = c->logn - i;
+        kp.key = c->key + (uint64_t)(j - 1) * kw;
+        kp.in = work;
+        kp.out = work;
+        kp.items = packs;
+        kp.in_stride = kp.out_stride = len * 2 * N;
+        kp.right_offset = 0;
+        kp.auto_index = (1u << j) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = 0;
+        tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+        if (s != TP_OK) return s;
+    }
+    TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
+    return TP_OK;
+}

@@ -167,6 +167,24 @@ tp_status tp_auto_eval_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, 
 tp_status tp_pack_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev, const uint64_t* in_dev,
                         void* stream);
 
+/* tp_pack_batch for callers that cannot allocate device memory when they call:
+ * a process whose HBM is owned by another allocator's pool, or a latency-bound
+ * loop that must not risk cudaMalloc/cudaFree blocking or synchronising the
+ * device. The packing-tree nodes live in a fixed device array of 16 MiB
+ * (2^21 words) instead of a cudaMalloc'd work area; calls with
+ * packs * len * 2N above 2^21 words fail with TP_ERR_PARAM. The call itself
+ * allocates nothing. Its first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture. Every GPU that loads the library holds the
+ * array until the process exits. All calls on a device share the one array:
+ * calls whose work overlaps on the GPU (different streams, or different
+ * contexts on the same device) race and corrupt each other, so order them.
+ * Nothing carries over between calls: the set-up kernel rewrites every node
+ * word a call reads. No counterpart in the reference, which always packs on
+ * host buffers it allocates itself. */
+tp_status tp_pack_batch_noalloc(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev,
+                                const uint64_t* in_dev, void* stream);
+
 typedef struct tp_lwe_ks_ctx tp_lwe_ks_ctx;
 
 /* LWE -> LWE key switching, LWEConversionContext(distr, modulus, n_in, n_out,
