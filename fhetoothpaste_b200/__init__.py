@@ -8,3 +8,4 @@ from .blind_rotation import (BlindRotationContext, GpuBlindRotator, ntt_backward
                              sample_extract_batch)
 from .key_switching import (GpuAutomorphismEvaluator, GpuLWEtoLWEConverter, GpuLWEtoRLWEPacker,  # noqa: F401,E402
                             GpuRLWEtoRLWEConverter)
+from .serving import BootstrapServer  # noqa: F401,E402

@@ -76,6 +76,20 @@ def lib() -> ctypes.CDLL:
         "tp_lwe_ks_key_words": (U64, [VP]),
         "tp_lwe_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
         "tp_lwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_server_create": (ctypes.c_int, [ctypes.c_int, U64, ctypes.POINTER(VP)]),
+        "tp_server_add_set": (ctypes.c_int, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),
+        "tp_server_start": (ctypes.c_int, [VP]),
+        "tp_server_submit": (ctypes.c_int, [VP, ctypes.c_uint32, U64P, U64P, U64P, ctypes.POINTER(U64)]),
+        "tp_server_wait": (ctypes.c_int, [VP, U64, ctypes.c_uint32]),
+        "tp_server_drain": (ctypes.c_int, [VP, ctypes.c_uint32]),
+        "tp_server_stats": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_double)]),
+        "tp_server_reset_stats": (ctypes.c_int, [VP]),
+        "tp_server_destroy": (ctypes.c_int, [VP]),
+        "tp_server_last_error": (ctypes.c_char_p, []),
+        "tp_server_run_poisson": (ctypes.c_int, [VP, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.c_uint32, ctypes.POINTER(U64P), ctypes.POINTER(U64P), U64P,
+                                                 U64]),
         "tp_debug_arith": (ctypes.c_int, [ctypes.c_int, U64, VP, VP, VP, VP, VP]),
         "tp_measure_int_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]),

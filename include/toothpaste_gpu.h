@@ -203,6 +203,51 @@ tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* ctx, const uint64_t* key_host, uin
  * pre-zeroed). Asynchronous. */
 tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev, void* stream);
 
+/* ---- Serving loop -------------------------------------------------------- */
+/* Continuous batching of single bootstrap requests over several resident
+ * parameter sets (no reference counterpart: the reference rotates one
+ * ciphertext per call on the calling thread). */
+typedef struct tp_server tp_server;
+
+/* max_queue bounds the requests waiting for a launch buffer; further submits
+ * are rejected (admission control). 0 = 2^20. */
+tp_status tp_server_create(int device, uint64_t max_queue, tp_server** out);
+
+/* Registers a parameter set served by `ctx` (created and keyed by the caller,
+ * kept alive until the server is destroyed): `buffers` launch buffers of
+ * `max_batch` requests each are reserved on the device and in pinned host
+ * memory now, which bounds how many of the set's requests are on the GPU at
+ * once. Results are NTT domain, or coefficients when out_coef != 0. */
+tp_status tp_server_add_set(tp_server* srv, tp_br_ctx* ctx, uint32_t ring_dim, uint32_t lwe_dim, uint32_t max_batch,
+                            uint32_t buffers, int out_coef, uint32_t* set_id);
+
+/* Starts the scheduler thread (after every tp_server_add_set). */
+tp_status tp_server_start(tp_server* srv);
+
+/* Queues one rotation of set `set_id`: lwe (n+1 words) and acc (2N words) are
+ * read and result (2N words) written by the scheduler, so the host buffers
+ * must stay valid until tp_server_wait returns for the ticket. Returns
+ * TP_ERR_STATE when the queue is full (the request is not admitted). */
+tp_status tp_server_submit(tp_server* srv, uint32_t set_id, const uint64_t* lwe, const uint64_t* acc,
+                           uint64_t* result, uint64_t* ticket);
+tp_status tp_server_wait(tp_server* srv, uint64_t ticket, uint32_t timeout_ms);
+/* Waits until no request is queued or in flight. */
+tp_status tp_server_drain(tp_server* srv, uint32_t timeout_ms);
+/* stats8 = {completed, rejected, launches, seconds from first submit to last
+ * completion, p50, p99, p99.9, max latency (ms, submit to result in host memory)}. */
+tp_status tp_server_stats(tp_server* srv, double* stats8);
+tp_status tp_server_reset_stats(tp_server* srv);
+tp_status tp_server_destroy(tp_server* srv);
+const char* tp_server_last_error(void);
+
+/* Open-loop load generator for the serving benchmark: Poisson arrivals at
+ * `rate` requests/s for `seconds`; set i with probability mix[i]; inputs taken
+ * round-robin from per-set pools (pool_n[i] rows). Waits for every admitted
+ * request to finish. */
+tp_status tp_server_run_poisson(tp_server* srv, double rate, double seconds, const double* mix, uint32_t nsets,
+                                const uint64_t* const* pool_lwe, const uint64_t* const* pool_acc,
+                                const uint64_t* pool_n, uint64_t seed);
+
 /* Diagnostic: element-wise Goldilocks primitives of the kernels on device
  * buffers, for testing them against exact integer arithmetic. op: 0 a+b,
  * 1 a-b, 2 a*b (a, b canonical); 3 c + a*b (any 64-bit a, b, c); 4 reduction
