@@ -233,7 +233,7 @@ def serving_run(device: int, rate: float, seconds: float) -> dict:
     out = {"sets": [f"N={N} n={n}" for N, n in SERVING_SETS], "mix": SERVING_MIX,
            "key_bytes_resident": sum(r.ctx.key_words() * 8 for r in rots), "duration_s": seconds}
     for label, r in (("offered", rate), ("sustainable", None)):
-        srv = BootstrapServer(device=device, max_queue=20000)
+        srv = BootstrapServer(device=device, max_queue=2500)
         for rot, mb in zip(rots, (296, 148, 148)):
             srv.add_set(rot, max_batch=mb, buffers=2)
         srv.start()
