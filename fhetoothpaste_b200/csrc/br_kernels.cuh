@@ -55,9 +55,24 @@ struct BrKernelParams {
     unsigned int* err;        // bit 0: an LWE word was outside [0, 2N)
 };
 
-// Shared memory of one block, in words: twiddles (2N), two exchange buffers
-// (2N), accumulator (2N), LWE vector (n+1, rounded up to an even count).
-__host__ __device__ constexpr size_t br_smem_words(int N, uint32_t n) { return 6 * (size_t)N + ((n + 2) & ~1u); }
+// Polynomials transformed together by the rotation kernel (the accumulator
+// halves, the gadget digits in pairs when 2). Two measured slower (4.4k vs 6.0k
+// ternary N = 2048 rotations/s): the doubled, fully unrolled transforms no longer
+// fit the instruction cache, so the kernel transforms one polynomial at a time.
+__host__ __device__ constexpr int br_ntt_width(int logn, int variant) {
+    return (void)logn, (void)variant, 1;
+}
+// Twiddles live in shared memory unless the exchange buffers of the wide
+// transforms leave no room for them (then they are read through L1).
+__host__ __device__ constexpr bool br_smem_twiddles(int logn) { return logn <= 11; }
+
+// Shared memory of one block, in words: twiddles (2N, if kept there), two
+// exchange areas of width*N words, the accumulator (2N), the LWE vector (n+1,
+// rounded up to an even count).
+__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n) {
+    return (size_t)(1 << logn) * ((br_smem_twiddles(logn) ? 2 : 0) + 2 * br_ntt_width(logn, variant) + 2) +
+           ((n + 2) & ~1u);
+}
 
 // Exponent e_k = 2 brv(k) + 1 of slot k: NTT(X^a)[k] = psi^(e_k a mod 2N).
 template <int LOGN>
@@ -73,9 +88,10 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
 // Resident blocks per SM the kernel is compiled for (register budget
 // 65536 / (T * blocks)). From N = 2048 up one block per SM with the full
 // register file measured faster than two blocks that spill (ternary N = 2048:
-// 6.0k vs 5.3k rotations/s); N = 4096 needs 200 KB of shared memory anyway.
+// 6.0k vs 5.3k rotations/s), and the wide transforms' shared memory leaves
+// room for one block there anyway.
 __host__ __device__ constexpr int br_min_blocks(int logn, int variant) {
-    return (logn >= 12 || (logn == 11 && variant != kCggiBinary) || variant == kBmmpBinary) ? 1 : 2;
+    return (logn >= 11 || variant == kBmmpBinary) ? 1 : 2;
 }
 
 template <int LOGN, int VARIANT>
@@ -86,25 +102,32 @@ br_kernel(const BrKernelParams prm) {
     constexpr int T = SH::T;
     constexpr int G = br_rgsw_per_group(VARIANT);
     constexpr int C = 2 * G;                 // key components per slot
+    constexpr int K = br_ntt_width(LOGN, VARIANT);  // polynomials per transform
+    constexpr bool TW_SMEM = br_smem_twiddles(LOGN);
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
 
     extern __shared__ __align__(16) uint64_t smem[];
-    uint64_t* tw_f = smem;
-    uint64_t* tw_i = smem + N;
-    uint64_t* xbuf0 = smem + 2 * N;
-    uint64_t* xbuf1 = smem + 3 * N;
-    uint64_t* acc = smem + 4 * N;            // [(h*8 + j)*T + t], canonical, NTT domain
-    uint64_t* lwe_s = smem + 6 * N;
+    uint64_t* base = smem;
+    const uint64_t* tw_f = prm.tw_fwd;
+    const uint64_t* tw_i = prm.tw_inv;
+    if constexpr (TW_SMEM) {
+        for (int i = threadIdx.x; i < N; i += T) {
+            base[i] = prm.tw_fwd[i];
+            base[N + i] = prm.tw_inv[i];
+        }
+        tw_f = base;
+        tw_i = base + N;
+        base += 2 * N;
+    }
+    uint64_t* xbuf0 = base;
+    uint64_t* xbuf1 = base + K * N;
+    uint64_t* acc = base + 2 * K * N;        // [(h*8 + j)*T + t], canonical, NTT domain
+    uint64_t* lwe_s = acc + 2 * N;
 
     const int t = threadIdx.x;
     const uint32_t n = prm.n;
     const uint32_t L = prm.digits;
-
-    for (int i = t; i < N; i += T) {
-        tw_f[i] = prm.tw_fwd[i];
-        tw_i[i] = prm.tw_inv[i];
-    }
 
     int sel = 0;
     auto xb = [&]() -> uint64_t* {
@@ -114,7 +137,7 @@ br_kernel(const BrKernelParams prm) {
     };
 
     for (uint64_t b = blockIdx.x; b < prm.batch; b += gridDim.x) {
-        __syncthreads();  // previous ciphertext done with lwe_s / acc
+        __syncthreads();  // previous ciphertext done with lwe_s / acc (and twiddles written)
         const uint64_t* lwe = prm.lwes + b * prm.lwe_stride;
         bool bad = false;
         for (uint32_t i = t; i <= n; i += T) {
@@ -130,14 +153,19 @@ br_kernel(const BrKernelParams prm) {
             const uint64_t* ain = prm.accs + b * prm.acc_stride;
             const uint32_t bb = (uint32_t)lwe_s[n];
 #pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                uint64_t x[8];
+            for (int h0 = 0; h0 < 2; h0 += K) {
+                uint64_t x[K][8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) x[j] = ain[h * N + t + j * T];
-                ntt_forward<LOGN>(x, t, xb(), tw_f);
+                for (int p = 0; p < K; ++p)
 #pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    acc[(h * 8 + j) * T + t] = gl_mul(x[j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j), bb));
+                    for (int j = 0; j < 8; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
+                ntt_forward_k<LOGN, K>(x, t, xb(), tw_f);
+#pragma unroll
+                for (int p = 0; p < K; ++p)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        acc[((h0 + p) * 8 + j) * T + t] =
+                            gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j), bb));
             }
         }
 
@@ -161,46 +189,70 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) o[c][j] = 0;
 
-            uint64_t cx[8];  // corrected coefficients of the half being decomposed
-#pragma unroll 1
-            for (uint32_t r = 0; r < 2 * L; ++r) {
-                if (r == 0 || r == L) {
-                    // Backward NTT of one accumulator half. Binary CGGI decomposes
-                    // (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the other variants
-                    // decompose acc itself (mux_operator.cpp:174-177, 219-224).
-                    const int h = r == 0 ? 0 : 1;
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        cx[j] = acc[(h * 8 + j) * T + t];
-                        if constexpr (VARIANT == kCggiBinary)
-                            cx[j] = gl_mul(cx[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j),
-                                                                    2u * N - a0), 1));
-                    }
-                    ntt_backward_unscaled<LOGN>(cx, t, xb(), tw_i);
-                    // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) cx[j] = gl_canon(gl_fma_lazy(prm.corr, cx[j], prm.n_inv));
-                }
-                const uint32_t d = r < L ? r : r - L;
-                const uint32_t sh = prm.dshift[d];
-                const uint64_t mk = prm.dmask[d];
-                const uint64_t dl = prm.ddelta[d];
-                uint64_t x[8];
+            // Backward NTT of an accumulator half into corrected coefficients. Binary
+            // CGGI decomposes (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the other
+            // variants decompose acc itself (mux_operator.cpp:174-177, 219-224).
+            uint64_t cx[2][8];
+            auto load_half = [&](uint64_t (&dst)[8], int h) {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const uint64_t raw = (cx[j] >> sh) & mk;
-                    x[j] = SIGNED ? gl_sub(raw, dl) : raw;
+                    dst[j] = acc[(h * 8 + j) * T + t];
+                    if constexpr (VARIANT == kCggiBinary)
+                        dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j),
+                                                                  2u * N - a0), 1));
                 }
-                ntt_forward<LOGN>(x, t, xb(), tw_f);
-                const uint64_t* kr = kit + (uint64_t)r * (N * C);
+            };
+            // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
+            auto finish_half = [&](uint64_t (&v)[8]) {
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
+                for (int j = 0; j < 8; ++j) v[j] = gl_canon(gl_fma_lazy(prm.corr, v[j], prm.n_inv));
+            };
+            if constexpr (K == 2) {
+                load_half(cx[0], 0);
+                load_half(cx[1], 1);
+                ntt_backward_unscaled_k<LOGN, 2>(cx, t, xb(), tw_i);
+                finish_half(cx[0]);
+                finish_half(cx[1]);
+            }
+#pragma unroll 1
+            for (uint32_t r = 0; r < 2 * L; r += K) {
+                if constexpr (K == 1) {
+                    if (r == 0 || r == L) {
+                        uint64_t (&c1)[1][8] = reinterpret_cast<uint64_t(&)[1][8]>(cx[0]);
+                        load_half(cx[0], r == 0 ? 0 : 1);
+                        ntt_backward_unscaled_k<LOGN, 1>(c1, t, xb(), tw_i);
+                        finish_half(cx[0]);
+                    }
+                }
+                uint64_t x[K][8];
 #pragma unroll
-                    for (int jp = 0; jp < 4; ++jp) {
-                        const ulonglong2 kv =
-                            __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
-                        o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[2 * jp], kv.x);
-                        o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[2 * jp + 1], kv.y);
+                for (int p = 0; p < K; ++p) {
+                    const uint32_t rr = r + p;
+                    const bool hb = K == 2 && rr >= L;          // digit of the B half
+                    const uint32_t d = rr < L ? rr : rr - L;
+                    const uint32_t sh = prm.dshift[d];
+                    const uint64_t mk = prm.dmask[d];
+                    const uint64_t dl = prm.ddelta[d];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const uint64_t c = hb ? cx[K - 1][j] : cx[0][j];
+                        const uint64_t raw = (c >> sh) & mk;
+                        x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
+                    }
+                }
+                ntt_forward_k<LOGN, K>(x, t, xb(), tw_f);
+#pragma unroll
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+#pragma unroll
+                        for (int jp = 0; jp < 4; ++jp) {
+                            const ulonglong2 kv =
+                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
+                            o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[p][2 * jp], kv.x);
+                            o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
+                        }
                     }
                 }
             }
@@ -241,18 +293,25 @@ br_kernel(const BrKernelParams prm) {
         // Epilogue (cggi_blind_rotation.cpp:258-261).
         uint64_t* res = prm.out + b * (2ull * N);
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            uint64_t x[8];
+        for (int h0 = 0; h0 < 2; h0 += K) {
+            uint64_t x[K][8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) x[j] = acc[(h * 8 + j) * T + t];
+            for (int p = 0; p < K; ++p)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) x[p][j] = acc[((h0 + p) * 8 + j) * T + t];
             if (prm.out_coef) {
-                ntt_backward_unscaled<LOGN>(x, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGN, K>(x, t, xb(), tw_i);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) res[h * N + t + j * T] = gl_mul(x[j], prm.n_inv);
+                for (int p = 0; p < K; ++p)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) res[(h0 + p) * N + t + j * T] = gl_mul(x[p][j], prm.n_inv);
             } else {
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    *reinterpret_cast<ulonglong2*>(res + h * N + 8 * t + 2 * c) = make_ulonglong2(x[2 * c], x[2 * c + 1]);
+                for (int p = 0; p < K; ++p)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        *reinterpret_cast<ulonglong2*>(res + (h0 + p) * N + 8 * t + 2 * c) =
+                            make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
             }
         }
     }

@@ -283,7 +283,7 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
     }
 
     c->kernel = tp::br_kernel_lookup(c->logn, p->variant);
-    c->smem_bytes = tp::br_smem_words((int)N, p->lwe_dim) * 8;
+    c->smem_bytes = tp::br_smem_words(c->logn, p->variant, p->lwe_dim) * 8;
     e = cudaFuncSetAttribute((const void*)c->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes);
     int per_sm = 0;
     if (e == cudaSuccess)

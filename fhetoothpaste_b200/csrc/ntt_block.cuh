@@ -74,9 +74,13 @@ __device__ __forceinline__ void ntt_sync(bool block_wide) {
     else __syncwarp();
 }
 
+// The functions below transform K polynomials at once (x[k] is polynomial k;
+// its exchange area is buf + k*N). The K transforms share every twiddle load
+// and every synchronisation, and their independent butterflies interleave.
+
 // Forward butterflies of pass P on the thread's registers.
-template <int LOGN, int P>
-__device__ __forceinline__ void fwd_pass_math(uint64_t x[8], int t, const uint64_t* __restrict__ tw) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][8], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN>;
     constexpr int S = SH::S(P);
     constexpr int G = 1 << S;
@@ -93,18 +97,21 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t x[8], int t, const uint64
             for (int j = 0; j < G; ++j) {
                 if (j & half) continue;
                 const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
-                const uint64_t u = x[q * G + j];
-                const uint64_t v = gl_mul(x[q * G + j + half], w);
-                x[q * G + j] = gl_add(u, v);
-                x[q * G + j + half] = gl_sub(u, v);
+#pragma unroll
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][q * G + j];
+                    const uint64_t v = gl_mul(x[p][q * G + j + half], w);
+                    x[p][q * G + j] = gl_add(u, v);
+                    x[p][q * G + j + half] = gl_sub(u, v);
+                }
             }
         }
     }
 }
 
 // Inverse butterflies of pass P (levels in reverse order).
-template <int LOGN, int P>
-__device__ __forceinline__ void inv_pass_math(uint64_t x[8], int t, const uint64_t* __restrict__ tw) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][8], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN>;
     constexpr int S = SH::S(P);
     constexpr int G = 1 << S;
@@ -121,83 +128,106 @@ __device__ __forceinline__ void inv_pass_math(uint64_t x[8], int t, const uint64
             for (int j = 0; j < G; ++j) {
                 if (j & half) continue;
                 const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
-                const uint64_t u = x[q * G + j];
-                const uint64_t v = x[q * G + j + half];
-                x[q * G + j] = gl_add(u, v);
-                x[q * G + j + half] = gl_mul(gl_sub(u, v), w);
+#pragma unroll
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][q * G + j];
+                    const uint64_t v = x[p][q * G + j + half];
+                    x[p][q * G + j] = gl_add(u, v);
+                    x[p][q * G + j + half] = gl_mul(gl_sub(u, v), w);
+                }
             }
         }
     }
 }
 
-template <int LOGN, int P>
-__device__ __forceinline__ void xstore(uint64_t* buf, const uint64_t x[8], int t) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void xstore(uint64_t* buf, const uint64_t (&x)[K][8], int t) {
     using SH = NttShape<LOGN>;
-    if constexpr (P == SH::NPASS - 1) {
-        // slot layout: 8 contiguous words, written as four 16-byte chunks
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int idx = 8 * t + 2 * c;
-            *reinterpret_cast<ulonglong2*>(buf + xpos(idx)) = make_ulonglong2(x[2 * c], x[2 * c + 1]);
+    for (int p = 0; p < K; ++p) {
+        uint64_t* b = buf + p * SH::N;
+        if constexpr (P == SH::NPASS - 1) {
+            // slot layout: 8 contiguous words, written as four 16-byte chunks
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int idx = 8 * t + 2 * c;
+                *reinterpret_cast<ulonglong2*>(b + xpos(idx)) = make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) b[xpos(pass_index<LOGN, P>(t, e))] = x[p][e];
         }
-    } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) buf[xpos(pass_index<LOGN, P>(t, e))] = x[e];
     }
 }
 
-template <int LOGN, int P>
-__device__ __forceinline__ void xload(const uint64_t* buf, uint64_t x[8], int t) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][8], int t) {
     using SH = NttShape<LOGN>;
-    if constexpr (P == SH::NPASS - 1) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int idx = 8 * t + 2 * c;
-            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(buf + xpos(idx));
-            x[2 * c] = v.x;
-            x[2 * c + 1] = v.y;
+    for (int p = 0; p < K; ++p) {
+        const uint64_t* b = buf + p * SH::N;
+        if constexpr (P == SH::NPASS - 1) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int idx = 8 * t + 2 * c;
+                const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(b + xpos(idx));
+                x[p][2 * c] = v.x;
+                x[p][2 * c + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) x[p][e] = b[xpos(pass_index<LOGN, P>(t, e))];
         }
-    } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) x[e] = buf[xpos(pass_index<LOGN, P>(t, e))];
     }
 }
 
-template <int LOGN, int P>
-__device__ __forceinline__ void fwd_passes_from(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw) {
     using SH = NttShape<LOGN>;
-    fwd_pass_math<LOGN, P>(x, t, tw);
+    fwd_pass_math<LOGN, P, K>(x, t, tw);
     if constexpr (P + 1 < SH::NPASS) {
-        xstore<LOGN, P>(buf, x, t);
+        xstore<LOGN, P, K>(buf, x, t);
         ntt_sync<LOGN>(!SH::WarpLocal(P));
-        xload<LOGN, P + 1>(buf, x, t);
-        fwd_passes_from<LOGN, P + 1>(x, t, buf, tw);
+        xload<LOGN, P + 1, K>(buf, x, t);
+        fwd_passes_from<LOGN, P + 1, K>(x, t, buf, tw);
     }
 }
 
-template <int LOGN, int P>
-__device__ __forceinline__ void inv_passes_from(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw) {
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw) {
     using SH = NttShape<LOGN>;
-    inv_pass_math<LOGN, P>(x, t, tw);
+    inv_pass_math<LOGN, P, K>(x, t, tw);
     if constexpr (P > 0) {
-        xstore<LOGN, P>(buf, x, t);
+        xstore<LOGN, P, K>(buf, x, t);
         ntt_sync<LOGN>(!SH::WarpLocal(P - 1));
-        xload<LOGN, P - 1>(buf, x, t);
-        inv_passes_from<LOGN, P - 1>(x, t, buf, tw);
+        xload<LOGN, P - 1, K>(buf, x, t);
+        inv_passes_from<LOGN, P - 1, K>(x, t, buf, tw);
     }
 }
 
-// Forward NTT: x in coefficient layout -> x in slot layout.
-template <int LOGN>
-__device__ __forceinline__ void ntt_forward(uint64_t x[8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
-    fwd_passes_from<LOGN, 0>(x, t, buf, tw_fwd);
+// Forward NTT of K polynomials: coefficient layout -> slot layout. buf holds K*N words.
+template <int LOGN, int K>
+__device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
+    fwd_passes_from<LOGN, 0, K>(x, t, buf, tw_fwd);
 }
 
-// Backward NTT without the 1/N factor: x in slot layout -> coefficient layout.
+// Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.
+template <int LOGN, int K>
+__device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][8], int t, uint64_t* buf,
+                                                        const uint64_t* tw_inv) {
+    inv_passes_from<LOGN, NttShape<LOGN>::NPASS - 1, K>(x, t, buf, tw_inv);
+}
+
+// One polynomial.
 template <int LOGN>
-__device__ __forceinline__ void ntt_backward_unscaled(uint64_t x[8], int t, uint64_t* buf,
+__device__ __forceinline__ void ntt_forward(uint64_t (&x)[8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
+    ntt_forward_k<LOGN, 1>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_fwd);
+}
+
+template <int LOGN>
+__device__ __forceinline__ void ntt_backward_unscaled(uint64_t (&x)[8], int t, uint64_t* buf,
                                                       const uint64_t* tw_inv) {
-    inv_passes_from<LOGN, NttShape<LOGN>::NPASS - 1>(x, t, buf, tw_inv);
+    ntt_backward_unscaled_k<LOGN, 1>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_inv);
 }
 
 }  // namespace tp
