@@ -23,6 +23,7 @@ GPU_LIB = PKG / "libtoothpaste_gpu.so"
 HOST_LIB = PKG / "libtoothpaste_host.so"
 
 NVCC = os.environ.get("NVCC", "nvcc")
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 CXX = os.environ.get("CXX", "g++")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -78,8 +79,8 @@ def build_host(force: bool = False) -> Path | None:
     deps = srcs + list(HOST.glob("*.h")) + [ROOT / "include" / "toothpaste_gpu.h", GPU_LIB]
     if force or not HOST_LIB.exists() or HOST_LIB.stat().st_mtime < _newest(deps):
         _run([CXX, "-std=c++20", "-O2", "-fPIC", "-shared", f"-I{ROOT / 'include'}", f"-I{HOST}",
-              *map(str, srcs), "-o", str(HOST_LIB), f"-L{PKG}", "-ltoothpaste_gpu",
-              "-Wl,-rpath,$ORIGIN"])
+              f"-I{CUDA_HOME / 'include'}", *map(str, srcs), "-o", str(HOST_LIB), f"-L{PKG}",
+              "-ltoothpaste_gpu", f"-L{CUDA_HOME / 'lib64'}", "-lcudart", "-Wl,-rpath,$ORIGIN"])
     return HOST_LIB
 
 

@@ -1,0 +1,194 @@
+// C++ drop-in operators over the B200 C ABI (include/toothpaste_gpu.h).
+//
+// These classes carry the reference's operator names, constructor parameters
+// and call signatures (lib/include/interfaces/blindrotation_operator.h:183-212,
+// lib/include/operators/cggi_blind_rotation.h:19-161,
+// lib/include/operators/bmmp_blind_rotation.h:18-176,
+// lib/include/operators/endo_glwe_conversion.h, automorphism_evaluation.h,
+// lwe_to_rlwe_packing.h), so host code written against the reference compiles
+// against them with a namespace change. ConstructOperator runs key generation
+// on the host (toothpaste_b200.cpp: the reference's MakeRLWE/MakeRGSW
+// steps with a seeded sampler) and uploads the key once; every BlindRotate /
+// Convert / Eval / Pack then runs on the GPU. A key produced elsewhere (for
+// instance by the reference's own operator) can be given to the Gpu* classes
+// directly in the reference's layout.
+//
+// Errors: a failing call throws std::runtime_error with tp_last_error().
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "toothpaste_gpu.h"
+
+namespace toothpaste_b200 {
+
+constexpr uint64_t kGoldilocks = 0xFFFFFFFF00000001ull;
+
+// lib/include/static/enum_ids.h
+enum KeyDistribution { BINARY, TERNARY, GAUSSIAN };
+
+inline void check(tp_status s) {
+    if (s != TP_OK) throw std::runtime_error(std::string("toothpaste_b200: ") + tp_last_error());
+}
+
+// Seeded stand-in for the reference's OpenFHE samplers (splitmix64 stream;
+// uniform by masked rejection, Gaussian by Box-Muller rounded to nearest).
+class Sampler {
+public:
+    explicit Sampler(uint64_t seed) : m_s(seed) {}
+    uint64_t Next();
+    uint64_t Uniform(uint64_t q);
+    uint64_t Gaussian(double std_dev, uint64_t q);
+
+private:
+    uint64_t m_s;
+};
+
+// Host key generation following the reference's RLWEEncryptor (lib/src/base_crypto.cpp:27-97)
+// and the operators' KeyGen loops. Outputs are in the reference's layouts.
+namespace keygen {
+std::vector<uint64_t> BlindRotationKey(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t basis_log2,
+                                       uint32_t digits, double std_dev, const std::vector<uint64_t>& lwe_key,
+                                       const std::vector<uint64_t>& rlwe_key);
+std::vector<uint64_t> RLWESwitchingKey(Sampler& rng, uint32_t N, uint32_t basis_log2, uint32_t digits, double std_dev,
+                                       const std::vector<uint64_t>& source_key, const std::vector<uint64_t>& target_key);
+std::vector<uint64_t> AutomorphismKey(Sampler& rng, uint32_t N, uint32_t basis_log2, uint32_t digits, double std_dev,
+                                      uint32_t index, const std::vector<uint64_t>& key);
+std::vector<uint64_t> PackingKeys(Sampler& rng, uint32_t N, uint32_t basis_log2, uint32_t digits, double std_dev,
+                                  const std::vector<uint64_t>& key);
+}  // namespace keygen
+
+// BlindRotator (lib/include/interfaces/blindrotation_operator.h:183-212).
+struct BlindRotator {
+    virtual void BlindRotate(std::vector<uint64_t>& result, const std::vector<uint64_t>& lwe_ciphertext,
+                             std::vector<uint64_t>& accumulator, bool output_as_coefficients = false) = 0;
+    virtual void BlindRotate(uint64_t* result, const uint64_t* lwe_vec, uint64_t* accumulator,
+                             bool output_as_coefficients = false) = 0;
+    virtual ~BlindRotator() = default;
+};
+
+// A blind-rotation key resident on one GPU (CGGI binary/ternary or BMMP).
+class GpuBlindRotator : public BlindRotator {
+public:
+    GpuBlindRotator(tp_br_variant variant, uint32_t N, uint32_t n, uint64_t basis, uint32_t digits,
+                    const std::vector<uint64_t>& brk, int device = 0);
+    ~GpuBlindRotator() override;
+    GpuBlindRotator(const GpuBlindRotator&) = delete;
+    GpuBlindRotator& operator=(const GpuBlindRotator&) = delete;
+
+    void BlindRotate(std::vector<uint64_t>& result, const std::vector<uint64_t>& lwe_ciphertext,
+                     std::vector<uint64_t>& accumulator, bool output_as_coefficients = false) override;
+    void BlindRotate(uint64_t* result, const uint64_t* lwe_vec, uint64_t* accumulator,
+                     bool output_as_coefficients = false) override;
+    // Many rotations at once on host buffers (lwe rows of n+1 words, acc rows of 2N words
+    // or one shared row when acc_stride == 0).
+    void BlindRotateBatch(uint64_t batch, uint64_t* results, const uint64_t* lwes, const uint64_t* accs,
+                          uint64_t acc_stride, bool output_as_coefficients = false);
+    tp_br_ctx* Handle() const { return m_ctx; }
+    uint32_t RingDimension() const { return m_N; }
+    uint32_t LWEDimension() const { return m_n; }
+
+private:
+    tp_br_ctx* m_ctx = nullptr;
+    uint32_t m_N, m_n;
+};
+
+// CGGIBlindRotationContext(distr, modulus, ring_dim, lwe_dim, basis, digits, std)
+// (lib/src/operators/cggi_blind_rotation.cpp:14-25).
+class CGGIBlindRotationContext : public std::enable_shared_from_this<CGGIBlindRotationContext> {
+public:
+    CGGIBlindRotationContext(KeyDistribution distr, uint64_t modulus, uint64_t ring_dim, uint64_t lwe_dim,
+                             uint64_t basis, uint64_t digits, double std_dev, int device = 0, uint64_t seed = 1);
+    // keys = {LWE key (n words; ternary -1 as any value other than 0/1), RLWE key (N words, coefficients)}
+    std::unique_ptr<GpuBlindRotator> ConstructOperator(const std::vector<std::vector<uint64_t>>& keys) const;
+    KeyDistribution GetKeyDistribution() const { return m_distr; }
+    uint64_t GetModulus() const { return m_q; }
+    uint64_t GetRingDimension() const { return m_N; }
+    uint64_t GetLWEDimension() const { return m_n; }
+    uint64_t GetBlindRotationBasis() const { return m_basis; }
+    uint64_t GetBlindRotationRGSWDigits() const { return m_digits; }
+    double GetStd() const { return m_std; }
+
+private:
+    KeyDistribution m_distr;
+    uint64_t m_q, m_N, m_n, m_basis, m_digits;
+    double m_std;
+    int m_device;
+    uint64_t m_seed;
+};
+
+// BMMPBlindRotationContext(distr, modulus, ring_dim, lwe_dim, basis, digits, std, step_size)
+// (lib/src/operators/bmmp_blind_rotation.cpp:13-37); binary keys, step size 2.
+class BMMPBlindRotationContext : public std::enable_shared_from_this<BMMPBlindRotationContext> {
+public:
+    BMMPBlindRotationContext(KeyDistribution distr, uint64_t modulus, uint64_t ring_dim, uint64_t lwe_dim,
+                             uint64_t basis, uint64_t digits, double std_dev, uint64_t step_size, int device = 0,
+                             uint64_t seed = 1);
+    std::unique_ptr<GpuBlindRotator> ConstructOperator(const std::vector<std::vector<uint64_t>>& keys) const;
+
+private:
+    uint64_t m_N, m_n, m_basis, m_digits;
+    double m_std;
+    int m_device;
+    uint64_t m_seed;
+};
+
+// RLWEtoRLWEConverter::Convert (lib/src/operators/rlwe_conversion.cpp:224-249).
+class GpuRLWEtoRLWEConverter {
+public:
+    GpuRLWEtoRLWEConverter(uint32_t N, uint64_t basis, uint32_t digits, const std::vector<uint64_t>& ksk,
+                           int device = 0);
+    ~GpuRLWEtoRLWEConverter();
+    // output -= KS(input.A); output.B += input.B  (output pre-zeroed by the caller, as in the reference)
+    void Convert(uint64_t* output, const uint64_t* input);
+    void Convert(std::vector<uint64_t>& output, const std::vector<uint64_t>& input);
+
+private:
+    tp_ks_ctx* m_ctx = nullptr;
+    uint32_t m_N;
+};
+
+// AutomorphismEvaluator::Eval (lib/src/operators/automorphism_evaluation.cpp:150-159).
+class GpuAutomorphismEvaluator {
+public:
+    GpuAutomorphismEvaluator(uint32_t N, uint64_t basis, uint32_t digits, uint32_t index,
+                             const std::vector<uint64_t>& ksk, int device = 0);
+    ~GpuAutomorphismEvaluator();
+    void Eval(uint64_t* output, const uint64_t* input);
+
+private:
+    tp_ks_ctx* m_ctx = nullptr;
+    uint32_t m_N;
+};
+
+// LWEtoRLWEPacker::Pack (lib/src/operators/lwe_to_rlwe_packing.cpp:129-236).
+class GpuLWEtoRLWEPacker {
+public:
+    GpuLWEtoRLWEPacker(uint32_t N, uint64_t basis, uint32_t digits, const std::vector<uint64_t>& keys,
+                       int device = 0);
+    ~GpuLWEtoRLWEPacker();
+    void Pack(uint64_t* output, const uint64_t* input, uint64_t len);
+
+private:
+    tp_ks_ctx* m_ctx = nullptr;
+    uint32_t m_N;
+};
+
+// LWEtoLWEConverter::Convert (lib/src/operators/lwe_conversion.cpp:205-239), Goldilocks modulus.
+class GpuLWEtoLWEConverter {
+public:
+    GpuLWEtoLWEConverter(uint32_t n_in, uint32_t n_out, uint64_t basis, uint32_t digits,
+                         const std::vector<uint64_t>& ksk, int device = 0);
+    ~GpuLWEtoLWEConverter();
+    void Convert(uint64_t* output, const uint64_t* input);
+
+private:
+    tp_lwe_ks_ctx* m_ctx = nullptr;
+    uint32_t m_n_in, m_n_out;
+};
+
+}  // namespace toothpaste_b200

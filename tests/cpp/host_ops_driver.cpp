@@ -1,0 +1,136 @@
+// Test driver for the C++ drop-in operators (fhetoothpaste_b200/host).
+//
+// Arrays travel as raw little-endian uint64 files; the Python tests write the
+// inputs, run one mode and compare the output file with the oracle.
+//
+//   keygen-br   variant N n beta digits std seed lwe_key rlwe_key out
+//   keygen-pack N beta digits std seed rlwe_key out
+//   rotate      variant N n beta digits std seed lwe_key rlwe_key lwes count accs out
+//   pack        N beta digits std seed rlwe_key lwes len out
+//   errors
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <string>
+
+#include "toothpaste_b200.hpp"
+
+using namespace toothpaste_b200;
+
+static std::vector<uint64_t> load(const char* path) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) throw std::runtime_error(std::string("cannot open ") + path);
+    const auto bytes = (size_t)f.tellg();
+    std::vector<uint64_t> v(bytes / 8);
+    f.seekg(0);
+    f.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(v.size() * 8));
+    return v;
+}
+
+static void save(const char* path, const uint64_t* p, size_t words) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(p), (std::streamsize)(words * 8));
+    if (!f) throw std::runtime_error(std::string("cannot write ") + path);
+}
+
+static uint64_t u(const char* s) { return std::strtoull(s, nullptr, 10); }
+
+template <class F>
+static bool throws(F&& f) {
+    try {
+        f();
+    } catch (const std::exception&) {
+        return true;
+    }
+    return false;
+}
+
+static int run(int argc, char** argv) {
+    const std::string mode = argc > 1 ? argv[1] : "";
+    if (mode == "keygen-br" && argc == 12) {
+        Sampler rng(u(argv[8]));
+        const auto brk = keygen::BlindRotationKey(rng, (int)u(argv[2]), (uint32_t)u(argv[3]), (uint32_t)u(argv[4]),
+                                                  (uint32_t)u(argv[5]), (uint32_t)u(argv[6]), std::atof(argv[7]),
+                                                  load(argv[9]), load(argv[10]));
+        save(argv[11], brk.data(), brk.size());
+        return 0;
+    }
+    if (mode == "keygen-pack" && argc == 9) {
+        Sampler rng(u(argv[6]));
+        const auto k = keygen::PackingKeys(rng, (uint32_t)u(argv[2]), (uint32_t)u(argv[3]), (uint32_t)u(argv[4]),
+                                           std::atof(argv[5]), load(argv[7]));
+        save(argv[8], k.data(), k.size());
+        return 0;
+    }
+    if (mode == "rotate" && argc == 15) {
+        const int variant = (int)u(argv[2]);
+        const uint64_t N = u(argv[3]), n = u(argv[4]), basis = 1ull << u(argv[5]), digits = u(argv[6]);
+        const double sd = std::atof(argv[7]);
+        const uint64_t seed = u(argv[8]), count = u(argv[12]);
+        const std::vector<std::vector<uint64_t>> keys{load(argv[9]), load(argv[10])};
+        std::unique_ptr<GpuBlindRotator> op;
+        if (variant == TP_BR_BMMP_BINARY) {
+            BMMPBlindRotationContext ctx(BINARY, kGoldilocks, N, n, basis, digits, sd, 2, 0, seed);
+            op = ctx.ConstructOperator(keys);
+        } else {
+            CGGIBlindRotationContext ctx(variant == TP_BR_CGGI_BINARY ? BINARY : TERNARY, kGoldilocks, N, n, basis,
+                                         digits, sd, 0, seed);
+            op = ctx.ConstructOperator(keys);
+        }
+        const auto lwes = load(argv[11]);
+        const auto accs = load(argv[13]);
+        std::vector<uint64_t> out(count * 2 * N);
+        // the first rotation through the reference's vector signature, in place like NegacyclicFunctionEvaluator
+        std::vector<uint64_t> lwe0(lwes.begin(), lwes.begin() + (n + 1));
+        std::vector<uint64_t> acc0(accs.begin(), accs.begin() + 2 * N);
+        op->BlindRotate(acc0, lwe0, acc0, false);
+        std::memcpy(out.data(), acc0.data(), 16 * N);
+        if (count > 1)
+            op->BlindRotateBatch(count - 1, out.data() + 2 * N, lwes.data() + (n + 1), accs.data() + 2 * N, 2 * N,
+                                 false);
+        save(argv[14], out.data(), out.size());
+        return 0;
+    }
+    if (mode == "pack" && argc == 11) {
+        const uint32_t N = (uint32_t)u(argv[2]), beta = (uint32_t)u(argv[3]), digits = (uint32_t)u(argv[4]);
+        Sampler rng(u(argv[6]));
+        const auto keys = keygen::PackingKeys(rng, N, beta, digits, std::atof(argv[5]), load(argv[7]));
+        GpuLWEtoRLWEPacker packer(N, 1ull << beta, digits, keys, 0);
+        const auto lwes = load(argv[8]);
+        std::vector<uint64_t> out(2ull * N);
+        packer.Pack(out.data(), lwes.data(), u(argv[9]));
+        save(argv[10], out.data(), out.size());
+        return 0;
+    }
+    if (mode == "errors") {
+        // parameter checks that the reference asserts (bmmp_blind_rotation.cpp:16-24) and
+        // C-ABI refusals surfacing as exceptions; none of these reaches a device
+        int bad = 0;
+        bad += !throws([] { BMMPBlindRotationContext(BINARY, kGoldilocks, 1024, 501, 1ull << 16, 3, 3.2, 2); });
+        bad += !throws([] { BMMPBlindRotationContext(TERNARY, kGoldilocks, 1024, 500, 1ull << 16, 3, 3.2, 2); });
+        bad += !throws([] { BMMPBlindRotationContext(BINARY, kGoldilocks, 1024, 500, 1ull << 16, 3, 3.2, 4); });
+        bad += !throws([] { CGGIBlindRotationContext(BINARY, (1ull << 61) - 1, 1024, 500, 1ull << 16, 3, 3.2); });
+        bad += !throws([] { CGGIBlindRotationContext(GAUSSIAN, kGoldilocks, 1024, 500, 1ull << 16, 3, 3.2); });
+        bad += !throws([] {
+            CGGIBlindRotationContext c(BINARY, kGoldilocks, 1024, 500, 1ull << 16, 3, 3.2);
+            c.ConstructOperator({{1, 0}, {}});
+        });
+        bad += !throws([] { GpuBlindRotator(TP_BR_CGGI_BINARY, 1000, 16, 1ull << 16, 3, {}, 0); });
+        bad += !throws([] { GpuBlindRotator(TP_BR_CGGI_BINARY, 1024, 16, 1ull << 16, 9, {}, 0); });
+        std::cout << (bad ? "FAIL " : "ok ") << bad << "\n";
+        return bad ? 1 : 0;
+    }
+    std::cerr << "bad arguments\n";
+    return 2;
+}
+
+int main(int argc, char** argv) {
+    try {
+        return run(argc, argv);
+    } catch (const std::exception& e) {
+        std::cerr << "error: " << e.what() << "\n";
+        return 1;
+    }
+}

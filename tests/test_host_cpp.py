@@ -1,0 +1,102 @@
+"""The C++ drop-in operators (fhetoothpaste_b200/host): key generation equals the
+oracle's for the same seed (CPU), the reference's parameter checks throw (CPU), and
+rotations / packing through the C++ classes equal the oracle (GPU)."""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.oracle import (CGGI_BINARY, CGGI_TERNARY, BMMP_BINARY, lwe_inputs, lwe_secret, random_acc,
+                           rlwe_secret, sm64)
+
+ROOT = Path(__file__).resolve().parents[1]
+PKG = ROOT / "fhetoothpaste_b200"
+
+
+@pytest.fixture(scope="session")
+def driver(tmp_path_factory):
+    from fhetoothpaste_b200 import build
+    build.build_gpu()
+    build.build_host()
+    exe = tmp_path_factory.mktemp("cpp") / "host_ops_driver"
+    subprocess.run(["g++", "-std=c++20", "-O2", f"-I{ROOT / 'include'}", f"-I{PKG / 'host'}",
+                    str(ROOT / "tests" / "cpp" / "host_ops_driver.cpp"), "-o", str(exe), f"-L{PKG}",
+                    "-ltoothpaste_host", "-ltoothpaste_gpu", f"-Wl,-rpath,{PKG}"], check=True)
+    return exe
+
+
+def run(exe, tmp, *args):
+    """Runs the driver; array arguments are written to files and the last one is read back."""
+    argv = [str(exe)]
+    for i, a in enumerate(args):
+        if isinstance(a, np.ndarray):
+            f = tmp / f"in{i}.bin"
+            np.ascontiguousarray(a, np.uint64).tofile(f)
+            argv.append(str(f))
+        else:
+            argv.append(str(a))
+    out = tmp / "out.bin"
+    argv.append(str(out))
+    res = subprocess.run(argv, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    return np.fromfile(out, dtype=np.uint64)
+
+
+BR_SMALL = [  # (variant, N, n, beta, digits, std)
+    (CGGI_BINARY, 256, 12, 16, 3, 3.2),
+    (CGGI_TERNARY, 128, 10, 20, 2, 3.2),
+    (BMMP_BINARY, 256, 12, 12, 4, 3.2),
+]
+
+
+@pytest.mark.parametrize("case", BR_SMALL, ids=["binary", "ternary", "bmmp"])
+def test_keygen_equals_oracle(driver, oracle, tmp_path, case):
+    variant, N, n, beta, digits, std = case
+    sk = lwe_secret(variant, n, N, seed=41)
+    z = rlwe_secret(N, seed=42)
+    got = run(driver, tmp_path, "keygen-br", variant, N, n, beta, digits, std, 7, sk, z)
+    want = oracle.br_keygen(variant, N, n, beta, digits, std, sk, z, seed=7)
+    assert got.size == want.size
+    assert np.array_equal(got, want)
+
+
+def test_packing_keygen_equals_oracle(driver, oracle, tmp_path):
+    N, beta, digits, std = 128, 16, 4, 3.2
+    z = rlwe_secret(N, seed=9)
+    got = run(driver, tmp_path, "keygen-pack", N, beta, digits, std, 11, z)
+    want = oracle.pack_keygen(N, beta, digits, std, z, seed=11)
+    assert np.array_equal(got, want)
+
+
+def test_parameter_checks_throw(driver):
+    res = subprocess.run([str(driver), "errors"], capture_output=True, text=True)
+    assert res.returncode == 0 and res.stdout.startswith("ok"), res.stdout + res.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", BR_SMALL, ids=["binary", "ternary", "bmmp"])
+def test_cpp_operator_rotates_like_oracle(driver, oracle, cuda, tmp_path, case):
+    variant, N, n, beta, digits, std = case
+    sk = lwe_secret(variant, n, N, seed=51)
+    z = rlwe_secret(N, seed=52)
+    count = 5
+    lwes = lwe_inputs(N, n, count, seed=53)
+    accs = random_acc(N, count, seed=54)
+    got = run(driver, tmp_path, "rotate", variant, N, n, beta, digits, std, 13, sk, z, lwes, count, accs)
+    brk = oracle.br_keygen(variant, N, n, beta, digits, std, sk, z, seed=13)
+    want = oracle.blind_rotate_many(variant, N, n, beta, digits, brk, lwes, accs, False, 2)
+    assert np.array_equal(got.reshape(count, 2 * N), want)
+
+
+@pytest.mark.gpu
+def test_cpp_packer_like_oracle(driver, oracle, cuda, tmp_path):
+    N, beta, digits, std, length = 128, 16, 4, 3.2, 4
+    z = rlwe_secret(N, seed=61)
+    lwes = (sm64(62, length * (N + 1)) % np.uint64(0xFFFFFFFF00000001)).reshape(length, N + 1)
+    got = run(driver, tmp_path, "pack", N, beta, digits, std, 17, z, lwes, length)
+    keys = oracle.pack_keygen(N, beta, digits, std, z, seed=17)
+    want = oracle.pack(N, beta, digits, keys, lwes, length)
+    assert np.array_equal(got, want)
