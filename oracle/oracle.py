@@ -130,6 +130,7 @@ class Oracle:
             "tpo_ntt_backward": (I, [U64, U64P, U64P]),
             "tpo_brk_words": (U64, [I, U64, U64, U64]),
             "tpo_br_keygen": (None, [R, I, U64, U64, U64, U64, D, U64P, U64P, U64P]),
+            "tpo_br_keygen_aligned": (None, [R, I, U64, U64, U64, U64, D, U64P, U64P, U64P]),
             "tpo_blind_rotate": (I, [I, U64, U64, U64, U64, U64P, U64P, U64P, U64P, I]),
             "tpo_blind_rotate_many": (I, [I, U64, U64, U64, U64, U64P, U64P, U64P, U64P, U64, I, I]),
             "tpo_phase_rlwe": (None, [U64, U64P, U64P, U64P]),
@@ -178,6 +179,23 @@ class Oracle:
                              ptr(np.ascontiguousarray(lwe_key, np.uint64)),
                              ptr(np.ascontiguousarray(rlwe_key, np.uint64)), ptr(brk))
         return brk
+
+    def br_keygen_aligned(self, variant, N, n, basis_log2, digits, std, lwe_key, rlwe_key, seed) -> np.ndarray:
+        """Key with RGSW rows scaled 2^(64 - beta(j+1)), aligned with the signed digits."""
+        r = Rng(seed)
+        brk = np.empty(self.L.tpo_brk_words(variant, N, n, digits), dtype=np.uint64)
+        self.L.tpo_br_keygen_aligned(ctypes.byref(r), variant, N, n, basis_log2, digits, std,
+                                     ptr(np.ascontiguousarray(lwe_key, np.uint64)),
+                                     ptr(np.ascontiguousarray(rlwe_key, np.uint64)), ptr(brk))
+        return brk
+
+    def make_rlwe(self, N, std, msg, sk, seed) -> np.ndarray:
+        """RLWE encryption (NTT domain) of a coefficient-domain message under sk (coefficients)."""
+        r = Rng(seed)
+        out = np.empty(2 * N, dtype=np.uint64)
+        self.L.tpo_make_rlwe(ctypes.byref(r), N, std, ptr(out), ptr(np.ascontiguousarray(msg, np.uint64)),
+                             ptr(self.ntt_forward(sk)), 0)
+        return out
 
     def blind_rotate(self, variant, N, n, basis_log2, digits, brk, lwe, acc, out_coef) -> np.ndarray:
         res = np.empty(2 * N, dtype=np.uint64)

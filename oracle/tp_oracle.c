@@ -298,32 +298,40 @@ void tpo_make_rlwe(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const 
     free(e);
 }
 
-/* RLWEEncryptor::MakeRGSW (lib/src/base_crypto.cpp:60-97): rows 0..l-1 encrypt
- * -s*m*g_j, rows l..2l-1 encrypt m*g_j, g_j = B^(max_digits-1-j). */
-void tpo_make_rgsw(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const uint64_t* msg,
-                   const uint64_t* sk_ntt, uint64_t basis, uint64_t digits, int msg_is_ntt) {
-    uint64_t* tmp = (uint64_t*)calloc(3 * N, 8);
-    /* ceil(log2(Q)/log2(basis)) in long double, as the reference computes it */
-    const uint64_t max_digits = (uint64_t)ceill(log2l((long double)P) / log2l((long double)basis));
+/* Rows of an RGSW with explicit gadget factors: rows 0..l-1 encrypt -s*m*g[j],
+ * rows l..2l-1 encrypt m*g[j], drawn in the order MakeRGSW draws them (smallest
+ * factor first). */
+static void make_rgsw_rows(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const uint64_t* msg,
+                           const uint64_t* sk_ntt, const uint64_t* g, uint64_t digits, int msg_is_ntt) {
+    uint64_t* m = (uint64_t*)calloc(3 * N, 8);
+    uint64_t* row = (uint64_t*)malloc(2 * N * 8);
     if (msg_is_ntt) {
-        for (uint64_t i = 0; i < N; ++i) tmp[i] = tpo_mul(msg[i], sk_ntt[i]);
-        for (uint64_t i = 0; i < N; ++i) tmp[N + i] = tpo_sub(tmp[N + i], tmp[i]);
-        memcpy(tmp, msg, N * 8);
+        memcpy(m, msg, N * 8);
     } else {
-        tpo_ntt_forward(N, tmp, msg);
-        for (uint64_t i = 0; i < N; ++i) tmp[2 * N + i] = tpo_mul(tmp[i], sk_ntt[i]);
-        for (uint64_t i = 0; i < N; ++i) tmp[N + i] = tpo_sub(tmp[N + i], tmp[2 * N + i]);
+        tpo_ntt_forward(N, m, msg);
     }
-    const uint64_t b = basis % P;
-    for (uint64_t d = 0; d < max_digits - digits; ++d)
-        for (uint64_t i = 0; i < 2 * N; ++i) tmp[i] = tpo_mul(tmp[i], b);
+    for (uint64_t i = 0; i < N; ++i) m[2 * N + i] = tpo_mul(m[i], sk_ntt[i]);
+    for (uint64_t i = 0; i < N; ++i) m[N + i] = tpo_sub(0, m[2 * N + i]);
     for (uint64_t d = 0; d < digits; ++d) {
         const uint64_t off = digits - d - 1;
-        tpo_make_rlwe(r, N, std_dev, out + off * 2 * N, tmp + N, sk_ntt, 1);
-        tpo_make_rlwe(r, N, std_dev, out + off * 2 * N + 2 * N * digits, tmp, sk_ntt, 1);
-        for (uint64_t i = 0; i < 2 * N; ++i) tmp[i] = tpo_mul(tmp[i], b);
+        const uint64_t f = g[off] % P;
+        for (uint64_t i = 0; i < 2 * N; ++i) row[i] = tpo_mul(m[i], f);
+        tpo_make_rlwe(r, N, std_dev, out + off * 2 * N, row + N, sk_ntt, 1);
+        tpo_make_rlwe(r, N, std_dev, out + off * 2 * N + 2 * N * digits, row, sk_ntt, 1);
     }
-    free(tmp);
+    free(m);
+    free(row);
+}
+
+/* RLWEEncryptor::MakeRGSW (lib/src/base_crypto.cpp:60-97): row j carries
+ * g_j = B^(max_digits-1-j), max_digits = ceil(log2(Q)/log2(B)) computed in long
+ * double as the reference computes it. */
+void tpo_make_rgsw(tpo_rng* r, uint64_t N, double std_dev, uint64_t* out, const uint64_t* msg,
+                   const uint64_t* sk_ntt, uint64_t basis, uint64_t digits, int msg_is_ntt) {
+    const uint64_t max_digits = (uint64_t)ceill(log2l((long double)P) / log2l((long double)basis));
+    uint64_t g[64];
+    for (uint64_t j = 0; j < digits; ++j) g[j] = tpo_pow(basis % P, max_digits - 1 - j);
+    make_rgsw_rows(r, N, std_dev, out, msg, sk_ntt, g, digits, msg_is_ntt);
 }
 
 /* RLWEEncryptor::PhaseRLWE (lib/src/base_crypto.cpp:99-108). */
@@ -341,41 +349,60 @@ uint64_t tpo_brk_words(int variant, uint64_t N, uint64_t n, uint64_t digits) {
     }
 }
 
-void tpo_br_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
-                   double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk) {
+static void br_keygen_rows(tpo_rng* r, int variant, uint64_t N, uint64_t n, const uint64_t* g, uint64_t digits,
+                           double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk) {
     uint64_t* sk = (uint64_t*)malloc(N * 8);
     uint64_t* data = (uint64_t*)calloc(2 * N, 8);
-    const uint64_t L = 1ULL << basis_log2;
     const uint64_t rg = 4 * N * digits;
     tpo_ntt_forward(N, sk, rlwe_key);
     if (variant == TPO_CGGI_BINARY) {
         /* cggi_blind_rotation.cpp:264-280 */
         for (uint64_t i = 0; i < n; ++i) {
             data[0] = lwe_key[i];
-            tpo_make_rgsw(r, N, std_dev, brk + i * rg, data, sk, L, digits, 0);
+            make_rgsw_rows(r, N, std_dev, brk + i * rg, data, sk, g, digits, 0);
         }
     } else if (variant == TPO_CGGI_TERNARY) {
         /* cggi_blind_rotation.cpp:282-311 */
         for (uint64_t i = 0; i < n; ++i) {
             data[0] = lwe_key[i] == 1;
             data[N] = lwe_key[i] != 0 && lwe_key[i] != 1;
-            tpo_make_rgsw(r, N, std_dev, brk + i * 2 * rg, data, sk, L, digits, 0);
-            tpo_make_rgsw(r, N, std_dev, brk + i * 2 * rg + rg, data + N, sk, L, digits, 0);
+            make_rgsw_rows(r, N, std_dev, brk + i * 2 * rg, data, sk, g, digits, 0);
+            make_rgsw_rows(r, N, std_dev, brk + i * 2 * rg + rg, data + N, sk, g, digits, 0);
         }
     } else {
         /* bmmp_blind_rotation.cpp:229-262 */
         for (uint64_t i = 0; i < n; i += 2) {
             uint64_t* chunk = brk + 3 * (i >> 1) * rg;
             data[0] = lwe_key[i];
-            tpo_make_rgsw(r, N, std_dev, chunk, data, sk, L, digits, 0);
+            make_rgsw_rows(r, N, std_dev, chunk, data, sk, g, digits, 0);
             data[0] = lwe_key[i + 1];
-            tpo_make_rgsw(r, N, std_dev, chunk + rg, data, sk, L, digits, 0);
+            make_rgsw_rows(r, N, std_dev, chunk + rg, data, sk, g, digits, 0);
             data[0] = lwe_key[i + 1] * lwe_key[i];
-            tpo_make_rgsw(r, N, std_dev, chunk + 2 * rg, data, sk, L, digits, 0);
+            make_rgsw_rows(r, N, std_dev, chunk + 2 * rg, data, sk, g, digits, 0);
         }
     }
     free(sk);
     free(data);
+}
+
+void tpo_br_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                   double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk) {
+    const uint64_t L = 1ULL << basis_log2;
+    const uint64_t max_digits = (uint64_t)ceill(log2l((long double)P) / log2l((long double)L));
+    uint64_t g[64];
+    for (uint64_t j = 0; j < digits; ++j) g[j] = tpo_pow(L, max_digits - 1 - j);
+    br_keygen_rows(r, variant, N, n, g, digits, std_dev, lwe_key, rlwe_key, brk);
+}
+
+/* Blind-rotation key whose RGSW rows carry g_j = 2^(64 - beta(j+1)), the weights of
+ * the signed decomposition's digits (gadget_decomp.h:176). Equal to the reference's
+ * key when beta divides 64; for other bases it is the consistent-gadget variant used
+ * only by the decryption tests. */
+void tpo_br_keygen_aligned(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                           double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk) {
+    uint64_t g[64];
+    for (uint64_t j = 0; j < digits; ++j) g[j] = 1ULL << (64 - basis_log2 * (j + 1));
+    br_keygen_rows(r, variant, N, n, g, digits, std_dev, lwe_key, rlwe_key, brk);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -74,6 +74,8 @@ uint64_t tpo_brk_words(int variant, uint64_t N, uint64_t n, uint64_t digits);
  * and BMMP KeyGenBinary (lib/src/operators/bmmp_blind_rotation.cpp:229-262). */
 void tpo_br_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
                    double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk);
+void tpo_br_keygen_aligned(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits,
+                           double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk);
 
 /* BlindRotate: CGGI (cggi_blind_rotation.cpp:236-262, 313-472) and BMMP
  * (bmmp_blind_rotation.cpp:325-335, 280-323, 354-419; MultiMux mux_operator.cpp:204-294).
