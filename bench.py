@@ -212,6 +212,89 @@ def run_reference(args, wl):
     print(json.dumps(line), flush=True)
 
 
+def _timed(torch, fn, warmup: int, reps: int, stream) -> float:
+    """Mean ms of fn() over reps launches on `stream` (CUDA events), after warmup."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _uniform_key(words: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 2**63, words, dtype=np.uint64)  # residues below p
+
+
+BMMP_BATCHES = (1, 37, 512, 2048, 8192)
+
+
+def bmmp_batch_sweep(device: int) -> dict:
+    """BMMP (binary n=768 as 384 pairs, N=2048, base 2^16 l=4) at uneven batch sizes,
+    identity test polynomials, one graph-recorded launch per batch."""
+    import torch
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    from oracle.oracle import lwe_inputs
+    N, n = 2048, 768
+    ctx = BlindRotationContext(2, N, n, 1 << 16, 4)
+    rot = GpuBlindRotator(ctx, _uniform_key(ctx.key_words(), 31), device=device)
+    stream = torch.cuda.current_stream().cuda_stream
+    ident = np.zeros(2 * N, np.uint64)
+    ident[N:] = np.arange(N, dtype=np.uint64)
+    out = {"workload": "BMMP n=768 (384 pairs), N=2048, base 2^16 l=4, identity LUT", "unit": "BR/s"}
+    launches = 0
+    lw_all = torch.from_numpy(lwe_inputs(N, n, max(BMMP_BATCHES), 33).view(np.int64)).cuda()
+    ac = torch.from_numpy(ident.view(np.int64)).cuda()
+    res = torch.empty((max(BMMP_BATCHES), 2 * N), dtype=torch.int64, device="cuda")
+    for b in BMMP_BATCHES:
+        g = rot.capture_batch(res.data_ptr(), lw_all.data_ptr(), n + 1, ac.data_ptr(), 0, b)
+        reps = 3 if b >= 512 else 5
+        ms = _timed(torch, lambda: g.launch(stream), 2, reps, stream)
+        launches += 2 + reps
+        g.close()
+        out[str(b)] = {"BR_per_s": round(b / (ms * 1e-3), 1), "ms_per_launch": round(ms, 3)}
+    rot.check(stream)
+    rot.close()
+    out["launches"] = launches
+    return out
+
+
+def packing_run(device: int) -> dict:
+    """Config-4 key switching: 2048 LWEs (n = N = 2048) packed into one RLWE with the
+    11 automorphism keys (base 2^16, l = 4), 64 packings per launch; then RLWE->RLWE
+    key switching of 1024 ciphertexts in one launch."""
+    import torch
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker, GpuRLWEtoRLWEConverter
+    N, L, packs, beta, l = 2048, 2048, 64, 16, 4
+    stream = torch.cuda.current_stream().cuda_stream
+    packer = GpuLWEtoRLWEPacker(N, 1 << beta, l, _uniform_key(11 * 2 * N * l, 41), device=device)
+    rng = np.random.default_rng(42)
+    lw = torch.from_numpy(rng.integers(0, 2**63, (packs * L, N + 1), dtype=np.uint64).view(np.int64)).cuda()
+    po = torch.empty((packs, 2 * N), dtype=torch.int64, device="cuda")
+    pack_ms = _timed(torch, lambda: packer.pack_batch(packs, L, po.data_ptr(), lw.data_ptr(), stream), 1, 2, stream)
+    del lw
+    packer.close()
+    conv = GpuRLWEtoRLWEConverter(N, 1 << beta, l, _uniform_key(2 * N * l, 43), device=device)
+    cts = 1024
+    ci = torch.from_numpy(rng.integers(0, 2**63, (cts, 2 * N), dtype=np.uint64).view(np.int64)).cuda()
+    co = torch.zeros((cts, 2 * N), dtype=torch.int64, device="cuda")
+    ks_ms = _timed(torch, lambda: conv.convert_batch(cts, co.data_ptr(), ci.data_ptr(), stream), 2, 5, stream)
+    conv.close()
+    levels = L.bit_length() - 1
+    per_pack_launch = 1 + levels + (N.bit_length() - 1 - levels)  # L0 setup, one launch per tree level, traces
+    return {"workload": "pack 2048 LWE (n=2048) -> RLWE N=2048, base 2^16 l=4; RLWE KS x1024",
+            "packs_per_launch": packs, "ms_per_pack_launch": round(pack_ms, 3),
+            "packs_per_s": round(packs / (pack_ms * 1e-3), 2),
+            "lwe_packed_per_s": round(packs * L / (pack_ms * 1e-3), 1),
+            "rlwe_ks_per_s": round(cts / (ks_ms * 1e-3), 1), "ms_per_ks_launch": round(ks_ms, 3),
+            "launches": 3 * per_pack_launch + 7}
+
+
 SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l = 3
 SERVING_MIX = [0.5, 0.35, 0.15]
 
@@ -264,6 +347,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--serve-rate", type=float, default=50000.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the BMMP batch sweep and the packing run")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -310,8 +394,11 @@ def main():
     out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
 
+    # one step = one replay of the recorded batch launch (CUDA graph)
+    graph = rot.capture_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch)
+
     def step():
-        rot.blind_rotate_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch, stream=stream)
+        graph.launch(stream)
 
     def barrier():
         torch.cuda.synchronize()
@@ -330,6 +417,7 @@ def main():
         barrier()
     rot.check(stream)
     ms = e0.elapsed_time(e1) / args.steps
+    graph.close()
     if args.mode == "kernel":
         if rank == 0:
             print(json.dumps({"mode": "kernel", "workload": wl, "batch": batch, "lwe_dim": n,
@@ -404,7 +492,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)", "data": "synthetic",
         "config": {"workload": DESCR[wl], "batch_per_gpu": batch, "ring_dim": N, "lwe_dim": n,
-                   "gadget": f"2^{bl} l={l}", "output": "NTT domain",
+                   "gadget": f"2^{bl} l={l}", "output": "NTT domain", "launch": "CUDA graph, one kernel per step",
                    "l2": f"inputs larger than L2: {key_bytes / 2**20:.0f} MiB key streamed per launch",
                    "key": "uniform random key words (timing does not depend on key values)"},
         "e2e": {"value": round(e2e_val, 2), "unit": "BR/s", "h2d_bytes_per_step": int(h2d),
@@ -424,6 +512,11 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = serving_run(local, args.serve_rate, args.serve_seconds)
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["bmmp_batches"] = bmmp_batch_sweep(local)
+        line["packing"] = packing_run(local)
+        launches += line["bmmp_batches"].pop("launches") + line["packing"].pop("launches")
+        line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, threads, count, secs = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,

@@ -57,6 +57,10 @@ def lib() -> ctypes.CDLL:
         "tp_br_blind_rotate_batch_host": (ctypes.c_int, [VP, U64, U64P, U64P, U64, U64P, U64, ctypes.c_int, VP]),
         "tp_br_check": (ctypes.c_int, [VP, VP]),
         "tp_sample_extract_batch": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
+        "tp_br_batch_graph_create": (ctypes.c_int, [VP, U64, VP, VP, U64, VP, U64, ctypes.c_int, VP,
+                                                    ctypes.POINTER(VP)]),
+        "tp_graph_launch": (ctypes.c_int, [VP, VP]),
+        "tp_graph_destroy": (ctypes.c_int, [VP]),
         "tp_ntt_forward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_ntt_backward": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_rlwe_ks_create": (ctypes.c_int, [ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(VP)]),

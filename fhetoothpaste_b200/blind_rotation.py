@@ -101,6 +101,36 @@ class GpuBlindRotator:
     def check(self, stream: int | None = None) -> None:
         nat.check(nat.lib().tp_br_check(self._h, stream))
 
+    def capture_batch(self, results_ptr: int, lwes_ptr: int, lwe_stride: int, accs_ptr: int, acc_stride: int,
+                      batch: int, out_coef: bool = False, extract_ptr: int | None = None) -> "BatchGraph":
+        """Records one batch launch (plus SampleExtract into extract_ptr) as a CUDA graph."""
+        g = ctypes.c_void_p()
+        nat.check(nat.lib().tp_br_batch_graph_create(self._h, batch, results_ptr, lwes_ptr, lwe_stride, accs_ptr,
+                                                     acc_stride, int(bool(out_coef)), extract_ptr, ctypes.byref(g)))
+        return BatchGraph(g, self)
+
+
+class BatchGraph:
+    """A recorded batch launch; replays read the device buffers' current contents."""
+
+    def __init__(self, handle: ctypes.c_void_p, owner: GpuBlindRotator):
+        self._g = handle
+        self._owner = owner  # keeps the key alive while the graph exists
+
+    def launch(self, stream: int | None = None) -> None:
+        nat.check(nat.lib().tp_graph_launch(self._g, stream))
+
+    def close(self) -> None:
+        if getattr(self, "_g", None):
+            nat.lib().tp_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 def ntt_forward(ring_dim: int, count: int, out_ptr: int, in_ptr: int, stream: int | None = None) -> None:
     nat.check(nat.lib().tp_ntt_forward(ring_dim, count, out_ptr, in_ptr, stream))

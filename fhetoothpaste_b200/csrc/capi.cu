@@ -450,6 +450,63 @@ tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* o
     return TP_OK;
 }
 
+struct tp_graph {
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+};
+
+tp_status tp_br_batch_graph_create(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                   uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
+                                   uint64_t* extract_out, tp_graph** out) {
+    if (!c || !out) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    if (batch == 0) return fail(TP_ERR_PARAM, "empty batch");
+    if (extract_out && !out_coef) return fail(TP_ERR_PARAM, "SampleExtract needs coefficient-domain results");
+    TP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = nullptr;
+    TP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s);
+        return fail(TP_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    }
+    tp_status st = tp_br_blind_rotate_batch(c, batch, results, lwes, lwe_stride, accs, acc_stride, out_coef, s);
+    if (st == TP_OK && extract_out) st = tp_sample_extract_batch(c->prm.ring_dim, batch, extract_out, results, s);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);  // always ends the capture, also after a failed launch
+    cudaStreamDestroy(s);
+    if (st != TP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    auto* gr = new tp_graph();
+    gr->device = c->device;
+    e = cudaGraphInstantiate(&gr->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        delete gr;
+        return fail(TP_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = gr;
+    return TP_OK;
+}
+
+tp_status tp_graph_launch(tp_graph* g, void* stream) {
+    if (!g) return fail(TP_ERR_PARAM, "null graph");
+    TP_CUDA(cudaSetDevice(g->device));
+    TP_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return TP_OK;
+}
+
+tp_status tp_graph_destroy(tp_graph* g) {
+    if (!g) return TP_OK;
+    cudaSetDevice(g->device);
+    cudaGraphExecDestroy(g->exec);
+    delete g;
+    return TP_OK;
+}
+
 tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out, const uint64_t* a, const uint64_t* b,
                          const uint64_t* c, void* stream) {
     if (op < 0 || op > 5) return fail(TP_ERR_PARAM, "unknown op %d", op);

@@ -111,6 +111,21 @@ tp_status tp_br_check(tp_br_ctx* ctx, void* stream);
 tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* out_dev, const uint64_t* rlwe_dev,
                                   void* stream);
 
+/* A batch launch recorded once as a CUDA graph and replayed many times, for
+ * loops that rotate fresh ciphertexts through the same device buffers (the
+ * graph reads the buffers' contents at replay time). With extract_out != NULL
+ * the graph also runs SampleExtract (index 0) on every result into
+ * extract_out (batch x (N+1) words), which needs out_coef = 1: rotation and
+ * extraction then cost one graph launch. No reference counterpart (the
+ * reference runs one rotation per call). Capture happens on a private stream;
+ * the context's key must be uploaded first. */
+typedef struct tp_graph tp_graph;
+tp_status tp_br_batch_graph_create(tp_br_ctx* ctx, uint64_t batch, uint64_t* results_dev, const uint64_t* lwes_dev,
+                                   uint64_t lwe_stride, const uint64_t* accs_dev, uint64_t acc_stride, int out_coef,
+                                   uint64_t* extract_out_dev, tp_graph** out);
+tp_status tp_graph_launch(tp_graph* graph, void* stream);
+tp_status tp_graph_destroy(tp_graph* graph);
+
 /* Batched negacyclic NTT on device buffers, `count` polynomials of N words,
  * in-place allowed. Replaces SolinasWorker::ForwardNTT / BackwardNTT
  * (lib/src/backend/solinas.cpp:228-313); backward includes 1/N. */

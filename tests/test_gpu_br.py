@@ -113,3 +113,52 @@ def test_result_may_alias_accumulator(native, oracle, golden, cuda):
     for b in range(3):
         exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], accs[b], 1)
         np.testing.assert_array_equal(got[b], exp)
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_graph_replays_read_fresh_inputs(native, oracle, golden, cuda, name):
+    """One recorded graph (rotation + SampleExtract), replayed over two different input sets."""
+    torch = cuda
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    batch = 150
+    d_lwe = torch.empty((batch, n + 1), dtype=torch.int64, device="cuda")
+    d_acc = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    d_res = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    d_ext = torch.empty((batch, N + 1), dtype=torch.int64, device="cuda")
+    graph = rot.capture_batch(d_res.data_ptr(), d_lwe.data_ptr(), n + 1, d_acc.data_ptr(), 2 * N, batch,
+                              out_coef=True, extract_ptr=d_ext.data_ptr())
+    for seed in (31, 41):
+        lwes = lwe_inputs(N, n, batch, seed)
+        accs = random_acc(N, batch, seed + 1)
+        d_lwe.copy_(torch.from_numpy(lwes.view(np.int64)))
+        d_acc.copy_(torch.from_numpy(accs.view(np.int64)))
+        graph.launch()
+        rot.check()
+        res = d_res.cpu().numpy().view(np.uint64)
+        ext = d_ext.cpu().numpy().view(np.uint64)
+        for b in (0, 77, batch - 1):
+            exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b],
+                                      accs[b], 1)
+            np.testing.assert_array_equal(res[b], exp)
+            lwe = np.zeros(N + 1, np.uint64)
+            oracle.L.tpo_sample_extract(oracle_ptr(lwe), oracle_ptr(exp), 0, N)
+            np.testing.assert_array_equal(ext[b], lwe)
+    graph.close()
+
+
+def test_graph_refuses_extract_without_coefficients(native, oracle, golden, cuda):
+    from fhetoothpaste_b200 import TpError
+    torch = cuda
+    case, rot = rotator(oracle, golden, "small_binary_n256")
+    N, n = case["N"], case["n"]
+    buf = torch.zeros(4 * (2 * N + n + 1), dtype=torch.int64, device="cuda")
+    with pytest.raises(TpError):
+        rot.capture_batch(buf.data_ptr(), buf.data_ptr(), n + 1, buf.data_ptr(), 2 * N, 1, out_coef=False,
+                          extract_ptr=buf.data_ptr())
+
+
+def oracle_ptr(a):
+    from oracle.oracle import ptr
+    return ptr(a)
