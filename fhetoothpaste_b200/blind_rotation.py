@@ -101,6 +101,20 @@ class GpuBlindRotator:
     def check(self, stream: int | None = None) -> None:
         nat.check(nat.lib().tp_br_check(self._h, stream))
 
+    @property
+    def tile(self) -> int:
+        """Coefficients per thread of the rotation kernel (8 or 4)."""
+        return int(nat.lib().tp_br_get_tile(self._h))
+
+    def set_tile(self, coef_per_thread: int) -> None:
+        nat.check(nat.lib().tp_br_set_tile(self._h, coef_per_thread))
+
+    def autotune(self, batch: int) -> tuple[int, float]:
+        """Times every tile on `batch` synthetic rotations and keeps the fastest."""
+        coef, rate = ctypes.c_uint32(), ctypes.c_double()
+        nat.check(nat.lib().tp_br_autotune(self._h, batch, ctypes.byref(coef), ctypes.byref(rate)))
+        return int(coef.value), float(rate.value)
+
     def capture_batch(self, results_ptr: int, lwes_ptr: int, lwe_stride: int, accs_ptr: int, acc_stride: int,
                       batch: int, out_coef: bool = False, extract_ptr: int | None = None) -> "BatchGraph":
         """Records one batch launch (plus SampleExtract into extract_ptr) as a CUDA graph."""

@@ -1,7 +1,8 @@
 // Batched blind rotation (CGGI binary / CGGI ternary / BMMP) for sm_100a.
 //
-// One thread block rotates one ciphertext at a time with T = N/8 threads and
-// loops over the batch (persistent grid, a few blocks per SM). The RLWE
+// One thread block rotates one ciphertext at a time with T = N/E threads (E =
+// 2^LOGE coefficients per thread, 8 or 4) and loops over the batch
+// (persistent grid, a few blocks per SM). The RLWE
 // accumulator [A | B] lives in shared memory, in the NTT domain, for all n
 // CMux iterations. Per iteration the block runs the reference's CMux with the
 // same residues (cggi_blind_rotation.cpp:313-472, bmmp_blind_rotation.cpp:354-419,
@@ -16,9 +17,9 @@
 // Key layout on the device (built by key_relayout_kernel from the reference's
 // m_brk): per iteration group `it` (an LWE index for CGGI, a pair for BMMP),
 // per gadget row r (0..2l-1; rows < l multiply digits of A, rows >= l digits
-// of B), the C = 2*G components (G RGSWs x {A, B} halves) of slot k = 8t + 2jp
-// + e sit at  ((c*4 + jp)*T + t)*2 + e,  so each thread's 16-byte loads are
-// contiguous across the warp.
+// of B), the C = 2*G components (G RGSWs x {A, B} halves) of slot k = E*t +
+// 2jp + e sit at  ((c*E/2 + jp)*T + t)*2 + e,  so each thread's 16-byte loads
+// are contiguous across the warp.
 #pragma once
 
 #include "gl_arith.cuh"
@@ -85,21 +86,33 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
     return __ldg(psi_pow + ((ek * a) & (2u * (1u << LOGN) - 1u)));
 }
 
-// Resident blocks per SM the kernel is compiled for (register budget
-// 65536 / (T * blocks)). From N = 2048 up one block per SM with the full
-// register file measured faster than two blocks that spill (ternary N = 2048:
-// 6.0k vs 5.3k rotations/s), and the wide transforms' shared memory leaves
-// room for one block there anyway.
-__host__ __device__ constexpr int br_min_blocks(int logn, int variant) {
-    return (logn >= 11 || variant == kBmmpBinary) ? 1 : 2;
+// Coefficients per thread (log2) a context starts with; tp_br_set_tile and
+// tp_br_autotune change it. 4 per thread measured faster than 8 for every
+// variant and ring size (rotations/s, full waves: ternary N = 2048 6361 vs
+// 6039, BMMP N = 2048 5317 vs 3893, ternary N = 1024 16437 vs 13729, ternary
+// N = 4096 1941 vs 1644): twice the warps per SM hide the integer pipes'
+// dependency latency that 8 per thread left exposed.
+__host__ __device__ constexpr int br_default_loge(int logn, int variant) {
+    return (void)logn, (void)variant, 2;
 }
 
-template <int LOGN, int VARIANT>
-__global__ void __launch_bounds__((1 << LOGN) / 8, br_min_blocks(LOGN, VARIANT))
+// Resident blocks per SM the kernel is compiled for (register budget
+// 65536 / (T * blocks)). With 8 coefficients per thread, from N = 2048 up one
+// block per SM with the full register file measured faster than two blocks
+// that spill (ternary N = 2048: 6.0k vs 5.3k rotations/s). With 4 per thread
+// the budget is 128 registers (two blocks of N/4 threads up to N = 1024, one
+// block of 512 threads at N = 2048).
+__host__ __device__ constexpr int br_min_blocks(int logn, int variant, int loge) {
+    return loge == 2 ? (logn <= 10 ? 2 : 1) : ((logn >= 11 || variant == kBmmpBinary) ? 1 : 2);
+}
+
+template <int LOGN, int VARIANT, int LOGE>
+__global__ void __launch_bounds__((1 << LOGN) >> LOGE, br_min_blocks(LOGN, VARIANT, LOGE))
 br_kernel(const BrKernelParams prm) {
-    using SH = NttShape<LOGN>;
+    using SH = NttShape<LOGN, LOGE>;
     constexpr int N = SH::N;
     constexpr int T = SH::T;
+    constexpr int E = SH::E;
     constexpr int G = br_rgsw_per_group(VARIANT);
     constexpr int C = 2 * G;                 // key components per slot
     constexpr int K = br_ntt_width(LOGN, VARIANT);  // polynomials per transform
@@ -122,7 +135,7 @@ br_kernel(const BrKernelParams prm) {
     }
     uint64_t* xbuf0 = base;
     uint64_t* xbuf1 = base + K * N;
-    uint64_t* acc = base + 2 * K * N;        // [(h*8 + j)*T + t], canonical, NTT domain
+    uint64_t* acc = base + 2 * K * N;        // [(h*E + j)*T + t], canonical, NTT domain
     uint64_t* lwe_s = acc + 2 * N;
 
     const int t = threadIdx.x;
@@ -154,18 +167,18 @@ br_kernel(const BrKernelParams prm) {
             const uint32_t bb = (uint32_t)lwe_s[n];
 #pragma unroll 1
             for (int h0 = 0; h0 < 2; h0 += K) {
-                uint64_t x[K][8];
+                uint64_t x[K][E];
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
-                ntt_forward_k<LOGN, K>(x, t, xb(), tw_f);
+                    for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
+                ntt_forward_k<LOGN, K, LOGE>(x, t, xb(), tw_f);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        acc[((h0 + p) * 8 + j) * T + t] =
-                            gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j), bb));
+                    for (int j = 0; j < E; ++j)
+                        acc[((h0 + p) * E + j) * T + t] =
+                            gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j), bb));
             }
         }
 
@@ -183,34 +196,34 @@ br_kernel(const BrKernelParams prm) {
             const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
 
             // MAC accumulators (lazy residues, any 64-bit value)
-            uint64_t o[C][8];
+            uint64_t o[C][E];
 #pragma unroll
             for (int c = 0; c < C; ++c)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) o[c][j] = 0;
+                for (int j = 0; j < E; ++j) o[c][j] = 0;
 
             // Backward NTT of an accumulator half into corrected coefficients. Binary
             // CGGI decomposes (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the other
             // variants decompose acc itself (mux_operator.cpp:174-177, 219-224).
-            uint64_t cx[2][8];
-            auto load_half = [&](uint64_t (&dst)[8], int h) {
+            uint64_t cx[2][E];
+            auto load_half = [&](uint64_t (&dst)[E], int h) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    dst[j] = acc[(h * 8 + j) * T + t];
+                for (int j = 0; j < E; ++j) {
+                    dst[j] = acc[(h * E + j) * T + t];
                     if constexpr (VARIANT == kCggiBinary)
-                        dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(8 * t + j),
+                        dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j),
                                                                   2u * N - a0), 1));
                 }
             };
             // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
-            auto finish_half = [&](uint64_t (&v)[8]) {
+            auto finish_half = [&](uint64_t (&v)[E]) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) v[j] = gl_canon(gl_fma_lazy(prm.corr, v[j], prm.n_inv));
+                for (int j = 0; j < E; ++j) v[j] = gl_canon(gl_fma_lazy(prm.corr, v[j], prm.n_inv));
             };
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
                 load_half(cx[1], 1);
-                ntt_backward_unscaled_k<LOGN, 2>(cx, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGN, 2, LOGE>(cx, t, xb(), tw_i);
                 finish_half(cx[0]);
                 finish_half(cx[1]);
             }
@@ -218,13 +231,13 @@ br_kernel(const BrKernelParams prm) {
             for (uint32_t r = 0; r < 2 * L; r += K) {
                 if constexpr (K == 1) {
                     if (r == 0 || r == L) {
-                        uint64_t (&c1)[1][8] = reinterpret_cast<uint64_t(&)[1][8]>(cx[0]);
+                        uint64_t (&c1)[1][E] = reinterpret_cast<uint64_t(&)[1][E]>(cx[0]);
                         load_half(cx[0], r == 0 ? 0 : 1);
-                        ntt_backward_unscaled_k<LOGN, 1>(c1, t, xb(), tw_i);
+                        ntt_backward_unscaled_k<LOGN, 1, LOGE>(c1, t, xb(), tw_i);
                         finish_half(cx[0]);
                     }
                 }
-                uint64_t x[K][8];
+                uint64_t x[K][E];
 #pragma unroll
                 for (int p = 0; p < K; ++p) {
                     const uint32_t rr = r + p;
@@ -234,22 +247,22 @@ br_kernel(const BrKernelParams prm) {
                     const uint64_t mk = prm.dmask[d];
                     const uint64_t dl = prm.ddelta[d];
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
+                    for (int j = 0; j < E; ++j) {
                         const uint64_t c = hb ? cx[K - 1][j] : cx[0][j];
                         const uint64_t raw = (c >> sh) & mk;
                         x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
                     }
                 }
-                ntt_forward_k<LOGN, K>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, K, LOGE>(x, t, xb(), tw_f);
 #pragma unroll
                 for (int p = 0; p < K; ++p) {
                     const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
 #pragma unroll
-                        for (int jp = 0; jp < 4; ++jp) {
+                        for (int jp = 0; jp < E / 2; ++jp) {
                             const ulonglong2 kv =
-                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
+                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
                             o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[p][2 * jp], kv.x);
                             o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
                         }
@@ -259,10 +272,10 @@ br_kernel(const BrKernelParams prm) {
 
             // Accumulator update.
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t ek = slot_exponent<LOGN>(8 * t + j);
+            for (int j = 0; j < E; ++j) {
+                const uint32_t ek = slot_exponent<LOGN>(E * t + j);
                 uint64_t ua = acc[j * T + t];
-                uint64_t ub = acc[(8 + j) * T + t];
+                uint64_t ub = acc[(E + j) * T + t];
                 if constexpr (VARIANT == kCggiBinary) {
                     // acc += ExtProd (mux_operator.cpp:151)
                     ua = gl_add(ua, gl_canon(o[0][j]));
@@ -286,7 +299,7 @@ br_kernel(const BrKernelParams prm) {
                     ub = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2));
                 }
                 acc[j * T + t] = ua;
-                acc[(8 + j) * T + t] = ub;
+                acc[(E + j) * T + t] = ub;
             }
         }
 
@@ -294,23 +307,23 @@ br_kernel(const BrKernelParams prm) {
         uint64_t* res = prm.out + b * (2ull * N);
 #pragma unroll 1
         for (int h0 = 0; h0 < 2; h0 += K) {
-            uint64_t x[K][8];
+            uint64_t x[K][E];
 #pragma unroll
             for (int p = 0; p < K; ++p)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) x[p][j] = acc[((h0 + p) * 8 + j) * T + t];
+                for (int j = 0; j < E; ++j) x[p][j] = acc[((h0 + p) * E + j) * T + t];
             if (prm.out_coef) {
-                ntt_backward_unscaled_k<LOGN, K>(x, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGN, K, LOGE>(x, t, xb(), tw_i);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) res[(h0 + p) * N + t + j * T] = gl_mul(x[p][j], prm.n_inv);
+                    for (int j = 0; j < E; ++j) res[(h0 + p) * N + t + j * T] = gl_mul(x[p][j], prm.n_inv);
             } else {
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                        *reinterpret_cast<ulonglong2*>(res + (h0 + p) * N + 8 * t + 2 * c) =
+                    for (int c = 0; c < E / 2; ++c)
+                        *reinterpret_cast<ulonglong2*>(res + (h0 + p) * N + E * t + 2 * c) =
                             make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
             }
         }

@@ -181,9 +181,10 @@ struct tp_br_ctx {
     bool key_ready = false;
     unsigned int* err = nullptr;  // device error word
     tp::BrKernelParams kp{};
-    const void* kernel = nullptr;
+    int loge = 3;                 // log2 coefficients per thread of the active tile
+    const void* kernels[4] = {};  // by loge (2, 3)
+    int grid_caps[4] = {};        // resident blocks on the device, by loge
     size_t smem_bytes = 0;
-    int grid_cap = 1;             // resident blocks on the device
     // workspace for host-pointer calls
     uint64_t* ws = nullptr;
     uint64_t ws_words = 0;
@@ -282,20 +283,24 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         }
     }
 
-    c->kernel = tp::br_kernel_lookup(c->logn, p->variant);
     c->smem_bytes = tp::br_smem_words(c->logn, p->variant, p->lwe_dim) * 8;
-    e = cudaFuncSetAttribute((const void*)c->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes);
-    int per_sm = 0;
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)c->kernel, (int)(N / 8), c->smem_bytes);
-    if (e != cudaSuccess || per_sm < 1) {
-        cudaFree(c->err);
-        delete c;
-        return fail(TP_ERR_PARAM, "blind-rotation kernel does not fit (N=%llu, n=%u, smem=%zu): %s",
-                    (unsigned long long)N, p->lwe_dim, (size_t)c->smem_bytes,
-                    e == cudaSuccess ? "no resident block" : cudaGetErrorString(e));
+    for (int lg = 2; lg <= 3; ++lg) {
+        const void* k = tp::br_kernel_lookup(c->logn, p->variant, lg);
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes);
+        int per_sm = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(N >> lg), c->smem_bytes);
+        if (e != cudaSuccess || per_sm < 1) {
+            cudaFree(c->err);
+            delete c;
+            return fail(TP_ERR_PARAM, "blind-rotation kernel does not fit (N=%llu, n=%u, smem=%zu, %d per thread): %s",
+                        (unsigned long long)N, p->lwe_dim, (size_t)c->smem_bytes, 1 << lg,
+                        e == cudaSuccess ? "no resident block" : cudaGetErrorString(e));
+        }
+        c->kernels[lg] = k;
+        c->grid_caps[lg] = per_sm * sm_count(device);
     }
-    c->grid_cap = per_sm * sm_count(device);
+    c->loge = tp::br_default_loge(c->logn, p->variant);
     *out = c;
     return TP_OK;
 }
@@ -337,7 +342,7 @@ tp_status tp_br_upload_key(tp_br_ctx* c, const uint64_t* brk, uint64_t words) {
             const int threads = 256;
             const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
             tp::key_relayout_kernel<<<(unsigned)blocks, threads>>>(c->key + g0 * per_group, stage, ng, c->G,
-                                                                    2 * c->prm.digits, c->logn);
+                                                                    2 * c->prm.digits, c->logn, c->loge);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -369,10 +374,115 @@ tp_status tp_br_blind_rotate_batch(tp_br_ctx* c, uint64_t batch, uint64_t* resul
     kp.out = results;
     kp.batch = batch;
     kp.out_coef = out_coef ? 1u : 0u;
-    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_cap);
+    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
     void* args[] = {&kp};
-    TP_CUDA(cudaLaunchKernel(c->kernel, dim3(grid), dim3(c->prm.ring_dim / 8), args, c->smem_bytes,
+    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args, c->smem_bytes,
                              (cudaStream_t)stream));
+    return TP_OK;
+}
+
+// Moves the resident key to the layout of another tile (2x key memory while it runs).
+static tp_status br_retile(tp_br_ctx* c, int loge) {
+    if (loge == c->loge) return TP_OK;
+    if (c->key_ready) {
+        uint64_t* nk = nullptr;
+        TP_CUDA(cudaMalloc(&nk, c->key_words * 8));
+        const uint64_t blocks = std::min<uint64_t>((c->key_words + 255) / 256, 65535);
+        tp::key_retile_kernel<<<(unsigned)blocks, 256>>>(nk, c->key, c->groups, c->G, 2 * c->prm.digits, c->logn,
+                                                          c->loge, loge);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            cudaFree(nk);
+            return fail(TP_ERR_CUDA, "key re-tiling: %s", cudaGetErrorString(e));
+        }
+        cudaFree(c->key);
+        c->key = nk;
+    }
+    c->loge = loge;
+    return TP_OK;
+}
+
+tp_status tp_br_set_tile(tp_br_ctx* c, uint32_t coef_per_thread) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (coef_per_thread != 4 && coef_per_thread != 8) return fail(TP_ERR_PARAM, "coefficients per thread must be 4 or 8");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    return br_retile(c, coef_per_thread == 4 ? 2 : 3);
+}
+
+uint32_t tp_br_get_tile(const tp_br_ctx* c) { return c ? 1u << c->loge : 0u; }
+
+tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_thread, double* best_rotations_per_s) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return fail(TP_ERR_PARAM, "empty batch");
+    const uint64_t N = c->prm.ring_dim, n = c->prm.lwe_dim;
+    const uint64_t cap = (uint64_t)std::max(c->grid_caps[2], c->grid_caps[3]);
+    const uint64_t tb = std::min<uint64_t>(batch, 2 * cap);  // at most two waves per trial
+    std::vector<uint64_t> lw(tb * (n + 1));
+    uint64_t z = 0x5eedull;
+    for (auto& w : lw) {  // splitmix64 words in [0, 2N): timing does not depend on the values
+        uint64_t x = (z += 0x9E3779B97F4A7C15ull);
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        w = (x ^ (x >> 31)) & (2 * N - 1);
+    }
+    TP_CUDA(cudaSetDevice(c->device));
+    uint64_t *d_lwe = nullptr, *d_acc = nullptr, *d_res = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    tp_status s = TP_OK;
+    double best_rate = 0.0;
+    int best = c->loge;
+    auto cleanup = [&]() {
+        cudaFree(d_lwe);
+        cudaFree(d_acc);
+        cudaFree(d_res);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+    };
+    cudaError_t e = cudaMalloc(&d_lwe, lw.size() * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&d_acc, 2 * N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&d_res, tb * 2 * N * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(d_lwe, lw.data(), lw.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_acc, 0, 2 * N * 8);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cleanup();
+        return fail(TP_ERR_CUDA, "autotune set-up: %s", cudaGetErrorString(e));
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    for (int lg : {3, 2}) {
+        s = br_retile(c, lg);
+        if (s != TP_OK) break;
+        for (int rep = 0; rep < 3 && s == TP_OK; ++rep) {  // one warm-up, two timed
+            if (rep == 1) cudaEventRecord(e0, st);
+            s = tp_br_blind_rotate_batch(c, tb, d_res, d_lwe, n + 1, d_acc, 0, 0, st);
+        }
+        if (s != TP_OK) break;
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+            s = fail(TP_ERR_CUDA, "autotune timing: %s", cudaGetErrorString(e));
+            break;
+        }
+        const double rate = 2.0 * tb / (ms * 1e-3);
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = lg;
+        }
+    }
+    if (s == TP_OK) s = br_retile(c, best);
+    cleanup();
+    if (s != TP_OK) return s;
+    if (best_coef_per_thread) *best_coef_per_thread = 1u << best;
+    if (best_rotations_per_s) *best_rotations_per_s = best_rate;
     return TP_OK;
 }
 
@@ -667,7 +777,7 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
         // each key: l rows of [A | B] (the reference's m_ksk) -> [row][c][jp][t][2]
         const uint64_t total = c->key_words;
         const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 65535);
-        tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn);
+        tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn, 3);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();

@@ -3,17 +3,17 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_7(int variant);
+const void* br_kernel_ptr_7(int variant, int loge);
 const void* ntt_kernel_ptr_7(bool forward);
-const void* br_kernel_ptr_8(int variant);
+const void* br_kernel_ptr_8(int variant, int loge);
 const void* ntt_kernel_ptr_8(bool forward);
-const void* br_kernel_ptr_9(int variant);
+const void* br_kernel_ptr_9(int variant, int loge);
 const void* ntt_kernel_ptr_9(bool forward);
-const void* br_kernel_ptr_10(int variant);
+const void* br_kernel_ptr_10(int variant, int loge);
 const void* ntt_kernel_ptr_10(bool forward);
-const void* br_kernel_ptr_11(int variant);
+const void* br_kernel_ptr_11(int variant, int loge);
 const void* ntt_kernel_ptr_11(bool forward);
-const void* br_kernel_ptr_12(int variant);
+const void* br_kernel_ptr_12(int variant, int loge);
 const void* ntt_kernel_ptr_12(bool forward);
 const void* ks_kernel_ptr_7(int mode);
 const void* ks_kernel_ptr_8(int mode);
@@ -22,14 +22,14 @@ const void* ks_kernel_ptr_10(int mode);
 const void* ks_kernel_ptr_11(int mode);
 const void* ks_kernel_ptr_12(int mode);
 
-inline const void* br_kernel_lookup(int logn, int variant) {
+inline const void* br_kernel_lookup(int logn, int variant, int loge) {
     switch (logn) {
-        case 7: return br_kernel_ptr_7(variant);
-        case 8: return br_kernel_ptr_8(variant);
-        case 9: return br_kernel_ptr_9(variant);
-        case 10: return br_kernel_ptr_10(variant);
-        case 11: return br_kernel_ptr_11(variant);
-        case 12: return br_kernel_ptr_12(variant);
+        case 7: return br_kernel_ptr_7(variant, loge);
+        case 8: return br_kernel_ptr_8(variant, loge);
+        case 9: return br_kernel_ptr_9(variant, loge);
+        case 10: return br_kernel_ptr_10(variant, loge);
+        case 11: return br_kernel_ptr_11(variant, loge);
+        case 12: return br_kernel_ptr_12(variant, loge);
         default: return nullptr;
     }
 }

@@ -7,11 +7,18 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_7(int variant) {
+const void* br_kernel_ptr_7(int variant, int loge) {
+    if (loge == 2) {
+        switch (variant) {
+            case kCggiBinary: return (const void*)br_kernel<7, kCggiBinary, 2>;
+            case kCggiTernary: return (const void*)br_kernel<7, kCggiTernary, 2>;
+            default: return (const void*)br_kernel<7, kBmmpBinary, 2>;
+        }
+    }
     switch (variant) {
-        case kCggiBinary: return (const void*)br_kernel<7, kCggiBinary>;
-        case kCggiTernary: return (const void*)br_kernel<7, kCggiTernary>;
-        default: return (const void*)br_kernel<7, kBmmpBinary>;
+        case kCggiBinary: return (const void*)br_kernel<7, kCggiBinary, 3>;
+        case kCggiTernary: return (const void*)br_kernel<7, kCggiTernary, 3>;
+        default: return (const void*)br_kernel<7, kBmmpBinary, 3>;
     }
 }
 

@@ -7,11 +7,18 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_11(int variant) {
+const void* br_kernel_ptr_11(int variant, int loge) {
+    if (loge == 2) {
+        switch (variant) {
+            case kCggiBinary: return (const void*)br_kernel<11, kCggiBinary, 2>;
+            case kCggiTernary: return (const void*)br_kernel<11, kCggiTernary, 2>;
+            default: return (const void*)br_kernel<11, kBmmpBinary, 2>;
+        }
+    }
     switch (variant) {
-        case kCggiBinary: return (const void*)br_kernel<11, kCggiBinary>;
-        case kCggiTernary: return (const void*)br_kernel<11, kCggiTernary>;
-        default: return (const void*)br_kernel<11, kBmmpBinary>;
+        case kCggiBinary: return (const void*)br_kernel<11, kCggiBinary, 3>;
+        case kCggiTernary: return (const void*)br_kernel<11, kCggiTernary, 3>;
+        default: return (const void*)br_kernel<11, kBmmpBinary, 3>;
     }
 }
 

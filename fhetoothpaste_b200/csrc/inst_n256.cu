@@ -7,11 +7,18 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_8(int variant) {
+const void* br_kernel_ptr_8(int variant, int loge) {
+    if (loge == 2) {
+        switch (variant) {
+            case kCggiBinary: return (const void*)br_kernel<8, kCggiBinary, 2>;
+            case kCggiTernary: return (const void*)br_kernel<8, kCggiTernary, 2>;
+            default: return (const void*)br_kernel<8, kBmmpBinary, 2>;
+        }
+    }
     switch (variant) {
-        case kCggiBinary: return (const void*)br_kernel<8, kCggiBinary>;
-        case kCggiTernary: return (const void*)br_kernel<8, kCggiTernary>;
-        default: return (const void*)br_kernel<8, kBmmpBinary>;
+        case kCggiBinary: return (const void*)br_kernel<8, kCggiBinary, 3>;
+        case kCggiTernary: return (const void*)br_kernel<8, kCggiTernary, 3>;
+        default: return (const void*)br_kernel<8, kBmmpBinary, 3>;
     }
 }
 

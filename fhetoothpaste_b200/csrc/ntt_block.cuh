@@ -1,5 +1,5 @@
 // Thread-block negacyclic NTT over Goldilocks for one polynomial of N = 2^LOGN
-// coefficients held 8 per thread by T = N/8 threads.
+// coefficients held E = 2^LOGE per thread (E = 8 or 4) by T = N/E threads.
 //
 // The transform is the reference's (lib/src/backend/solinas.cpp:228-313):
 // forward = Cooley-Tukey, natural-order coefficients in, evaluations out in
@@ -9,57 +9,68 @@
 // exact residue, any evaluation order of the same butterflies gives the same
 // words as the reference.
 //
-// Levels are processed in passes of up to three (radix-8 groups in registers).
+// Levels are processed in passes of up to LOGE (radix-E groups in registers).
 // Between passes the data goes through a shared-memory exchange buffer of N
-// words. Passes whose blocks span at most 256 coefficients touch only their
-// own warp's 256-word region, so those exchanges need only __syncwarp; the
+// words. Passes whose blocks span at most 32*E coefficients touch only their
+// own warp's 32*E-word region, so those exchanges need only __syncwarp; the
 // others use __syncthreads.
 //
 // Register layouts ("where thread t holds what"):
 //   coefficient layout: x[j] = coefficient t + j*T            (pass 0 groups)
-//   slot layout:        x[j] = slot 8t + j                     (last pass groups)
+//   slot layout:        x[j] = slot E*t + j                    (last pass groups)
 // forward: coefficient layout -> slot layout; backward: slot -> coefficient.
 //
 // Exchange-buffer hazards: a transform's first shared-memory write may race
 // with another warp still reading the previous transform's last exchange, so
-// callers alternate between two buffers; every transform of N >= 512 contains
-// a block-wide barrier, which orders transform k's reads before transform
-// k+2's writes to the same buffer.
+// callers alternate between two buffers; every transform run by more than one
+// warp contains a block-wide barrier (its first exchange spans the whole
+// polynomial), which orders transform k's reads before transform k+2's writes
+// to the same buffer.
 #pragma once
 
 #include "gl_arith.cuh"
 
 namespace tp {
 
-template <int LOGN>
+template <int LOGN, int LOGE = 3>
 struct NttShape {
     static constexpr int N = 1 << LOGN;
-    static constexpr int T = N / 8;
-    static constexpr int NPASS = (LOGN + 2) / 3;
-    __host__ __device__ static constexpr int L0(int p) { return 3 * p; }
-    __host__ __device__ static constexpr int S(int p) { return 3 * p + 3 <= LOGN ? 3 : LOGN - 3 * p; }
-    // A pass whose level-L0 blocks have at most 256 coefficients stays inside
-    // the 256-word region of its warp.
-    __host__ __device__ static constexpr bool WarpLocal(int p) { return LOGN - L0(p) <= 8; }
+    static constexpr int E = 1 << LOGE;       // coefficients per thread
+    static constexpr int T = N / E;
+    static constexpr int NPASS = (LOGN + LOGE - 1) / LOGE;
+    __host__ __device__ static constexpr int L0(int p) { return LOGE * p; }
+    __host__ __device__ static constexpr int S(int p) { return LOGE * p + LOGE <= LOGN ? LOGE : LOGN - LOGE * p; }
+    // A pass whose level-L0 blocks have at most 32*E coefficients stays inside
+    // the 32*E-word region of its warp.
+    __host__ __device__ static constexpr bool WarpLocal(int p) { return LOGN - L0(p) <= 5 + LOGE; }
     static constexpr bool SingleWarp = (T <= 32);
 };
 
-// Swizzled position of coefficient/slot `idx` in an exchange buffer: 16-byte
-// chunk c = idx/2 is stored at chunk c ^ ((c >> 3) & 7). Keeps every pass's
-// 8-byte accesses (per half-warp) and 16-byte accesses (per quarter-warp)
-// free of bank conflicts.
+// Swizzled position of coefficient/slot `idx` in an exchange buffer.
+//  E = 8: 16-byte chunk c = idx/2 is stored at chunk c ^ ((c >> 3) & 7); keeps
+//         every pass's 8-byte accesses (per half-warp) and the last pass's
+//         16-byte accesses (per quarter-warp) free of bank conflicts.
+//  E = 4: word idx is stored at idx ^ (5 * ((idx >> 4) & 3)) inside its 16-word
+//         row. A half-warp's 8-byte accesses then hit 16 distinct bank pairs
+//         for every pass shape (runs of 1, 2, 4, 8 or >= 16 consecutive words
+//         at a stride of 4x the run); the last pass uses 8-byte accesses too.
+template <int LOGE>
 __device__ __forceinline__ int xpos(int idx) {
-    const int c = idx >> 1;
-    return ((c ^ ((c >> 3) & 7)) << 1) | (idx & 1);
+    if constexpr (LOGE == 3) {
+        const int c = idx >> 1;
+        return ((c ^ ((c >> 3) & 7)) << 1) | (idx & 1);
+    } else {
+        return idx ^ (5 * ((idx >> 4) & 3));
+    }
 }
 
-// Index of the e-th register (0..7) of thread t in pass P.
-template <int LOGN, int P>
+// Index of the e-th register (0..E-1) of thread t in pass P.
+template <int LOGN, int LOGE, int P>
 __device__ __forceinline__ int pass_index(int t, int e) {
-    using SH = NttShape<LOGN>;
+    using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
     constexpr int G = 1 << S;
-    constexpr int PER = 8 / G;
+    constexpr int PER = SH::E / G;
     constexpr int TMIN = SH::N >> (SH::L0(P) + S);
     const int q = e / G, j = e % G;
     const int g = PER * t + q;
@@ -67,9 +78,9 @@ __device__ __forceinline__ int pass_index(int t, int e) {
     return blk * G * TMIN + off + j * TMIN;
 }
 
-template <int LOGN>
+template <int LOGN, int LOGE>
 __device__ __forceinline__ void ntt_sync(bool block_wide) {
-    using SH = NttShape<LOGN>;
+    using SH = NttShape<LOGN, LOGE>;
     if (SH::T < 32 || block_wide) __syncthreads();
     else __syncwarp();
 }
@@ -79,12 +90,12 @@ __device__ __forceinline__ void ntt_sync(bool block_wide) {
 // and every synchronisation, and their independent butterflies interleave.
 
 // Forward butterflies of pass P on the thread's registers.
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][8], int t, const uint64_t* __restrict__ tw) {
-    using SH = NttShape<LOGN>;
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
     constexpr int G = 1 << S;
-    constexpr int PER = 8 / G;
+    constexpr int PER = SH::E / G;
     constexpr int TMIN = SH::N >> (SH::L0(P) + S);
     constexpr int L0 = SH::L0(P);
 #pragma unroll
@@ -110,12 +121,12 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][8], int t, const 
 }
 
 // Inverse butterflies of pass P (levels in reverse order).
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][8], int t, const uint64_t* __restrict__ tw) {
-    using SH = NttShape<LOGN>;
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
     constexpr int G = 1 << S;
-    constexpr int PER = 8 / G;
+    constexpr int PER = SH::E / G;
     constexpr int TMIN = SH::N >> (SH::L0(P) + S);
     constexpr int L0 = SH::L0(P);
 #pragma unroll
@@ -140,94 +151,97 @@ __device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][8], int t, const 
     }
 }
 
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void xstore(uint64_t* buf, const uint64_t (&x)[K][8], int t) {
-    using SH = NttShape<LOGN>;
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void xstore(uint64_t* buf, const uint64_t (&x)[K][1 << LOGE], int t) {
+    using SH = NttShape<LOGN, LOGE>;
 #pragma unroll
     for (int p = 0; p < K; ++p) {
         uint64_t* b = buf + p * SH::N;
-        if constexpr (P == SH::NPASS - 1) {
+        if constexpr (P == SH::NPASS - 1 && LOGE == 3) {
             // slot layout: 8 contiguous words, written as four 16-byte chunks
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int idx = 8 * t + 2 * c;
-                *reinterpret_cast<ulonglong2*>(b + xpos(idx)) = make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
+                *reinterpret_cast<ulonglong2*>(b + xpos<LOGE>(idx)) = make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
             }
         } else {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) b[xpos(pass_index<LOGN, P>(t, e))] = x[p][e];
+            for (int e = 0; e < SH::E; ++e) b[xpos<LOGE>(pass_index<LOGN, LOGE, P>(t, e))] = x[p][e];
         }
     }
 }
 
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][8], int t) {
-    using SH = NttShape<LOGN>;
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][1 << LOGE], int t) {
+    using SH = NttShape<LOGN, LOGE>;
 #pragma unroll
     for (int p = 0; p < K; ++p) {
         const uint64_t* b = buf + p * SH::N;
-        if constexpr (P == SH::NPASS - 1) {
+        if constexpr (P == SH::NPASS - 1 && LOGE == 3) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int idx = 8 * t + 2 * c;
-                const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(b + xpos(idx));
+                const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(b + xpos<LOGE>(idx));
                 x[p][2 * c] = v.x;
                 x[p][2 * c + 1] = v.y;
             }
         } else {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) x[p][e] = b[xpos(pass_index<LOGN, P>(t, e))];
+            for (int e = 0; e < SH::E; ++e) x[p][e] = b[xpos<LOGE>(pass_index<LOGN, LOGE, P>(t, e))];
         }
     }
 }
 
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw) {
-    using SH = NttShape<LOGN>;
-    fwd_pass_math<LOGN, P, K>(x, t, tw);
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
+                                                const uint64_t* tw) {
+    using SH = NttShape<LOGN, LOGE>;
+    fwd_pass_math<LOGN, P, K, LOGE>(x, t, tw);
     if constexpr (P + 1 < SH::NPASS) {
-        xstore<LOGN, P, K>(buf, x, t);
-        ntt_sync<LOGN>(!SH::WarpLocal(P));
-        xload<LOGN, P + 1, K>(buf, x, t);
-        fwd_passes_from<LOGN, P + 1, K>(x, t, buf, tw);
+        xstore<LOGN, P, K, LOGE>(buf, x, t);
+        ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P));
+        xload<LOGN, P + 1, K, LOGE>(buf, x, t);
+        fwd_passes_from<LOGN, P + 1, K, LOGE>(x, t, buf, tw);
     }
 }
 
-template <int LOGN, int P, int K>
-__device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw) {
-    using SH = NttShape<LOGN>;
-    inv_pass_math<LOGN, P, K>(x, t, tw);
+template <int LOGN, int P, int K, int LOGE>
+__device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
+                                                const uint64_t* tw) {
+    using SH = NttShape<LOGN, LOGE>;
+    inv_pass_math<LOGN, P, K, LOGE>(x, t, tw);
     if constexpr (P > 0) {
-        xstore<LOGN, P, K>(buf, x, t);
-        ntt_sync<LOGN>(!SH::WarpLocal(P - 1));
-        xload<LOGN, P - 1, K>(buf, x, t);
-        inv_passes_from<LOGN, P - 1, K>(x, t, buf, tw);
+        xstore<LOGN, P, K, LOGE>(buf, x, t);
+        ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P - 1));
+        xload<LOGN, P - 1, K, LOGE>(buf, x, t);
+        inv_passes_from<LOGN, P - 1, K, LOGE>(x, t, buf, tw);
     }
 }
 
 // Forward NTT of K polynomials: coefficient layout -> slot layout. buf holds K*N words.
-template <int LOGN, int K>
-__device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
-    fwd_passes_from<LOGN, 0, K>(x, t, buf, tw_fwd);
+template <int LOGN, int K, int LOGE = 3>
+__device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
+                                              const uint64_t* tw_fwd) {
+    fwd_passes_from<LOGN, 0, K, LOGE>(x, t, buf, tw_fwd);
 }
 
 // Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.
-template <int LOGN, int K>
-__device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][8], int t, uint64_t* buf,
+template <int LOGN, int K, int LOGE = 3>
+__device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                         const uint64_t* tw_inv) {
-    inv_passes_from<LOGN, NttShape<LOGN>::NPASS - 1, K>(x, t, buf, tw_inv);
+    inv_passes_from<LOGN, NttShape<LOGN, LOGE>::NPASS - 1, K, LOGE>(x, t, buf, tw_inv);
 }
 
-// One polynomial.
+// One polynomial, 8 coefficients per thread.
 template <int LOGN>
 __device__ __forceinline__ void ntt_forward(uint64_t (&x)[8], int t, uint64_t* buf, const uint64_t* tw_fwd) {
-    ntt_forward_k<LOGN, 1>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_fwd);
+    ntt_forward_k<LOGN, 1, 3>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_fwd);
 }
 
 template <int LOGN>
 __device__ __forceinline__ void ntt_backward_unscaled(uint64_t (&x)[8], int t, uint64_t* buf,
                                                       const uint64_t* tw_inv) {
-    ntt_backward_unscaled_k<LOGN, 1>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_inv);
+    ntt_backward_unscaled_k<LOGN, 1, 3>(reinterpret_cast<uint64_t(&)[1][8]>(x), t, buf, tw_inv);
 }
 
 }  // namespace tp

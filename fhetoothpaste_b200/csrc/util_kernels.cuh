@@ -6,30 +6,47 @@
 
 namespace tp {
 
-// Reference m_brk layout -> device layout, one word per thread.
-// Reference: word (it, g, r, h, k) at ((it*G + g)*2l + r)*2N + h*N + k
-// (MakeRGSW rows, base_crypto.cpp:90-95; per-iteration RGSW order,
-// cggi_blind_rotation.cpp:277,306-309 and bmmp_blind_rotation.cpp:241-258).
-__global__ void key_relayout_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
-                                    uint32_t G, uint32_t rows, uint32_t logn) {
+// Device position of key word (group it, gadget row r, component c = 2g + h,
+// slot k) for a rotation kernel with 2^loge coefficients per thread: slot
+// k = E*t + 2jp + e sits at ((c*E/2 + jp)*T + t)*2 + e inside the (it, r) row.
+__device__ __forceinline__ uint64_t key_device_pos(uint64_t it, uint64_t r, uint64_t c, uint64_t k, uint32_t G,
+                                                   uint32_t rows, uint32_t logn, uint32_t loge) {
     const uint64_t N = 1ull << logn;
-    const uint64_t T = N / 8;
-    const uint64_t per_group = (uint64_t)G * rows * 2 * N;
-    const uint64_t total = groups * per_group;
+    const uint64_t E = 1ull << loge;
+    const uint64_t T = N >> loge;
+    const uint64_t t = k >> loge, jp = (k & (E - 1)) >> 1, e = k & 1;
+    return (it * rows + r) * 2 * G * N + ((c * (E / 2) + jp) * T + t) * 2 + e;
+}
+
+// Reference m_brk layout ((it*G + g)*rows + r)*2N + h*N + k  ->  device layout.
+__global__ void key_relayout_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
+                                    uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge) {
+    const uint64_t N = 1ull << logn;
+    const uint64_t total = groups * G * rows * 2 * N;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t it = w / per_group;
-        uint64_t rem = w % per_group;
-        const uint64_t r = rem / (2 * G * N);
-        rem %= 2 * G * N;
-        // rem = ((c*4 + jp)*T + t)*2 + e
-        const uint64_t e = rem & 1;
-        const uint64_t tt = (rem >> 1) % T;
-        const uint64_t cj = (rem >> 1) / T;
-        const uint64_t jp = cj % 4, c = cj / 4;
-        const uint64_t g = c >> 1, h = c & 1;
-        const uint64_t k = 8 * tt + 2 * jp + e;
-        dst[w] = src[((it * G + g) * rows + r) * 2 * N + h * N + k];
+        const uint64_t k = w % N;
+        const uint64_t h = (w / N) & 1;
+        const uint64_t r = (w / (2 * N)) % rows;
+        const uint64_t ig = w / (2 * N * rows);
+        const uint64_t g = ig % G, it = ig / G;
+        dst[key_device_pos(it, r, 2 * g + h, k, G, rows, logn, loge)] = src[w];
+    }
+}
+
+// Device layout for one coefficients-per-thread count -> another (same key).
+__global__ void key_retile_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
+                                  uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge_src, uint32_t loge_dst) {
+    const uint64_t N = 1ull << logn;
+    const uint64_t total = groups * G * rows * 2 * N;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = w % N;
+        const uint64_t c = (w / N) % (2 * G);
+        const uint64_t r = (w / (2 * G * N)) % rows;
+        const uint64_t it = w / (2 * G * N * rows);
+        dst[key_device_pos(it, r, c, k, G, rows, logn, loge_dst)] =
+            src[key_device_pos(it, r, c, k, G, rows, logn, loge_src)];
     }
 }
 

@@ -99,6 +99,21 @@ tp_status tp_br_blind_rotate_batch_host(tp_br_ctx* ctx, uint64_t batch, uint64_t
                                         const uint64_t* lwes, uint64_t lwe_stride, const uint64_t* accs,
                                         uint64_t acc_stride, int out_coef, void* stream);
 
+/* Tile of the rotation kernel: coefficients per thread (8: N/8 threads per
+ * rotation with radix-8 NTT passes; 4: N/4 threads, radix-4 passes, fewer
+ * registers per thread so more warps per SM). Changing it after the key is
+ * uploaded re-lays the key out on the device (twice the key's memory while it
+ * runs). Not thread-safe against concurrent launches on the same context. No
+ * reference counterpart (tiling is a property of the GPU kernel). */
+tp_status tp_br_set_tile(tp_br_ctx* ctx, uint32_t coef_per_thread);
+uint32_t tp_br_get_tile(const tp_br_ctx* ctx);
+
+/* Times every tile on up to two waves of `batch` synthetic rotations with the
+ * uploaded key, keeps the fastest and reports it (either output may be NULL).
+ * Blocks until done; the context must be idle. */
+tp_status tp_br_autotune(tp_br_ctx* ctx, uint64_t batch, uint32_t* best_coef_per_thread,
+                         double* best_rotations_per_s);
+
 /* Waits for the context's work on `stream` and reports device-side input
  * errors seen since the last check (TP_ERR_PARAM for out-of-range LWE words). */
 tp_status tp_br_check(tp_br_ctx* ctx, void* stream);

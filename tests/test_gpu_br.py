@@ -162,3 +162,28 @@ def test_graph_refuses_extract_without_coefficients(native, oracle, golden, cuda
 def oracle_ptr(a):
     from oracle.oracle import ptr
     return ptr(a)
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_tile_of_four_matches_reference(native, oracle, golden, name):
+    """4 coefficients per thread (radix-4 passes), key re-tiled on the device after upload."""
+    case, rot = rotator(oracle, golden, name)
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for tile in (4, 8):
+        rot.set_tile(tile)
+        assert rot.tile == tile
+        for oc in (0, 1):
+            idx = [i for i, c in enumerate(coefs) if c == oc]
+            got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+            np.testing.assert_array_equal(got, expect[idx], err_msg=f"tile {tile}")
+
+
+def test_autotune_picks_a_tile_and_keeps_results(native, oracle, golden):
+    name = "small_bmmp_n512"
+    case, rot = rotator(oracle, golden, name)
+    coef, rate = rot.autotune(300)
+    assert coef in (4, 8) and rot.tile == coef and rate > 0
+    lwes, accs, coefs = case_inputs(name, case)
+    idx = [i for i, c in enumerate(coefs) if c == 0]
+    np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[idx], accs[idx]), golden[1][f"br_{name}"][idx])
