@@ -36,8 +36,8 @@ __host__ __device__ constexpr int br_rgsw_per_group(int variant) {
 
 struct BrKernelParams {
     const uint64_t* key;      // device layout, see above
-    const uint64_t* tw_fwd;   // N: psi^brv(k)
-    const uint64_t* tw_inv;   // N: psi^-brv(k)
+    const uint64_t* tw_fwd;   // psi^brv(k) (k < N), then tw[i] tw[2i] (i < N/2)
+    const uint64_t* tw_inv;   // psi^-brv(k), then the same products
     const uint64_t* psi_pow;  // 2N: psi^k
     const uint64_t* lwes;
     uint64_t lwe_stride;
@@ -67,12 +67,18 @@ __host__ __device__ constexpr int br_ntt_width(int logn, int variant) {
 // transforms leave no room for them (then they are read through L1).
 __host__ __device__ constexpr bool br_smem_twiddles(int logn) { return logn <= 11; }
 
-// Shared memory of one block, in words: twiddles (2N, if kept there), two
-// exchange areas of width*N words, the accumulator (2N), the LWE vector (n+1,
-// rounded up to an even count).
-__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n) {
-    return (size_t)(1 << logn) * ((br_smem_twiddles(logn) ? 2 : 0) + 2 * br_ntt_width(logn, variant) + 2) +
-           ((n + 2) & ~1u);
+// Twiddle words per direction: psi^(+-brv(k)) for k < N, plus for radix-4
+// passes the products tw[i] tw[2i] (i < N/2) at N + i.
+__host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
+    return loge == 2 ? (1 << logn) + (1 << (logn - 1)) : (1 << logn);
+}
+
+// Shared memory of one block, in words: twiddles (both directions, if kept
+// there), two exchange areas of width*N words, the accumulator (2N), the LWE
+// vector (n+1, rounded up to an even count).
+__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge) {
+    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
+           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) + ((n + 2) & ~1u);
 }
 
 // Exponent e_k = 2 brv(k) + 1 of slot k: NTT(X^a)[k] = psi^(e_k a mod 2N).
@@ -84,6 +90,14 @@ __device__ __forceinline__ uint32_t slot_exponent(int k) {
 template <int LOGN>
 __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, uint32_t ek, uint32_t a) {
     return __ldg(psi_pow + ((ek * a) & (2u * (1u << LOGN) - 1u)));
+}
+
+// Fused radix-4 NTT passes (three products and a shift per two levels, see
+// ntt_block.cuh) for 4 coefficients per thread. Measured against plain radix-2
+// butterflies, rotations/s: BMMP N = 2048 5570 vs 5438; CGGI ternary N = 2048
+// 6247 vs 6443, binary N = 1024 15675 vs 16249, ternary N = 1024 and 4096 equal.
+__host__ __device__ constexpr bool br_fused_radix4(int loge, int variant) {
+    return loge == 2 && variant == kBmmpBinary;
 }
 
 // Coefficients per thread (log2) a context starts with; tp_br_set_tile and
@@ -119,19 +133,21 @@ br_kernel(const BrKernelParams prm) {
     constexpr bool TW_SMEM = br_smem_twiddles(LOGN);
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
+    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT);
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
     const uint64_t* tw_f = prm.tw_fwd;
     const uint64_t* tw_i = prm.tw_inv;
     if constexpr (TW_SMEM) {
-        for (int i = threadIdx.x; i < N; i += T) {
+        constexpr int TWW = br_twiddle_words(LOGN, LOGE);
+        for (int i = threadIdx.x; i < TWW; i += T) {
             base[i] = prm.tw_fwd[i];
-            base[N + i] = prm.tw_inv[i];
+            base[TWW + i] = prm.tw_inv[i];
         }
         tw_f = base;
-        tw_i = base + N;
-        base += 2 * N;
+        tw_i = base + TWW;
+        base += 2 * TWW;
     }
     uint64_t* xbuf0 = base;
     uint64_t* xbuf1 = base + K * N;
@@ -172,7 +188,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
-                ntt_forward_k<LOGN, K, LOGE>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_f);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
@@ -223,7 +239,7 @@ br_kernel(const BrKernelParams prm) {
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
                 load_half(cx[1], 1);
-                ntt_backward_unscaled_k<LOGN, 2, LOGE>(cx, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGN, 2, LOGE, R4>(cx, t, xb(), tw_i);
                 finish_half(cx[0]);
                 finish_half(cx[1]);
             }
@@ -233,7 +249,7 @@ br_kernel(const BrKernelParams prm) {
                     if (r == 0 || r == L) {
                         uint64_t (&c1)[1][E] = reinterpret_cast<uint64_t(&)[1][E]>(cx[0]);
                         load_half(cx[0], r == 0 ? 0 : 1);
-                        ntt_backward_unscaled_k<LOGN, 1, LOGE>(c1, t, xb(), tw_i);
+                        ntt_backward_unscaled_k<LOGN, 1, LOGE, R4>(c1, t, xb(), tw_i);
                         finish_half(cx[0]);
                     }
                 }
@@ -253,7 +269,7 @@ br_kernel(const BrKernelParams prm) {
                         x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
                     }
                 }
-                ntt_forward_k<LOGN, K, LOGE>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_f);
 #pragma unroll
                 for (int p = 0; p < K; ++p) {
                     const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
@@ -313,7 +329,7 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) x[p][j] = acc[((h0 + p) * E + j) * T + t];
             if (prm.out_coef) {
-                ntt_backward_unscaled_k<LOGN, K, LOGE>(x, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_i);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll

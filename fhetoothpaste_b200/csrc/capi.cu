@@ -93,7 +93,8 @@ tp_status get_tables(int device, int logn, const Tables** out) {
     // psi = 7^((p-1)/2N) (lib/src/backend/solinas.cpp:176)
     const uint64_t psi = hpow(7, (kP - 1) >> (logn + 1));
     const uint64_t psi_inv = hinv(psi);
-    std::vector<uint64_t> pw(2 * N), pwi(N), tf(N), ti(N);
+    // twiddles psi^(+-brv(k)), k < N, followed by the radix-4 products tw[i] tw[2i], i < N/2
+    std::vector<uint64_t> pw(2 * N), pwi(N), tf(N + N / 2, 0), ti(N + N / 2, 0);
     pw[0] = 1;
     for (uint64_t i = 1; i < 2 * N; ++i) pw[i] = hmul(pw[i - 1], psi);
     pwi[0] = 1;
@@ -102,15 +103,23 @@ tp_status get_tables(int device, int logn, const Tables** out) {
         tf[k] = pw[brv((uint32_t)k, logn)];
         ti[k] = pwi[brv((uint32_t)k, logn)];
     }
+    for (uint64_t i = 1; i < N / 2; ++i) {
+        tf[N + i] = hmul(tf[i], tf[2 * i]);
+        ti[N + i] = hmul(ti[i], ti[2 * i]);
+    }
+    // The radix-4 kernels multiply by the first levels' twiddles as shifts:
+    // psi^(N/2) = 2^48, psi^(N/4) = 2^120 (and their inverses 2^144, 2^72).
+    if (tf[1] != hpow(2, 48) || tf[2] != hpow(2, 120) || ti[1] != hpow(2, 144) || ti[2] != hpow(2, 72))
+        return fail(TP_ERR_PARAM, "unexpected NTT roots of unity (shift twiddles do not apply)");
     auto* t = new Tables();
     t->device = device;
     t->logn = logn;
     t->n_inv = hinv(N);
-    cudaError_t e = cudaMalloc(&t->tw_fwd, N * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&t->tw_inv, N * 8);
+    cudaError_t e = cudaMalloc(&t->tw_fwd, tf.size() * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&t->tw_inv, ti.size() * 8);
     if (e == cudaSuccess) e = cudaMalloc(&t->psi_pow, 2 * N * 8);
-    if (e == cudaSuccess) e = cudaMemcpy(t->tw_fwd, tf.data(), N * 8, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(t->tw_inv, ti.data(), N * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->tw_fwd, tf.data(), tf.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t->tw_inv, ti.data(), ti.size() * 8, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t->psi_pow, pw.data(), 2 * N * 8, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaFree(t->tw_fwd);
@@ -184,7 +193,7 @@ struct tp_br_ctx {
     int loge = 3;                 // log2 coefficients per thread of the active tile
     const void* kernels[4] = {};  // by loge (2, 3)
     int grid_caps[4] = {};        // resident blocks on the device, by loge
-    size_t smem_bytes = 0;
+    size_t smem[4] = {};          // dynamic shared memory bytes, by loge
     // workspace for host-pointer calls
     uint64_t* ws = nullptr;
     uint64_t ws_words = 0;
@@ -283,21 +292,22 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         }
     }
 
-    c->smem_bytes = tp::br_smem_words(c->logn, p->variant, p->lwe_dim) * 8;
     for (int lg = 2; lg <= 3; ++lg) {
         const void* k = tp::br_kernel_lookup(c->logn, p->variant, lg);
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes);
+        const size_t smem = tp::br_smem_words(c->logn, p->variant, p->lwe_dim, lg) * 8;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int per_sm = 0;
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(N >> lg), c->smem_bytes);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(N >> lg), smem);
         if (e != cudaSuccess || per_sm < 1) {
             cudaFree(c->err);
             delete c;
             return fail(TP_ERR_PARAM, "blind-rotation kernel does not fit (N=%llu, n=%u, smem=%zu, %d per thread): %s",
-                        (unsigned long long)N, p->lwe_dim, (size_t)c->smem_bytes, 1 << lg,
+                        (unsigned long long)N, p->lwe_dim, smem, 1 << lg,
                         e == cudaSuccess ? "no resident block" : cudaGetErrorString(e));
         }
         c->kernels[lg] = k;
+        c->smem[lg] = smem;
         c->grid_caps[lg] = per_sm * sm_count(device);
     }
     c->loge = tp::br_default_loge(c->logn, p->variant);
@@ -376,8 +386,8 @@ tp_status tp_br_blind_rotate_batch(tp_br_ctx* c, uint64_t batch, uint64_t* resul
     kp.out_coef = out_coef ? 1u : 0u;
     const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
     void* args[] = {&kp};
-    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args, c->smem_bytes,
-                             (cudaStream_t)stream));
+    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args,
+                             c->smem[c->loge], (cudaStream_t)stream));
     return TP_OK;
 }
 

@@ -53,6 +53,9 @@ __device__ __forceinline__ uint64_t gl_sub(uint64_t a, uint64_t b) {
     return pack64(dl, dh);
 }
 
+// Canonical residue of any 64-bit value.
+__device__ __forceinline__ uint64_t gl_canon(uint64_t x) { return x >= kP ? x - kP : x; }
+
 // -a mod p.
 __device__ __forceinline__ uint64_t gl_neg(uint64_t a) { return a == 0 ? 0 : kP - a; }
 
@@ -75,32 +78,30 @@ __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t& r0, u
 }
 
 // Reduces x = r0 + r1 2^32 + r2 2^64 + r3 2^96 (any 128-bit value) to [0, p).
+//   t = (r1:r0) - r3            (a borrow takes eps off: t stays >= 2^64 - 2^32)
+//   s = t + r2 (2^32 - 1)       (65 bits: carry c)
+//   result = s + eps (mod 2^64) if c or s >= p, else s
+// With a carry the wrapped s is below r2 (2^32 - 1) <= 2^64 - 2^33 + 1, so
+// s + eps neither overflows nor reaches p; without one, s >= p exactly when
+// s + eps carries, and then s + eps (mod 2^64) = s - p.
 __device__ __forceinline__ uint64_t gl_reduce128(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
     uint32_t s0, s1;
     asm("{\n\t"
-        ".reg .u32 t0, t1, m, m1, u0, u1, c, x0, x1;\n\t"
+        ".reg .u32 t0, t1, b, u0, u1, c, x0, x1;\n\t"
         ".reg .pred pc;\n\t"
-        // t = (r1:r0) - r3; on borrow add p (t stays below 2^64)
         "sub.cc.u32 t0, %2, %5;\n\t"
         "subc.cc.u32 t1, %3, 0;\n\t"
-        "subc.u32 m, 0, 0;\n\t"
-        "and.b32 m1, m, 1;\n\t"
-        "add.cc.u32 t0, t0, m1;\n\t"
-        "addc.u32 t1, t1, m;\n\t"
-        // u = r2 * (2^32 - 1) = (r2 : 0) - (0 : r2)
+        "subc.u32 b, 0, 0;\n\t"
+        "sub.cc.u32 t0, t0, b;\n\t"
+        "subc.u32 t1, t1, 0;\n\t"
         "sub.cc.u32 u0, 0, %4;\n\t"
         "subc.u32 u1, %4, 0;\n\t"
-        // s = t + u; on carry add eps (cannot carry again)
         "add.cc.u32 %0, t0, u0;\n\t"
         "addc.cc.u32 %1, t1, u1;\n\t"
         "addc.u32 c, 0, 0;\n\t"
-        "neg.s32 c, c;\n\t"
-        "add.cc.u32 %0, %0, c;\n\t"
-        "addc.u32 %1, %1, 0;\n\t"
-        // canonical: s >= p  <=>  s + eps carries; then s - p = s + eps (mod 2^64)
         "add.cc.u32 x0, %0, 0xFFFFFFFF;\n\t"
         "addc.cc.u32 x1, %1, 0;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
+        "addc.u32 c, c, 0;\n\t"
         "setp.ne.u32 pc, c, 0;\n\t"
         "selp.b32 %0, x0, %0, pc;\n\t"
         "selp.b32 %1, x1, %1, pc;\n\t"
@@ -170,7 +171,37 @@ __device__ __forceinline__ uint64_t gl_fma_lazy(uint64_t acc, uint64_t a, uint64
     return gl_reduce128_lazy(r0, r1, r2, r3);
 }
 
-// Canonical residue of any 64-bit value.
-__device__ __forceinline__ uint64_t gl_canon(uint64_t x) { return x >= kP ? x - kP : x; }
+// hi * 2^64 + lo mod p as a 64-bit representative (not necessarily below p),
+// for any hi, lo: hi 2^64 = h0 2^64 + h1 2^96 = h0 (2^32 - 1) - h1.
+__device__ __forceinline__ uint64_t gl_fold(uint64_t hi, uint64_t lo) {
+    const uint64_t h0 = hi & 0xFFFFFFFFull, h1 = hi >> 32;
+    uint64_t t = lo - h1;
+    if (lo < h1) t -= kEps;              // t was >= 2^64 - 2^32: no underflow
+    const uint64_t u = (h0 << 32) - h0;  // h0 (2^32 - 1) < 2^64
+    uint64_t s = t + u;
+    if (s < u) s += kEps;                // wrapped s < u <= 2^64 - 2^33 + 1: no overflow
+    return s;
+}
+
+// x * 2^K mod p for a compile-time K (canonical in and out), with shifts and
+// adds only. Every root of unity of order dividing 64 is a power of two in this
+// field (2 has order 192), so the twiddles of the first NTT levels are such
+// shifts.
+template <int K>
+__device__ __forceinline__ uint64_t gl_mul_pow2(uint64_t x) {
+    static_assert(K >= 0 && K < 192, "exponent out of range");
+    if constexpr (K >= 96) {
+        return gl_neg(gl_mul_pow2<K - 96>(x));  // 2^96 = -1
+    } else if constexpr (K == 0) {
+        return x;
+    } else if constexpr (K < 64) {
+        return gl_canon(gl_fold(x >> (64 - K), x << K));
+    } else if constexpr (K == 64) {
+        return gl_canon(gl_fold(x, 0));
+    } else {
+        return gl_canon(gl_fold(gl_fold(x >> (128 - K), x << (K - 64)), 0));
+    }
+}
+
 
 }  // namespace tp

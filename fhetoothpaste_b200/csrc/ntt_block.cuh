@@ -10,6 +10,7 @@
 // words as the reference.
 //
 // Levels are processed in passes of up to LOGE (radix-E groups in registers).
+// Radix-4 passes read a second table of twiddle products at tw + N (below).
 // Between passes the data goes through a shared-memory exchange buffer of N
 // words. Passes whose blocks span at most 32*E coefficients touch only their
 // own warp's 32*E-word region, so those exchanges need only __syncwarp; the
@@ -89,31 +90,114 @@ __device__ __forceinline__ void ntt_sync(bool block_wide) {
 // its exchange area is buf + k*N). The K transforms share every twiddle load
 // and every synchronisation, and their independent butterflies interleave.
 
-// Forward butterflies of pass P on the thread's registers.
-template <int LOGN, int P, int K, int LOGE>
+// Fused radix-4 passes (E = 4, optional) combine their two levels. With W1 = tw[m + b] (level L0,
+// m = 2^L0, block b), W2 = tw[2m + 2b] and W3 = tw[2m + 2b + 1] = W2 w4, where
+// w4 = psi^(N/2) = 2^48 is the 4th root of unity (brv(2i+1) = brv(2i) + N/2),
+// the four outputs of the forward levels are
+//   t1 = W1 x2, t2 = W2 x1, t3 = W1W2 x3
+//   y0 = (x0 + t1) + (t2 + t3)     y1 = (x0 + t1) - (t2 + t3)
+//   y2 = (x0 - t1) + w4 (t2 - t3)  y3 = (x0 - t1) - w4 (t2 - t3)
+// three general products and one shift instead of four products. W1W2 is read
+// from the product table at tw[N + m + b]. In pass 0 (b = 0) the twiddles are
+// 2^48, 2^120, 2^168 and every product is a shift. This trades IMADs (FMA
+// pipe) for shifts and adds (ALU pipe); it measured faster only where the FMA
+// pipe is the busier one (BMMP, whose key MAC is 1.5x CGGI ternary's).
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void fwd_radix4(uint64_t (&x)[K][4], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN, 2>;
+    constexpr int TMIN = SH::N >> (SH::L0(P) + 2);
+    constexpr int M = 1 << SH::L0(P);
+    const int b = t / TMIN;
+    uint64_t w1 = 0, w2 = 0, w12 = 0;
+    if constexpr (P > 0) {
+        w1 = tw[M + b];
+        w2 = tw[2 * M + 2 * b];
+        w12 = tw[SH::N + M + b];
+    }
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+        uint64_t t1, t2, t3;
+        if constexpr (P == 0) {
+            t1 = gl_mul_pow2<48>(x[p][2]);
+            t2 = gl_mul_pow2<120>(x[p][1]);
+            t3 = gl_mul_pow2<168>(x[p][3]);
+        } else {
+            t1 = gl_mul(x[p][2], w1);
+            t2 = gl_mul(x[p][1], w2);
+            t3 = gl_mul(x[p][3], w12);
+        }
+        const uint64_t a = gl_add(x[p][0], t1), bb = gl_sub(x[p][0], t1);
+        const uint64_t c = gl_add(t2, t3), d = gl_mul_pow2<48>(gl_sub(t2, t3));
+        x[p][0] = gl_add(a, c);
+        x[p][1] = gl_sub(a, c);
+        x[p][2] = gl_add(bb, d);
+        x[p][3] = gl_sub(bb, d);
+    }
+}
+
+// Inverse of the above (Gentleman-Sande, levels L0+1 then L0) with V = tw_inv:
+//   g = x0 + x1, h = x2 + x3, e = x0 - x1, f = w4^-1 (x2 - x3)
+//   y0 = g + h, y2 = V1 (g - h), y1 = V2 (e + f), y3 = V1V2 (e - f)
+// In pass 0 the twiddles are 2^144, 2^72, 2^24 (w4^-1 = 2^144).
+template <int LOGN, int P, int K>
+__device__ __forceinline__ void inv_radix4(uint64_t (&x)[K][4], int t, const uint64_t* __restrict__ tw) {
+    using SH = NttShape<LOGN, 2>;
+    constexpr int TMIN = SH::N >> (SH::L0(P) + 2);
+    constexpr int M = 1 << SH::L0(P);
+    const int b = t / TMIN;
+    uint64_t v1 = 0, v2 = 0, v12 = 0;
+    if constexpr (P > 0) {
+        v1 = tw[M + b];
+        v2 = tw[2 * M + 2 * b];
+        v12 = tw[SH::N + M + b];
+    }
+#pragma unroll
+    for (int p = 0; p < K; ++p) {
+        const uint64_t g = gl_add(x[p][0], x[p][1]), h = gl_add(x[p][2], x[p][3]);
+        const uint64_t e = gl_sub(x[p][0], x[p][1]), f = gl_mul_pow2<144>(gl_sub(x[p][2], x[p][3]));
+        x[p][0] = gl_add(g, h);
+        if constexpr (P == 0) {
+            x[p][2] = gl_mul_pow2<144>(gl_sub(g, h));
+            x[p][1] = gl_mul_pow2<72>(gl_add(e, f));
+            x[p][3] = gl_mul_pow2<24>(gl_sub(e, f));
+        } else {
+            x[p][2] = gl_mul(gl_sub(g, h), v1);
+            x[p][1] = gl_mul(gl_add(e, f), v2);
+            x[p][3] = gl_mul(gl_sub(e, f), v12);
+        }
+    }
+}
+
+// Forward butterflies of pass P on the thread's registers (R4: use the fused
+// radix-4 form for radix-4 passes).
+template <int LOGN, int P, int K, int LOGE, bool R4>
 __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
-    constexpr int G = 1 << S;
-    constexpr int PER = SH::E / G;
-    constexpr int TMIN = SH::N >> (SH::L0(P) + S);
-    constexpr int L0 = SH::L0(P);
+    if constexpr (R4 && LOGE == 2 && S == 2) {
+        fwd_radix4<LOGN, P, K>(x, t, tw);
+    } else {
+        constexpr int G = 1 << S;
+        constexpr int PER = SH::E / G;
+        constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+        constexpr int L0 = SH::L0(P);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int blk = (PER * t + q) / TMIN;
+        for (int q = 0; q < PER; ++q) {
+            const int blk = (PER * t + q) / TMIN;
 #pragma unroll
-        for (int k = 0; k < S; ++k) {
-            const int half = G >> (k + 1);
+            for (int k = 0; k < S; ++k) {
+                const int half = G >> (k + 1);
 #pragma unroll
-            for (int j = 0; j < G; ++j) {
-                if (j & half) continue;
-                const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
+                for (int j = 0; j < G; ++j) {
+                    if (j & half) continue;
+                    const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
 #pragma unroll
-                for (int p = 0; p < K; ++p) {
-                    const uint64_t u = x[p][q * G + j];
-                    const uint64_t v = gl_mul(x[p][q * G + j + half], w);
-                    x[p][q * G + j] = gl_add(u, v);
-                    x[p][q * G + j + half] = gl_sub(u, v);
+                    for (int p = 0; p < K; ++p) {
+                        const uint64_t u = x[p][q * G + j];
+                        const uint64_t v = gl_mul(x[p][q * G + j + half], w);
+                        x[p][q * G + j] = gl_add(u, v);
+                        x[p][q * G + j + half] = gl_sub(u, v);
+                    }
                 }
             }
         }
@@ -121,30 +205,34 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t
 }
 
 // Inverse butterflies of pass P (levels in reverse order).
-template <int LOGN, int P, int K, int LOGE>
+template <int LOGN, int P, int K, int LOGE, bool R4>
 __device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
-    constexpr int G = 1 << S;
-    constexpr int PER = SH::E / G;
-    constexpr int TMIN = SH::N >> (SH::L0(P) + S);
-    constexpr int L0 = SH::L0(P);
+    if constexpr (R4 && LOGE == 2 && S == 2) {
+        inv_radix4<LOGN, P, K>(x, t, tw);
+    } else {
+        constexpr int G = 1 << S;
+        constexpr int PER = SH::E / G;
+        constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+        constexpr int L0 = SH::L0(P);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int blk = (PER * t + q) / TMIN;
+        for (int q = 0; q < PER; ++q) {
+            const int blk = (PER * t + q) / TMIN;
 #pragma unroll
-        for (int k = S - 1; k >= 0; --k) {
-            const int half = G >> (k + 1);
+            for (int k = S - 1; k >= 0; --k) {
+                const int half = G >> (k + 1);
 #pragma unroll
-            for (int j = 0; j < G; ++j) {
-                if (j & half) continue;
-                const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
+                for (int j = 0; j < G; ++j) {
+                    if (j & half) continue;
+                    const uint64_t w = tw[(1 << (L0 + k)) + (blk << k) + (j >> (S - k))];
 #pragma unroll
-                for (int p = 0; p < K; ++p) {
-                    const uint64_t u = x[p][q * G + j];
-                    const uint64_t v = x[p][q * G + j + half];
-                    x[p][q * G + j] = gl_add(u, v);
-                    x[p][q * G + j + half] = gl_mul(gl_sub(u, v), w);
+                    for (int p = 0; p < K; ++p) {
+                        const uint64_t u = x[p][q * G + j];
+                        const uint64_t v = x[p][q * G + j + half];
+                        x[p][q * G + j] = gl_add(u, v);
+                        x[p][q * G + j + half] = gl_mul(gl_sub(u, v), w);
+                    }
                 }
             }
         }
@@ -192,44 +280,46 @@ __device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][1 <<
     }
 }
 
-template <int LOGN, int P, int K, int LOGE>
+template <int LOGN, int P, int K, int LOGE, bool R4>
 __device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                 const uint64_t* tw) {
     using SH = NttShape<LOGN, LOGE>;
-    fwd_pass_math<LOGN, P, K, LOGE>(x, t, tw);
+    fwd_pass_math<LOGN, P, K, LOGE, R4>(x, t, tw);
     if constexpr (P + 1 < SH::NPASS) {
         xstore<LOGN, P, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P));
         xload<LOGN, P + 1, K, LOGE>(buf, x, t);
-        fwd_passes_from<LOGN, P + 1, K, LOGE>(x, t, buf, tw);
+        fwd_passes_from<LOGN, P + 1, K, LOGE, R4>(x, t, buf, tw);
     }
 }
 
-template <int LOGN, int P, int K, int LOGE>
+template <int LOGN, int P, int K, int LOGE, bool R4>
 __device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                 const uint64_t* tw) {
     using SH = NttShape<LOGN, LOGE>;
-    inv_pass_math<LOGN, P, K, LOGE>(x, t, tw);
+    inv_pass_math<LOGN, P, K, LOGE, R4>(x, t, tw);
     if constexpr (P > 0) {
         xstore<LOGN, P, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P - 1));
         xload<LOGN, P - 1, K, LOGE>(buf, x, t);
-        inv_passes_from<LOGN, P - 1, K, LOGE>(x, t, buf, tw);
+        inv_passes_from<LOGN, P - 1, K, LOGE, R4>(x, t, buf, tw);
     }
 }
 
 // Forward NTT of K polynomials: coefficient layout -> slot layout. buf holds K*N words.
-template <int LOGN, int K, int LOGE = 3>
+// R4 (4 coefficients per thread only) selects the fused radix-4 butterflies,
+// whose twiddle products sit at tw_fwd + N.
+template <int LOGN, int K, int LOGE = 3, bool R4 = false>
 __device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                               const uint64_t* tw_fwd) {
-    fwd_passes_from<LOGN, 0, K, LOGE>(x, t, buf, tw_fwd);
+    fwd_passes_from<LOGN, 0, K, LOGE, R4>(x, t, buf, tw_fwd);
 }
 
 // Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.
-template <int LOGN, int K, int LOGE = 3>
+template <int LOGN, int K, int LOGE = 3, bool R4 = false>
 __device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                         const uint64_t* tw_inv) {
-    inv_passes_from<LOGN, NttShape<LOGN, LOGE>::NPASS - 1, K, LOGE>(x, t, buf, tw_inv);
+    inv_passes_from<LOGN, NttShape<LOGN, LOGE>::NPASS - 1, K, LOGE, R4>(x, t, buf, tw_inv);
 }
 
 // One polynomial, 8 coefficients per thread.
