@@ -73,13 +73,27 @@ __host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
     return loge == 2 ? (1 << logn) + (1 << (logn - 1)) : (1 << logn);
 }
 
+// Key rows staged in shared memory: each thread copies its own slots of the
+// next gadget row with cp.async before the digit's transforms and reads them
+// after, so the L2 latency of the key stream hides behind the NTTs. Needs C*N
+// more words; off at N = 4096 where they do not fit.
+__host__ __device__ constexpr bool br_key_prefetch(int logn) { return logn <= 11; }
+
 // Shared memory of one block, in words: twiddles (both directions, if kept
-// there), two exchange areas of width*N words, the accumulator (2N), the LWE
-// vector (n+1, rounded up to an even count).
+// there), two exchange areas of width*N words, the accumulator (2N), the key
+// row stage (C*N, if used), the LWE vector (n+1, rounded up to an even count).
 __host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge) {
     return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
-           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) + ((n + 2) & ~1u);
+           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
+           (br_key_prefetch(logn) ? (size_t)(1 << logn) * 2 * br_rgsw_per_group(variant) : 0) + ((n + 2) & ~1u);
 }
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Exponent e_k = 2 brv(k) + 1 of slot k: NTT(X^a)[k] = psi^(e_k a mod 2N).
 template <int LOGN>
@@ -134,6 +148,7 @@ br_kernel(const BrKernelParams prm) {
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
     constexpr bool R4 = br_fused_radix4(LOGE, VARIANT);
+    constexpr bool PF = br_key_prefetch(LOGN);
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
@@ -152,7 +167,8 @@ br_kernel(const BrKernelParams prm) {
     uint64_t* xbuf0 = base;
     uint64_t* xbuf1 = base + K * N;
     uint64_t* acc = base + 2 * K * N;        // [(h*E + j)*T + t], canonical, NTT domain
-    uint64_t* lwe_s = acc + 2 * N;
+    uint64_t* kst = acc + 2 * N;             // key row stage, device layout of one row (C*N words)
+    uint64_t* lwe_s = kst + (PF ? C * N : 0);
 
     const int t = threadIdx.x;
     const uint32_t n = prm.n;
@@ -245,6 +261,18 @@ br_kernel(const BrKernelParams prm) {
             }
 #pragma unroll 1
             for (uint32_t r = 0; r < 2 * L; r += K) {
+                if constexpr (PF && K == 1) {
+                    // this thread's slots of key row r; read back by this thread only
+                    const uint64_t* kr = kit + (uint64_t)r * (N * C);
+#pragma unroll
+                    for (int c = 0; c < C; ++c)
+#pragma unroll
+                        for (int jp = 0; jp < E / 2; ++jp) {
+                            const int ko = ((c * (E / 2) + jp) * T + t) * 2;
+                            cp_async16(kst + ko, kr + ko);
+                        }
+                    cp_async_commit();
+                }
                 if constexpr (K == 1) {
                     if (r == 0 || r == L) {
                         uint64_t (&c1)[1][E] = reinterpret_cast<uint64_t(&)[1][E]>(cx[0]);
@@ -270,6 +298,7 @@ br_kernel(const BrKernelParams prm) {
                     }
                 }
                 ntt_forward_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_f);
+                if constexpr (PF && K == 1) cp_async_wait_all();
 #pragma unroll
                 for (int p = 0; p < K; ++p) {
                     const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
@@ -277,8 +306,10 @@ br_kernel(const BrKernelParams prm) {
                     for (int c = 0; c < C; ++c) {
 #pragma unroll
                         for (int jp = 0; jp < E / 2; ++jp) {
-                            const ulonglong2 kv =
-                                __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
+                            const int ko = ((c * (E / 2) + jp) * T + t) * 2;
+                            const ulonglong2 kv = (PF && K == 1)
+                                                      ? *reinterpret_cast<const ulonglong2*>(kst + ko)
+                                                      : __ldg(reinterpret_cast<const ulonglong2*>(kr + ko));
                             o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[p][2 * jp], kv.x);
                             o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
                         }

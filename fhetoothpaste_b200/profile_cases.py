@@ -1,0 +1,171 @@
+"""Runs each GPU kernel of the library on one small case, for profiler captures.
+
+    python -m fhetoothpaste_b200.profile_cases CASE [CASE ...]   (or: all)
+
+Every case launches its kernel(s) twice: one warm-up launch, then the launch to
+capture (so `ncu -s <launches per warm-up> -c <launches>` selects the second).
+Inputs are seeded uniform residues; keys are uniform words (the kernels' timing
+does not depend on their values). Sizes keep device memory to a few GB while the
+streamed operands stay larger than L2 where the kernel streams them.
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+
+import numpy as np
+
+P = 0xFFFFFFFF00000001
+
+
+def _u64(seed: int, shape, bound: int = P) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, 2**63, shape, dtype=np.uint64) % np.uint64(bound)
+
+
+def _dev(torch, a: np.ndarray):
+    return torch.from_numpy(np.ascontiguousarray(a, np.uint64).view(np.int64)).cuda()
+
+
+def _rotation(torch, variant: int, N: int, n: int, beta: int, digits: int, batch: int, tile: int = 0):
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    ctx = BlindRotationContext(variant, N, n, 1 << beta, digits)
+    rot = GpuBlindRotator(ctx, _u64(1, ctx.key_words()))  # key_relayout_kernel
+    if tile:
+        rot.set_tile(tile)                                 # key_retile_kernel
+    lw = _dev(torch, _u64(2, (batch, n + 1), 2 * N))
+    ac = _dev(torch, _u64(3, (batch, 2 * N)))
+    out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        rot.blind_rotate_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch)
+    rot.check()
+    rot.close()
+
+
+def case_br_ternary_n2048(torch):
+    """br_kernel, CGGI ternary N=2048 base 2^12 l=3, n reduced to 64, one wave (148)."""
+    _rotation(torch, 1, 2048, 64, 12, 3, 148)
+
+
+def case_br_binary_n1024(torch):
+    """br_kernel, CGGI binary N=1024 base 2^16 l=4, n reduced to 64, one wave (296)."""
+    _rotation(torch, 0, 1024, 64, 16, 4, 296)
+
+
+def case_br_bmmp_n2048(torch):
+    """br_kernel, BMMP N=2048 base 2^16 l=4, n reduced to 64 (32 pairs), one wave (148)."""
+    _rotation(torch, 2, 2048, 64, 16, 4, 148)
+
+
+def case_br_ternary_n4096(torch):
+    """br_kernel, CGGI ternary N=4096 base 2^12 l=3, n reduced to 32, one wave (148)."""
+    _rotation(torch, 1, 4096, 32, 12, 3, 148)
+
+
+def case_ntt_n2048(torch):
+    """ntt_batch_kernel forward then backward, 8192 polynomials of N=2048 (134 MB)."""
+    from fhetoothpaste_b200 import ntt_backward, ntt_forward
+    N, count = 2048, 8192
+    x = _dev(torch, _u64(4, (count, N)))
+    for _ in range(2):
+        ntt_forward(N, count, x.data_ptr(), x.data_ptr())
+        ntt_backward(N, count, x.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+
+
+def case_rlwe_ks_n2048(torch):
+    """ks_kernel (RLWE->RLWE), 4096 ciphertexts of N=2048, base 2^16 l=4."""
+    from fhetoothpaste_b200 import GpuRLWEtoRLWEConverter
+    N, l, batch = 2048, 4, 4096
+    conv = GpuRLWEtoRLWEConverter(N, 1 << 16, l, _u64(5, 2 * N * l))
+    x = _dev(torch, _u64(6, (batch, 2 * N)))
+    y = torch.zeros((batch, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        conv.convert_batch(batch, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+    conv.close()
+
+
+def case_auto_n2048(torch):
+    """ks_kernel (automorphism X -> X^5 + key switch), 4096 ciphertexts of N=2048, l=4."""
+    from fhetoothpaste_b200 import GpuAutomorphismEvaluator
+    N, l, batch = 2048, 4, 4096
+    ev = GpuAutomorphismEvaluator(N, 1 << 16, l, 5, _u64(7, 2 * N * l))
+    x = _dev(torch, _u64(8, (batch, 2 * N)))
+    y = torch.zeros((batch, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        ev.eval_batch(batch, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+    ev.close()
+
+
+def case_pack_n2048(torch):
+    """pack_l0_kernel + ks_kernel merge levels: 8 packs of 2048 LWEs (n=N=2048), l=4."""
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker
+    N, L, packs, l = 2048, 2048, 8, 4
+    packer = GpuLWEtoRLWEPacker(N, 1 << 16, l, _u64(9, 11 * 2 * N * l))
+    x = _dev(torch, _u64(10, (packs * L, N + 1)))
+    y = torch.empty((packs, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        packer.pack_batch(packs, L, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+    packer.close()
+
+
+def case_lwe_ks_2048_630(torch):
+    """lwe_ks_kernel: 4096 LWE ciphertexts n=2048 -> n=630, base 2^16 l=4 (41 MB key)."""
+    from fhetoothpaste_b200 import GpuLWEtoLWEConverter
+    n_in, n_out, l, batch = 2048, 630, 4, 4096
+    conv = GpuLWEtoLWEConverter(n_in, n_out, 1 << 16, l, _u64(11, n_in * l * (n_out + 1)))
+    x = _dev(torch, _u64(12, (batch, n_in + 1)))
+    y = torch.zeros((batch, n_out + 1), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        conv.convert_batch(batch, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+    conv.close()
+
+
+def case_sample_extract_n2048(torch):
+    """sample_extract0_kernel, 16384 ciphertexts of N=2048 (537 MB in)."""
+    from fhetoothpaste_b200 import sample_extract_batch
+    N, batch = 2048, 16384
+    x = _dev(torch, _u64(13, (batch, 2 * N)))
+    y = torch.empty((batch, N + 1), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        sample_extract_batch(N, batch, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+
+
+def case_key_retile_n2048(torch):
+    """key_relayout_kernel (upload) and key_retile_kernel (tile 4 -> 8 -> 4), ternary N=2048 n=630 key."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    ctx = BlindRotationContext(1, 2048, 630, 1 << 12, 3)
+    rot = GpuBlindRotator(ctx, _u64(14, ctx.key_words()))
+    rot.set_tile(8)
+    rot.set_tile(4)
+    rot.close()
+
+
+CASES = {name[5:]: fn for name, fn in globals().items() if name.startswith("case_")}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("cases", nargs="+", help="case names or 'all': " + ", ".join(sorted(CASES)))
+    args = ap.parse_args(argv)
+    names = sorted(CASES) if args.cases == ["all"] else args.cases
+    unknown = [c for c in names if c not in CASES]
+    if unknown:
+        ap.error(f"unknown case(s): {unknown}")
+    import torch
+    if not torch.cuda.is_available():
+        print("profile_cases needs a CUDA device", file=sys.stderr)
+        return 2
+    for name in names:
+        CASES[name](torch)
+        print(f"{name}: ok", flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
