@@ -350,9 +350,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the BMMP batch sweep and the packing run")
     args = ap.parse_args()
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from fhetoothpaste_b200.dist_util import aggregate_rate, env_ranks, init, max_over_ranks, weak_seed
+    rank, world, local = env_ranks()
     wl = args.workload
 
     if args.impl == "reference":
@@ -362,12 +361,7 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = init("nccl", timeout_s=120.0)  # None on one GPU
 
     from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator, _native
     from oracle.oracle import lwe_inputs
@@ -381,14 +375,14 @@ def main():
     # Key words are uniform residues: timing does not depend on their values
     # (parity with real keys is covered by the test suite).
     kw = ctx.key_words()
-    rng = np.random.default_rng(1234 + rank)
+    rng = np.random.default_rng(weak_seed(1234, rank))
     brk = rng.integers(0, 2**63, kw, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, kw, dtype=np.uint64)
     brk = np.where(brk >= np.uint64(P), brk - np.uint64(P), brk)
     rot = GpuBlindRotator(ctx, brk, device=local)
     del brk
 
-    lwes_h = lwe_inputs(N, n, batch, 7 + 1000 * rank)
-    accs_h = lut_polys(N, batch, 8 + 1000 * rank)
+    lwes_h = lwe_inputs(N, n, batch, weak_seed(7, rank))   # each rank rotates its own batch
+    accs_h = lut_polys(N, batch, weak_seed(8, rank))
     lw = torch.from_numpy(lwes_h.view(np.int64)).cuda()
     ac = torch.from_numpy(accs_h.view(np.int64)).cuda()
     out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
@@ -426,11 +420,8 @@ def main():
         if dist:
             dist.destroy_process_group()
         return
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = batch * world / (ms * 1e-3)
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = aggregate_rate(batch, world, ms * 1e-3)
     launches = args.steps
 
     # end-to-end through the host-buffer call: pinned host inputs, copies inside
@@ -449,16 +440,15 @@ def main():
     for _ in range(1):
         e2e_step()
     barrier()
-    t0 = time.perf_counter()
+    # CUDA events on the launching stream: the call's host->device copies, the
+    # launch and the device->host copy of the results are all on this stream
+    e0.record()
     for _ in range(e2e_steps):
         e2e_step()
+    e1.record()
     barrier()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_val = batch * world / e2e_s
+    e2e_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / e2e_steps, dist, "cuda")
+    e2e_val = aggregate_rate(batch, world, e2e_s)
     launches += e2e_steps + 1
     h2d = lwes_h.nbytes + accs_h.nbytes
     d2h = batch * 2 * N * 8
