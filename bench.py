@@ -236,7 +236,8 @@ BMMP_BATCHES = (1, 37, 512, 2048, 8192)
 
 def bmmp_batch_sweep(device: int) -> dict:
     """BMMP (binary n=768 as 384 pairs, N=2048, base 2^16 l=4) at uneven batch sizes,
-    identity test polynomials, one graph-recorded launch per batch."""
+    identity test polynomials; per batch size the autotuner picks the tile and the
+    blocks per rotation, then one graph-recorded launch per step is timed."""
     import torch
     from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
     from oracle.oracle import lwe_inputs
@@ -252,12 +253,17 @@ def bmmp_batch_sweep(device: int) -> dict:
     ac = torch.from_numpy(ident.view(np.int64)).cuda()
     res = torch.empty((max(BMMP_BATCHES), 2 * N), dtype=torch.int64, device="cuda")
     for b in BMMP_BATCHES:
+        prev = rot.tile
+        coef, _ = rot.autotune(b)
+        # three candidates x three launches, plus the key re-tilings between them
+        launches += 9 + (prev != 8) + 1 + (coef == 8)
         g = rot.capture_batch(res.data_ptr(), lw_all.data_ptr(), n + 1, ac.data_ptr(), 0, b)
         reps = 3 if b >= 512 else 5
         ms = _timed(torch, lambda: g.launch(stream), 2, reps, stream)
         launches += 2 + reps
         g.close()
-        out[str(b)] = {"BR_per_s": round(b / (ms * 1e-3), 1), "ms_per_launch": round(ms, 3)}
+        out[str(b)] = {"BR_per_s": round(b / (ms * 1e-3), 1), "ms_per_launch": round(ms, 3),
+                       "tile": {"coef_per_thread": coef, "blocks_per_rotation": rot.split}}
     rot.check(stream)
     rot.close()
     out["launches"] = launches
@@ -453,19 +459,27 @@ def main():
     h2d = lwes_h.nbytes + accs_h.nbytes
     d2h = batch * 2 * N * 8
 
-    # plain form: one rotation per launch
+    # plain form: one rotation per launch (one thread block, as the batched kernel
+    # runs it), and the same with the rotation split over two SMs
     one_out = torch.empty((1, 2 * N), dtype=torch.int64, device="cuda")
     plain_reps = 3
-    rot.blind_rotate_batch(one_out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, 1, stream=stream)
-    torch.cuda.synchronize()
-    e0.record()
-    for i in range(plain_reps):
-        rot.blind_rotate_batch(one_out.data_ptr(), lw[i:].data_ptr(), n + 1, ac[i:].data_ptr(), 2 * N, 1,
-                               stream=stream)
-    e1.record()
-    torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / plain_reps
-    launches += plain_reps + 1
+
+    def plain_time() -> float:
+        rot.blind_rotate_batch(one_out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, 1, stream=stream)
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(plain_reps):
+            rot.blind_rotate_batch(one_out.data_ptr(), lw[i:].data_ptr(), n + 1, ac[i:].data_ptr(), 2 * N, 1,
+                                   stream=stream)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / plain_reps
+
+    plain_ms = plain_time()
+    rot.set_split(2)
+    plain2_ms = plain_time()
+    rot.set_split(1)
+    launches += 2 * (plain_reps + 1)
 
     # roofline: algorithmic modmuls per launch over the kernel's launch time,
     # against the measured 64x64->128 product rate of this GPU
@@ -488,7 +502,9 @@ def main():
         "e2e": {"value": round(e2e_val, 2), "unit": "BR/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "plain": {"value": round(1e3 / plain_ms, 3), "unit": "BR/s", "ms_per_rotation": round(plain_ms, 3),
-                  "batched_over_plain": round(value / world / (1e3 / plain_ms), 1)},
+                  "batched_over_plain": round(value / world / (1e3 / plain_ms), 1),
+                  "two_blocks": {"value": round(1e3 / plain2_ms, 3), "ms_per_rotation": round(plain2_ms, 3),
+                                 "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)}},
         "gpu_launches": launches,
         "roofline": {"bound": "int32", "achieved": round(achieved / 1e9, 1), "peak": round(prod.value / 1e9, 1),
                      "unit": "Gmodmul/s", "frac": round(achieved / prod.value, 4), "traffic": traffic,

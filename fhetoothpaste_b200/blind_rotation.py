@@ -109,8 +109,16 @@ class GpuBlindRotator:
     def set_tile(self, coef_per_thread: int) -> None:
         nat.check(nat.lib().tp_br_set_tile(self._h, coef_per_thread))
 
+    @property
+    def split(self) -> int:
+        """Thread blocks per rotation (1, or 2 for the two-SM cluster kernel)."""
+        return int(nat.lib().tp_br_get_split(self._h))
+
+    def set_split(self, blocks_per_rotation: int) -> None:
+        nat.check(nat.lib().tp_br_set_split(self._h, blocks_per_rotation))
+
     def autotune(self, batch: int) -> tuple[int, float]:
-        """Times every tile on `batch` synthetic rotations and keeps the fastest."""
+        """Times every tile (and the two-block split) on `batch` synthetic rotations and keeps the fastest."""
         coef, rate = ctypes.c_uint32(), ctypes.c_double()
         nat.check(nat.lib().tp_br_autotune(self._h, batch, ctypes.byref(coef), ctypes.byref(rate)))
         return int(coef.value), float(rate.value)

@@ -1,0 +1,20 @@
+// Library-internal launch of the rotation kernels with an explicit split, for
+// callers inside the library that choose the kernel per launch (the serving
+// loop). Not part of the C ABI.
+#pragma once
+
+#include "toothpaste_gpu.h"
+
+namespace tp {
+
+// split 0: the context's setting; 1: one block per rotation; 2: the two-block
+// cluster kernel when the context's tile and the device allow it (else 1).
+tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                          uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef, void* stream,
+                          int split);
+
+// Rotations the device runs at once with one (split 1) or two (split 2) blocks
+// per rotation; 0 when that kernel is not available for the context.
+uint64_t br_concurrency(const tp_br_ctx* c, int split);
+
+}  // namespace tp

@@ -11,7 +11,9 @@
 
 #include "toothpaste_gpu.h"
 #include "br_kernels.cuh"
+#include "br_pair_kernel.cuh"
 #include "dispatch.h"
+#include "br_launch.h"
 #include "misc_kernels.cuh"
 #include "util_kernels.cuh"
 #include "ks_kernels.cuh"
@@ -194,6 +196,10 @@ struct tp_br_ctx {
     const void* kernels[4] = {};  // by loge (2, 3)
     int grid_caps[4] = {};        // resident blocks on the device, by loge
     size_t smem[4] = {};          // dynamic shared memory bytes, by loge
+    int split = 1;                // thread blocks per rotation (2: cluster kernel, tile 4 only)
+    const void* pair_kernel = nullptr;
+    size_t pair_smem = 0;
+    int pair_cap = 0;             // resident two-CTA clusters on the device (0: unavailable)
     // workspace for host-pointer calls
     uint64_t* ws = nullptr;
     uint64_t ws_words = 0;
@@ -311,6 +317,27 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         c->grid_caps[lg] = per_sm * sm_count(device);
     }
     c->loge = tp::br_default_loge(c->logn, p->variant);
+    {
+        // two-CTA cluster kernel; optional: a parameter set it does not fit keeps pair_cap = 0
+        const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant);
+        const size_t smem = tp::br_pair_smem_words(c->logn, p->variant, p->lwe_dim, 2) * 8;
+        cudaError_t pe = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int clusters = 0;
+        if (pe == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(2 * (unsigned)sm_count(device));
+            cfg.blockDim = dim3((unsigned)(N >> 2));
+            cfg.dynamicSmemBytes = smem;
+            pe = cudaOccupancyMaxActiveClusters(&clusters, k, &cfg);
+        }
+        if (pe == cudaSuccess && clusters > 0) {
+            c->pair_kernel = k;
+            c->pair_smem = smem;
+            c->pair_cap = clusters;
+        } else {
+            cudaGetLastError();  // clear the optional probe's error
+        }
+    }
     *out = c;
     return TP_OK;
 }
@@ -366,29 +393,7 @@ tp_status tp_br_upload_key(tp_br_ctx* c, const uint64_t* brk, uint64_t words) {
 tp_status tp_br_blind_rotate_batch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
                                    uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
                                    void* stream) {
-    if (!c) return fail(TP_ERR_PARAM, "null context");
-    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
-    if (batch == 0) return TP_OK;
-    if (!results || !lwes || !accs) return fail(TP_ERR_PARAM, "null buffer");
-    if (lwe_stride < (uint64_t)c->prm.lwe_dim + 1) return fail(TP_ERR_PARAM, "lwe_stride below n+1");
-    if (acc_stride != 0 && acc_stride < 2ull * c->prm.ring_dim) return fail(TP_ERR_PARAM, "acc_stride below 2N");
-    if (((uintptr_t)results & 15) || ((uintptr_t)accs & 7) || ((uintptr_t)lwes & 7))
-        return fail(TP_ERR_PARAM, "results must be 16-byte aligned, lwes/accs 8-byte aligned");
-    TP_CUDA(cudaSetDevice(c->device));
-    tp::BrKernelParams kp = c->kp;
-    kp.key = c->key;
-    kp.lwes = lwes;
-    kp.lwe_stride = lwe_stride;
-    kp.accs = accs;
-    kp.acc_stride = acc_stride;
-    kp.out = results;
-    kp.batch = batch;
-    kp.out_coef = out_coef ? 1u : 0u;
-    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
-    void* args[] = {&kp};
-    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args,
-                             c->smem[c->loge], (cudaStream_t)stream));
-    return TP_OK;
+    return tp::br_batch_launch(c, batch, results, lwes, lwe_stride, accs, acc_stride, out_coef, stream, 0);
 }
 
 // Moves the resident key to the layout of another tile (2x key memory while it runs).
@@ -417,18 +422,37 @@ tp_status tp_br_set_tile(tp_br_ctx* c, uint32_t coef_per_thread) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
     if (coef_per_thread != 4 && coef_per_thread != 8) return fail(TP_ERR_PARAM, "coefficients per thread must be 4 or 8");
     std::lock_guard<std::mutex> lk(c->mu);
+    if (coef_per_thread == 8 && c->split == 2)
+        return fail(TP_ERR_STATE, "the two-block kernel runs with 4 coefficients per thread; set the split to 1 first");
     TP_CUDA(cudaSetDevice(c->device));
     return br_retile(c, coef_per_thread == 4 ? 2 : 3);
 }
 
 uint32_t tp_br_get_tile(const tp_br_ctx* c) { return c ? 1u << c->loge : 0u; }
 
+tp_status tp_br_set_split(tp_br_ctx* c, uint32_t blocks_per_rotation) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (blocks_per_rotation != 1 && blocks_per_rotation != 2)
+        return fail(TP_ERR_PARAM, "blocks per rotation must be 1 or 2");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (blocks_per_rotation == 2) {
+        if (c->pair_cap == 0)
+            return fail(TP_ERR_PARAM, "the two-block kernel does not fit this parameter set on this device");
+        if (c->loge != 2)
+            return fail(TP_ERR_STATE, "the two-block kernel runs with 4 coefficients per thread; set the tile first");
+    }
+    c->split = (int)blocks_per_rotation;
+    return TP_OK;
+}
+
+uint32_t tp_br_get_split(const tp_br_ctx* c) { return c ? (uint32_t)c->split : 0u; }
+
 tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_thread, double* best_rotations_per_s) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
     if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
     if (batch == 0) return fail(TP_ERR_PARAM, "empty batch");
     const uint64_t N = c->prm.ring_dim, n = c->prm.lwe_dim;
-    const uint64_t cap = (uint64_t)std::max(c->grid_caps[2], c->grid_caps[3]);
+    const uint64_t cap = (uint64_t)std::max(std::max(c->grid_caps[2], c->grid_caps[3]), c->pair_cap);
     const uint64_t tb = std::min<uint64_t>(batch, 2 * cap);  // at most two waves per trial
     std::vector<uint64_t> lw(tb * (n + 1));
     uint64_t z = 0x5eedull;
@@ -466,9 +490,14 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
         return fail(TP_ERR_CUDA, "autotune set-up: %s", cudaGetErrorString(e));
     }
     std::lock_guard<std::mutex> lk(c->mu);
-    for (int lg : {3, 2}) {
-        s = br_retile(c, lg);
+    int best_split = c->split;
+    struct Cand { int loge, split; };
+    const Cand cands[] = {{3, 1}, {2, 1}, {2, 2}};
+    for (const Cand& cd : cands) {
+        if (cd.split == 2 && c->pair_cap == 0) continue;
+        s = br_retile(c, cd.loge);
         if (s != TP_OK) break;
+        c->split = cd.split;
         for (int rep = 0; rep < 3 && s == TP_OK; ++rep) {  // one warm-up, two timed
             if (rep == 1) cudaEventRecord(e0, st);
             s = tp_br_blind_rotate_batch(c, tb, d_res, d_lwe, n + 1, d_acc, 0, 0, st);
@@ -485,10 +514,13 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
         const double rate = 2.0 * tb / (ms * 1e-3);
         if (rate > best_rate) {
             best_rate = rate;
-            best = lg;
+            best = cd.loge;
+            best_split = cd.split;
         }
     }
+    c->split = 1;
     if (s == TP_OK) s = br_retile(c, best);
+    if (s == TP_OK) c->split = best_split;
     cleanup();
     if (s != TP_OK) return s;
     if (best_coef_per_thread) *best_coef_per_thread = 1u << best;
@@ -1126,3 +1158,49 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
     TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
     return TP_OK;
 }
+
+namespace tp {
+
+uint64_t br_concurrency(const tp_br_ctx* c, int split) {
+    if (!c) return 0;
+    if (split == 2) return c->loge == 2 ? (uint64_t)c->pair_cap : 0;
+    return (uint64_t)c->grid_caps[c->loge];
+}
+
+tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                          uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef, void* stream,
+                          int split) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (batch == 0) return TP_OK;
+    if (!results || !lwes || !accs) return fail(TP_ERR_PARAM, "null buffer");
+    if (lwe_stride < (uint64_t)c->prm.lwe_dim + 1) return fail(TP_ERR_PARAM, "lwe_stride below n+1");
+    if (acc_stride != 0 && acc_stride < 2ull * c->prm.ring_dim) return fail(TP_ERR_PARAM, "acc_stride below 2N");
+    if (((uintptr_t)results & 15) || ((uintptr_t)accs & 7) || ((uintptr_t)lwes & 7))
+        return fail(TP_ERR_PARAM, "results must be 16-byte aligned, lwes/accs 8-byte aligned");
+    if (split == 0) split = c->split;
+    if (split == 2 && br_concurrency(c, 2) == 0) split = 1;
+    TP_CUDA(cudaSetDevice(c->device));
+    BrKernelParams kp = c->kp;
+    kp.key = c->key;
+    kp.lwes = lwes;
+    kp.lwe_stride = lwe_stride;
+    kp.accs = accs;
+    kp.acc_stride = acc_stride;
+    kp.out = results;
+    kp.batch = batch;
+    kp.out_coef = out_coef ? 1u : 0u;
+    void* args[] = {&kp};
+    if (split == 2) {
+        const unsigned pairs = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->pair_cap);
+        TP_CUDA(cudaLaunchKernel(c->pair_kernel, dim3(2 * pairs), dim3(c->prm.ring_dim >> 2), args, c->pair_smem,
+                                 (cudaStream_t)stream));
+        return TP_OK;
+    }
+    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
+    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args,
+                             c->smem[c->loge], (cudaStream_t)stream));
+    return TP_OK;
+}
+
+}  // namespace tp

@@ -15,6 +15,12 @@ const void* br_kernel_ptr_11(int variant, int loge);
 const void* ntt_kernel_ptr_11(bool forward);
 const void* br_kernel_ptr_12(int variant, int loge);
 const void* ntt_kernel_ptr_12(bool forward);
+const void* br_pair_kernel_ptr_7(int variant);
+const void* br_pair_kernel_ptr_8(int variant);
+const void* br_pair_kernel_ptr_9(int variant);
+const void* br_pair_kernel_ptr_10(int variant);
+const void* br_pair_kernel_ptr_11(int variant);
+const void* br_pair_kernel_ptr_12(int variant);
 const void* ks_kernel_ptr_7(int mode);
 const void* ks_kernel_ptr_8(int mode);
 const void* ks_kernel_ptr_9(int mode);
@@ -30,6 +36,19 @@ inline const void* br_kernel_lookup(int logn, int variant, int loge) {
         case 10: return br_kernel_ptr_10(variant, loge);
         case 11: return br_kernel_ptr_11(variant, loge);
         case 12: return br_kernel_ptr_12(variant, loge);
+        default: return nullptr;
+    }
+}
+
+// Two-CTA (cluster) rotation kernel, 4 coefficients per thread.
+inline const void* br_pair_kernel_lookup(int logn, int variant) {
+    switch (logn) {
+        case 7: return br_pair_kernel_ptr_7(variant);
+        case 8: return br_pair_kernel_ptr_8(variant);
+        case 9: return br_pair_kernel_ptr_9(variant);
+        case 10: return br_pair_kernel_ptr_10(variant);
+        case 11: return br_pair_kernel_ptr_11(variant);
+        case 12: return br_pair_kernel_ptr_12(variant);
         default: return nullptr;
     }
 }

@@ -1,6 +1,7 @@
 // Kernel instantiations for N = 128 (compiled as a separate unit so the
 // ring sizes build in parallel).
 #include "br_kernels.cuh"
+#include "br_pair_kernel.cuh"
 #include "dispatch.h"
 #include "ks_kernels.cuh"
 #include "misc_kernels.cuh"
@@ -19,6 +20,14 @@ const void* br_kernel_ptr_7(int variant, int loge) {
         case kCggiBinary: return (const void*)br_kernel<7, kCggiBinary, 3>;
         case kCggiTernary: return (const void*)br_kernel<7, kCggiTernary, 3>;
         default: return (const void*)br_kernel<7, kBmmpBinary, 3>;
+    }
+}
+
+const void* br_pair_kernel_ptr_7(int variant) {
+    switch (variant) {
+        case kCggiBinary: return (const void*)br_pair_kernel<7, kCggiBinary, 2>;
+        case kCggiTernary: return (const void*)br_pair_kernel<7, kCggiTernary, 2>;
+        default: return (const void*)br_pair_kernel<7, kBmmpBinary, 2>;
     }
 }
 

@@ -11,7 +11,8 @@
 // while the earlier launches are still in flight (different streams, so their
 // blocks overlap on the SMs). Keys and tables stay resident in the contexts.
 // A request's result depends only on its own inputs: batching changes which
-// launch and slot it runs in, never the words it produces.
+// launch, slot and kernel (one or two blocks per rotation, chosen per launch by
+// its size) it runs in, never the words it produces.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +28,7 @@
 #include <vector>
 
 #include "toothpaste_gpu.h"
+#include "br_launch.h"
 
 namespace {
 
@@ -124,8 +126,11 @@ void launch_pending(tp_server* srv, uint32_t si) {
         srv->queued -= take;
         cudaError_t e = cudaMemcpyAsync(b.d_lwe, b.h_lwe, take * lw * 8, cudaMemcpyHostToDevice, b.stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b.d_acc, b.h_acc, take * aw * 8, cudaMemcpyHostToDevice, b.stream);
-        tp_status st = e == cudaSuccess ? tp_br_blind_rotate_batch(s.ctx, take, b.d_res, b.d_lwe, lw, b.d_acc, aw,
-                                                                  s.out_coef, b.stream)
+        // A launch that leaves SMs idle runs each rotation on two SMs (half the
+        // latency); a launch of a full wave or more runs one block per rotation.
+        const int split = take <= tp::br_concurrency(s.ctx, 2) ? 2 : 1;
+        tp_status st = e == cudaSuccess ? tp::br_batch_launch(s.ctx, take, b.d_res, b.d_lwe, lw, b.d_acc, aw,
+                                                               s.out_coef, b.stream, split)
                                         : TP_ERR_CUDA;
         if (st == TP_OK) e = cudaMemcpyAsync(b.h_res, b.d_res, take * aw * 8, cudaMemcpyDeviceToHost, b.stream);
         if (st == TP_OK && e == cudaSuccess) e = cudaEventRecord(b.done, b.stream);

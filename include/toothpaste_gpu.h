@@ -108,9 +108,22 @@ tp_status tp_br_blind_rotate_batch_host(tp_br_ctx* ctx, uint64_t batch, uint64_t
 tp_status tp_br_set_tile(tp_br_ctx* ctx, uint32_t coef_per_thread);
 uint32_t tp_br_get_tile(const tp_br_ctx* ctx);
 
-/* Times every tile on up to two waves of `batch` synthetic rotations with the
- * uploaded key, keeps the fastest and reports it (either output may be NULL).
- * Blocks until done; the context must be idle. */
+/* Thread blocks per rotation: 1 (default) or 2. With 2, a cluster of two
+ * blocks on two SMs rotates each ciphertext, each block owning one accumulator
+ * half and its gadget rows and exchanging partial sums with the other through
+ * distributed shared memory: half the latency per rotation, for batches smaller
+ * than the number of SMs (large batches run faster with 1). Needs the tile of
+ * 4 coefficients per thread; TP_ERR_PARAM if the parameter set does not fit the
+ * two-block kernel on this device. Same output words either way. No reference
+ * counterpart. */
+tp_status tp_br_set_split(tp_br_ctx* ctx, uint32_t blocks_per_rotation);
+uint32_t tp_br_get_split(const tp_br_ctx* ctx);
+
+/* Times every tile (8 or 4 coefficients per thread, and 4 with two blocks per
+ * rotation) on up to two waves of `batch` synthetic rotations with the uploaded
+ * key, keeps the fastest and reports it (either output may be NULL; the split
+ * is read back with tp_br_get_split). Blocks until done; the context must be
+ * idle. */
 tp_status tp_br_autotune(tp_br_ctx* ctx, uint64_t batch, uint32_t* best_coef_per_thread,
                          double* best_rotations_per_s);
 

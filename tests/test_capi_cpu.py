@@ -51,4 +51,7 @@ def test_null_context_calls_fail_cleanly(native):
     assert native.tp_br_blind_rotate(None, None, None, None, 0) == _native.TP_ERR_PARAM
     assert native.tp_br_check(None, None) == _native.TP_ERR_PARAM
     assert native.tp_br_key_words(None) == 0
+    assert native.tp_br_set_split(None, 2) == _native.TP_ERR_PARAM
+    assert native.tp_br_get_split(None) == 0
+    assert native.tp_br_set_tile(None, 4) == _native.TP_ERR_PARAM
     assert native.tp_ntt_forward(1000, 1, None, None, None) == _native.TP_ERR_PARAM

@@ -187,3 +187,53 @@ def test_autotune_picks_a_tile_and_keeps_results(native, oracle, golden):
     lwes, accs, coefs = case_inputs(name, case)
     idx = [i for i, c in enumerate(coefs) if c == 0]
     np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[idx], accs[idx]), golden[1][f"br_{name}"][idx])
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_two_block_rotation_matches_reference(native, oracle, golden, name):
+    """Two thread blocks per ciphertext (cluster kernel): same words as the reference."""
+    case, rot = rotator(oracle, golden, name)
+    rot.set_tile(4)
+    rot.set_split(2)
+    assert rot.split == 2
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for oc in (0, 1):
+        idx = [i for i, c in enumerate(coefs) if c == oc]
+        got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+        np.testing.assert_array_equal(got, expect[idx], err_msg="two blocks per rotation")
+    # one ciphertext through the reference-signature call, result aliasing the accumulator
+    res = np.ascontiguousarray(accs[0])
+    rot.BlindRotate(res, np.ascontiguousarray(lwes[0]), res, bool(coefs[0]))
+    np.testing.assert_array_equal(res, expect[0])
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_two_block_batches_of_any_size(native, oracle, golden, name):
+    """Batch 1, 37 and more pairs than fit on the device (pairs loop over ciphertexts)."""
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    rot.set_split(2)
+    for batch in (1, 37, 2 * 148 + 3):
+        lwes = lwe_inputs(N, n, batch, 500 + batch)
+        accs = random_acc(N, batch, 600 + batch)
+        got = rot.blind_rotate_batch_host(lwes, accs, out_coef=False)
+        for b in sorted({0, batch // 2, batch - 1}):
+            exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b],
+                                      accs[b], 0)
+            np.testing.assert_array_equal(got[b], exp, err_msg=f"batch {batch}, ciphertext {b}")
+
+
+def test_two_block_split_needs_tile_of_four(native, oracle, golden):
+    from fhetoothpaste_b200 import TpError
+    case, rot = rotator(oracle, golden, "small_binary_n256")
+    rot.set_tile(8)
+    with pytest.raises(TpError):
+        rot.set_split(2)
+    rot.set_tile(4)
+    rot.set_split(2)
+    with pytest.raises(TpError):
+        rot.set_tile(8)
+    rot.set_split(1)
+    rot.set_tile(8)
