@@ -7,5 +7,5 @@ from ._native import GOLDILOCKS, TP_BR_BMMP_BINARY, TP_BR_CGGI_BINARY, TP_BR_CGG
 from .blind_rotation import (BatchGraph, BlindRotationContext, GpuBlindRotator, ntt_backward, ntt_forward,  # noqa: F401
                              sample_extract_batch)
 from .key_switching import (GpuAutomorphismEvaluator, GpuLWEtoLWEConverter, GpuLWEtoRLWEPacker,  # noqa: F401,E402
-                            GpuRLWEtoRLWEConverter)
+                            GpuRLWEtoRLWEConverter, modulus_switch_batch)
 from .serving import BootstrapServer  # noqa: F401,E402

@@ -22,6 +22,7 @@ STATUS_NAMES = {0: "TP_OK", 1: "TP_ERR_PARAM", 2: "TP_ERR_OOM", 3: "TP_ERR_CUDA"
                 5: "TP_ERR_LAYOUT", 6: "TP_ERR_STATE"}
 
 TP_BR_CGGI_BINARY, TP_BR_CGGI_TERNARY, TP_BR_BMMP_BINARY = 0, 1, 2
+TP_MS_ROUND, TP_MS_FLOOR, TP_MS_CEIL = 0, 1, 2
 GOLDILOCKS = 0xFFFFFFFF00000001
 
 
@@ -85,6 +86,9 @@ def lib() -> ctypes.CDLL:
         "tp_lwe_ks_key_words": (U64, [VP]),
         "tp_lwe_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
         "tp_lwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_modulus_switch_batch": (ctypes.c_int, [U64, VP, U64, U64, ctypes.c_int, VP]),
+        "tp_pbs_epilogue_batch": (ctypes.c_int, [VP, U64, VP, VP, U64, VP]),
+        "tp_pbs_graph_create": (ctypes.c_int, [VP, VP, U64, VP, VP, VP, U64, VP, ctypes.POINTER(VP)]),
         "tp_server_create": (ctypes.c_int, [ctypes.c_int, U64, ctypes.POINTER(VP)]),
         "tp_server_add_set": (ctypes.c_int, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),

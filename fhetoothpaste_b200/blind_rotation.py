@@ -131,6 +131,14 @@ class GpuBlindRotator:
                                                      acc_stride, int(bool(out_coef)), extract_ptr, ctypes.byref(g)))
         return BatchGraph(g, self)
 
+    def capture_bootstrap(self, key_switch, batch: int, rlwe_scratch_ptr: int, lwes_ptr: int, accs_ptr: int,
+                          acc_stride: int, out_lwe_ptr: int) -> "BatchGraph":
+        """Records rotation (coefficient output) + SampleExtract + LWE key switch + FLOOR switch to 2N."""
+        g = ctypes.c_void_p()
+        nat.check(nat.lib().tp_pbs_graph_create(self._h, key_switch._h, batch, rlwe_scratch_ptr, lwes_ptr, accs_ptr,
+                                                acc_stride, out_lwe_ptr, ctypes.byref(g)))
+        return BatchGraph(g, (self, key_switch))
+
 
 class BatchGraph:
     """A recorded batch launch; replays read the device buffers' current contents."""

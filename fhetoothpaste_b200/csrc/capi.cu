@@ -1026,6 +1026,96 @@ tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* c, uint64_t batch, uint64_t* out, const
     return TP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Modulus switch and the bootstrap epilogue
+// ---------------------------------------------------------------------------
+static int pow2_log2(uint64_t t) {
+    if (t < 2 || (t & (t - 1)) || t > (1ull << 32)) return 0;
+    return ilog2(t);
+}
+
+tp_status tp_modulus_switch_batch(uint64_t count, uint64_t* vec, uint64_t source_modulus, uint64_t target_modulus,
+                                  int type, void* stream) {
+    if (source_modulus != kP) return fail(TP_ERR_PARAM, "the GPU modulus switch takes the Goldilocks modulus as source");
+    const int k = pow2_log2(target_modulus);
+    if (!k) return fail(TP_ERR_PARAM, "target modulus must be a power of two in [2, 2^32]");
+    if (type != TP_MS_FLOOR)
+        return fail(TP_ERR_PARAM, "only FLOOR is computed on the GPU (the type the bootstrap path uses)");
+    if (count == 0) return TP_OK;
+    if (!vec) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 65535);
+    tp::ms_floor_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vec, count, (uint32_t)k);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
+tp_status tp_pbs_epilogue_batch(tp_lwe_ks_ctx* c, uint64_t batch, uint64_t* out_lwe, const uint64_t* rlwe_coef,
+                                uint64_t target_modulus, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
+    if (c->n_in < 2 || (c->n_in & (c->n_in - 1)))
+        return fail(TP_ERR_PARAM, "the key switch's input dimension must be the ring dimension N (a power of two)");
+    const int k = pow2_log2(target_modulus);
+    if (!k) return fail(TP_ERR_PARAM, "target modulus must be a power of two in [2, 2^32]");
+    if (batch == 0) return TP_OK;
+    if (!out_lwe || !rlwe_coef) return fail(TP_ERR_PARAM, "null buffer");
+    if (batch > 65535ull * tp::kLweKsRows) return fail(TP_ERR_PARAM, "batch too large for one launch");
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::LweKsParams kp = c->kp;
+    kp.ksk = c->key;
+    kp.in = rlwe_coef;
+    kp.out = out_lwe;
+    kp.batch = batch;
+    kp.rlwe_in = 1;
+    kp.ms_log2 = (uint32_t)k;
+    dim3 grid((c->n_out + 1 + tp::kLweKsCols - 1) / tp::kLweKsCols,
+              (unsigned)((batch + tp::kLweKsRows - 1) / tp::kLweKsRows));
+    tp::lwe_ks_kernel<<<grid, tp::kLweKsCols, 0, (cudaStream_t)stream>>>(kp);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
+tp_status tp_pbs_graph_create(tp_br_ctx* br, tp_lwe_ks_ctx* ks, uint64_t batch, uint64_t* rlwe_scratch,
+                              const uint64_t* lwes, const uint64_t* accs, uint64_t acc_stride, uint64_t* out_lwe,
+                              tp_graph** out) {
+    if (!br || !ks || !out) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    if (batch == 0) return fail(TP_ERR_PARAM, "empty batch");
+    if (ks->n_in != br->prm.ring_dim)
+        return fail(TP_ERR_PARAM, "the key switch's input dimension (%u) must be the rotation's ring dimension (%u)",
+                    ks->n_in, br->prm.ring_dim);
+    if (ks->device != br->device) return fail(TP_ERR_PARAM, "contexts live on different devices");
+    TP_CUDA(cudaSetDevice(br->device));
+    cudaStream_t s = nullptr;
+    TP_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s);
+        return fail(TP_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    }
+    tp_status st = tp_br_blind_rotate_batch(br, batch, rlwe_scratch, lwes, (uint64_t)br->prm.lwe_dim + 1, accs,
+                                            acc_stride, 1, s);
+    if (st == TP_OK) st = tp_pbs_epilogue_batch(ks, batch, out_lwe, rlwe_scratch, 2ull * br->prm.ring_dim, s);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);
+    cudaStreamDestroy(s);
+    if (st != TP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(TP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    auto* gr = new tp_graph();
+    gr->device = br->device;
+    e = cudaGraphInstantiate(&gr->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        delete gr;
+        return fail(TP_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = gr;
+    return TP_OK;
+}
+
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd) {
     if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))

@@ -36,10 +36,12 @@ __global__ void pack_l0_kernel(uint64_t* __restrict__ nodes, const uint64_t* __r
 // ---------------------------------------------------------------------------
 struct LweKsParams {
     const uint64_t* ksk;      // reference layout: [i][j][n_out + 1]
-    const uint64_t* in;       // batch x (n_in + 1)
+    const uint64_t* in;       // batch x (n_in + 1); or, with rlwe_in, batch x 2N RLWEs (coefficients)
     uint64_t* out;            // batch x (n_out + 1)
     uint64_t batch;
     uint32_t n_in, n_out, digits;
+    uint32_t rlwe_in;         // 1: input row = SampleExtract(index 0) of an RLWE with N = n_in
+    uint32_t ms_log2;         // k > 0: write floor(out * 2^k / p) into a fresh output (PBS epilogue)
     uint64_t corr;
     uint32_t dshift[8];
     uint64_t dmask[8];
@@ -49,6 +51,35 @@ struct LweKsParams {
 constexpr int kLweKsRows = 16;     // ciphertexts per block
 constexpr int kLweKsCols = 128;    // output words per block (= threads)
 constexpr int kLweKsChunk = 32;    // input coefficients staged per round
+
+// floor(v 2^k / p) for 1 <= k <= 32: v 2^k = hi 2^64 + lo and v 2^k - hi p =
+// lo + hi (2^32 - 1) lies in [0, 2p), so the quotient is hi or hi + 1. This is
+// also the reference's long-double FLOOR switch (modulus_switching.cpp:43-48):
+// with p = 1 (mod 2^k) every quotient q is at least q/p away from the integer
+// above it, more than half a 64-bit-mantissa ulp, so rounding the quotient to
+// long double never carries it over an integer.
+__device__ __forceinline__ uint64_t ms_floor_pow2(uint64_t v, uint32_t k) {
+    const uint64_t hi = v >> (64 - k), lo = v << k;
+    const uint64_t m = (hi << 32) - hi;
+    const uint64_t r = lo + m;
+    return hi + ((r < lo || r >= kP) ? 1u : 0u);
+}
+
+__global__ void ms_floor_kernel(uint64_t* __restrict__ vec, uint64_t count, uint32_t k) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
+        vec[i] = ms_floor_pow2(vec[i], k);
+}
+
+// Input word i (< n_in) and the body word of ciphertext row `row`: an LWE row, or
+// SampleExtract at index 0 of an RLWE [A | B] (a_0 = A[0], a_i = -A[N - i], b = B[0]).
+__device__ __forceinline__ uint64_t lwe_ks_in_word(const LweKsParams& prm, uint64_t row, uint32_t i) {
+    if (!prm.rlwe_in) return prm.in[row * (prm.n_in + 1) + i];
+    const uint64_t* r = prm.in + row * 2ull * prm.n_in;
+    return i == 0 ? r[0] : gl_neg(r[prm.n_in - i]);
+}
+__device__ __forceinline__ uint64_t lwe_ks_in_body(const LweKsParams& prm, uint64_t row) {
+    return prm.rlwe_in ? prm.in[row * 2ull * prm.n_in + prm.n_in] : prm.in[row * (prm.n_in + 1) + prm.n_in];
+}
 
 __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams prm) {
     __shared__ uint64_t dig[kLweKsRows][kLweKsChunk * 8];
@@ -66,7 +97,7 @@ __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams pr
         for (uint32_t e = t; e < kLweKsRows * ni; e += kLweKsCols) {
             const uint32_t r = e / ni, ii = e % ni;
             uint64_t x = 0;
-            if (row0 + r < prm.batch) x = gl_add(prm.in[(row0 + r) * (prm.n_in + 1) + i0 + ii], prm.corr);
+            if (row0 + r < prm.batch) x = gl_add(lwe_ks_in_word(prm, row0 + r, i0 + ii), prm.corr);
             for (uint32_t j = 0; j < L; ++j)
                 dig[r][ii * L + j] = row0 + r < prm.batch ? gl_sub((x >> prm.dshift[j]) & prm.dmask[j], prm.ddelta[j]) : 0;
         }
@@ -85,8 +116,13 @@ __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams pr
             const uint64_t row = row0 + r;
             if (row >= prm.batch) break;
             uint64_t* o = prm.out + row * width;
-            const uint64_t base = col == prm.n_out ? prm.in[row * (prm.n_in + 1) + prm.n_in] : o[col];
-            o[col] = gl_sub(base, gl_canon(acc[r]));
+            if (prm.ms_log2) {
+                const uint64_t base = col == prm.n_out ? lwe_ks_in_body(prm, row) : 0;
+                o[col] = ms_floor_pow2(gl_sub(base, gl_canon(acc[r])), prm.ms_log2);
+            } else {
+                const uint64_t base = col == prm.n_out ? lwe_ks_in_body(prm, row) : o[col];
+                o[col] = gl_sub(base, gl_canon(acc[r]));
+            }
         }
     }
 }

@@ -120,8 +120,18 @@ class GpuLWEtoLWEConverter:
     def convert_batch(self, batch: int, out_ptr: int, in_ptr: int, stream=None) -> None:
         nat.check(nat.lib().tp_lwe_ks_batch(self._h, batch, out_ptr, in_ptr, stream))
 
+    def pbs_epilogue_batch(self, batch: int, out_ptr: int, rlwe_ptr: int, target_modulus: int, stream=None) -> None:
+        """SampleExtract(0) of each RLWE (coefficients, N = n_in) -> this key switch -> FLOOR switch to target."""
+        nat.check(nat.lib().tp_pbs_epilogue_batch(self._h, batch, out_ptr, rlwe_ptr, target_modulus, stream))
+
     def Convert(self, out: np.ndarray, inp: np.ndarray) -> None:
         import torch
         d_in, d_out = _dev(torch, inp), _dev(torch, out)
         self.convert_batch(d_in.numel() // (self.n_in + 1), d_out.data_ptr(), d_in.data_ptr())
         out[...] = d_out.cpu().numpy().view(np.uint64).reshape(out.shape)
+
+
+def modulus_switch_batch(count: int, vec_ptr: int, target_modulus: int, stream=None) -> None:
+    """In-place FLOOR modulus switch of `count` device words from p to a power of two."""
+    nat.check(nat.lib().tp_modulus_switch_batch(count, vec_ptr, nat.GOLDILOCKS, target_modulus, nat.TP_MS_FLOOR,
+                                                stream))

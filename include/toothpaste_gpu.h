@@ -246,6 +246,37 @@ tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* ctx, const uint64_t* key_host, uin
  * pre-zeroed). Asynchronous. */
 tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev, void* stream);
 
+/* ModulusSwitch (lib/src/static/modulus_switching.cpp:36-93) in place on a
+ * device vector: source must be the Goldilocks prime p, target a power of two
+ * up to 2^32 (2N), type TP_MS_FLOOR. The result equals the reference's 80-bit
+ * long-double floorl((target * v) / p) word for word; ROUND and CEIL are not
+ * computed here (TP_ERR_PARAM). */
+#define TP_MS_ROUND 0
+#define TP_MS_FLOOR 1
+#define TP_MS_CEIL 2
+tp_status tp_modulus_switch_batch(uint64_t count, uint64_t* vec_dev, uint64_t source_modulus,
+                                  uint64_t target_modulus, int type, void* stream);
+
+/* The bootstrap epilogue, fused: SampleExtract at index 0 of each RLWE
+ * (coefficient domain, batch x 2N words), LWE->LWE key switch with `ks`
+ * (n_in = N, fresh output), then the FLOOR switch to `target_modulus` (2N to
+ * feed the next blind rotation): out gets batch x (n_out + 1) words. This is
+ * the refresh step of SAPDecomposer (lib/src/operators/sap_decomposer.cpp:353-
+ * 369: SampleExtract, LWEtoLWEConverter::Convert, ModulusSwitch FLOOR to 2N)
+ * for Qks = Q. */
+tp_status tp_pbs_epilogue_batch(tp_lwe_ks_ctx* ks, uint64_t batch, uint64_t* out_lwe_dev,
+                                const uint64_t* rlwe_coef_dev, uint64_t target_modulus, void* stream);
+
+/* One graph for a whole bootstrap batch: blind rotation (coefficient output
+ * into rlwe_scratch_dev, batch x 2N words) followed by tp_pbs_epilogue_batch
+ * to 2N. The output LWEs (dimension n_out of `ks`) feed the next rotation with
+ * a context whose lwe_dim is n_out. Replay with tp_graph_launch. No reference
+ * counterpart as one call. */
+tp_status tp_pbs_graph_create(tp_br_ctx* br, tp_lwe_ks_ctx* ks, uint64_t batch, uint64_t* rlwe_scratch_dev,
+                              const uint64_t* lwes_dev, const uint64_t* accs_dev, uint64_t acc_stride,
+                              uint64_t* out_lwe_dev, tp_graph** out);
+
+
 /* ---- Serving loop -------------------------------------------------------- */
 /* Continuous batching of single bootstrap requests over several resident
  * parameter sets (no reference counterpart: the reference rotates one

@@ -149,6 +149,7 @@ class Oracle:
             "tpo_pack_keygen": (None, [R, U64, U64, U64, D, U64P, U64P]),
             "tpo_pack": (I, [U64, U64, U64, U64P, U64P, U64P, U64]),
             "tpo_sample_extract": (None, [U64P, U64P, U64, U64]),
+            "tpo_modulus_switch": (I, [U64P, U64, U64, U64, I]),
             "tpo_psi": (U64, [U64]),
             "tpo_mul": (U64, [U64, U64]),
         }
@@ -265,6 +266,25 @@ class Oracle:
         self.L.tpo_lwe_ks(q, n_in, n_out, bl, dg, ptr(ksk), ptr(out), ptr(np.ascontiguousarray(inp, np.uint64)))
         return out
 
+    def modulus_switch(self, vec, source, target, kind) -> np.ndarray:
+        """ModulusSwitch; kind 'round' | 'floor' | 'ceil'."""
+        out = np.array(vec, dtype=np.uint64)
+        assert self.L.tpo_modulus_switch(ptr(out), out.size, source, target,
+                                         {"round": 0, "floor": 1, "ceil": 2}[kind]) == 0
+        return out
+
+    def sample_extract(self, rlwe: np.ndarray) -> np.ndarray:
+        N = rlwe.size // 2
+        out = np.zeros(N + 1, np.uint64)
+        self.L.tpo_sample_extract(ptr(out), ptr(np.ascontiguousarray(rlwe, np.uint64)), 0, N)
+        return out
+
+    def pbs_epilogue(self, rlwe_coef, n_out, bl, dg, ksk, target):
+        """SampleExtract (index 0) -> LWE key switch (fresh output) -> FLOOR switch to `target`."""
+        N = rlwe_coef.size // 2
+        ks = self.lwe_ks(P, N, n_out, bl, dg, ksk, self.sample_extract(rlwe_coef))
+        return self.modulus_switch(ks, P, target, "floor")
+
     def phase_rlwe(self, rlwe_ntt: np.ndarray, sk: np.ndarray) -> np.ndarray:
         N = sk.size
         sk_ntt = self.ntt_forward(sk)
@@ -316,6 +336,7 @@ class Reference:
             "ref_pack_key_copy": (None, [VP, U64P]),
             "ref_pack_destroy": (None, [VP]),
             "ref_sample_extract": (None, [U64P, U64P, U64, U64]),
+            "ref_modulus_switch": (None, [U64P, U64, U64, U64, I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

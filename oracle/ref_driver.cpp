@@ -24,6 +24,7 @@
 #include "operators/endo_glwe_conversion.h"
 #include "operators/lwe_to_rlwe_packing.h"
 #include "static/keys.h"
+#include "static/modulus_switching.h"
 #include "static/sample_extraction.h"
 #undef private
 #undef protected
@@ -223,6 +224,12 @@ void ref_pack_destroy(void* hp) { delete (LWEtoRLWEPacker*)hp; }
 
 void ref_sample_extract(uint64_t* out_lwe, uint64_t* rlwe, uint64_t index, uint64_t N) {
     SampleExtract<uint64_t>(out_lwe, rlwe, index, N, kQ);
+}
+
+// type: 0 ROUND, 1 FLOOR, 2 CEIL (ModulusSwitchType order)
+void ref_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type) {
+    const ModulusSwitchType t[] = {ModulusSwitchType::ROUND, ModulusSwitchType::FLOOR, ModulusSwitchType::CEIL};
+    ModulusSwitch(vec, n, source, target, t[type]);
 }
 
 }  // extern "C"

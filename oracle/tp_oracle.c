@@ -832,3 +832,27 @@ void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index,
     }
     out_lwe[N] = rlwe[N + index];
 }
+
+/* ------------------------------------------------------------------------- */
+/* modulus switching                                                         */
+/* ------------------------------------------------------------------------- */
+
+/* ModulusSwitch (lib/src/static/modulus_switching.cpp:36-93) for the FLOOR,
+ * CEIL and ROUND types, in x86 80-bit long double exactly as the reference
+ * computes it: (target * (long double)v) / source, then floorl / ceill /
+ * roundl, then one conditional subtraction of the target. type: 0 ROUND,
+ * 1 FLOOR, 2 CEIL (lib/include/static/modulus_switching.h:24-29). */
+int tpo_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type) {
+    const long double sM = (long double)source, tM = (long double)target;
+    for (uint64_t i = 0; i < n; ++i) {
+        const long double v = (tM * (long double)vec[i]) / sM;
+        uint64_t r;
+        if (type == 0) r = (uint64_t)roundl(v);
+        else if (type == 1) r = (uint64_t)floorl(v);
+        else if (type == 2) r = (uint64_t)ceill(v);
+        else return -1;
+        if (r >= target) r -= target;
+        vec[i] = r;
+    }
+    return 0;
+}

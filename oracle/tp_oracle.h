@@ -125,6 +125,10 @@ int tpo_pack(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* k
  * where the source coefficient is zero (the caller pre-zeroes). */
 void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index, uint64_t N);
 
+/* ModulusSwitch (lib/src/static/modulus_switching.cpp:36-93), types 0 ROUND,
+ * 1 FLOOR, 2 CEIL, in 80-bit long double like the reference; in place. */
+int tpo_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type);
+
 #ifdef __cplusplus
 }
 #endif
