@@ -301,6 +301,37 @@ def packing_run(device: int) -> dict:
             "launches": 3 * per_pack_launch + 7}
 
 
+def bootstrap_run(device: int) -> dict:
+    """Whole bootstraps (config-1 shape: CGGI binary n=500, N=1024, base 2^16 l=4): blind rotation
+    with coefficient output, SampleExtract, LWE key switch N=1024 -> n=500 (base 2^16, l=4) and the
+    FLOOR switch to 2N, recorded as one graph over a batch of 4096; the output LWEs are valid inputs
+    of the next rotation."""
+    import torch
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator, GpuLWEtoLWEConverter
+    from oracle.oracle import lwe_inputs
+    N, n, beta, l, batch = 1024, 500, 16, 4, 4096
+    stream = torch.cuda.current_stream().cuda_stream
+    ctx = BlindRotationContext(0, N, n, 1 << beta, l)
+    rot = GpuBlindRotator(ctx, _uniform_key(ctx.key_words(), 51), device=device)
+    conv = GpuLWEtoLWEConverter(N, n, 1 << beta, l, _uniform_key(N * l * (n + 1), 52), device=device)
+    lw = torch.from_numpy(lwe_inputs(N, n, batch, 53).view(np.int64)).cuda()
+    ac = torch.from_numpy(lut_polys(N, batch, 54).view(np.int64)).cuda()
+    rl = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    out = torch.empty((batch, n + 1), dtype=torch.int64, device="cuda")
+    g = rot.capture_bootstrap(conv, batch, rl.data_ptr(), lw.data_ptr(), ac.data_ptr(), 2 * N, out.data_ptr())
+    ms = _timed(torch, lambda: g.launch(stream), 2, 3, stream)
+    g.close()
+    rot.check(stream)
+    # the epilogue alone, for its share of the bootstrap
+    ep = _timed(torch, lambda: conv.pbs_epilogue_batch(batch, out.data_ptr(), rl.data_ptr(), 2 * N, stream), 1, 3,
+                stream)
+    rot.close()
+    conv.close()
+    return {"workload": "bootstrap: CGGI binary n=500 N=1024 2^16 l=4 + extract + LWE KS 1024->500 + switch to 2N",
+            "batch": batch, "bootstraps_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
+            "epilogue_ms": round(ep, 3), "launches": 2 * 5 + 4 + 1}  # graphs x 2 kernels, epilogues, key upload
+
+
 SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l = 3
 SERVING_MIX = [0.5, 0.35, 0.15]
 
@@ -521,7 +552,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         line["bmmp_batches"] = bmmp_batch_sweep(local)
         line["packing"] = packing_run(local)
-        launches += line["bmmp_batches"].pop("launches") + line["packing"].pop("launches")
+        line["bootstrap"] = bootstrap_run(local)
+        launches += (line["bmmp_batches"].pop("launches") + line["packing"].pop("launches") +
+                     line["bootstrap"].pop("launches"))
         line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
