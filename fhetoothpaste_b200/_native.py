@@ -86,6 +86,12 @@ def lib() -> ctypes.CDLL:
         "tp_lwe_ks_key_words": (U64, [VP]),
         "tp_lwe_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
         "tp_lwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_key_file_write": (ctypes.c_int, [ctypes.c_char_p, VP, U64P]),
+        "tp_key_file_info": (ctypes.c_int, [ctypes.c_char_p, VP]),
+        "tp_key_file_read": (ctypes.c_int, [ctypes.c_char_p, VP, U64P, U64]),
+        "tp_br_upload_key_file": (ctypes.c_int, [VP, ctypes.c_char_p]),
+        "tp_ks_upload_key_file": (ctypes.c_int, [VP, ctypes.c_char_p]),
+        "tp_lwe_ks_upload_key_file": (ctypes.c_int, [VP, ctypes.c_char_p]),
         "tp_modulus_switch_batch": (ctypes.c_int, [U64, VP, U64, U64, ctypes.c_int, VP]),
         "tp_pbs_epilogue_batch": (ctypes.c_int, [VP, U64, VP, VP, U64, VP]),
         "tp_pbs_graph_create": (ctypes.c_int, [VP, VP, U64, VP, VP, VP, U64, VP, ctypes.POINTER(VP)]),

@@ -43,7 +43,8 @@ class BlindRotationContext:
 class GpuBlindRotator:
     """A blind-rotation key resident on one GPU plus its launch context."""
 
-    def __init__(self, ctx: BlindRotationContext, brk: np.ndarray, device: int = 0):
+    def __init__(self, ctx: BlindRotationContext, brk: np.ndarray | None, device: int = 0, key_file=None):
+        """`brk` in the reference's m_brk layout, or `key_file` (a key file of kind blind_rotation)."""
         L = nat.lib()
         self.ctx = ctx
         self.device = device
@@ -51,8 +52,19 @@ class GpuBlindRotator:
         prm = ctx.params()
         nat.check(L.tp_br_create(ctypes.byref(prm), device, ctypes.byref(h)))
         self._h = h
-        brk = np.ascontiguousarray(brk, dtype=np.uint64)
-        nat.check(L.tp_br_upload_key(self._h, nat.ptr(brk), brk.size))
+        if key_file is not None:
+            nat.check(L.tp_br_upload_key_file(self._h, str(key_file).encode()))
+        else:
+            brk = np.ascontiguousarray(brk, dtype=np.uint64)
+            nat.check(L.tp_br_upload_key(self._h, nat.ptr(brk), brk.size))
+
+    @classmethod
+    def from_key_file(cls, path, device: int = 0) -> "GpuBlindRotator":
+        """Context and key from a key file (parameters read from its header)."""
+        from .keyfile import key_file_info
+        i = key_file_info(path)
+        ctx = BlindRotationContext(i["variant"], i["ring_dim"], i["lwe_dim"], i["basis"], i["digits"], i["modulus"])
+        return cls(ctx, None, device=device, key_file=path)
 
     def close(self) -> None:
         if getattr(self, "_h", None):

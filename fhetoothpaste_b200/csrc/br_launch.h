@@ -1,6 +1,6 @@
-// Library-internal launch of the rotation kernels with an explicit split, for
-// callers inside the library that choose the kernel per launch (the serving
-// loop). Not part of the C ABI.
+// Library-internal helpers shared between translation units: the rotation
+// launch with an explicit split (the serving loop chooses the kernel per
+// launch) and the error recorder. Not part of the C ABI.
 #pragma once
 
 #include "toothpaste_gpu.h"
@@ -12,6 +12,10 @@ namespace tp {
 tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
                           uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef, void* stream,
                           int split);
+
+// Records an error message for tp_last_error() (the calling thread's) and
+// returns `s`; for the library's other translation units.
+tp_status set_error(tp_status s, const char* fmt, ...);
 
 // Rotations the device runs at once with one (split 1) or two (split 2) blocks
 // per rotation; 0 when that kernel is not available for the context.

@@ -713,6 +713,7 @@ struct tp_ks_ctx {
     uint32_t N = 0;
     uint32_t digits = 0;
     uint32_t index = 0;           // automorphism index (kind 1)
+    uint64_t basis = 0;
     int nkeys = 1;                // packing: logN keys, index 2^j + 1, j = 1..logN
     uint64_t key_words = 0;
     const Tables* tab = nullptr;
@@ -743,6 +744,7 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     auto* c = new tp_ks_ctx();
     c->kind = kind;
     c->device = device;
+    c->basis = basis;
     c->N = ring_dim;
     c->logn = ilog2(ring_dim);
     c->digits = digits;
@@ -937,6 +939,7 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
 struct tp_lwe_ks_ctx {
     int device = 0;
     uint32_t n_in = 0, n_out = 0, digits = 0;
+    uint64_t basis = 0;
     uint64_t key_words = 0;
     uint64_t* key = nullptr;
     bool key_ready = false;
@@ -961,6 +964,7 @@ tp_status tp_lwe_ks_create(uint64_t modulus, uint32_t n_in, uint32_t n_out, uint
     c->n_in = n_in;
     c->n_out = n_out;
     c->digits = digits;
+    c->basis = basis;
     c->key_words = (uint64_t)n_in * digits * (n_out + 1);
     tp::LweKsParams& kp = c->kp;
     kp.n_in = n_in;
@@ -1116,6 +1120,74 @@ tp_status tp_pbs_graph_create(tp_br_ctx* br, tp_lwe_ks_ctx* ks, uint64_t batch, 
     return TP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Key files (format in keyfile.cu): header checked against the context, then
+// the payload read, hashed and uploaded like a key from memory
+// ---------------------------------------------------------------------------
+static tp_status key_file_payload(const char* path, const tp_key_info& want, std::vector<uint64_t>& words) {
+    tp_key_info got{};
+    tp_status s = tp_key_file_info(path, &got);
+    if (s != TP_OK) return s;
+    if (got.kind != want.kind || got.variant != want.variant || got.ring_dim != want.ring_dim ||
+        got.lwe_dim != want.lwe_dim || got.digits != want.digits || got.modulus != want.modulus ||
+        got.basis != want.basis || got.index != want.index || got.words != want.words)
+        return fail(TP_ERR_LAYOUT,
+                    "%s: key for kind %u variant %u N %u n %u digits %u basis %llu index %u (%llu words); the context "
+                    "needs kind %u variant %u N %u n %u digits %u basis %llu index %u (%llu words)",
+                    path, got.kind, got.variant, got.ring_dim, got.lwe_dim, got.digits,
+                    (unsigned long long)got.basis, got.index, (unsigned long long)got.words, want.kind, want.variant,
+                    want.ring_dim, want.lwe_dim, want.digits, (unsigned long long)want.basis, want.index,
+                    (unsigned long long)want.words);
+    words.resize(got.words);
+    return tp_key_file_read(path, &got, words.data(), words.size());
+}
+
+tp_status tp_br_upload_key_file(tp_br_ctx* c, const char* path) {
+    if (!c || !path) return fail(TP_ERR_PARAM, "null argument");
+    tp_key_info want{};
+    want.kind = TP_KEY_BLIND_ROTATION;
+    want.variant = (uint32_t)c->prm.variant;
+    want.ring_dim = c->prm.ring_dim;
+    want.lwe_dim = c->prm.lwe_dim;
+    want.digits = c->prm.digits;
+    want.modulus = c->prm.modulus;
+    want.basis = c->prm.basis;
+    want.words = c->key_words;
+    std::vector<uint64_t> w;
+    tp_status s = key_file_payload(path, want, w);
+    return s == TP_OK ? tp_br_upload_key(c, w.data(), w.size()) : s;
+}
+
+tp_status tp_ks_upload_key_file(tp_ks_ctx* c, const char* path) {
+    if (!c || !path) return fail(TP_ERR_PARAM, "null argument");
+    tp_key_info want{};
+    want.kind = c->kind == 0 ? TP_KEY_RLWE_SWITCH : (c->kind == 1 ? TP_KEY_AUTOMORPHISM : TP_KEY_PACKING);
+    want.ring_dim = c->N;
+    want.digits = c->digits;
+    want.modulus = kP;
+    want.basis = c->basis;
+    want.index = c->kind == 1 ? c->index : 0;
+    want.words = c->key_words;
+    std::vector<uint64_t> w;
+    tp_status s = key_file_payload(path, want, w);
+    return s == TP_OK ? tp_ks_upload_key(c, w.data(), w.size()) : s;
+}
+
+tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* c, const char* path) {
+    if (!c || !path) return fail(TP_ERR_PARAM, "null argument");
+    tp_key_info want{};
+    want.kind = TP_KEY_LWE_SWITCH;
+    want.ring_dim = c->n_in;
+    want.lwe_dim = c->n_out;
+    want.digits = c->digits;
+    want.modulus = kP;
+    want.basis = c->basis;
+    want.words = c->key_words;
+    std::vector<uint64_t> w;
+    tp_status s = key_file_payload(path, want, w);
+    return s == TP_OK ? tp_lwe_ks_upload_key(c, w.data(), w.size()) : s;
+}
+
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd) {
     if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
@@ -1250,6 +1322,16 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
 }
 
 namespace tp {
+
+tp_status set_error(tp_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
 
 uint64_t br_concurrency(const tp_br_ctx* c, int split) {
     if (!c) return 0;

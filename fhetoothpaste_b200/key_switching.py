@@ -97,14 +97,17 @@ class GpuLWEtoRLWEPacker(_KsBase):
 
 
 class GpuLWEtoLWEConverter:
-    def __init__(self, n_in: int, n_out: int, basis: int, digits: int, ksk: np.ndarray, device: int = 0,
-                 modulus: int = nat.GOLDILOCKS):
+    def __init__(self, n_in: int, n_out: int, basis: int, digits: int, ksk: np.ndarray | None, device: int = 0,
+                 modulus: int = nat.GOLDILOCKS, key_file=None):
         h = ctypes.c_void_p()
         nat.check(nat.lib().tp_lwe_ks_create(modulus, n_in, n_out, basis, digits, device, ctypes.byref(h)))
         self._h = h
         self.n_in, self.n_out = n_in, n_out
-        ksk = np.ascontiguousarray(ksk, dtype=np.uint64)
-        nat.check(nat.lib().tp_lwe_ks_upload_key(self._h, nat.ptr(ksk), ksk.size))
+        if key_file is not None:
+            nat.check(nat.lib().tp_lwe_ks_upload_key_file(self._h, str(key_file).encode()))
+        else:
+            ksk = np.ascontiguousarray(ksk, dtype=np.uint64)
+            nat.check(nat.lib().tp_lwe_ks_upload_key(self._h, nat.ptr(ksk), ksk.size))
 
     def close(self) -> None:
         if getattr(self, "_h", None):

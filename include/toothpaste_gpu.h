@@ -337,6 +337,34 @@ tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out_dev, const uint64
  * counterpart. */
 tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_per_s);
 
+/* ---- Key files ------------------------------------------------------------
+ * The reference keeps keys only in memory (no serialization). A key file holds
+ * one key in the reference's own layout (the words tp_*_upload_key takes)
+ * behind a 128-byte header: magic "TPKEYv1", kind, parameters, word count and
+ * the SHA-256 of the payload; all fields little-endian. Reading checks the
+ * magic, the layout tag and the hash (TP_ERR_LAYOUT on a mismatch); the
+ * *_upload_key_file calls also check the header against the context's
+ * parameters before uploading. Host-only, no device needed to read or write. */
+typedef enum {
+    TP_KEY_BLIND_ROTATION = 1, /* m_brk: variant, ring_dim N, lwe_dim n */
+    TP_KEY_RLWE_SWITCH = 2,    /* RLWEtoRLWEConverter m_ksk: ring_dim */
+    TP_KEY_AUTOMORPHISM = 3,   /* AutomorphismEvaluator key: ring_dim, index */
+    TP_KEY_PACKING = 4,        /* LWEtoRLWEPacker: log2 N automorphism keys, ring_dim */
+    TP_KEY_LWE_SWITCH = 5      /* LWEtoLWEConverter m_ksk: ring_dim = n_in, lwe_dim = n_out */
+} tp_key_kind;
+
+typedef struct {
+    uint32_t kind, variant, ring_dim, lwe_dim, digits, index;
+    uint64_t modulus, basis, words;
+} tp_key_info;
+
+tp_status tp_key_file_write(const char* path, const tp_key_info* info, const uint64_t* words);
+tp_status tp_key_file_info(const char* path, tp_key_info* info);
+tp_status tp_key_file_read(const char* path, tp_key_info* info, uint64_t* words, uint64_t capacity);
+tp_status tp_br_upload_key_file(tp_br_ctx* ctx, const char* path);
+tp_status tp_ks_upload_key_file(tp_ks_ctx* ctx, const char* path);
+tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* ctx, const char* path);
+
 /* Message for the last failing call on this thread ("" if none). */
 const char* tp_last_error(void);
 
