@@ -75,9 +75,21 @@ __host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
 
 // Key rows staged in shared memory: each thread copies its own slots of the
 // next gadget row with cp.async before the digit's transforms and reads them
-// after, so the L2 latency of the key stream hides behind the NTTs. Needs C*N
-// more words; off at N = 4096 where they do not fit.
-__host__ __device__ constexpr bool br_key_prefetch(int logn) { return logn <= 11; }
+// after, so the L2 latency of the key stream hides behind the NTTs. The stage
+// needs C*N words and is used where it fits (not for ternary and BMMP at
+// N = 4096). Keeping the accumulator in registers there to make room measured
+// slower (ternary N = 4096: 1856 vs 1977 rotations/s; the spills cost more).
+__host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge) {
+    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
+           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
+           1024;  // LWE area budget for the plan; the host adds the real size
+}
+__host__ __device__ constexpr size_t br_stage_words(int logn, int variant) {
+    return (size_t)(1 << logn) * 2 * br_rgsw_per_group(variant);
+}
+__host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int loge) {
+    return (br_base_words(logn, variant, loge) + br_stage_words(logn, variant)) * 8 <= 227u * 1024u;
+}
 
 // Shared memory of one block, in words: twiddles (both directions, if kept
 // there), two exchange areas of width*N words, the accumulator (2N), the key
@@ -85,7 +97,7 @@ __host__ __device__ constexpr bool br_key_prefetch(int logn) { return logn <= 11
 __host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge) {
     return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
            (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
-           (br_key_prefetch(logn) ? (size_t)(1 << logn) * 2 * br_rgsw_per_group(variant) : 0) + ((n + 2) & ~1u);
+           (br_key_prefetch(logn, variant, loge) ? br_stage_words(logn, variant) : 0) + ((n + 2) & ~1u);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
@@ -148,7 +160,7 @@ br_kernel(const BrKernelParams prm) {
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
     constexpr bool R4 = br_fused_radix4(LOGE, VARIANT);
-    constexpr bool PF = br_key_prefetch(LOGN);
+    constexpr bool PF = br_key_prefetch(LOGN, VARIANT, LOGE);
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
@@ -173,6 +185,9 @@ br_kernel(const BrKernelParams prm) {
     const int t = threadIdx.x;
     const uint32_t n = prm.n;
     const uint32_t L = prm.digits;
+    // slot j of accumulator half h of this thread
+    auto acc_ld = [&](int h, int j) -> uint64_t { return acc[(h * E + j) * T + t]; };
+    auto acc_st = [&](int h, int j, uint64_t v) { acc[(h * E + j) * T + t] = v; };
 
     int sel = 0;
     auto xb = [&]() -> uint64_t* {
@@ -209,8 +224,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int j = 0; j < E; ++j)
-                        acc[((h0 + p) * E + j) * T + t] =
-                            gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j), bb));
+                        acc_st(h0 + p, j, gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j), bb)));
             }
         }
 
@@ -241,7 +255,7 @@ br_kernel(const BrKernelParams prm) {
             auto load_half = [&](uint64_t (&dst)[E], int h) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
-                    dst[j] = acc[(h * E + j) * T + t];
+                    dst[j] = acc_ld(h, j);
                     if constexpr (VARIANT == kCggiBinary)
                         dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j),
                                                                   2u * N - a0), 1));
@@ -321,8 +335,8 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const uint32_t ek = slot_exponent<LOGN>(E * t + j);
-                uint64_t ua = acc[j * T + t];
-                uint64_t ub = acc[(E + j) * T + t];
+                uint64_t ua = acc_ld(0, j);
+                uint64_t ub = acc_ld(1, j);
                 if constexpr (VARIANT == kCggiBinary) {
                     // acc += ExtProd (mux_operator.cpp:151)
                     ua = gl_add(ua, gl_canon(o[0][j]));
@@ -345,8 +359,8 @@ br_kernel(const BrKernelParams prm) {
                     ua = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ua, o[0][j], w0), o[2][j], w1), o[4][j], w2));
                     ub = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2));
                 }
-                acc[j * T + t] = ua;
-                acc[(E + j) * T + t] = ub;
+                acc_st(0, j, ua);
+                acc_st(1, j, ub);
             }
         }
 
@@ -358,7 +372,7 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
             for (int p = 0; p < K; ++p)
 #pragma unroll
-                for (int j = 0; j < E; ++j) x[p][j] = acc[((h0 + p) * E + j) * T + t];
+                for (int j = 0; j < E; ++j) x[p][j] = acc_ld(h0 + p, j);
             if (prm.out_coef) {
                 ntt_backward_unscaled_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_i);
 #pragma unroll
