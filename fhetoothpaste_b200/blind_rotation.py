@@ -152,6 +152,49 @@ class GpuBlindRotator:
         return BatchGraph(g, (self, key_switch))
 
 
+class NegacyclicFunctionEvaluator:
+    """NegacyclicFunctionEvaluator (lib/src/operators/negacyclic_function_evaluator.cpp:72-101):
+    BlindRotate with coefficient output, then SampleExtract at index 0 into the caller's buffer
+    (words stay untouched where the rotated A coefficient is 0, as in the reference)."""
+
+    def __init__(self, rotator: GpuBlindRotator):
+        self.rot = rotator
+        self.N = rotator.ctx.N
+
+    @staticmethod
+    def _extract(out: np.ndarray, rl: np.ndarray) -> None:
+        N = rl.size // 2
+        out[0] = rl[0]
+        a = rl[N - np.arange(1, N)]
+        nz = a != 0
+        idx = np.arange(1, N)[nz]
+        out[idx] = np.uint64(nat.GOLDILOCKS) - a[nz]
+        out[N] = rl[N]
+
+    def EvalFunc(self, result: np.ndarray, input_lwe: np.ndarray, lut) -> None:
+        """lut: an RLWE [A | B] (2N words), or a function f: the test RLWE is then built as the
+        reference builds it (f(0) at A[0], -f(N - i) at B[i], lines 82-84)."""
+        N = self.N
+        if callable(lut):
+            rl = np.zeros(2 * N, np.uint64)
+            rl[0] = int(lut(0)) % nat.GOLDILOCKS
+            for i in range(1, N):
+                rl[i + N] = (nat.GOLDILOCKS - int(lut(N - i)) % nat.GOLDILOCKS) % nat.GOLDILOCKS
+            lut = rl
+        acc = np.empty(2 * N, np.uint64)
+        self.rot.BlindRotate(acc, np.ascontiguousarray(input_lwe, np.uint64), np.ascontiguousarray(lut, np.uint64),
+                             True)
+        self._extract(result, acc)
+
+    def eval_func_batch(self, lwes: np.ndarray, luts: np.ndarray, results: np.ndarray | None = None) -> np.ndarray:
+        """Many at once: lwes batch x (n+1), luts batch x 2N or one 2N row; returns batch x (N+1)."""
+        rl = self.rot.blind_rotate_batch_host(lwes, luts, out_coef=True)
+        out = np.zeros((rl.shape[0], self.N + 1), np.uint64) if results is None else results
+        for b in range(rl.shape[0]):
+            self._extract(out[b], rl[b])
+        return out
+
+
 class BatchGraph:
     """A recorded batch launch; replays read the device buffers' current contents."""
 

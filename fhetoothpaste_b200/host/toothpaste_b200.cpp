@@ -309,6 +309,60 @@ std::unique_ptr<GpuBlindRotator> BMMPBlindRotationContext::ConstructOperator(
                                              (uint32_t)m_digits, brk, m_device);
 }
 
+// ---- programmable bootstrap ----
+
+namespace {
+// SampleExtract at index 0 (lib/include/static/sample_extraction.h:20-36): a word of the
+// result is written only where the source coefficient is non-zero.
+void sample_extract0(uint64_t* out, const uint64_t* rlwe, uint64_t N) {
+    out[0] = rlwe[0];
+    for (uint64_t i = 1; i < N; ++i)
+        if (rlwe[N - i] != 0) out[i] = P - rlwe[N - i];
+    out[N] = rlwe[N];
+}
+}  // namespace
+
+GpuNegacyclicFunctionEvaluator::GpuNegacyclicFunctionEvaluator(std::unique_ptr<GpuBlindRotator> rotator)
+    : m_rot(std::move(rotator)) {
+    if (!m_rot) throw std::invalid_argument("toothpaste_b200: null rotator");
+    m_acc.assign(2ull * m_rot->RingDimension(), 0);
+}
+
+void GpuNegacyclicFunctionEvaluator::EvalFunc(uint64_t* result, const uint64_t* input_lwe, uint64_t* lut_rlwe) {
+    const uint64_t N = m_rot->RingDimension();
+    m_rot->BlindRotate(m_acc.data(), input_lwe, lut_rlwe, true);
+    sample_extract0(result, m_acc.data(), N);
+}
+
+void GpuNegacyclicFunctionEvaluator::EvalFunc(uint64_t* result, const uint64_t* input_lwe,
+                                              std::function<uint64_t(uint64_t)>& function) {
+    const uint64_t N = m_rot->RingDimension();
+    std::vector<uint64_t> tmp(2 * N, 0);
+    tmp[0] = function(0);  // negacyclic_function_evaluator.cpp:82-84, as the reference places it
+    for (uint64_t i = 1; i < N; ++i) tmp[i + N] = subp(0, function(N - i) % P);
+    EvalFunc(result, input_lwe, tmp.data());
+}
+
+void GpuNegacyclicFunctionEvaluator::EvalFunc(std::vector<uint64_t>& result, const std::vector<uint64_t>& input,
+                                              std::vector<uint64_t>& lut_rlwe) {
+    result.resize(m_rot->RingDimension() + 1ull);
+    EvalFunc(result.data(), input.data(), lut_rlwe.data());
+}
+
+void GpuNegacyclicFunctionEvaluator::EvalFunc(std::vector<uint64_t>& result, const std::vector<uint64_t>& input,
+                                              std::function<uint64_t(uint64_t)>& function) {
+    result.resize(m_rot->RingDimension() + 1ull);
+    EvalFunc(result.data(), input.data(), function);
+}
+
+void GpuNegacyclicFunctionEvaluator::EvalFuncBatch(uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                                   const uint64_t* luts, uint64_t lut_stride) {
+    const uint64_t N = m_rot->RingDimension();
+    std::vector<uint64_t> rl(batch * 2 * N);
+    m_rot->BlindRotateBatch(batch, rl.data(), lwes, luts, lut_stride, true);
+    for (uint64_t b = 0; b < batch; ++b) sample_extract0(results + b * (N + 1), rl.data() + b * 2 * N, N);
+}
+
 // ---- key switching wrappers (synchronous, host buffers) ----
 
 namespace {

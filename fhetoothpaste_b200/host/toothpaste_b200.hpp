@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -135,6 +136,31 @@ private:
     double m_std;
     int m_device;
     uint64_t m_seed;
+};
+
+// NegacyclicFunctionEvaluator (lib/src/operators/negacyclic_function_evaluator.cpp:72-101):
+// a programmable bootstrap = BlindRotate with coefficient output, then SampleExtract at 0.
+// The result is an LWE of dimension N mod Q (N + 1 words). As in the reference,
+// SampleExtract leaves a result word untouched where the rotated A coefficient is 0,
+// and EvalFunc(function) builds the test RLWE with f(0) at A[0] and -f(N - i) at B[i]
+// (lines 82-84), reproduced word for word.
+class GpuNegacyclicFunctionEvaluator {
+public:
+    explicit GpuNegacyclicFunctionEvaluator(std::unique_ptr<GpuBlindRotator> rotator);
+    void EvalFunc(uint64_t* result, const uint64_t* input_lwe, uint64_t* lut_rlwe);
+    void EvalFunc(uint64_t* result, const uint64_t* input_lwe, std::function<uint64_t(uint64_t)>& function);
+    void EvalFunc(std::vector<uint64_t>& result, const std::vector<uint64_t>& input, std::vector<uint64_t>& lut_rlwe);
+    void EvalFunc(std::vector<uint64_t>& result, const std::vector<uint64_t>& input,
+                  std::function<uint64_t(uint64_t)>& function);
+    // Many at once on host buffers: lwes rows of n+1 words, luts rows of 2N words (lut_stride 0:
+    // one shared test RLWE), results rows of N+1 words (extracted in place of what they hold).
+    void EvalFuncBatch(uint64_t batch, uint64_t* results, const uint64_t* lwes, const uint64_t* luts,
+                       uint64_t lut_stride);
+    GpuBlindRotator& Rotator() { return *m_rot; }
+
+private:
+    std::unique_ptr<GpuBlindRotator> m_rot;
+    std::vector<uint64_t> m_acc;
 };
 
 // RLWEtoRLWEConverter::Convert (lib/src/operators/rlwe_conversion.cpp:224-249).

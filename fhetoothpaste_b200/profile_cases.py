@@ -62,6 +62,36 @@ def case_br_ternary_n4096(torch):
     _rotation(torch, 1, 4096, 32, 12, 3, 148)
 
 
+def case_br_pair_ternary_n2048(torch):
+    """br_pair_kernel (two blocks per rotation), CGGI ternary N=2048 l=3, n reduced to 64, batch 37."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    N, n, batch = 2048, 64, 37
+    ctx = BlindRotationContext(1, N, n, 1 << 12, 3)
+    rot = GpuBlindRotator(ctx, _u64(1, ctx.key_words()))
+    rot.set_split(2)
+    lw = _dev(torch, _u64(2, (batch, n + 1), 2 * N))
+    ac = _dev(torch, _u64(3, (batch, 2 * N)))
+    out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        rot.blind_rotate_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch)
+    rot.check()
+    rot.close()
+
+
+def case_pbs_epilogue_n1024(torch):
+    """lwe_ks_kernel as the bootstrap epilogue: 4096 RLWEs N=1024 -> extract -> KS to n=500
+    (base 2^16, l=4, 16 MB key) -> FLOOR switch to 2N."""
+    from fhetoothpaste_b200 import GpuLWEtoLWEConverter
+    N, n, l, batch = 1024, 500, 4, 4096
+    conv = GpuLWEtoLWEConverter(N, n, 1 << 16, l, _u64(15, N * l * (n + 1)))
+    x = _dev(torch, _u64(16, (batch, 2 * N)))
+    y = torch.empty((batch, n + 1), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        conv.pbs_epilogue_batch(batch, y.data_ptr(), x.data_ptr(), 2 * N)
+    torch.cuda.synchronize()
+    conv.close()
+
+
 def case_ntt_n2048(torch):
     """ntt_batch_kernel forward then backward, 8192 polynomials of N=2048 (134 MB)."""
     from fhetoothpaste_b200 import ntt_backward, ntt_forward

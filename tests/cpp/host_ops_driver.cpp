@@ -7,6 +7,7 @@
 //   keygen-pack N beta digits std seed rlwe_key out
 //   rotate      variant N n beta digits std seed lwe_key rlwe_key lwes count accs out
 //   pack        N beta digits std seed rlwe_key lwes len out
+//   evalfunc    N n beta digits seed lwe_key rlwe_key lwes(3 rows) lut out
 //   errors
 #include <cstdio>
 #include <cstdlib>
@@ -91,6 +92,22 @@ static int run(int argc, char** argv) {
             op->BlindRotateBatch(count - 1, out.data() + 2 * N, lwes.data() + (n + 1), accs.data() + 2 * N, 2 * N,
                                  false);
         save(argv[14], out.data(), out.size());
+        return 0;
+    }
+    if (mode == "evalfunc" && argc == 12) {
+        // binary CGGI; results: 1 LWE from a LUT RLWE, 1 from f(x) = (3x + 1) mod 5, the batch of `count`
+        const uint64_t N = u(argv[2]), n = u(argv[3]), basis = 1ull << u(argv[4]), digits = u(argv[5]);
+        const std::vector<std::vector<uint64_t>> keys{load(argv[7]), load(argv[8])};
+        CGGIBlindRotationContext ctx(BINARY, kGoldilocks, N, n, basis, digits, 3.2, 0, u(argv[6]));
+        GpuNegacyclicFunctionEvaluator ev(ctx.ConstructOperator(keys));
+        const auto lwes = load(argv[9]);
+        auto lut = load(argv[10]);
+        std::vector<uint64_t> out(3 * (N + 1), 7);  // untouched words keep this value, as in the reference
+        ev.EvalFunc(out.data(), lwes.data(), lut.data());
+        std::function<uint64_t(uint64_t)> f = [](uint64_t x) { return (3 * x + 1) % 5; };
+        ev.EvalFunc(out.data() + (N + 1), lwes.data() + (n + 1), f);
+        ev.EvalFuncBatch(1, out.data() + 2 * (N + 1), lwes.data() + 2 * (n + 1), lut.data(), 0);
+        save(argv[11], out.data(), out.size());
         return 0;
     }
     if (mode == "pack" && argc == 11) {

@@ -237,3 +237,30 @@ def test_two_block_split_needs_tile_of_four(native, oracle, golden):
         rot.set_tile(8)
     rot.set_split(1)
     rot.set_tile(8)
+
+
+def test_function_evaluator_like_oracle(native, oracle, golden):
+    from fhetoothpaste_b200 import NegacyclicFunctionEvaluator
+    from oracle.oracle import ptr
+    name = "small_binary_n256"
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    ev = NegacyclicFunctionEvaluator(rot)
+    lwes = lwe_inputs(N, n, 3, 81)
+    f = lambda x: (5 * x + 2) % 11  # noqa: E731
+    res = np.full(N + 1, 9, np.uint64)
+    ev.EvalFunc(res, lwes[0], f)
+    acc = np.zeros(2 * N, np.uint64)
+    acc[0] = 2
+    for i in range(1, N):
+        acc[i + N] = (0xFFFFFFFF00000001 - (5 * (N - i) + 2) % 11) % 0xFFFFFFFF00000001
+    rl = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[0], acc, 1)
+    want = np.full(N + 1, 9, np.uint64)
+    oracle.L.tpo_sample_extract(ptr(want), ptr(rl), 0, N)
+    np.testing.assert_array_equal(res, want)
+    luts = random_acc(N, 3, 82)
+    batch = ev.eval_func_batch(lwes, luts)
+    for b in range(3):
+        rl = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], luts[b], 1)
+        np.testing.assert_array_equal(batch[b], oracle.sample_extract(rl))

@@ -100,3 +100,28 @@ def test_cpp_packer_like_oracle(driver, oracle, cuda, tmp_path):
     keys = oracle.pack_keygen(N, beta, digits, std, z, seed=17)
     want = oracle.pack(N, beta, digits, keys, lwes, length)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_cpp_function_evaluator_like_oracle(driver, oracle, cuda, tmp_path):
+    """GpuNegacyclicFunctionEvaluator: BlindRotate (coefficient output) + SampleExtract into a
+    caller buffer whose words stay where the rotated A coefficient is 0, as in the reference."""
+    from oracle.oracle import P, ptr
+    N, n, beta, digits = 256, 12, 16, 4
+    sk = lwe_secret(CGGI_BINARY, n, N, seed=71)
+    z = rlwe_secret(N, seed=72)
+    lwes = lwe_inputs(N, n, 3, seed=73)
+    lut = random_acc(N, 1, seed=74)[0]
+    lut[:N] = 0                                        # trivial RLWE of a test polynomial
+    lut[N + 5] = 0                                     # and a zero coefficient
+    got = run(driver, tmp_path, "evalfunc", N, n, beta, digits, 19, sk, z, lwes, lut).reshape(3, N + 1)
+    brk = oracle.br_keygen(CGGI_BINARY, N, n, beta, digits, 3.2, sk, z, seed=19)
+    f_rlwe = np.zeros(2 * N, np.uint64)
+    f_rlwe[0] = 1                                      # f(0) = 1 placed at A[0], as the reference does
+    for i in range(1, N):
+        f_rlwe[i + N] = (P - (3 * (N - i) + 1) % 5) % P
+    for row, acc in ((0, lut), (1, f_rlwe), (2, lut)):
+        rl = oracle.blind_rotate(CGGI_BINARY, N, n, beta, digits, brk, lwes[row], acc, 1)
+        want = np.full(N + 1, 7, np.uint64)
+        oracle.L.tpo_sample_extract(ptr(want), ptr(rl), 0, N)
+        np.testing.assert_array_equal(got[row], want, err_msg=f"row {row}")
