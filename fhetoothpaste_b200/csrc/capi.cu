@@ -942,6 +942,7 @@ struct tp_lwe_ks_ctx {
     uint64_t basis = 0;
     uint64_t key_words = 0;
     uint64_t* key = nullptr;
+    uint64_t* cterm = nullptr;    // n_out + 1 words, from the key (see lwe_ks_kernel)
     bool key_ready = false;
     tp::LweKsParams kp{};
 };
@@ -959,6 +960,8 @@ tp_status tp_lwe_ks_create(uint64_t modulus, uint32_t n_in, uint32_t n_out, uint
     // (lwe_conversion.cpp:226-236); every shift must stay non-negative.
     if (digits < 1 || digits > 8 || (uint64_t)digits * beta > 64)
         return fail(TP_ERR_PARAM, "digits * log2(basis) must be at most 64 (and digits at most 8)");
+    if ((uint64_t)n_in * digits > (1ull << 30))
+        return fail(TP_ERR_PARAM, "n_in * digits above 2^30 is not supported");
     auto* c = new tp_lwe_ks_ctx();
     c->device = device;
     c->n_in = n_in;
@@ -993,6 +996,7 @@ tp_status tp_lwe_ks_destroy(tp_lwe_ks_ctx* c) {
     if (!c) return TP_OK;
     cudaSetDevice(c->device);
     cudaFree(c->key);
+    cudaFree(c->cterm);
     delete c;
     return TP_OK;
 }
@@ -1005,8 +1009,17 @@ tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* c, const uint64_t* ksk, uint64_t w
         return fail(TP_ERR_LAYOUT, "key has %llu words, context expects %llu", (unsigned long long)words,
                     (unsigned long long)c->key_words);
     TP_CUDA(cudaSetDevice(c->device));
+    c->key_ready = false;
     if (!c->key) TP_CUDA(cudaMalloc(&c->key, c->key_words * 8));
+    if (!c->cterm) TP_CUDA(cudaMalloc(&c->cterm, ((uint64_t)c->n_out + 1) * 8));
     TP_CUDA(cudaMemcpy(c->key, ksk, c->key_words * 8, cudaMemcpyHostToDevice));
+    tp::LweKsParams kp = c->kp;
+    kp.ksk = c->key;
+    const unsigned blocks = (c->n_out + 1 + 127) / 128;
+    tp::lwe_ks_cterm_kernel<<<blocks, 128>>>(c->cterm, kp);
+    TP_CUDA(cudaGetLastError());
+    TP_CUDA(cudaDeviceSynchronize());
+    c->kp.cterm = c->cterm;
     c->key_ready = true;
     return TP_OK;
 }

@@ -42,6 +42,7 @@ struct LweKsParams {
     uint32_t n_in, n_out, digits;
     uint32_t rlwe_in;         // 1: input row = SampleExtract(index 0) of an RLWE with N = n_in
     uint32_t ms_log2;         // k > 0: write floor(out * 2^k / p) into a fresh output (PBS epilogue)
+    const uint64_t* cterm;    // per output word: sum_j ddelta[j] * sum_i ksk[i][j][col] mod p
     uint64_t corr;
     uint32_t dshift[8];
     uint64_t dmask[8];
@@ -81,16 +82,37 @@ __device__ __forceinline__ uint64_t lwe_ks_in_body(const LweKsParams& prm, uint6
     return prm.rlwe_in ? prm.in[row * 2ull * prm.n_in + prm.n_in] : prm.in[row * (prm.n_in + 1) + prm.n_in];
 }
 
+// a (128-bit, four 32-bit limbs) += raw * k exactly, raw < 2^32: two 32x64-bit
+// partial products folded into the limbs' carry chains.
+__device__ __forceinline__ void mac_raw(uint32_t (&a)[4], uint32_t raw, uint64_t k) {
+    asm("mad.lo.cc.u32 %0, %4, %5, %0;\n\t"
+        "madc.hi.cc.u32 %1, %4, %5, %1;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.u32 %3, %3, 0;\n\t"
+        "mad.lo.cc.u32 %1, %4, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %4, %6, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3])
+        : "r"(raw), "r"(lo32(k)), "r"(hi32(k)));
+}
+
+// The signed digits are d_ij = raw_ij - ddelta[j] with raw_ij in [0, 2^beta), so
+//   sum_ij d_ij k_ij = sum_ij raw_ij k_ij - sum_j ddelta[j] (sum_i k_ij)   (mod p).
+// The kernel accumulates the first sum exactly in 128 bits (no reduction per
+// term: n_in * l terms below 2^94 each) and takes off the second, which depends
+// only on the key and the output word (cterm, computed at key upload).
 __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams prm) {
-    __shared__ uint64_t dig[kLweKsRows][kLweKsChunk * 8];
+    __shared__ uint32_t dig[kLweKsRows][kLweKsChunk * 8];
     const int t = threadIdx.x;
     const uint64_t row0 = (uint64_t)blockIdx.y * kLweKsRows;
     const uint32_t col = blockIdx.x * kLweKsCols + t;
     const uint32_t width = prm.n_out + 1;
     const uint32_t L = prm.digits;
-    uint64_t acc[kLweKsRows];
+    uint32_t acc[kLweKsRows][4];
 #pragma unroll
-    for (int r = 0; r < kLweKsRows; ++r) acc[r] = 0;
+    for (int r = 0; r < kLweKsRows; ++r)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) acc[r][w] = 0;
     for (uint32_t i0 = 0; i0 < prm.n_in; i0 += kLweKsChunk) {
         const uint32_t ni = min((uint32_t)kLweKsChunk, prm.n_in - i0);
         __syncthreads();
@@ -99,31 +121,48 @@ __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams pr
             uint64_t x = 0;
             if (row0 + r < prm.batch) x = gl_add(lwe_ks_in_word(prm, row0 + r, i0 + ii), prm.corr);
             for (uint32_t j = 0; j < L; ++j)
-                dig[r][ii * L + j] = row0 + r < prm.batch ? gl_sub((x >> prm.dshift[j]) & prm.dmask[j], prm.ddelta[j]) : 0;
+                dig[r][ii * L + j] = row0 + r < prm.batch ? (uint32_t)((x >> prm.dshift[j]) & prm.dmask[j]) : 0u;
         }
         __syncthreads();
         if (col < width) {
             for (uint32_t ij = 0; ij < ni * L; ++ij) {
                 const uint64_t kv = __ldg(prm.ksk + (uint64_t)(i0 * L + ij) * width + col);
 #pragma unroll
-                for (int r = 0; r < kLweKsRows; ++r) acc[r] = gl_fma_lazy(acc[r], dig[r][ij], kv);
+                for (int r = 0; r < kLweKsRows; ++r) mac_raw(acc[r], dig[r][ij], kv);
             }
         }
     }
     if (col < width) {
+        const uint64_t ct = prm.cterm[col];
 #pragma unroll
         for (int r = 0; r < kLweKsRows; ++r) {
             const uint64_t row = row0 + r;
             if (row >= prm.batch) break;
+            const uint64_t sum = gl_sub(gl_reduce128(acc[r][0], acc[r][1], acc[r][2], acc[r][3]), ct);
             uint64_t* o = prm.out + row * width;
             if (prm.ms_log2) {
                 const uint64_t base = col == prm.n_out ? lwe_ks_in_body(prm, row) : 0;
-                o[col] = ms_floor_pow2(gl_sub(base, gl_canon(acc[r])), prm.ms_log2);
+                o[col] = ms_floor_pow2(gl_sub(base, sum), prm.ms_log2);
             } else {
                 const uint64_t base = col == prm.n_out ? lwe_ks_in_body(prm, row) : o[col];
-                o[col] = gl_sub(base, gl_canon(acc[r]));
+                o[col] = gl_sub(base, sum);
             }
         }
+    }
+}
+
+// cterm[col] = sum_j ddelta[j] * (sum_i ksk[i][j][col]) mod p, one thread per output word.
+__global__ void lwe_ks_cterm_kernel(uint64_t* __restrict__ cterm, const LweKsParams prm) {
+    const uint32_t width = prm.n_out + 1;
+    for (uint32_t col = blockIdx.x * blockDim.x + threadIdx.x; col < width; col += gridDim.x * blockDim.x) {
+        uint64_t total = 0;
+        for (uint32_t j = 0; j < prm.digits; ++j) {
+            uint64_t s = 0;
+            for (uint32_t i = 0; i < prm.n_in; ++i)
+                s = gl_add(s, gl_canon(prm.ksk[((uint64_t)i * prm.digits + j) * width + col]));
+            total = gl_add(total, gl_mul(s, gl_canon(prm.ddelta[j])));
+        }
+        cterm[col] = total;
     }
 }
 
