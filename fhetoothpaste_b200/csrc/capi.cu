@@ -4,6 +4,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -18,6 +19,7 @@
 #include "util_kernels.cuh"
 #include "ks_kernels.cuh"
 #include "ks_util_kernels.cuh"
+#include "ss_kernels.cuh"
 
 namespace {
 
@@ -873,6 +875,31 @@ tp_status tp_auto_eval_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const 
     return ks_launch(c, tp::kKsAuto, kp, (cudaStream_t)stream);
 }
 
+// Trace steps j = j_hi down to j_lo over `items` RLWEs (coefficient domain, in
+// place, `stride` words apart): x <- x + INTT(AutoKS_{2^j+1}(x)) with the
+// packing context's key for index 2^j + 1 (lwe_to_rlwe_packing.cpp:228-234,
+// trace_evaluation.cpp:145-153).
+static tp_status ks_trace_steps(tp_ks_ctx* c, uint64_t items, uint64_t* data, uint64_t stride, int j_hi, int j_lo,
+                                cudaStream_t st) {
+    const uint64_t N = c->N;
+    const uint64_t kw = (uint64_t)c->digits * 2 * N;
+    tp::KsKernelParams kp = c->kp;
+    for (int j = j_hi; j >= j_lo; --j) {
+        kp.key = c->key + (uint64_t)(j - 1) * kw;
+        kp.in = data;
+        kp.out = data;
+        kp.items = items;
+        kp.in_stride = kp.out_stride = stride;
+        kp.right_offset = 0;
+        kp.auto_index = (1u << j) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = 0;
+        tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+        if (s != TP_OK) return s;
+    }
+    return TP_OK;
+}
+
 tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out, const uint64_t* in, void* stream) {
     if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
     if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
@@ -915,18 +942,8 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
         if (s != TP_OK) return s;
     }
     // trailing traces when len < N (lwe_to_rlwe_packing.cpp:228-234)
-    for (int i = 0; i < c->logn - log_len; ++i) {
-        const int j = c->logn - i;
-        kp.key = c->key + (uint64_t)(j - 1) * kw;
-        kp.in = c->work;
-        kp.out = c->work;
-        kp.items = packs;
-        kp.in_stride = kp.out_stride = len * 2 * N;
-        kp.right_offset = 0;
-        kp.auto_index = (1u << j) + 1;
-        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
-        kp.shift = 0;
-        tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+    {
+        tp_status s = ks_trace_steps(c, packs, c->work, len * 2 * N, c->logn, log_len + 1, st);
         if (s != TP_OK) return s;
     }
     TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, c->work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
@@ -1202,7 +1219,7 @@ tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* c, const char* path) {
 }
 
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
-                            bool fwd) {
+                            bool fwd, uint64_t in_stride = 0, uint64_t out_stride = 0) {
     if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
         return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
     if (count == 0) return TP_OK;
@@ -1222,7 +1239,9 @@ static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, co
     const uint64_t grid = std::min<uint64_t>(count, (uint64_t)std::max(1, per_sm) * sm_count(device));
     const uint64_t* tw = fwd ? tab->tw_fwd : tab->tw_inv;
     uint64_t n_inv = tab->n_inv;
-    void* args[] = {&out, &in, &count, &tw, &n_inv};
+    if (!in_stride) in_stride = ring_dim;
+    if (!out_stride) out_stride = ring_dim;
+    void* args[] = {&out, &in, &count, &tw, &n_inv, &in_stride, &out_stride};
     TP_CUDA(cudaLaunchKernel(k, dim3((unsigned)grid), dim3(ring_dim / 8), args, smem, (cudaStream_t)stream));
     return TP_OK;
 }
@@ -1233,6 +1252,171 @@ tp_status tp_ntt_forward(uint32_t ring_dim, uint64_t count, uint64_t* out, const
 
 tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream) {
     return ntt_launch(ring_dim, count, out, in, stream, false);
+}
+
+// ---------------------------------------------------------------------------
+// LWE -> RGSW scheme switching (lib/src/operators/lwe_to_rgsw_conversion.cpp)
+// ---------------------------------------------------------------------------
+struct tp_ss_ctx {
+    int device = 0;
+    uint32_t N = 0, n = 0, D = 0, logn = 0;
+    tp_br_ctx* br = nullptr;      // CGGI binary rotation
+    tp_ks_ctx* trace = nullptr;   // packing-kind context: automorphism keys 2^j + 1, j = 1..log2 N
+    tp_ks_ctx* sq = nullptr;      // RLWE key switch s^2 -> s
+    std::vector<uint64_t> acc_host;  // the converter's m_acc: [0 | -tp | tp], 3N words
+    uint64_t* acc = nullptr;      // device copy
+    uint64_t *rot = nullptr, *rows = nullptr, *sqin = nullptr, *sqout = nullptr;
+    uint64_t cap = 0;             // ciphertexts the scratch holds
+    bool ready = false;
+    std::mutex mu;
+};
+
+// The test polynomial of LWEtoRGSWConverter's constructor (lines 120-160), in the
+// reference's own integer arithmetic (the first scale is an int shift there).
+static bool ss_test_polynomial(uint32_t N, uint32_t D, int basebits, std::vector<uint64_t>& acc) {
+    const uint64_t bs = N / D;
+    const uint64_t max_digits = (uint64_t)std::ceil(std::log2((long double)kP) / (long double)basebits);
+    const uint64_t sh = (uint64_t)basebits * (max_digits - D);
+    if (max_digits < D || sh >= 31) return false;
+    uint64_t scale = (uint64_t)(1 << sh);
+    acc.assign(3ull * N, 0);
+    for (uint64_t i = 0; i < bs / 2; ++i) {
+        acc[N + i] = scale;
+        acc[2 * N - i - 1] = kP - scale;
+    }
+    for (uint64_t b = 1; b < D; ++b) {
+        scale <<= basebits;
+        for (uint64_t j = 0; j < bs; ++j) acc[N + b * bs + j - bs / 2] = scale;
+    }
+    const uint64_t two_inv = hinv(2);
+    for (uint64_t i = 0; i < N; ++i) acc[N + i] = hmul(acc[N + i] % kP, two_inv);
+    for (uint64_t i = 0; i < N; ++i) acc[2 * N + i] = acc[N + i];
+    for (uint64_t i = 0; i < N; ++i) acc[N + i] = hmul(acc[2 * N + i], kP - 1);
+    return true;
+}
+
+tp_status tp_ss_destroy(tp_ss_ctx* c) {
+    if (!c) return TP_OK;
+    cudaSetDevice(c->device);
+    tp_br_destroy(c->br);
+    tp_ks_destroy(c->trace);
+    tp_ks_destroy(c->sq);
+    cudaFree(c->acc);
+    cudaFree(c->rot);
+    cudaFree(c->rows);
+    cudaFree(c->sqin);
+    cudaFree(c->sqout);
+    delete c;
+    return TP_OK;
+}
+
+tp_status tp_ss_create(const tp_br_params* rotation, uint64_t trace_basis, uint32_t trace_digits,
+                       uint64_t square_basis, uint32_t square_digits, uint32_t out_digits, uint64_t out_basis,
+                       int device, tp_ss_ctx** out) {
+    if (!out || !rotation) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    const uint32_t ring_dim = rotation->ring_dim, lwe_dim = rotation->lwe_dim;
+    if (out_digits < 1 || (ring_dim % out_digits) || ((ring_dim / out_digits) & 1))
+        return fail(TP_ERR_PARAM, "out_digits must divide N into blocks of even size");
+    if (out_basis < 2 || (out_basis & (out_basis - 1))) return fail(TP_ERR_PARAM, "out_basis must be a power of two");
+    auto* c = new tp_ss_ctx();
+    c->device = device;
+    c->N = ring_dim;
+    c->n = lwe_dim;
+    c->D = out_digits;
+    c->logn = ilog2(ring_dim);
+    if (!ss_test_polynomial(ring_dim, out_digits, ilog2(out_basis), c->acc_host)) {
+        delete c;
+        return fail(TP_ERR_PARAM, "output gadget (out_digits, out_basis) not supported: its first scale overflows");
+    }
+    tp_status s = tp_br_create(rotation, device, &c->br);
+    if (s == TP_OK) s = tp_pack_create(ring_dim, trace_basis, trace_digits, device, &c->trace);
+    if (s == TP_OK) s = tp_rlwe_ks_create(ring_dim, square_basis, square_digits, device, &c->sq);
+    if (s != TP_OK) {
+        tp_ss_destroy(c);
+        return s;
+    }
+    cudaError_t e = cudaMalloc(&c->acc, c->acc_host.size() * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(c->acc, c->acc_host.data(), c->acc_host.size() * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        tp_ss_destroy(c);
+        return fail(TP_ERR_CUDA, "test polynomial: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return TP_OK;
+}
+
+uint64_t tp_ss_key_words(const tp_ss_ctx* c, int which) {
+    if (!c) return 0;
+    return which == 0 ? tp_br_key_words(c->br) : tp_ks_key_words(which == 1 ? c->trace : c->sq);
+}
+
+tp_status tp_ss_upload_keys(tp_ss_ctx* c, const uint64_t* brk, uint64_t brk_words, const uint64_t* trace_keys,
+                            uint64_t trace_words, const uint64_t* square_key, uint64_t square_words) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->ready = false;
+    tp_status s = tp_br_upload_key(c->br, brk, brk_words);
+    if (s == TP_OK) s = tp_ks_upload_key(c->trace, trace_keys, trace_words);
+    if (s == TP_OK) s = tp_ks_upload_key(c->sq, square_key, square_words);
+    if (s == TP_OK) c->ready = true;
+    return s;
+}
+
+tp_status tp_ss_accumulator(const tp_ss_ctx* c, uint64_t* out_host) {
+    if (!c || !out_host) return fail(TP_ERR_PARAM, "null argument");
+    std::copy(c->acc_host.begin(), c->acc_host.end(), out_host);
+    return TP_OK;
+}
+
+tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* lwes, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->ready) return fail(TP_ERR_STATE, "keys not uploaded");
+    if (batch == 0) return TP_OK;
+    if (!out || !lwes) return fail(TP_ERR_PARAM, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    const uint64_t N = c->N, D = c->D;
+    if (c->cap < batch) {
+        cudaFree(c->rot);
+        cudaFree(c->rows);
+        cudaFree(c->sqin);
+        cudaFree(c->sqout);
+        c->rot = c->rows = c->sqin = c->sqout = nullptr;
+        c->cap = 0;
+        TP_CUDA(cudaMalloc(&c->rot, batch * 2 * N * 8));
+        TP_CUDA(cudaMalloc(&c->rows, batch * D * 2 * N * 8));
+        TP_CUDA(cudaMalloc(&c->sqin, batch * D * 2 * N * 8));
+        TP_CUDA(cudaMalloc(&c->sqout, batch * D * 2 * N * 8));
+        c->cap = batch;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t rowsn = batch * D;
+    const uint64_t total = rowsn * 2 * N;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 65535);
+    // 1. rotation of [0 | -tp] with coefficient output (line 178)
+    tp_status s = tp_br_blind_rotate_batch(c->br, batch, c->rot, lwes, (uint64_t)c->n + 1, c->acc, 0, 1, stream);
+    if (s != TP_OK) return s;
+    // 2. + (0, tp), Lev rows, times N^-1 (lines 180-200; trace_evaluation.cpp:143)
+    tp::ss_rows_kernel<<<blocks, 256, 0, st>>>(c->rows, c->rot, c->acc + 2 * N, batch, (uint32_t)D, (uint32_t)N,
+                                                 (uint32_t)(N / D), c->br->tab->n_inv);
+    TP_CUDA(cudaGetLastError());
+    // 3. trace: automorphisms N+1 down to 3 (trace_evaluation.cpp:145-153), then NTT of both halves
+    s = ks_trace_steps(c->trace, rowsn, c->rows, 2 * N, (int)c->logn, 1, st);
+    if (s != TP_OK) return s;
+    s = ntt_launch((uint32_t)N, 2 * rowsn, c->rows, c->rows, stream, true);
+    if (s != TP_OK) return s;
+    // 4. squaring input [INTT(row.A) | 0], key switch s^2 -> s into zero rows (lines 212-216)
+    s = ntt_launch((uint32_t)N, rowsn, c->sqin, c->rows, stream, false, 2 * N, 2 * N);
+    if (s != TP_OK) return s;
+    TP_CUDA(cudaMemset2DAsync(c->sqin + N, 2 * N * 8, 0, N * 8, rowsn, st));
+    TP_CUDA(cudaMemsetAsync(c->sqout, 0, total * 8, st));
+    s = tp_rlwe_ks_batch(c->sq, rowsn, c->sqout, c->sqin, stream);
+    if (s != TP_OK) return s;
+    // 5. RGSW = [lev_left | lev_right] (lines 218-224)
+    tp::ss_assemble_kernel<<<blocks, 256, 0, st>>>(out, c->rows, c->sqout, batch, (uint32_t)D, (uint32_t)N);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
 }
 
 }  // extern "C"

@@ -6,11 +6,13 @@
 
 namespace tp {
 
-// count polynomials; block b handles polynomials b, b + gridDim.x, ...
+// count polynomials, polynomial p at in + p*in_stride / out + p*out_stride;
+// block b handles polynomials b, b + gridDim.x, ...
 // Shared memory: twiddles (N) + two exchange buffers (2N).
 template <int LOGN, bool FORWARD>
 __global__ void __launch_bounds__((1 << LOGN) / 8) ntt_batch_kernel(uint64_t* out, const uint64_t* in, uint64_t count,
-                                                                     const uint64_t* tw, uint64_t n_inv) {
+                                                                     const uint64_t* tw, uint64_t n_inv,
+                                                                     uint64_t in_stride, uint64_t out_stride) {
     using SH = NttShape<LOGN>;
     constexpr int N = SH::N;
     constexpr int T = SH::T;
@@ -22,8 +24,8 @@ __global__ void __launch_bounds__((1 << LOGN) / 8) ntt_batch_kernel(uint64_t* ou
     __syncthreads();
     int sel = 0;
     for (uint64_t p = blockIdx.x; p < count; p += gridDim.x) {
-        const uint64_t* src = in + p * N;
-        uint64_t* dst = out + p * N;
+        const uint64_t* src = in + p * in_stride;
+        uint64_t* dst = out + p * out_stride;
         uint64_t x[8];
         if constexpr (FORWARD) {
 #pragma unroll

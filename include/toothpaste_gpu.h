@@ -337,6 +337,32 @@ tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out_dev, const uint64
  * counterpart. */
 tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_per_s);
 
+/* ---- LWE -> RGSW scheme switching -------------------------------------------
+ * LWEtoRGSWConverter::Convert (lib/src/operators/lwe_to_rgsw_conversion.cpp:168-
+ * 225) of a SchemeSwitchingContext(rotation, trace, squaring, out_digits,
+ * out_basis) on the Goldilocks modulus. Lines 10-110 build the context from a
+ * rotation context of any variant, a TraceEvaluationContext and an
+ * RLWEConversionContext, each with its own gadget. Per LWE: a blind rotation of the context's test polynomial, Lev extraction,
+ * a trace over the automorphisms N+1 .. 3 and a key switch from s^2 to s per
+ * row. Keys in the reference's layouts: the blind-rotation key (m_brk), the
+ * trace's automorphism keys for indices 3, 5, 9, .., N+1 concatenated (as the
+ * packer takes them), and the squaring converter's m_ksk. Output per LWE:
+ * 4 N out_digits words [lev_left rows | lev_right rows], NTT domain.
+ * out_digits must divide N into even blocks. */
+typedef struct tp_ss_ctx tp_ss_ctx;
+tp_status tp_ss_create(const tp_br_params* rotation, uint64_t trace_basis, uint32_t trace_digits,
+                       uint64_t square_basis, uint32_t square_digits, uint32_t out_digits, uint64_t out_basis,
+                       int device, tp_ss_ctx** out);
+tp_status tp_ss_destroy(tp_ss_ctx* ctx);
+/* which: 0 blind-rotation key, 1 trace keys, 2 squaring key */
+uint64_t tp_ss_key_words(const tp_ss_ctx* ctx, int which);
+tp_status tp_ss_upload_keys(tp_ss_ctx* ctx, const uint64_t* brk, uint64_t brk_words, const uint64_t* trace_keys,
+                            uint64_t trace_words, const uint64_t* square_key, uint64_t square_words);
+/* The converter's accumulator (3N words: [0 | -tp | tp]), for checks. */
+tp_status tp_ss_accumulator(const tp_ss_ctx* ctx, uint64_t* out_host);
+tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* lwes_dev,
+                               void* stream);
+
 /* ---- Key files ------------------------------------------------------------
  * The reference keeps keys only in memory (no serialization). A key file holds
  * one key in the reference's own layout (the words tp_*_upload_key takes)

@@ -150,6 +150,11 @@ class Oracle:
             "tpo_pack": (I, [U64, U64, U64, U64P, U64P, U64P, U64]),
             "tpo_sample_extract": (None, [U64P, U64P, U64, U64]),
             "tpo_modulus_switch": (I, [U64P, U64, U64, U64, I]),
+            "tpo_ss_test_poly": (I, [U64, U64, U64, U64P]),
+            "tpo_ss_keygen": (None, [R, I, U64, U64, U64, U64, U64, U64, U64, U64, D, U64P, U64P, U64P, U64P,
+                                     U64P]),
+            "tpo_lwe_to_rgsw": (I, [I, U64, U64, U64, U64, U64P, U64, U64, U64P, U64, U64, U64P, U64, U64, U64P,
+                                    U64P]),
             "tpo_psi": (U64, [U64]),
             "tpo_mul": (U64, [U64, U64]),
         }
@@ -285,6 +290,32 @@ class Oracle:
         ks = self.lwe_ks(P, N, n_out, bl, dg, ksk, self.sample_extract(rlwe_coef))
         return self.modulus_switch(ks, P, target, "floor")
 
+    def ss_test_poly(self, N, out_digits, out_basis_log2) -> np.ndarray:
+        """LWEtoRGSWConverter's m_acc = [0 | -tp | tp] (3N words)."""
+        acc = np.empty(3 * N, np.uint64)
+        assert self.L.tpo_ss_test_poly(N, out_digits, out_basis_log2, ptr(acc)) == 0
+        return acc
+
+    def ss_keygen(self, variant, N, n, br, tr, sq, std, lwe_key, rlwe_key, seed):
+        """(rotation key, trace keys, squaring key) from one sampler stream, as the reference makes them."""
+        r = Rng(seed)
+        brk = np.empty(self.L.tpo_brk_words(variant, N, n, br[1]), np.uint64)
+        logn = N.bit_length() - 1
+        trk = np.empty(logn * tr[1] * 2 * N, np.uint64)
+        sqk = np.empty(sq[1] * 2 * N, np.uint64)
+        self.L.tpo_ss_keygen(ctypes.byref(r), variant, N, n, br[0], br[1], tr[0], tr[1], sq[0], sq[1], std,
+                             ptr(np.ascontiguousarray(lwe_key, np.uint64)),
+                             ptr(np.ascontiguousarray(rlwe_key, np.uint64)), ptr(brk), ptr(trk), ptr(sqk))
+        return brk, trk, sqk
+
+    def lwe_to_rgsw(self, variant, N, n, br, brk, tr, trace_keys, sq, sq_key, out_digits, out_basis_log2, lwe):
+        """LWEtoRGSWConverter::Convert of one LWE; br/tr/sq = (basis_log2, digits) of each component."""
+        out = np.empty(4 * N * out_digits, np.uint64)
+        assert self.L.tpo_lwe_to_rgsw(variant, N, n, br[0], br[1], ptr(brk), tr[0], tr[1], ptr(trace_keys), sq[0],
+                                      sq[1], ptr(sq_key), out_digits, out_basis_log2,
+                                      ptr(np.ascontiguousarray(lwe, np.uint64)), ptr(out)) == 0
+        return out
+
     def phase_rlwe(self, rlwe_ntt: np.ndarray, sk: np.ndarray) -> np.ndarray:
         N = sk.size
         sk_ntt = self.ntt_forward(sk)
@@ -337,6 +368,12 @@ class Reference:
             "ref_pack_destroy": (None, [VP]),
             "ref_sample_extract": (None, [U64P, U64P, U64, U64]),
             "ref_modulus_switch": (None, [U64P, U64, U64, U64, I]),
+            "ref_ss_create": (VP, [I, U64, U64, U64, U64, U64, U64, U64, U64, D, U64, U64, U64P, U64P]),
+            "ref_ss_key_words": (U64, [VP, I]),
+            "ref_ss_key_copy": (None, [VP, I, U64P]),
+            "ref_ss_convert": (None, [VP, U64P, U64P]),
+            "ref_ss_test_poly": (None, [VP, U64P]),
+            "ref_ss_destroy": (None, [VP]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

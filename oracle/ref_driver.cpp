@@ -22,7 +22,9 @@
 #include "operators/bmmp_blind_rotation.h"
 #include "operators/cggi_blind_rotation.h"
 #include "operators/endo_glwe_conversion.h"
+#include "operators/lwe_to_rgsw_conversion.h"
 #include "operators/lwe_to_rlwe_packing.h"
+#include "operators/trace_evaluation.h"
 #include "static/keys.h"
 #include "static/modulus_switching.h"
 #include "static/sample_extraction.h"
@@ -225,6 +227,90 @@ void ref_pack_destroy(void* hp) { delete (LWEtoRLWEPacker*)hp; }
 void ref_sample_extract(uint64_t* out_lwe, uint64_t* rlwe, uint64_t index, uint64_t N) {
     SampleExtract<uint64_t>(out_lwe, rlwe, index, N, kQ);
 }
+
+// LWE -> RGSW scheme switching (lib/src/operators/lwe_to_rgsw_conversion.cpp): CGGI binary
+// rotation, trace and squaring contexts all with (base 2^basis_log2, digits), output RGSW
+// with (out_digits, 2^out_basis_log2), as tests/scheme_switch_tests.cpp builds them.
+struct SSHandle {
+    std::shared_ptr<SchemeSwitchingContext> ctx;
+    std::unique_ptr<LWEtoRGSWConverter> op;
+    uint64_t N = 0, out_digits = 0;
+};
+
+// variant as in ref_br_create; each component has its own gadget (basis 2^b, digits)
+void* ref_ss_create(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                    uint64_t tr_basis_log2, uint64_t tr_digits, uint64_t sq_basis_log2, uint64_t sq_digits,
+                    double std_dev, uint64_t out_digits, uint64_t out_basis_log2, const uint64_t* lwe_key,
+                    const uint64_t* rlwe_key) {
+    auto* h = new SSHandle();
+    h->N = N;
+    h->out_digits = out_digits;
+    std::shared_ptr<OperatorContext<BlindRotator>> rot;
+    std::shared_ptr<MathWorker> ntt;
+    if (variant == 2) {
+        auto br = std::make_shared<BMMPBlindRotationContext>(KeyDistribution::BINARY, kQ, N, n, 1ULL << br_basis_log2,
+                                                             br_digits, std_dev, 2);
+        ntt = br->GetNTT();
+        rot = std::reinterpret_pointer_cast<OperatorContext<BlindRotator>>(br);
+    } else {
+        auto br = std::make_shared<CGGIBlindRotationContext>(
+            variant == 0 ? KeyDistribution::BINARY : KeyDistribution::TERNARY, kQ, N, n, 1ULL << br_basis_log2,
+            br_digits, std_dev);
+        ntt = br->GetNTT();
+        rot = std::reinterpret_pointer_cast<OperatorContext<BlindRotator>>(br);
+    }
+    auto tr = std::make_shared<TraceEvaluationContext>(BINARY, ntt, 1ULL << tr_basis_log2, tr_digits, std_dev);
+    auto sq = std::make_shared<RLWEConversionContext>(BINARY, ntt, 1ULL << sq_basis_log2, sq_digits, std_dev);
+    h->ctx = std::make_shared<SchemeSwitchingContext>(rot, tr, sq, out_digits, 1ULL << out_basis_log2);
+    std::vector<GenericKey> keys = {{"LWE", lwe_key, n}, {"RLWE", rlwe_key, N}};
+    h->op = h->ctx->ConstructOperator(keys);
+    return h;
+}
+
+static const AlignedBuffer& ss_brk(SSHandle* h) {
+    if (auto* c = dynamic_cast<CGGIBlindRotator*>(h->op->m_rotator.get())) return c->m_brk;
+    return dynamic_cast<BMMPBlindRotator*>(h->op->m_rotator.get())->m_brk;
+}
+
+// what: 0 blind-rotation key, 1 trace keys (indices 3, 5, 9, .., N+1 concatenated), 2 squaring key
+uint64_t ref_ss_key_words(void* hp, int what) {
+    auto* h = (SSHandle*)hp;
+    if (what == 0) return ss_brk(h).size();
+    if (what == 1) {
+        uint64_t w = 0;
+        for (auto& e : h->op->m_trace_eval->m_trace_evaluators) w += e->m_converter->m_ksk.size();
+        return w;
+    }
+    return h->op->m_square_eval->m_ksk.size();
+}
+
+void ref_ss_key_copy(void* hp, int what, uint64_t* out) {
+    auto* h = (SSHandle*)hp;
+    if (what == 0) {
+        const auto& k = ss_brk(h);
+        std::copy(k.begin(), k.end(), out);
+    } else if (what == 1) {
+        for (auto& e : h->op->m_trace_eval->m_trace_evaluators)
+            out = std::copy(e->m_converter->m_ksk.begin(), e->m_converter->m_ksk.end(), out);
+    } else {
+        const auto& k = h->op->m_square_eval->m_ksk;
+        std::copy(k.begin(), k.end(), out);
+    }
+}
+
+// out: 4 N out_digits words (pre-zeroed here), [lev_left | lev_right], NTT domain
+void ref_ss_convert(void* hp, uint64_t* out, const uint64_t* lwe) {
+    auto* h = (SSHandle*)hp;
+    std::fill(out, out + 4 * h->N * h->out_digits, 0);
+    h->op->Convert(out, lwe);
+}
+
+void ref_ss_test_poly(void* hp, uint64_t* out) {  // the converter's m_acc (3N words)
+    auto* h = (SSHandle*)hp;
+    std::copy(h->op->m_acc.begin(), h->op->m_acc.end(), out);
+}
+
+void ref_ss_destroy(void* hp) { delete (SSHandle*)hp; }
 
 // type: 0 ROUND, 1 FLOOR, 2 CEIL (ModulusSwitchType order)
 void ref_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type) {

@@ -856,3 +856,105 @@ int tpo_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t targ
     }
     return 0;
 }
+
+/* ---- LWE -> RGSW scheme switching ------------------------------------------ */
+
+/* LWEtoRGSWConverter's constructor (lwe_to_rgsw_conversion.cpp:120-160): block
+ * size N/D; the first block holds +-scale centred on X^0, block b >= 1 holds
+ * scale * 2^(b*basebits) starting at X^(b*bs - bs/2); then times 2^-1, and the
+ * copy at [N, 2N) negated. max_digits = ceil(log2(p)/basebits) = ceil(64/basebits)
+ * (log2(p) is within 2^-31 of 64). */
+int tpo_ss_test_poly(uint64_t N, uint64_t D, uint64_t basebits, uint64_t* acc) {
+    if (D == 0 || basebits == 0 || N % D || ((N / D) & 1)) return -1;
+    const uint64_t max_digits = (64 + basebits - 1) / basebits;
+    if (max_digits < D || basebits * (max_digits - D) >= 31) return -1;
+    const uint64_t bs = N / D;
+    uint64_t scale = 1ULL << (basebits * (max_digits - D));
+    memset(acc, 0, 3 * N * 8);
+    for (uint64_t i = 0; i < bs / 2; ++i) {
+        acc[N + i] = scale;
+        acc[2 * N - i - 1] = P - scale;
+    }
+    for (uint64_t b = 1; b < D; ++b) {
+        scale <<= basebits;
+        for (uint64_t j = 0; j < bs; ++j) acc[N + b * bs + j - bs / 2] = scale;
+    }
+    const uint64_t half = tpo_inv(2);
+    for (uint64_t i = 0; i < N; ++i) {
+        acc[2 * N + i] = tpo_mul(acc[N + i], half);
+        acc[N + i] = tpo_sub(0, acc[2 * N + i]);
+    }
+    return 0;
+}
+
+/* TraceEvaluator::Eval (trace_evaluation.cpp:138-156), in place on [A | B]
+ * coefficients: x *= N^-1; for index N+1 down to 3: x += INTT(Auto_index(x));
+ * then both halves to the NTT domain. */
+static void trace_eval(uint64_t N, uint64_t bl, uint64_t dg, const uint64_t* keys, uint64_t* x, uint64_t* tmp) {
+    const uint64_t ninv = tpo_inv(N);
+    const uint64_t logn = int_log2(N);
+    for (uint64_t i = 0; i < 2 * N; ++i) x[i] = tpo_mul(x[i], ninv);
+    for (uint64_t j = logn; j >= 1; --j) {
+        memset(tmp, 0, 2 * N * 8);
+        tpo_auto_eval(N, bl, dg, (1ULL << j) + 1, keys + (j - 1) * 2 * N * dg, tmp, x);
+        tpo_ntt_backward(N, tmp, tmp);
+        tpo_ntt_backward(N, tmp + N, tmp + N);
+        for (uint64_t i = 0; i < 2 * N; ++i) x[i] = tpo_add(x[i], tmp[i]);
+    }
+    tpo_ntt_forward(N, x, x);
+    tpo_ntt_forward(N, x + N, x + N);
+}
+
+int tpo_lwe_to_rgsw(int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, const uint64_t* brk,
+                    uint64_t tr_bl, uint64_t tr_dg, const uint64_t* trace_keys, uint64_t sq_bl, uint64_t sq_dg,
+                    const uint64_t* sq_key, uint64_t D, uint64_t out_bl, const uint64_t* lwe, uint64_t* out) {
+    uint64_t* acc = (uint64_t*)malloc(3 * N * 8);
+    uint64_t* buf = (uint64_t*)malloc(4 * N * 8);
+    int rc = tpo_ss_test_poly(N, D, out_bl, acc);
+    uint64_t* left = out;
+    uint64_t* right = out + 2 * N * D;
+    const uint64_t bs = N / D;
+    if (rc == 0) rc = tpo_blind_rotate(variant, N, n, br_bl, br_dg, brk, right, lwe, acc, 1);
+    if (rc == 0) {
+        /* B += tp (line 180); [A, -A, B, -B] and the row rotations (lines 188-200) */
+        for (uint64_t i = 0; i < N; ++i) right[N + i] = tpo_add(right[N + i], acc[2 * N + i]);
+        for (uint64_t i = 0; i < N; ++i) {
+            buf[i] = right[i];
+            buf[N + i] = tpo_sub(0, right[i]);
+            buf[2 * N + i] = right[N + i];
+            buf[3 * N + i] = tpo_sub(0, right[N + i]);
+        }
+        for (uint64_t d = 1; d < D; ++d) {
+            memcpy(right + d * 2 * N, buf + d * bs, N * 8);
+            memcpy(right + d * 2 * N + N, buf + 2 * N + d * bs, N * 8);
+        }
+        for (uint64_t d = 0; d < D; ++d) trace_eval(N, tr_bl, tr_dg, trace_keys, right + d * 2 * N, buf);
+        /* RLWE(-s m) from RLWE(m) per row (lines 208-224) */
+        for (uint64_t d = 0; d < D; ++d) {
+            uint64_t* m = right + d * 2 * N;
+            uint64_t* sm = left + d * 2 * N;
+            memset(buf, 0, 2 * N * 8);
+            tpo_ntt_backward(N, buf, m);
+            memset(sm, 0, 2 * N * 8);
+            tpo_rlwe_ks(N, sq_bl, sq_dg, sq_key, sm, buf);
+            for (uint64_t i = 0; i < 2 * N; ++i) sm[i] = tpo_sub(0, sm[i]);
+            for (uint64_t i = 0; i < N; ++i) sm[i] = tpo_add(sm[i], m[N + i]);
+        }
+    }
+    free(acc);
+    free(buf);
+    return rc;
+}
+
+void tpo_ss_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, uint64_t tr_bl,
+                   uint64_t tr_dg, uint64_t sq_bl, uint64_t sq_dg, double std_dev, const uint64_t* lwe_key,
+                   const uint64_t* rlwe_key, uint64_t* brk, uint64_t* trace_keys, uint64_t* sq_key) {
+    tpo_br_keygen(r, variant, N, n, br_bl, br_dg, std_dev, lwe_key, rlwe_key, brk);
+    tpo_pack_keygen(r, N, tr_bl, tr_dg, std_dev, rlwe_key, trace_keys);
+    uint64_t* sq = (uint64_t*)malloc(N * 8);
+    tpo_ntt_forward(N, sq, rlwe_key);
+    for (uint64_t i = 0; i < N; ++i) sq[i] = tpo_mul(sq[i], sq[i]);
+    tpo_ntt_backward(N, sq, sq);
+    tpo_rlwe_ks_keygen(r, N, sq_bl, sq_dg, std_dev, sq, rlwe_key, sq_key);
+    free(sq);
+}

@@ -129,6 +129,26 @@ void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index,
  * 1 FLOOR, 2 CEIL, in 80-bit long double like the reference; in place. */
 int tpo_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type);
 
+/* ---- LWE -> RGSW scheme switching (lib/src/operators/lwe_to_rgsw_conversion.cpp) ---- */
+/* The converter's accumulator m_acc = [0 | -tp | tp] (3N words; lines 120-160).
+ * Returns -1 where the reference's first scale (an int shift) would overflow
+ * or out_digits does not split N into even blocks. */
+int tpo_ss_test_poly(uint64_t N, uint64_t out_digits, uint64_t out_basis_log2, uint64_t* acc);
+/* Convert (lines 168-225) of one LWE (n+1 words mod 2N) into 4 N out_digits
+ * words [lev_left | lev_right], NTT domain. trace_keys: automorphism keys for
+ * indices 2^j + 1, j = 1..logN, concatenated; sq_key: RLWE key switch s^2 -> s. */
+/* SchemeSwitchingContext::ConstructOperator (lwe_to_rgsw_conversion.cpp:72-108)
+ * from one sampler stream: the rotation key, the trace's automorphism keys
+ * (indices 3, 5, .., N+1), then the key switch from s^2 = INTT(NTT(s)^2) to s. */
+void tpo_ss_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                   uint64_t tr_basis_log2, uint64_t tr_digits, uint64_t sq_basis_log2, uint64_t sq_digits,
+                   double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk,
+                   uint64_t* trace_keys, uint64_t* sq_key);
+int tpo_lwe_to_rgsw(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                    const uint64_t* brk, uint64_t tr_basis_log2, uint64_t tr_digits, const uint64_t* trace_keys,
+                    uint64_t sq_basis_log2, uint64_t sq_digits, const uint64_t* sq_key, uint64_t out_digits,
+                    uint64_t out_basis_log2, const uint64_t* lwe, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

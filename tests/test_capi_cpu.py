@@ -55,3 +55,20 @@ def test_null_context_calls_fail_cleanly(native):
     assert native.tp_br_get_split(None) == 0
     assert native.tp_br_set_tile(None, 4) == _native.TP_ERR_PARAM
     assert native.tp_ntt_forward(1000, 1, None, None, None) == _native.TP_ERR_PARAM
+    assert native.tp_ss_create(None, 1 << 16, 4, 1 << 16, 4, 4, 1 << 16, 0, None) == _native.TP_ERR_PARAM
+    assert native.tp_ss_upload_keys(None, None, 0, None, 0, None, 0) == _native.TP_ERR_PARAM
+    assert native.tp_ss_accumulator(None, None) == _native.TP_ERR_PARAM
+    assert native.tp_lwe_to_rgsw_batch(None, 1, None, None, None) == _native.TP_ERR_PARAM
+    assert native.tp_ss_key_words(None, 0) == 0
+    assert native.tp_ss_destroy(None) == _native.TP_OK
+
+
+def test_scheme_switch_rejects_bad_output_gadget(native):
+    """Parameter checks run before any device call, so they answer on a machine without a GPU."""
+    from fhetoothpaste_b200 import _native
+    prm = _native.BrParams(0, _native.GOLDILOCKS, 256, 16, 1 << 16, 4)
+    h = ctypes.c_void_p()
+    for digits, basis in ((3, 1 << 16), (2, 1 << 16), (4, 3 << 10)):
+        assert native.tp_ss_create(ctypes.byref(prm), 1 << 16, 4, 1 << 16, 4, digits, basis, 0,
+                                   ctypes.byref(h)) == _native.TP_ERR_PARAM
+        assert not h.value
