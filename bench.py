@@ -332,6 +332,30 @@ def bootstrap_run(device: int) -> dict:
             "epilogue_ms": round(ep, 3), "launches": 2 * 5 + 4 + 1}  # graphs x 2 kernels, epilogues, key upload
 
 
+def scheme_switch_run(device: int) -> dict:
+    """LWE -> RGSW scheme switching at the shape of the reference's scheme-switch tests (CGGI
+    binary n=100, N=2048; rotation, trace and squaring gadgets base 2^14 l=4; output 4 digits of
+    base 2^14), 1024 conversions per call: rotation of the test polynomial, Lev rows, the trace
+    (11 automorphism key switches per row) and the s^2 -> s key switch."""
+    import torch
+    from fhetoothpaste_b200 import BlindRotationContext, GpuLWEtoRGSWConverter
+    from oracle.oracle import lwe_inputs
+    N, n, beta, l, D, batch = 2048, 100, 14, 4, 4, 1024
+    stream = torch.cuda.current_stream().cuda_stream
+    brk_words = BlindRotationContext(0, N, n, 1 << beta, l).key_words()
+    conv = GpuLWEtoRGSWConverter((0, N, n, 1 << beta, l), (1 << beta, l), (1 << beta, l), D, 1 << beta,
+                                 _uniform_key(brk_words, 61), _uniform_key(11 * 2 * N * l, 62),
+                                 _uniform_key(2 * N * l, 63), device=device)
+    lw = torch.from_numpy(lwe_inputs(N, n, batch, 64).view(np.int64)).cuda()
+    out = torch.empty((batch, 4 * N * D), dtype=torch.int64, device="cuda")
+    ms = _timed(torch, lambda: conv.convert_batch(batch, out.data_ptr(), lw.data_ptr(), stream), 1, 3, stream)
+    conv.close()
+    per_call = 1 + 1 + 11 + 1 + 1 + 1 + 1  # rotation, rows, 11 traces, NTT, INTT, key switch, assembly
+    return {"workload": "LWE->RGSW: CGGI binary n=100 N=2048, gadgets 2^14 l=4, out 4 digits 2^14",
+            "batch": batch, "conversions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
+            "launches": per_call * 4 + 3}  # + the three key re-layouts
+
+
 SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l = 3
 SERVING_MIX = [0.5, 0.35, 0.15]
 
@@ -553,8 +577,9 @@ def main():
         line["bmmp_batches"] = bmmp_batch_sweep(local)
         line["packing"] = packing_run(local)
         line["bootstrap"] = bootstrap_run(local)
+        line["scheme_switch"] = scheme_switch_run(local)
         launches += (line["bmmp_batches"].pop("launches") + line["packing"].pop("launches") +
-                     line["bootstrap"].pop("launches"))
+                     line["bootstrap"].pop("launches") + line["scheme_switch"].pop("launches"))
         line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

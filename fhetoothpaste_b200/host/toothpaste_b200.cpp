@@ -222,6 +222,29 @@ std::vector<uint64_t> PackingKeys(Sampler& rng, uint32_t N, uint32_t basis_log2,
     return all;
 }
 
+SchemeSwitchingKeySet SchemeSwitchingKeys(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t br_bl,
+                                          uint32_t br_dg, uint32_t tr_bl, uint32_t tr_dg, uint32_t sq_bl,
+                                          uint32_t sq_dg, double sd, const std::vector<uint64_t>& lwe_key,
+                                          const std::vector<uint64_t>& rlwe_key) {
+    SchemeSwitchingKeySet k;
+    k.rotation = BlindRotationKey(rng, variant, N, n, br_bl, br_dg, sd, lwe_key, rlwe_key);
+    k.trace = PackingKeys(rng, N, tr_bl, tr_dg, sd, rlwe_key);
+    // s^2 in Z_p[X]/(X^N + 1) (the reference's INTT(NTT(s)^2), lines 91-94), schoolbook
+    std::vector<uint64_t> sq(N, 0);
+    for (uint32_t i = 0; i < N; ++i) {
+        const uint64_t a = rlwe_key[i] % P;
+        if (!a) continue;
+        for (uint32_t j = 0; j < N; ++j) {
+            const uint64_t t = mulp(a, rlwe_key[j] % P);
+            const uint32_t d = i + j;
+            if (d < N) sq[d] = addp(sq[d], t);
+            else sq[d - N] = subp(sq[d - N], t);
+        }
+    }
+    k.square = RLWESwitchingKey(rng, N, sq_bl, sq_dg, sd, sq, rlwe_key);
+    return k;
+}
+
 }  // namespace keygen
 
 // ---- GpuBlindRotator ----
@@ -446,6 +469,74 @@ void GpuLWEtoLWEConverter::Convert(uint64_t* output, const uint64_t* input) {
     check(tp_lwe_ks_batch(m_ctx, 1, dout.p, din.p, nullptr));
     if (cudaMemcpy(output, dout.p, (m_n_out + 1ull) * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
         throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
+// ---- scheme switching ----
+
+static uint32_t log2_of(uint64_t b) {
+    uint32_t k = 0;
+    while ((1ull << k) < b) ++k;
+    return k;
+}
+
+GpuLWEtoRGSWConverter::GpuLWEtoRGSWConverter(const tp_br_params& rotation, uint64_t trace_basis,
+                                             uint32_t trace_digits, uint64_t square_basis, uint32_t square_digits,
+                                             uint32_t out_digits, uint64_t out_basis, const std::vector<uint64_t>& brk,
+                                             const std::vector<uint64_t>& trace_keys,
+                                             const std::vector<uint64_t>& square_key, int device)
+    : m_N(rotation.ring_dim), m_n(rotation.lwe_dim), m_D(out_digits) {
+    check(tp_ss_create(&rotation, trace_basis, trace_digits, square_basis, square_digits, out_digits, out_basis,
+                       device, &m_ctx));
+    tp_status s = tp_ss_upload_keys(m_ctx, brk.data(), brk.size(), trace_keys.data(), trace_keys.size(),
+                                    square_key.data(), square_key.size());
+    if (s != TP_OK) {
+        tp_ss_destroy(m_ctx);
+        check(s);
+    }
+}
+GpuLWEtoRGSWConverter::~GpuLWEtoRGSWConverter() { tp_ss_destroy(m_ctx); }
+
+void GpuLWEtoRGSWConverter::ConvertBatch(uint64_t batch, uint64_t* outputs, const uint64_t* lwes) {
+    if (batch == 0) return;
+    DevBuf din(batch * (m_n + 1ull)), dout(batch * OutputWords());
+    if (cudaMemcpy(din.p, lwes, batch * (m_n + 1ull) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_lwe_to_rgsw_batch(m_ctx, batch, dout.p, din.p, nullptr));
+    if (cudaMemcpy(outputs, dout.p, batch * OutputWords() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
+void GpuLWEtoRGSWConverter::Convert(uint64_t* output, const uint64_t* input) { ConvertBatch(1, output, input); }
+
+void GpuLWEtoRGSWConverter::Convert(std::vector<uint64_t>& output, const std::vector<uint64_t>& input) {
+    output.resize(OutputWords());
+    ConvertBatch(1, output.data(), input.data());
+}
+
+SchemeSwitchingContext::SchemeSwitchingContext(const tp_br_params& rotation, uint64_t trace_basis,
+                                               uint64_t trace_digits, uint64_t square_basis, uint64_t square_digits,
+                                               uint64_t output_digits, uint64_t output_basis, double std_dev,
+                                               int device, uint64_t seed)
+    : m_rot(rotation), m_tr_basis(trace_basis), m_tr_digits(trace_digits), m_sq_basis(square_basis),
+      m_sq_digits(square_digits), m_out_digits(output_digits), m_out_basis(output_basis), m_std(std_dev),
+      m_device(device), m_seed(seed) {
+    if (rotation.modulus != kGoldilocks)
+        throw std::invalid_argument("toothpaste_b200: modulus must be 2^64 - 2^32 + 1");
+    for (uint64_t b : {rotation.basis, trace_basis, square_basis, output_basis})
+        if (b < 2 || (b & (b - 1))) throw std::invalid_argument("toothpaste_b200: gadget bases must be powers of two");
+}
+
+std::unique_ptr<GpuLWEtoRGSWConverter> SchemeSwitchingContext::ConstructOperator(
+    const std::vector<std::vector<uint64_t>>& keys) const {
+    if (keys.size() < 2 || keys[0].size() < m_rot.lwe_dim || keys[1].size() < m_rot.ring_dim)
+        throw std::invalid_argument("toothpaste_b200: keys = {LWE key (n), RLWE key (N)}");
+    Sampler rng(m_seed);
+    auto k = keygen::SchemeSwitchingKeys(rng, m_rot.variant, m_rot.ring_dim, m_rot.lwe_dim, log2_of(m_rot.basis),
+                                         m_rot.digits, log2_of(m_tr_basis), (uint32_t)m_tr_digits,
+                                         log2_of(m_sq_basis), (uint32_t)m_sq_digits, m_std, keys[0], keys[1]);
+    return std::make_unique<GpuLWEtoRGSWConverter>(m_rot, m_tr_basis, (uint32_t)m_tr_digits, m_sq_basis,
+                                                   (uint32_t)m_sq_digits, (uint32_t)m_out_digits, m_out_basis,
+                                                   k.rotation, k.trace, k.square, m_device);
 }
 
 }  // namespace toothpaste_b200

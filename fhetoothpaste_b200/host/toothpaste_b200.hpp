@@ -61,6 +61,16 @@ std::vector<uint64_t> AutomorphismKey(Sampler& rng, uint32_t N, uint32_t basis_l
                                       uint32_t index, const std::vector<uint64_t>& key);
 std::vector<uint64_t> PackingKeys(Sampler& rng, uint32_t N, uint32_t basis_log2, uint32_t digits, double std_dev,
                                   const std::vector<uint64_t>& key);
+// SchemeSwitchingContext::ConstructOperator (lib/src/operators/lwe_to_rgsw_conversion.cpp:72-108)
+// from one sampler stream: the rotation key, the trace's automorphism keys (indices 3, 5, .., N+1),
+// then the key switch from s^2 to s.
+struct SchemeSwitchingKeySet {
+    std::vector<uint64_t> rotation, trace, square;
+};
+SchemeSwitchingKeySet SchemeSwitchingKeys(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t br_basis_log2,
+                                          uint32_t br_digits, uint32_t tr_basis_log2, uint32_t tr_digits,
+                                          uint32_t sq_basis_log2, uint32_t sq_digits, double std_dev,
+                                          const std::vector<uint64_t>& lwe_key, const std::vector<uint64_t>& rlwe_key);
 }  // namespace keygen
 
 // BlindRotator (lib/include/interfaces/blindrotation_operator.h:183-212).
@@ -215,6 +225,53 @@ public:
 private:
     tp_lwe_ks_ctx* m_ctx = nullptr;
     uint32_t m_n_in, m_n_out;
+};
+
+// LWEtoRGSWConverter (lib/src/operators/lwe_to_rgsw_conversion.cpp:115-225): Convert writes
+// 4 N out_digits words [lev_left rows | lev_right rows] in the NTT domain. The reference
+// accumulates the squaring step into the caller's lev_left rows, so its callers pass a zeroed
+// output; here those rows are written fresh, which is the same result.
+class GpuLWEtoRGSWConverter {
+public:
+    GpuLWEtoRGSWConverter(const tp_br_params& rotation, uint64_t trace_basis, uint32_t trace_digits,
+                          uint64_t square_basis, uint32_t square_digits, uint32_t out_digits, uint64_t out_basis,
+                          const std::vector<uint64_t>& brk, const std::vector<uint64_t>& trace_keys,
+                          const std::vector<uint64_t>& square_key, int device = 0);
+    ~GpuLWEtoRGSWConverter();
+    GpuLWEtoRGSWConverter(const GpuLWEtoRGSWConverter&) = delete;
+    GpuLWEtoRGSWConverter& operator=(const GpuLWEtoRGSWConverter&) = delete;
+    void Convert(uint64_t* output, const uint64_t* input);
+    void Convert(std::vector<uint64_t>& output, const std::vector<uint64_t>& input);
+    // Many at once on host buffers: lwes rows of n+1 words, outputs rows of 4 N out_digits words.
+    void ConvertBatch(uint64_t batch, uint64_t* outputs, const uint64_t* lwes);
+    uint64_t OutputWords() const { return 4ull * m_N * m_D; }
+
+private:
+    tp_ss_ctx* m_ctx = nullptr;
+    uint32_t m_N, m_n, m_D;
+};
+
+// SchemeSwitchingContext(rotation, trace, squaring, output_digits, output_basis)
+// (lib/src/operators/lwe_to_rgsw_conversion.cpp:10-108): the rotation context's parameters, the
+// trace's and the squaring converter's gadgets, and the output gadget of the RGSW.
+class SchemeSwitchingContext {
+public:
+    SchemeSwitchingContext(const tp_br_params& rotation, uint64_t trace_basis, uint64_t trace_digits,
+                           uint64_t square_basis, uint64_t square_digits, uint64_t output_digits,
+                           uint64_t output_basis, double std_dev, int device = 0, uint64_t seed = 1);
+    // keys = {LWE key (n words), RLWE key (N words, coefficients)}
+    std::unique_ptr<GpuLWEtoRGSWConverter> ConstructOperator(const std::vector<std::vector<uint64_t>>& keys) const;
+    uint64_t GetOutputDigits() const { return m_out_digits; }
+    uint64_t GetOutputBasis() const { return m_out_basis; }
+    void SetOutputDigits(uint64_t d) { m_out_digits = d; }
+    void SetOutputBasis(uint64_t b) { m_out_basis = b; }
+
+private:
+    tp_br_params m_rot;
+    uint64_t m_tr_basis, m_tr_digits, m_sq_basis, m_sq_digits, m_out_digits, m_out_basis;
+    double m_std;
+    int m_device;
+    uint64_t m_seed;
 };
 
 }  // namespace toothpaste_b200

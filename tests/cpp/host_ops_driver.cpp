@@ -8,7 +8,11 @@
 //   rotate      variant N n beta digits std seed lwe_key rlwe_key lwes count accs out
 //   pack        N beta digits std seed rlwe_key lwes len out
 //   evalfunc    N n beta digits seed lwe_key rlwe_key lwes(3 rows) lut out
+//   keygen-ss   variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed lwe_key rlwe_key out
+//   ss          variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed out_digits out_beta
+//               lwe_key rlwe_key lwes count out
 //   errors
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -121,6 +125,38 @@ static int run(int argc, char** argv) {
         save(argv[10], out.data(), out.size());
         return 0;
     }
+    if (mode == "keygen-ss" && argc == 16) {
+        Sampler rng(u(argv[12]));
+        const auto k = keygen::SchemeSwitchingKeys(
+            rng, (int)u(argv[2]), (uint32_t)u(argv[3]), (uint32_t)u(argv[4]), (uint32_t)u(argv[5]),
+            (uint32_t)u(argv[6]), (uint32_t)u(argv[7]), (uint32_t)u(argv[8]), (uint32_t)u(argv[9]),
+            (uint32_t)u(argv[10]), std::atof(argv[11]), load(argv[13]), load(argv[14]));
+        std::vector<uint64_t> all(k.rotation);
+        all.insert(all.end(), k.trace.begin(), k.trace.end());
+        all.insert(all.end(), k.square.begin(), k.square.end());
+        save(argv[15], all.data(), all.size());
+        return 0;
+    }
+    if (mode == "ss" && argc == 20) {
+        // SchemeSwitchingContext -> ConstructOperator -> Convert one by one, then ConvertBatch;
+        // both must agree. Output: the batch result.
+        const tp_br_params rot{(int32_t)u(argv[2]), kGoldilocks, (uint32_t)u(argv[3]), (uint32_t)u(argv[4]),
+                               1ull << u(argv[5]), (uint32_t)u(argv[6])};
+        SchemeSwitchingContext ctx(rot, 1ull << u(argv[7]), u(argv[8]), 1ull << u(argv[9]), u(argv[10]), u(argv[13]),
+                                   1ull << u(argv[14]), std::atof(argv[11]), 0, u(argv[12]));
+        auto conv = ctx.ConstructOperator({load(argv[15]), load(argv[16])});
+        const auto lwes = load(argv[17]);
+        const uint64_t count = u(argv[18]), n = rot.lwe_dim;
+        std::vector<uint64_t> batch(count * conv->OutputWords()), one;
+        conv->ConvertBatch(count, batch.data(), lwes.data());
+        for (uint64_t i = 0; i < count; ++i) {
+            conv->Convert(one, std::vector<uint64_t>(lwes.begin() + i * (n + 1), lwes.begin() + (i + 1) * (n + 1)));
+            if (!std::equal(one.begin(), one.end(), batch.begin() + i * conv->OutputWords()))
+                throw std::runtime_error("Convert and ConvertBatch differ");
+        }
+        save(argv[19], batch.data(), batch.size());
+        return 0;
+    }
     if (mode == "errors") {
         // parameter checks that the reference asserts (bmmp_blind_rotation.cpp:16-24) and
         // C-ABI refusals surfacing as exceptions; none of these reaches a device
@@ -136,6 +172,13 @@ static int run(int argc, char** argv) {
         });
         bad += !throws([] { GpuBlindRotator(TP_BR_CGGI_BINARY, 1000, 16, 1ull << 16, 3, {}, 0); });
         bad += !throws([] { GpuBlindRotator(TP_BR_CGGI_BINARY, 1024, 16, 1ull << 16, 9, {}, 0); });
+        const tp_br_params rot{TP_BR_CGGI_BINARY, kGoldilocks, 256, 16, 1ull << 16, 4};
+        bad += !throws([&] { SchemeSwitchingContext(rot, 1ull << 16, 4, 3ull << 10, 4, 4, 1ull << 16, 3.2); });
+        bad += !throws([&] {
+            SchemeSwitchingContext c(rot, 1ull << 16, 4, 1ull << 16, 4, 4, 1ull << 16, 3.2);
+            c.ConstructOperator({{1, 0}, {}});
+        });
+        bad += !throws([&] { GpuLWEtoRGSWConverter(rot, 1ull << 16, 4, 1ull << 16, 4, 3, 1ull << 16, {}, {}, {}); });
         std::cout << (bad ? "FAIL " : "ok ") << bad << "\n";
         return bad ? 1 : 0;
     }

@@ -125,3 +125,31 @@ def test_cpp_function_evaluator_like_oracle(driver, oracle, cuda, tmp_path):
         want = np.full(N + 1, 7, np.uint64)
         oracle.L.tpo_sample_extract(ptr(want), ptr(rl), 0, N)
         np.testing.assert_array_equal(got[row], want, err_msg=f"row {row}")
+
+
+SS_CASE = (CGGI_BINARY, 256, 16, (16, 4), (14, 4), (20, 3), 3.2)
+
+
+def test_scheme_switch_keygen_equals_oracle(driver, oracle, tmp_path):
+    """keygen::SchemeSwitchingKeys draws the three keys from one stream in the reference's order."""
+    variant, N, n, br, tr, sq, std = SS_CASE
+    sk = lwe_secret(variant, n, N, seed=81)
+    z = rlwe_secret(N, seed=82)
+    got = run(driver, tmp_path, "keygen-ss", variant, N, n, *br, *tr, *sq, std, 23, sk, z)
+    want = np.concatenate(oracle.ss_keygen(variant, N, n, br, tr, sq, std, sk, z, 23))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", [CGGI_BINARY, BMMP_BINARY], ids=["cggi", "bmmp"])
+def test_cpp_scheme_switch_like_oracle(driver, oracle, cuda, tmp_path, variant):
+    _, N, n, br, tr, sq, std = SS_CASE
+    D, ob, count = 4, 10, 3
+    sk = lwe_secret(variant, n, N, seed=91)
+    z = rlwe_secret(N, seed=92)
+    lwes = lwe_inputs(N, n, count, seed=93)
+    got = run(driver, tmp_path, "ss", variant, N, n, *br, *tr, *sq, std, 29, D, ob, sk, z, lwes, count)
+    keys = oracle.ss_keygen(variant, N, n, br, tr, sq, std, sk, z, 29)
+    for j in range(count):
+        want = oracle.lwe_to_rgsw(variant, N, n, br, keys[0], tr, keys[1], sq, keys[2], D, ob, lwes[j])
+        np.testing.assert_array_equal(got.reshape(count, -1)[j], want, err_msg=f"input {j}")
