@@ -176,6 +176,23 @@ def case_key_retile_n2048(torch):
     rot.close()
 
 
+def case_lwe_to_rgsw_n2048(torch):
+    """LWE -> RGSW scheme switching, 256 LWEs (CGGI binary n=100, N=2048, gadgets 2^14 l=4, out 4
+    digits): br_kernel, ss_rows_kernel, 11 trace ks_kernel launches, ntt_batch_kernel x2,
+    ks_kernel (s^2 -> s), ss_assemble_kernel per conversion call."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuLWEtoRGSWConverter
+    N, n, beta, l, D, batch = 2048, 100, 14, 4, 4, 256
+    words = BlindRotationContext(0, N, n, 1 << beta, l).key_words()
+    conv = GpuLWEtoRGSWConverter((0, N, n, 1 << beta, l), (1 << beta, l), (1 << beta, l), D, 1 << beta,
+                                 _u64(61, words), _u64(62, 11 * 2 * N * l), _u64(63, 2 * N * l))
+    lw = _dev(torch, _u64(64, (batch, n + 1), 2 * N))
+    out = torch.empty((batch, 4 * N * D), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        conv.convert_batch(batch, out.data_ptr(), lw.data_ptr())
+    torch.cuda.synchronize()
+    conv.close()
+
+
 CASES = {name[5:]: fn for name, fn in globals().items() if name.startswith("case_")}
 
 
