@@ -102,6 +102,13 @@ def lib() -> ctypes.CDLL:
         "tp_ss_upload_keys": (ctypes.c_int, [VP, U64P, U64, U64P, U64, U64P, U64]),
         "tp_ss_accumulator": (ctypes.c_int, [VP, U64P]),
         "tp_lwe_to_rgsw_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_sap_create": (ctypes.c_int, [ctypes.POINTER(BrParams), U64, ctypes.c_uint32, U64, ctypes.c_uint32,
+                                         ctypes.c_int, ctypes.POINTER(VP)]),
+        "tp_sap_destroy": (ctypes.c_int, [VP]),
+        "tp_sap_key_words": (U64, [VP, ctypes.c_int]),
+        "tp_sap_upload_keys": (ctypes.c_int, [VP, U64P, U64, U64P, U64, U64P, U64]),
+        "tp_sap_decompose_batch": (ctypes.c_int, [VP, U64, VP, U64, VP, U64, U64, U64,
+                                                  ctypes.POINTER(ctypes.c_uint32), VP]),
         "tp_server_create": (ctypes.c_int, [ctypes.c_int, U64, ctypes.POINTER(VP)]),
         "tp_server_add_set": (ctypes.c_int, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),

@@ -19,6 +19,7 @@
 #include "util_kernels.cuh"
 #include "ks_kernels.cuh"
 #include "ks_util_kernels.cuh"
+#include "sap_kernels.cuh"
 #include "ss_kernels.cuh"
 
 namespace {
@@ -723,7 +724,7 @@ struct tp_ks_ctx {
     bool key_ready = false;
     tp::KsKernelParams kp{};
     size_t smem = 0;
-    int per_sm[4] = {0, 0, 0, 0};
+    int per_sm[tp::kKsModes] = {};
     uint64_t* work = nullptr;     // packing tree nodes
     uint64_t work_words = 0;
     std::mutex mu;
@@ -770,7 +771,7 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     kp.n_inv = c->tab->n_inv;
     signed_digit_consts(beta, digits, kp.corr, kp.dshift, kp.dmask, kp.ddelta);
     c->smem = tp::ks_smem_words(ring_dim) * 8;
-    for (int mode = 0; mode < 4; ++mode) {
+    for (int mode = 0; mode < tp::kKsModes; ++mode) {
         const void* k = tp::ks_kernel_lookup(c->logn, mode);
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem);
         if (e == cudaSuccess)
@@ -1416,6 +1417,243 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     // 5. RGSW = [lev_left | lev_right] (lines 218-224)
     tp::ss_assemble_kernel<<<blocks, 256, 0, st>>>(out, c->rows, c->sqout, batch, (uint32_t)D, (uint32_t)N);
     TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SAP digit decomposition (lib/src/operators/sap_decomposer.cpp)
+// ---------------------------------------------------------------------------
+struct tp_sap_ctx {
+    int device = 0;
+    uint32_t N = 0, n = 0, logn = 0;
+    tp_br_ctx* br = nullptr;          // rotation of any variant
+    tp_ks_ctx* trace = nullptr;       // automorphism keys 2^j + 1, j = 1..log2 N
+    tp_lwe_ks_ctx* lks = nullptr;     // LWE key switch N -> n (the reset)
+    bool ready = false;
+    // constants: [extract poly | pad poly | overflow poly] in the NTT domain, fresh acc (0, Q/2N)
+    uint64_t* consts = nullptr;
+    uint64_t* fresh = nullptr;
+    uint64_t radix = 0;               // radix the constants were made for
+    // scratch, sized for `cap` LWEs and `leaves` tree leaves per LWE
+    uint64_t *copy = nullptr, *sub = nullptr, *modulus = nullptr, *acc = nullptr, *ext = nullptr, *lw = nullptr,
+             *tree = nullptr;
+    uint8_t* flags = nullptr;
+    uint64_t cap = 0, leaves = 0;
+    std::mutex mu;
+};
+
+tp_status tp_sap_destroy(tp_sap_ctx* c) {
+    if (!c) return TP_OK;
+    cudaSetDevice(c->device);
+    tp_br_destroy(c->br);
+    tp_ks_destroy(c->trace);
+    tp_lwe_ks_destroy(c->lks);
+    for (void* p : {(void*)c->consts, (void*)c->fresh, (void*)c->copy, (void*)c->sub, (void*)c->modulus,
+                    (void*)c->acc, (void*)c->ext, (void*)c->lw, (void*)c->tree, (void*)c->flags})
+        cudaFree(p);
+    delete c;
+    return TP_OK;
+}
+
+tp_status tp_sap_create(const tp_br_params* rotation, uint64_t trace_basis, uint32_t trace_digits, uint64_t ks_basis,
+                        uint32_t ks_digits, int device, tp_sap_ctx** out) {
+    if (!out || !rotation) return fail(TP_ERR_PARAM, "null argument");
+    *out = nullptr;
+    auto* c = new tp_sap_ctx();
+    c->device = device;
+    c->N = rotation->ring_dim;
+    c->n = rotation->lwe_dim;
+    tp_status s = tp_br_create(rotation, device, &c->br);
+    if (s == TP_OK) {
+        c->logn = ilog2(c->N);
+        s = tp_pack_create(c->N, trace_basis, trace_digits, device, &c->trace);
+    }
+    if (s == TP_OK) s = tp_lwe_ks_create(kP, c->N, c->n, ks_basis, ks_digits, device, &c->lks);
+    if (s != TP_OK) {
+        tp_sap_destroy(c);
+        return s;
+    }
+    std::vector<uint64_t> fresh(2ull * c->N, 0);
+    fresh[c->N] = kP / (2ull * c->N);
+    cudaError_t e = cudaMalloc(&c->fresh, fresh.size() * 8);
+    if (e == cudaSuccess) e = cudaMemcpy(c->fresh, fresh.data(), fresh.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&c->consts, 3ull * c->N * 8);
+    if (e != cudaSuccess) {
+        tp_sap_destroy(c);
+        return fail(TP_ERR_CUDA, "SAP constants: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return TP_OK;
+}
+
+uint64_t tp_sap_key_words(const tp_sap_ctx* c, int which) {
+    if (!c) return 0;
+    if (which == 0) return tp_br_key_words(c->br);
+    if (which == 1) return tp_ks_key_words(c->trace);
+    return tp_lwe_ks_key_words(c->lks);
+}
+
+tp_status tp_sap_upload_keys(tp_sap_ctx* c, const uint64_t* brk, uint64_t brk_words, const uint64_t* trace_keys,
+                             uint64_t trace_words, const uint64_t* lwe_ksk, uint64_t lwe_ksk_words) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->ready = false;
+    tp_status s = tp_br_upload_key(c->br, brk, brk_words);
+    if (s == TP_OK) s = tp_ks_upload_key(c->trace, trace_keys, trace_words);
+    if (s == TP_OK) s = tp_lwe_ks_upload_key(c->lks, lwe_ksk, lwe_ksk_words);
+    if (s == TP_OK) c->ready = true;
+    return s;
+}
+
+// Constants for `radix` (NTT domain): the extraction polynomial x -> x mod radix,
+// reversed (lines 394-399), the truncation pad sum_{i<radix} X^(i-(radix-1))
+// (lines 212-217) and the reset's overflow polynomial (lines 320-324, radix 0 as
+// Decompose passes it, so IntLog2(0) = 0: -(N - i) at X^i).
+static tp_status sap_constants(tp_sap_ctx* c, uint64_t radix, cudaStream_t st) {
+    if (c->radix == radix) return TP_OK;
+    const uint64_t N = c->N;
+    std::vector<uint64_t> h(3 * N, 0);
+    for (uint64_t i = 1; i < N; ++i) h[N - i] = (kP - (i & (radix - 1))) % kP;
+    for (uint64_t i = N - (radix - 1); i < N; ++i) h[N + i] = kP - 1;
+    h[N] = 1;
+    for (uint64_t i = 1; i < N; ++i) h[2 * N + i] = kP - (N - i);
+    TP_CUDA(cudaMemcpyAsync(c->consts, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
+    tp_status s = ntt_launch((uint32_t)N, 3, c->consts, c->consts, st, true);
+    if (s != TP_OK) return s;
+    TP_CUDA(cudaStreamSynchronize(st));
+    c->radix = radix;
+    return TP_OK;
+}
+
+static unsigned sap_blocks(uint64_t work) { return (unsigned)std::min<uint64_t>((work + 255) / 256, 65535); }
+
+tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, uint64_t out_digits,
+                                 const uint64_t* lwes, uint64_t radix, uint64_t hamming_weight,
+                                 uint64_t restart_period, uint32_t* digits_host, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->ready) return fail(TP_ERR_STATE, "keys not uploaded");
+    const uint64_t N = c->N, n = c->n;
+    if (radix < 2 || radix > N || (radix & (radix - 1)))
+        return fail(TP_ERR_PARAM, "radix must be a power of two in [2, N]");
+    if (restart_period == 0) return fail(TP_ERR_PARAM, "restart period must be positive (UINT64_MAX: never)");
+    if (batch == 0) return TP_OK;
+    if (!out || !lwes) return fail(TP_ERR_PARAM, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t logr = (uint32_t)ilog2(radix);
+    const uint32_t L = c->logn - logr;
+    const uint64_t leaves = 1ull << L;
+    if (c->cap < batch || c->leaves < leaves) {
+        for (void* p : {(void*)c->copy, (void*)c->sub, (void*)c->modulus, (void*)c->acc, (void*)c->ext,
+                        (void*)c->lw, (void*)c->tree, (void*)c->flags})
+            cudaFree(p);
+        c->copy = c->sub = c->modulus = c->acc = c->ext = c->lw = c->tree = nullptr;
+        c->flags = nullptr;
+        c->cap = c->leaves = 0;
+        const uint64_t B = std::max(batch, c->cap);
+        TP_CUDA(cudaMalloc(&c->copy, B * (n + 1) * 8));
+        TP_CUDA(cudaMalloc(&c->sub, B * (n + 1) * 8));
+        TP_CUDA(cudaMalloc(&c->lw, B * (n + 1) * 8));
+        TP_CUDA(cudaMalloc(&c->modulus, B * 8));
+        TP_CUDA(cudaMalloc(&c->flags, B));
+        TP_CUDA(cudaMalloc(&c->acc, B * 2 * N * 8));
+        TP_CUDA(cudaMalloc(&c->ext, B * 2 * N * 8));
+        TP_CUDA(cudaMalloc(&c->tree, B * leaves * 2 * N * 8));
+        c->cap = B;
+        c->leaves = leaves;
+    }
+    tp_status s = sap_constants(c, radix, st);
+    if (s != TP_OK) return s;
+    const uint64_t* xpoly = c->consts;
+    const uint64_t* pad = c->consts + N;
+    const uint64_t* ovf = c->consts + 2 * N;
+
+    // input moduli and digit counts (lines 409-416); one read-back to plan the steps
+    tp::sap_init_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(c->copy, c->modulus, c->acc, lwes, batch,
+                                                                       (uint32_t)n, (uint32_t)N);
+    TP_CUDA(cudaGetLastError());
+    std::vector<uint64_t> M(batch);
+    TP_CUDA(cudaMemcpyAsync(M.data(), c->modulus, batch * 8, cudaMemcpyDeviceToHost, st));
+    TP_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> digits(batch, 0);
+    uint32_t steps = 0;
+    for (uint64_t b = 0; b < batch; ++b) {
+        for (uint64_t m = M[b]; m > 1; m >>= logr) ++digits[b];
+        steps = std::max(steps, digits[b]);
+    }
+    if (digits_host) std::copy(digits.begin(), digits.end(), digits_host);
+    for (uint64_t b = 0; b < batch; ++b)
+        if (digits[b] > out_digits)
+            return fail(TP_ERR_PARAM, "LWE %llu needs %u digits, the output holds %llu", (unsigned long long)b,
+                        digits[b], (unsigned long long)out_digits);
+
+    const uint64_t out_stride = out_digits * (N + 1);
+    const uint64_t S = leaves * 2 * N;  // words of one LWE's tree
+    for (uint32_t d = 0; d < steps; ++d) {
+        bool any_reset = false, more = false;
+        for (uint64_t b = 0; b < batch; ++b) {
+            if (d < digits[b] && (d + 1) % restart_period == 0 && (M[b] >> (logr * (d + 1ull))) != 0)
+                any_reset = true;
+            if (d + 1 < digits[b]) more = true;
+        }
+        tp::sap_digit_kernel<<<sap_blocks(batch * (n + 1)), 256, 0, st>>>(
+            c->copy, c->sub, c->modulus, c->flags, batch, (uint32_t)n, (uint32_t)N, logr, hamming_weight, d,
+            restart_period);
+        TP_CUDA(cudaGetLastError());
+        // rotation of the coefficient-domain accumulator in place, NTT output (lines 432-434)
+        s = tp_br_blind_rotate_batch(c->br, batch, c->acc, c->sub, n + 1, c->acc, 2 * N, 0, stream);
+        if (s != TP_OK) return s;
+        // digit d = SampleExtract(INTT(acc (.) extract poly)) (lines 438-445)
+        tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, xpoly, 1, batch,
+                                                                         (uint32_t)N);
+        TP_CUDA(cudaGetLastError());
+        s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
+        if (s != TP_OK) return s;
+        tp::sap_extract_kernel<<<sap_blocks(batch * (N + 1)), 256, 0, st>>>(out, out_stride, d, c->ext, c->flags,
+                                                                          batch, (uint32_t)N);
+        TP_CUDA(cudaGetLastError());
+        if (any_reset) {
+            // ResetAccumulator (lines 293-351): overflow extraction, SampleExtract, LWE key
+            // switch, FLOOR switch to 2N, rotation of (0, Q/2N); taken where flagged
+            tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, ovf, 1, batch,
+                                                                             (uint32_t)N);
+            TP_CUDA(cudaGetLastError());
+            s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
+            if (s == TP_OK) s = tp_pbs_epilogue_batch(c->lks, batch, c->lw, c->ext, 2 * N, stream);
+            if (s == TP_OK) s = tp_br_blind_rotate_batch(c->br, batch, c->ext, c->lw, n + 1, c->fresh, 0, 0, stream);
+            if (s != TP_OK) return s;
+            tp::sap_select_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->ext, c->flags, batch,
+                                                                           (uint32_t)N);
+            TP_CUDA(cudaGetLastError());
+        }
+        if (!more) break;
+        // HomTrunc (lines 189-291) in coefficients: N^-1 and the pad, INTT, partial trace
+        // over N+1 .. 2^(L+1)+1, the truncation tree level by level, the leaf sum
+        tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->tree, S, c->acc, pad,
+                                                                         c->br->tab->n_inv, batch, (uint32_t)N);
+        TP_CUDA(cudaGetLastError());
+        s = ntt_launch((uint32_t)N, batch, c->tree, c->tree, stream, false, S, S);
+        if (s == TP_OK) s = ntt_launch((uint32_t)N, batch, c->tree + N, c->tree + N, stream, false, S, S);
+        if (s == TP_OK) s = ks_trace_steps(c->trace, batch, c->tree, S, (int)c->logn, (int)(L + 1), st);
+        if (s != TP_OK) return s;
+        for (uint32_t l = L; l >= 1; --l) {
+            tp::KsKernelParams kp = c->trace->kp;
+            kp.key = c->trace->key + (uint64_t)(l - 1) * c->trace->digits * 2 * N;
+            kp.in = c->tree;
+            kp.out = c->tree;
+            kp.items = batch << (L - l);
+            kp.in_stride = kp.out_stride = (2 * N) << l;
+            kp.right_offset = (2 * N) << (l - 1);
+            kp.auto_index = (1u << l) + 1;
+            kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+            kp.shift = (uint32_t)(N >> l);
+            s = ks_launch(c->trace, tp::kKsSplit, kp, st);
+            if (s != TP_OK) return s;
+        }
+        tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->tree, batch, (uint32_t)N, L);
+        TP_CUDA(cudaGetLastError());
+    }
     return TP_OK;
 }
 

@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_10(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<10, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<10, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<10, kKsMerge>;
-        default: return (const void*)ks_kernel<10, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<10, kKsTrace>;
+        default: return (const void*)ks_kernel<10, kKsSplit>;
     }
 }
 

@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_7(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<7, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<7, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<7, kKsMerge>;
-        default: return (const void*)ks_kernel<7, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<7, kKsTrace>;
+        default: return (const void*)ks_kernel<7, kKsSplit>;
     }
 }
 

@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_11(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<11, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<11, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<11, kKsMerge>;
-        default: return (const void*)ks_kernel<11, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<11, kKsTrace>;
+        default: return (const void*)ks_kernel<11, kKsSplit>;
     }
 }
 

@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_8(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<8, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<8, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<8, kKsMerge>;
-        default: return (const void*)ks_kernel<8, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<8, kKsTrace>;
+        default: return (const void*)ks_kernel<8, kKsSplit>;
     }
 }
 

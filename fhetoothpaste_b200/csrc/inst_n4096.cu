@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_12(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<12, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<12, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<12, kKsMerge>;
-        default: return (const void*)ks_kernel<12, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<12, kKsTrace>;
+        default: return (const void*)ks_kernel<12, kKsSplit>;
     }
 }
 

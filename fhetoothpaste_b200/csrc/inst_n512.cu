@@ -40,7 +40,8 @@ const void* ks_kernel_ptr_9(int mode) {
         case kKsRlwe: return (const void*)ks_kernel<9, kKsRlwe>;
         case kKsAuto: return (const void*)ks_kernel<9, kKsAuto>;
         case kKsMerge: return (const void*)ks_kernel<9, kKsMerge>;
-        default: return (const void*)ks_kernel<9, kKsTrace>;
+        case kKsTrace: return (const void*)ks_kernel<9, kKsTrace>;
+        default: return (const void*)ks_kernel<9, kKsSplit>;
     }
 }
 

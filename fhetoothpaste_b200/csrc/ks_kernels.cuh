@@ -18,8 +18,10 @@ enum KsMode : int {
     kKsRlwe = 0,   // out -= KS(in.A coef); out.B += in.B (NTT)
     kKsAuto = 1,   // out -= KS(aut_t(in.A)); out.B += NTT(aut_t(in.B)); in coefficient domain
     kKsMerge = 2,  // packing merge: left <- (right + X^s left) + INTT(AutoKS(right - X^s left))
-    kKsTrace = 3   // trace step:    x <- x + INTT(AutoKS(x))
+    kKsTrace = 3,  // trace step:    x <- x + INTT(AutoKS(x))
+    kKsSplit = 4   // SAP truncation tree node: y = INTT(AutoKS(x)); x <- x + y; out1 <- X^-s (x - y)
 };
+constexpr int kKsModes = 5;
 
 struct KsKernelParams {
     const uint64_t* key;      // device layout: [digit][c][jp][t][2], C = 2
@@ -30,11 +32,11 @@ struct KsKernelParams {
     uint64_t items;           // ciphertexts (or merges)
     uint64_t in_stride;       // words between items' inputs
     uint64_t out_stride;      // words between items' outputs
-    uint64_t right_offset;    // kKsMerge: words from left node to right node
+    uint64_t right_offset;    // kKsMerge: words from left node to right node; kKsSplit: to the second child
     uint32_t digits;
     uint32_t auto_index;      // t (odd)
     uint32_t auto_index_inv;  // t^-1 mod 2N
-    uint32_t shift;           // kKsMerge: X^shift rotation of the left node
+    uint32_t shift;           // kKsMerge: X^shift rotation of the left node; kKsSplit: X^-shift of the difference
     uint64_t n_inv;
     uint64_t corr;
     uint32_t dshift[8];
@@ -188,9 +190,25 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
                                                               : gl_sub(bb[j], gl_canon(o[1][j]));
                     ntt_backward_unscaled<LOGN>(r, t, sel ? buf1 : buf0, tw_i);
                     sel ^= 1;
+                    if constexpr (MODE == kKsSplit) {
+                        // children of a truncation-tree node (sap_decomposer.cpp:266-284, in the
+                        // coefficient domain): x + y in place, X^-s (x - y) at right_offset
+                        uint64_t* out1 = out + prm.right_offset + h * N;
+                        const uint32_t s = prm.shift;
 #pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[j], prm.n_inv));
+                        for (int j = 0; j < 8; ++j) {
+                            const uint32_t m = t + j * T;
+                            const uint64_t y = gl_mul(r[j], prm.n_inv);
+                            out[h * N + m] = gl_add(base[h][j], y);
+                            const uint64_t z = gl_sub(base[h][j], y);
+                            if (m >= s) out1[m - s] = z;
+                            else out1[m + N - s] = gl_neg(z);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[j], prm.n_inv));
+                    }
                 }
             }
         }

@@ -363,6 +363,39 @@ tp_status tp_ss_accumulator(const tp_ss_ctx* ctx, uint64_t* out_host);
 tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* lwes_dev,
                                void* stream);
 
+/* ---- SAP digit decomposition ---------------------------------------------
+ * SAPDecomposer::Decompose (lib/src/operators/sap_decomposer.cpp:353-464) of a
+ * SAPDecompositionContext(rotation, trace, LWE conversion N -> n, radix) on the
+ * Goldilocks modulus, for a batch of LWEs per call. Per digit: a blind rotation
+ * of the LWE's running accumulator by its next radix digit, the digit's
+ * SampleExtract, optionally ResetAccumulator (lines 293-351: overflow
+ * extraction, LWE key switch, FLOOR switch to 2N, a fresh rotation), and
+ * HomTrunc (lines 189-291: partial trace and the truncation tree of automorphism
+ * key switches). Keys in the reference's layouts: the rotator's m_brk, the trace
+ * evaluators' m_ksk for indices 3, 5, 9, .., N+1 concatenated, and the LWE
+ * converter's m_ksk (N -> n). */
+typedef struct tp_sap_ctx tp_sap_ctx;
+tp_status tp_sap_create(const tp_br_params* rotation, uint64_t trace_basis, uint32_t trace_digits, uint64_t ks_basis,
+                        uint32_t ks_digits, int device, tp_sap_ctx** out);
+tp_status tp_sap_destroy(tp_sap_ctx* ctx);
+/* which: 0 blind-rotation key, 1 trace keys, 2 LWE key switch */
+uint64_t tp_sap_key_words(const tp_sap_ctx* ctx, int which);
+tp_status tp_sap_upload_keys(tp_sap_ctx* ctx, const uint64_t* brk, uint64_t brk_words, const uint64_t* trace_keys,
+                             uint64_t trace_words, const uint64_t* lwe_ksk, uint64_t lwe_ksk_words);
+/* Decomposes `batch` LWEs (device, rows of n+1 words; the input modulus of each
+ * is read from its words as the reference does) in base `radix` (a power of two
+ * in [2, N]) with the LWE key's Hamming weight `hamming_weight` (the reference's
+ * m_beta) and the accumulator reset every `restart_period` digits (the
+ * context's GetRestartIteration(); UINT64_MAX: never). Output (device): LWE b's
+ * digit d at out + (b out_digits + d)(N+1), an LWE of dimension N mod Q; words
+ * past an LWE's digit count are left untouched. digits_host (optional, batch
+ * entries) receives each LWE's digit count. Reads the input moduli back once
+ * (synchronising `stream`); the rest is asynchronous. Refuses the call if an LWE
+ * needs more than out_digits digits. */
+tp_status tp_sap_decompose_batch(tp_sap_ctx* ctx, uint64_t batch, uint64_t* out_dev, uint64_t out_digits,
+                                 const uint64_t* lwes_dev, uint64_t radix, uint64_t hamming_weight,
+                                 uint64_t restart_period, uint32_t* digits_host, void* stream);
+
 /* ---- Key files ------------------------------------------------------------
  * The reference keeps keys only in memory (no serialization). A key file holds
  * one key in the reference's own layout (the words tp_*_upload_key takes)

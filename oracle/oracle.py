@@ -155,6 +155,13 @@ class Oracle:
                                      U64P]),
             "tpo_lwe_to_rgsw": (I, [I, U64, U64, U64, U64, U64P, U64, U64, U64P, U64, U64, U64P, U64, U64, U64P,
                                     U64P]),
+            "tpo_ref_int_log2": (U64, [U64]),
+            "tpo_sap_keygen": (None, [R, I, U64, U64, U64, U64, U64, U64, U64, U64, D, U64P, U64P, U64P, U64P,
+                                      U64P]),
+            "tpo_sap_homtrunc": (I, [U64, U64, U64, U64P, U64, U64P, U64P]),
+            "tpo_sap_reset": (I, [I, U64, U64, U64, U64, U64P, U64, U64, U64P, U64, U64P]),
+            "tpo_sap_decompose": (I, [I, U64, U64, U64, U64, U64P, U64, U64, U64P, U64, U64, U64P, U64, U64, U64,
+                                      U64P, U64P, U64]),
             "tpo_psi": (U64, [U64]),
             "tpo_mul": (U64, [U64, U64]),
         }
@@ -316,6 +323,39 @@ class Oracle:
                                       ptr(np.ascontiguousarray(lwe, np.uint64)), ptr(out)) == 0
         return out
 
+    def sap_keygen(self, variant, N, n, br, tr, ks, std, lwe_key, rlwe_key, seed):
+        """(rotation key, trace keys, LWE key switch N -> n) from one sampler stream, as the reference makes them."""
+        r = Rng(seed)
+        brk = np.empty(self.L.tpo_brk_words(variant, N, n, br[1]), np.uint64)
+        trk = np.empty((N.bit_length() - 1) * tr[1] * 2 * N, np.uint64)
+        ksk = np.empty(N * ks[1] * (n + 1), np.uint64)
+        self.L.tpo_sap_keygen(ctypes.byref(r), variant, N, n, br[0], br[1], tr[0], tr[1], ks[0], ks[1], std,
+                              ptr(np.ascontiguousarray(lwe_key, np.uint64)),
+                              ptr(np.ascontiguousarray(rlwe_key, np.uint64)), ptr(brk), ptr(trk), ptr(ksk))
+        return brk, trk, ksk
+
+    def sap_homtrunc(self, N, tr, trace_keys, radix, rlwe_ntt) -> np.ndarray:
+        out = np.empty(2 * N, np.uint64)
+        assert self.L.tpo_sap_homtrunc(N, tr[0], tr[1], ptr(trace_keys), radix, ptr(out),
+                                       ptr(np.ascontiguousarray(rlwe_ntt, np.uint64))) == 0
+        return out
+
+    def sap_reset(self, variant, N, n, br, brk, ks, ksk, radix, acc_ntt) -> np.ndarray:
+        acc = np.array(acc_ntt, dtype=np.uint64)
+        assert self.L.tpo_sap_reset(variant, N, n, br[0], br[1], ptr(brk), ks[0], ks[1], ptr(ksk), radix,
+                                    ptr(acc)) == 0
+        return acc
+
+    def sap_decompose(self, variant, N, n, br, brk, tr, trace_keys, ks, ksk, radix, beta, restart, lwe,
+                      out_digits) -> np.ndarray:
+        """SAPDecomposer::Decompose of one LWE: (digits, out_digits x (N+1) words, zero past the digits)."""
+        out = np.zeros(out_digits * (N + 1), np.uint64)
+        d = self.L.tpo_sap_decompose(variant, N, n, br[0], br[1], ptr(brk), tr[0], tr[1], ptr(trace_keys), ks[0],
+                                     ks[1], ptr(ksk), radix, beta, restart,
+                                     ptr(np.ascontiguousarray(lwe, np.uint64)), ptr(out), out_digits)
+        assert d >= 0
+        return d, out.reshape(out_digits, N + 1)
+
     def phase_rlwe(self, rlwe_ntt: np.ndarray, sk: np.ndarray) -> np.ndarray:
         N = sk.size
         sk_ntt = self.ntt_forward(sk)
@@ -374,6 +414,16 @@ class Reference:
             "ref_ss_convert": (None, [VP, U64P, U64P]),
             "ref_ss_test_poly": (None, [VP, U64P]),
             "ref_ss_destroy": (None, [VP]),
+            "ref_sap_create": (VP, [I, U64, U64, U64, U64, U64, U64, U64, U64, D, U64, U64P, U64P]),
+            "ref_sap_restart": (U64, [VP]),
+            "ref_sap_set_restart": (None, [VP, U64]),
+            "ref_sap_beta": (U64, [VP]),
+            "ref_sap_key_words": (U64, [VP, I]),
+            "ref_sap_key_copy": (None, [VP, I, U64P]),
+            "ref_sap_decompose": (None, [VP, U64P, U64, U64P, U64]),
+            "ref_sap_homtrunc": (None, [VP, U64P, U64P, U64]),
+            "ref_sap_reset": (None, [VP, U64P, U64]),
+            "ref_sap_destroy": (None, [VP]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

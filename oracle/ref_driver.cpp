@@ -24,6 +24,7 @@
 #include "operators/endo_glwe_conversion.h"
 #include "operators/lwe_to_rgsw_conversion.h"
 #include "operators/lwe_to_rlwe_packing.h"
+#include "operators/sap_decomposition.h"
 #include "operators/trace_evaluation.h"
 #include "static/keys.h"
 #include "static/modulus_switching.h"
@@ -311,6 +312,100 @@ void ref_ss_test_poly(void* hp, uint64_t* out) {  // the converter's m_acc (3N w
 }
 
 void ref_ss_destroy(void* hp) { delete (SSHandle*)hp; }
+
+struct SAPHandle {
+    std::shared_ptr<SAPDecompositionContext> ctx;
+    std::unique_ptr<SAPDecomposer> op;
+    uint64_t N = 0, n = 0;
+};
+
+// SAPDecompositionContext(rotation, trace, LWE conversion N -> n, radix) and its operator.
+void* ref_sap_create(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                     uint64_t tr_basis_log2, uint64_t tr_digits, uint64_t ks_basis_log2, uint64_t ks_digits,
+                     double std_dev, uint64_t radix, const uint64_t* lwe_key, const uint64_t* rlwe_key) {
+    auto* h = new SAPHandle();
+    h->N = N;
+    h->n = n;
+    std::shared_ptr<OperatorContext<BlindRotator>> rot;
+    std::shared_ptr<MathWorker> ntt;
+    if (variant == 2) {
+        auto br = std::make_shared<BMMPBlindRotationContext>(KeyDistribution::BINARY, kQ, N, n, 1ULL << br_basis_log2,
+                                                             br_digits, std_dev, 2);
+        ntt = br->GetNTT();
+        rot = std::reinterpret_pointer_cast<OperatorContext<BlindRotator>>(br);
+    } else {
+        auto br = std::make_shared<CGGIBlindRotationContext>(
+            variant == 0 ? KeyDistribution::BINARY : KeyDistribution::TERNARY, kQ, N, n, 1ULL << br_basis_log2,
+            br_digits, std_dev);
+        ntt = br->GetNTT();
+        rot = std::reinterpret_pointer_cast<OperatorContext<BlindRotator>>(br);
+    }
+    auto tr = std::make_shared<TraceEvaluationContext>(BINARY, ntt, 1ULL << tr_basis_log2, tr_digits, std_dev);
+    auto cv = std::make_shared<LWEConversionContext>(BINARY, kQ, N, n, 1ULL << ks_basis_log2, ks_digits, std_dev);
+    h->ctx = std::make_shared<SAPDecompositionContext>(rot, tr, cv, radix);
+    std::vector<GenericKey> keys = {{"LWE", lwe_key, n}, {"RLWE", rlwe_key, N}};
+    h->op = h->ctx->ConstructOperator(keys);
+    return h;
+}
+
+uint64_t ref_sap_restart(void* hp) { return ((SAPHandle*)hp)->op->m_restart_iteration; }
+void ref_sap_set_restart(void* hp, uint64_t r) { ((SAPHandle*)hp)->op->m_restart_iteration = r; }
+uint64_t ref_sap_beta(void* hp) { return ((SAPHandle*)hp)->op->m_beta; }
+
+static const AlignedBuffer& sap_brk(SAPHandle* h) {
+    if (auto* c = dynamic_cast<CGGIBlindRotator*>(h->op->m_rotator.get())) return c->m_brk;
+    return dynamic_cast<BMMPBlindRotator*>(h->op->m_rotator.get())->m_brk;
+}
+
+// what: 0 blind-rotation key, 1 trace keys (indices 3, 5, 9, .., N+1 concatenated), 2 LWE key switch
+uint64_t ref_sap_key_words(void* hp, int what) {
+    auto* h = (SAPHandle*)hp;
+    if (what == 0) return sap_brk(h).size();
+    if (what == 1) {
+        uint64_t w = 0;
+        for (auto& e : h->op->m_packer->m_trace_evaluators) w += e->m_converter->m_ksk.size();
+        return w;
+    }
+    return h->op->m_lwe_converter->m_ksk.size();
+}
+
+void ref_sap_key_copy(void* hp, int what, uint64_t* out) {
+    auto* h = (SAPHandle*)hp;
+    if (what == 0) {
+        const auto& k = sap_brk(h);
+        std::copy(k.begin(), k.end(), out);
+    } else if (what == 1) {
+        for (auto& e : h->op->m_packer->m_trace_evaluators)
+            out = std::copy(e->m_converter->m_ksk.begin(), e->m_converter->m_ksk.end(), out);
+    } else {
+        const auto& k = h->op->m_lwe_converter->m_ksk;
+        std::copy(k.begin(), k.end(), out);
+    }
+}
+
+// Decompose with the LWE converter's accumulator fully cleared first (its own clear is
+// partial, lwe_conversion.cpp:217), so a reset inside behaves as on a fresh converter.
+// out: out_words words, zeroed here (SampleExtract writes only nonzero words).
+void ref_sap_decompose(void* hp, uint64_t* out, uint64_t out_words, const uint64_t* in, uint64_t radix) {
+    auto* h = (SAPHandle*)hp;
+    auto& acc = h->op->m_lwe_converter->m_acc;
+    std::fill(acc.begin(), acc.end(), 0);
+    std::fill(out, out + out_words, 0);
+    h->op->Decompose(out, in, radix);
+}
+
+void ref_sap_homtrunc(void* hp, uint64_t* out, uint64_t* in, uint64_t radix) {
+    ((SAPHandle*)hp)->op->HomTrunc(out, in, radix);
+}
+
+void ref_sap_reset(void* hp, uint64_t* acc, uint64_t radix) {
+    auto* h = (SAPHandle*)hp;
+    auto& a = h->op->m_lwe_converter->m_acc;
+    std::fill(a.begin(), a.end(), 0);
+    h->op->ResetAccumulator(acc, radix);
+}
+
+void ref_sap_destroy(void* hp) { delete (SAPHandle*)hp; }
 
 // type: 0 ROUND, 1 FLOOR, 2 CEIL (ModulusSwitchType order)
 void ref_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t target, int type) {

@@ -958,3 +958,195 @@ void tpo_ss_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t br_
     tpo_rlwe_ks_keygen(r, N, sq_bl, sq_dg, std_dev, sq, rlwe_key, sq_key);
     free(sq);
 }
+
+/* ---- SAP digit decomposition ------------------------------------------------ */
+
+uint64_t tpo_ref_int_log2(uint64_t x) { return int_log2(x); }
+
+static void ntt_pair(uint64_t N, uint64_t* x, int forward) {
+    if (forward) {
+        tpo_ntt_forward(N, x, x);
+        tpo_ntt_forward(N, x + N, x + N);
+    } else {
+        tpo_ntt_backward(N, x, x);
+        tpo_ntt_backward(N, x + N, x + N);
+    }
+}
+
+static void mul_pair(uint64_t N, uint64_t* x, const uint64_t* poly) {
+    for (uint64_t i = 0; i < N; ++i) {
+        x[i] = tpo_mul(x[i], poly[i]);
+        x[N + i] = tpo_mul(x[N + i], poly[i]);
+    }
+}
+
+static uint64_t brev_bits(uint64_t x, uint64_t bits) {
+    uint64_t r = 0;
+    for (uint64_t b = 0; b < bits; ++b) r |= ((x >> b) & 1) << (bits - 1 - b);
+    return r;
+}
+
+/* One node of the truncation tree (lines 243-289), depth first like the reference:
+ * a leaf adds x * X^brev(e) to out; an inner node at level l splits x into
+ * x + Auto(x) (exponent 2e) and (x - Auto(x)) * X^-(N >> l) (exponent 2e + 1),
+ * Auto = Auto_{2^l + 1} of INTT(x), all in the NTT domain. */
+static void trunc_node(uint64_t N, uint64_t bl, uint64_t dg, const uint64_t* keys, uint64_t L, uint64_t level,
+                       uint64_t e, uint64_t* x, uint64_t* out) {
+    uint64_t* poly = (uint64_t*)calloc(N, 8);
+    if (level == 0) {
+        poly[brev_bits(e, L)] = 1;
+        tpo_ntt_forward(N, poly, poly);
+        mul_pair(N, x, poly);
+        for (uint64_t i = 0; i < 2 * N; ++i) out[i] = tpo_add(out[i], x[i]);
+        free(poly);
+        return;
+    }
+    poly[N - (N >> level)] = P - 1;
+    tpo_ntt_forward(N, poly, poly);
+    uint64_t* c = (uint64_t*)malloc(2 * N * 8);
+    uint64_t* a = (uint64_t*)calloc(2 * N, 8);
+    uint64_t* t = (uint64_t*)malloc(2 * N * 8);
+    memcpy(c, x, 2 * N * 8);
+    ntt_pair(N, c, 0);
+    const uint64_t j = level;                       /* index 2^level + 1 is key j - 1 */
+    tpo_auto_eval(N, bl, dg, (1ULL << j) + 1, keys + (j - 1) * 2 * N * dg, a, c);
+    for (uint64_t i = 0; i < 2 * N; ++i) {
+        t[i] = tpo_sub(x[i], a[i]);
+        x[i] = tpo_add(x[i], a[i]);
+    }
+    mul_pair(N, t, poly);
+    trunc_node(N, bl, dg, keys, L, level - 1, 2 * e + 1, t, out);
+    trunc_node(N, bl, dg, keys, L, level - 1, 2 * e, x, out);
+    free(c);
+    free(a);
+    free(t);
+    free(poly);
+}
+
+int tpo_sap_homtrunc(uint64_t N, uint64_t bl, uint64_t dg, const uint64_t* keys, uint64_t radix, uint64_t* out,
+                     const uint64_t* in) {
+    if (radix < 1 || (radix & (radix - 1)) || radix > N || !get_tables(N)) return -1;
+    const uint64_t logn = int_log2(N), logr = tpo_ref_int_log2(radix);
+    uint64_t* pad = (uint64_t*)calloc(N, 8);
+    uint64_t* x = (uint64_t*)malloc(2 * N * 8);
+    uint64_t* c = (uint64_t*)malloc(2 * N * 8);
+    uint64_t* a = (uint64_t*)malloc(2 * N * 8);
+    /* sum_{i < radix} X^(i - (radix - 1)) (lines 212-217) */
+    for (uint64_t i = N - (radix - 1); i < N; ++i) pad[i] = P - 1;
+    pad[0] = 1;
+    tpo_ntt_forward(N, pad, pad);
+    const uint64_t ninv = tpo_inv(N);
+    for (uint64_t i = 0; i < 2 * N; ++i) x[i] = tpo_mul(in[i], ninv);
+    mul_pair(N, x, pad);
+    /* partial trace (lines 229-238) */
+    for (uint64_t i = 0; i < logr; ++i) {
+        const uint64_t j = logn - i;
+        memcpy(c, x, 2 * N * 8);
+        ntt_pair(N, c, 0);
+        memset(a, 0, 2 * N * 8);
+        tpo_auto_eval(N, bl, dg, (1ULL << j) + 1, keys + (j - 1) * 2 * N * dg, a, c);
+        for (uint64_t k = 0; k < 2 * N; ++k) x[k] = tpo_add(x[k], a[k]);
+    }
+    memset(out, 0, 2 * N * 8);
+    trunc_node(N, bl, dg, keys, logn - logr, logn - logr, 0, x, out);
+    free(pad);
+    free(x);
+    free(c);
+    free(a);
+    return 0;
+}
+
+int tpo_sap_reset(int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, const uint64_t* brk,
+                  uint64_t ks_bl, uint64_t ks_dg, const uint64_t* ksk, uint64_t radix, uint64_t* acc) {
+    if (!get_tables(N)) return -1;
+    const uint64_t r = tpo_ref_int_log2(radix);
+    uint64_t* poly = (uint64_t*)calloc(N, 8);
+    uint64_t* ext = (uint64_t*)calloc(N + 1, 8);
+    uint64_t* lwe = (uint64_t*)calloc(n + 1, 8);
+    uint64_t* fresh = (uint64_t*)calloc(2 * N, 8);
+    /* overflow extraction polynomial (lines 320-324) */
+    for (uint64_t i = 1; i < N; ++i) poly[i] = tpo_sub(0, ((N - i) >> r) << r);
+    tpo_ntt_forward(N, poly, poly);
+    mul_pair(N, acc, poly);
+    ntt_pair(N, acc, 0);
+    tpo_sample_extract(ext, acc, 0, N);
+    tpo_lwe_ks(P, N, n, ks_bl, ks_dg, ksk, lwe, ext);
+    tpo_modulus_switch(lwe, n + 1, P, 2 * N, 1);
+    fresh[N] = P / (2 * N);
+    const int rc = tpo_blind_rotate(variant, N, n, br_bl, br_dg, brk, acc, lwe, fresh, 0);
+    free(poly);
+    free(ext);
+    free(lwe);
+    free(fresh);
+    return rc;
+}
+
+int tpo_sap_decompose(int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, const uint64_t* brk,
+                      uint64_t tr_bl, uint64_t tr_dg, const uint64_t* keys, uint64_t ks_bl, uint64_t ks_dg,
+                      const uint64_t* ksk, uint64_t radix, uint64_t beta, uint64_t restart, const uint64_t* in,
+                      uint64_t* out, uint64_t out_digits) {
+    if (radix < 2 || (radix & (radix - 1)) || radix > N || !get_tables(N) || restart == 0) return -1;
+    const uint64_t r = tpo_ref_int_log2(radix), mask = radix - 1, q_in = 2 * N;
+    uint64_t* acc = (uint64_t*)calloc(2 * N, 8);
+    uint64_t* ext = (uint64_t*)malloc(2 * N * 8);
+    uint64_t* xp = (uint64_t*)calloc(N, 8);
+    uint64_t* copy = (uint64_t*)malloc((n + 1) * 8);
+    uint64_t* sub = (uint64_t*)malloc((n + 1) * 8);
+    int rc = 0;
+    /* acc = (0, Q/2N), B in the NTT domain (lines 389-392) */
+    acc[N] = P / (2 * N);
+    tpo_ntt_forward(N, acc + N, acc + N);
+    /* x -> x mod radix, reversed (lines 394-399) */
+    for (uint64_t i = 1; i < N; ++i) xp[N - i] = tpo_sub(0, i & mask);
+    tpo_ntt_forward(N, xp, xp);
+    memcpy(copy, in, (n + 1) * 8);
+    /* input modulus from the words themselves (lines 409-416) */
+    uint64_t M = 1ULL << tpo_ref_int_log2(in[0]);
+    for (uint64_t i = 1; i <= n; ++i)
+        if (M <= in[i]) M <<= 1;
+    uint64_t d = 0;
+    while (M > 1) {
+        for (uint64_t i = 0; i <= n; ++i) {
+            sub[i] = copy[i] & mask;
+            copy[i] >>= r;
+        }
+        M >>= r;
+        sub[n] = (uint64_t)(((unsigned __int128)sub[n] + radix * beta) % q_in);
+        copy[n] = copy[n] >= beta ? copy[n] - beta : copy[n] + M - beta;
+        ntt_pair(N, acc, 0);
+        rc = tpo_blind_rotate(variant, N, n, br_bl, br_dg, brk, acc, sub, acc, 0);
+        if (rc) break;
+        for (uint64_t i = 0; i < N; ++i) {
+            ext[i] = tpo_mul(acc[i], xp[i]);
+            ext[N + i] = tpo_mul(acc[N + i], xp[i]);
+        }
+        ntt_pair(N, ext, 0);
+        if (d >= out_digits) {
+            rc = -1;
+            break;
+        }
+        tpo_sample_extract(out + d * (N + 1), ext, 0, N);
+        if ((d + 1) % restart == 0 && M != 0) {
+            rc = tpo_sap_reset(variant, N, n, br_bl, br_dg, brk, ks_bl, ks_dg, ksk, 0, acc);
+            if (rc) break;
+        }
+        rc = tpo_sap_homtrunc(N, tr_bl, tr_dg, keys, radix, ext, acc);
+        if (rc) break;
+        memcpy(acc, ext, 2 * N * 8);
+        ++d;
+    }
+    free(acc);
+    free(ext);
+    free(xp);
+    free(copy);
+    free(sub);
+    return rc ? -1 : (int)d;
+}
+
+void tpo_sap_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, uint64_t tr_bl,
+                    uint64_t tr_dg, uint64_t ks_bl, uint64_t ks_dg, double std_dev, const uint64_t* lwe_key,
+                    const uint64_t* rlwe_key, uint64_t* brk, uint64_t* trace_keys, uint64_t* lwe_ksk) {
+    tpo_br_keygen(r, variant, N, n, br_bl, br_dg, std_dev, lwe_key, rlwe_key, brk);
+    tpo_pack_keygen(r, N, tr_bl, tr_dg, std_dev, rlwe_key, trace_keys);
+    tpo_lwe_ks_keygen(r, P, N, n, ks_bl, ks_dg, std_dev, rlwe_key, lwe_key, lwe_ksk);
+}

@@ -149,6 +149,33 @@ int tpo_lwe_to_rgsw(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2,
                     uint64_t sq_basis_log2, uint64_t sq_digits, const uint64_t* sq_key, uint64_t out_digits,
                     uint64_t out_basis_log2, const uint64_t* lwe, uint64_t* out);
 
+/* ---- SAP digit decomposition (lib/src/operators/sap_decomposer.cpp) ---- */
+/* The reference's IntLog2 (math_utils.cpp:11-25): ceil(log2 x), 0 for x <= 1. */
+uint64_t tpo_ref_int_log2(uint64_t x);
+/* SAPDecompositionContext::ConstructOperator (lines 166-186) from one sampler
+ * stream: the rotation key, the trace's automorphism keys (indices 3, 5, .., N+1),
+ * then the LWE key switch from the RLWE key's coefficients (N) to the LWE key (n). */
+void tpo_sap_keygen(tpo_rng* r, int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                    uint64_t tr_basis_log2, uint64_t tr_digits, uint64_t ks_basis_log2, uint64_t ks_digits,
+                    double std_dev, const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t* brk,
+                    uint64_t* trace_keys, uint64_t* lwe_ksk);
+/* HomTrunc (lines 189-291): out (2N, NTT domain) from in (2N, NTT domain); trace_keys
+ * for indices 2^j + 1, j = 1..logN. */
+int tpo_sap_homtrunc(uint64_t N, uint64_t tr_basis_log2, uint64_t tr_digits, const uint64_t* trace_keys,
+                     uint64_t radix, uint64_t* out, const uint64_t* in);
+/* ResetAccumulator (lines 293-351) on acc (2N, NTT domain, in place), with the LWE key
+ * switch N -> n of a fresh converter (its accumulator cleared). */
+int tpo_sap_reset(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                  const uint64_t* brk, uint64_t ks_basis_log2, uint64_t ks_digits, const uint64_t* lwe_ksk,
+                  uint64_t radix, uint64_t* acc);
+/* Decompose (lines 353-464): digits of `in` (n+1 words) written to out + d (N+1) (only
+ * nonzero words, the caller zeroes out), at most out_digits; returns the digit count,
+ * or -1 on bad parameters / too small an output. */
+int tpo_sap_decompose(int variant, uint64_t N, uint64_t n, uint64_t br_basis_log2, uint64_t br_digits,
+                      const uint64_t* brk, uint64_t tr_basis_log2, uint64_t tr_digits, const uint64_t* trace_keys,
+                      uint64_t ks_basis_log2, uint64_t ks_digits, const uint64_t* lwe_ksk, uint64_t radix,
+                      uint64_t beta, uint64_t restart, const uint64_t* in, uint64_t* out, uint64_t out_digits);
+
 #ifdef __cplusplus
 }
 #endif
