@@ -356,6 +356,33 @@ def scheme_switch_run(device: int) -> dict:
             "launches": per_call * 4 + 3}  # + the three key re-layouts
 
 
+def sap_run(device: int) -> dict:
+    """SAP digit decomposition at the shape of the reference's SAP tests (CGGI binary n=10,
+    N=4096, rotation / trace / LWE key-switch gadgets base 2^16 l=4, radix 32, inputs mod 2^40:
+    8 digits, each a rotation, an extraction and a truncation of 5 trace steps and a 127-node
+    key-switch tree), 64 LWEs per call."""
+    import torch
+    from fhetoothpaste_b200 import BlindRotationContext, GpuSAPDecomposer
+    N, n, beta, l, radix, batch = 4096, 10, 16, 4, 32, 64
+    stream = torch.cuda.current_stream().cuda_stream
+    brk_words = BlindRotationContext(0, N, n, 1 << beta, l).key_words()
+    dec = GpuSAPDecomposer((0, N, n, 1 << beta, l), (1 << beta, l), (1 << beta, l), _uniform_key(brk_words, 71),
+                           _uniform_key(12 * 2 * N * l, 72), _uniform_key(N * l * (n + 1), 73), hamming_weight=5,
+                           device=device)
+    rng = np.random.default_rng(74)
+    lw = torch.from_numpy(rng.integers(0, 1 << 40, (batch, n + 1), dtype=np.uint64).view(np.int64)).cuda()
+    out = torch.zeros((batch, 9, N + 1), dtype=torch.int64, device="cuda")
+    ms = _timed(torch, lambda: dec.decompose_batch(batch, out.data_ptr(), 9, lw.data_ptr(), radix, stream), 1, 3,
+                stream)
+    dec.close()
+    # per digit: digit, rotation, multiply, NTT, extract; per truncation (7 of them): multiply, 2 NTT,
+    # 5 trace steps, 7 tree levels, leaf sum; once: init, 3 constants
+    per_call = 1 + 8 * 5 + 7 * (1 + 2 + 5 + 7 + 1)
+    return {"workload": "SAP: CGGI binary n=10 N=4096, gadgets 2^16 l=4, radix 32, inputs mod 2^40 (8 digits)",
+            "batch": batch, "decompositions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
+            "launches": per_call * 4 + 3 + 1 + 3}  # + constants, key re-layouts
+
+
 SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l = 3
 SERVING_MIX = [0.5, 0.35, 0.15]
 
@@ -578,8 +605,10 @@ def main():
         line["packing"] = packing_run(local)
         line["bootstrap"] = bootstrap_run(local)
         line["scheme_switch"] = scheme_switch_run(local)
+        line["sap"] = sap_run(local)
         launches += (line["bmmp_batches"].pop("launches") + line["packing"].pop("launches") +
-                     line["bootstrap"].pop("launches") + line["scheme_switch"].pop("launches"))
+                     line["bootstrap"].pop("launches") + line["scheme_switch"].pop("launches") +
+                     line["sap"].pop("launches"))
         line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -222,6 +222,34 @@ std::vector<uint64_t> PackingKeys(Sampler& rng, uint32_t N, uint32_t basis_log2,
     return all;
 }
 
+std::vector<uint64_t> LWESwitchingKey(Sampler& rng, uint32_t n_in, uint32_t n_out, uint32_t basis_log2,
+                                      uint32_t digits, double sd, const std::vector<uint64_t>& source_key,
+                                      const std::vector<uint64_t>& target_key) {
+    std::vector<uint64_t> ksk((uint64_t)n_in * digits * (n_out + 1ull));
+    for (uint32_t i = 0; i < n_in; ++i) {
+        uint64_t g = 1ull << (64 - basis_log2);  // IntLog2(p) = 64
+        for (uint32_t j = 0; j < digits; ++j, g >>= basis_log2) {
+            uint64_t* row = ksk.data() + ((uint64_t)i * digits + j) * (n_out + 1ull);
+            // LWEEncryptor::MakeLWE (base_crypto.cpp:137-155): a uniform, b = e + <a, t> + msg
+            for (uint32_t k = 0; k < n_out; ++k) row[k] = rng.Uniform(P);
+            uint64_t b = rng.Gaussian(sd, P);
+            for (uint32_t k = 0; k < n_out; ++k) b = addp(b, mulp(row[k], target_key[k] % P));
+            row[n_out] = addp(b, mulp(g % P, source_key[i] % P));
+        }
+    }
+    return ksk;
+}
+
+SAPKeySet SAPKeys(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t br_bl, uint32_t br_dg, uint32_t tr_bl,
+                  uint32_t tr_dg, uint32_t ks_bl, uint32_t ks_dg, double sd, const std::vector<uint64_t>& lwe_key,
+                  const std::vector<uint64_t>& rlwe_key) {
+    SAPKeySet k;
+    k.rotation = BlindRotationKey(rng, variant, N, n, br_bl, br_dg, sd, lwe_key, rlwe_key);
+    k.trace = PackingKeys(rng, N, tr_bl, tr_dg, sd, rlwe_key);
+    k.lwe_switch = LWESwitchingKey(rng, N, n, ks_bl, ks_dg, sd, rlwe_key, lwe_key);
+    return k;
+}
+
 SchemeSwitchingKeySet SchemeSwitchingKeys(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t br_bl,
                                           uint32_t br_dg, uint32_t tr_bl, uint32_t tr_dg, uint32_t sq_bl,
                                           uint32_t sq_dg, double sd, const std::vector<uint64_t>& lwe_key,
@@ -537,6 +565,84 @@ std::unique_ptr<GpuLWEtoRGSWConverter> SchemeSwitchingContext::ConstructOperator
     return std::make_unique<GpuLWEtoRGSWConverter>(m_rot, m_tr_basis, (uint32_t)m_tr_digits, m_sq_basis,
                                                    (uint32_t)m_sq_digits, (uint32_t)m_out_digits, m_out_basis,
                                                    k.rotation, k.trace, k.square, m_device);
+}
+
+// ---- SAP decomposition ----
+
+GpuSAPDecomposer::GpuSAPDecomposer(const tp_br_params& rotation, uint64_t trace_basis, uint32_t trace_digits,
+                                   uint64_t ks_basis, uint32_t ks_digits, const std::vector<uint64_t>& brk,
+                                   const std::vector<uint64_t>& trace_keys, const std::vector<uint64_t>& lwe_ksk,
+                                   uint64_t hamming_weight, uint64_t restart_period, uint64_t max_digits, int device)
+    : m_N(rotation.ring_dim), m_n(rotation.lwe_dim), m_beta(hamming_weight), m_restart(restart_period),
+      m_max_digits(max_digits) {
+    check(tp_sap_create(&rotation, trace_basis, trace_digits, ks_basis, ks_digits, device, &m_ctx));
+    tp_status s = tp_sap_upload_keys(m_ctx, brk.data(), brk.size(), trace_keys.data(), trace_keys.size(),
+                                     lwe_ksk.data(), lwe_ksk.size());
+    if (s != TP_OK) {
+        tp_sap_destroy(m_ctx);
+        check(s);
+    }
+}
+GpuSAPDecomposer::~GpuSAPDecomposer() { tp_sap_destroy(m_ctx); }
+
+std::vector<uint32_t> GpuSAPDecomposer::DecomposeBatch(uint64_t batch, uint64_t* outputs, uint64_t out_digits,
+                                                       const uint64_t* lwes, uint64_t radix) {
+    std::vector<uint32_t> digits(batch, 0);
+    if (batch == 0) return digits;
+    const uint64_t in_words = batch * (m_n + 1ull), out_words = batch * out_digits * (m_N + 1ull);
+    DevBuf din(in_words), dout(out_words);
+    if (cudaMemcpy(din.p, lwes, in_words * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dout.p, outputs, out_words * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_sap_decompose_batch(m_ctx, batch, dout.p, out_digits, din.p, radix, m_beta, m_restart, digits.data(),
+                                 nullptr));
+    if (cudaMemcpy(outputs, dout.p, out_words * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+    return digits;
+}
+
+void GpuSAPDecomposer::Decompose(uint64_t* output, const uint64_t* input, uint64_t radix) {
+    // the output holds as many digits as the input implies; stage through a buffer of the
+    // context's maximum and copy those back
+    std::vector<uint64_t> buf(m_max_digits * (m_N + 1ull), 0);
+    const auto d = DecomposeBatch(1, buf.data(), m_max_digits, input, radix);
+    std::copy(buf.begin(), buf.begin() + d[0] * (m_N + 1ull), output);
+}
+
+void GpuSAPDecomposer::Decompose(std::vector<uint64_t>& output, const std::vector<uint64_t>& input, uint64_t radix) {
+    std::vector<uint64_t> buf(m_max_digits * (m_N + 1ull), 0);
+    const auto d = DecomposeBatch(1, buf.data(), m_max_digits, input.data(), radix);
+    if (output.size() < d[0] * (m_N + 1ull)) output.resize(d[0] * (m_N + 1ull));
+    std::copy(buf.begin(), buf.begin() + d[0] * (m_N + 1ull), output.begin());
+}
+
+SAPDecompositionContext::SAPDecompositionContext(const tp_br_params& rotation, uint64_t trace_basis,
+                                                 uint64_t trace_digits, uint64_t ks_basis, uint64_t ks_digits,
+                                                 uint64_t default_radix, double std_dev, uint64_t restart_period,
+                                                 int device, uint64_t seed)
+    : m_rot(rotation), m_tr_basis(trace_basis), m_tr_digits(trace_digits), m_ks_basis(ks_basis),
+      m_ks_digits(ks_digits), m_radix(default_radix), m_std(std_dev), m_restart(restart_period), m_device(device),
+      m_seed(seed) {
+    if (rotation.modulus != kGoldilocks)
+        throw std::invalid_argument("toothpaste_b200: modulus must be 2^64 - 2^32 + 1");
+    for (uint64_t b : {rotation.basis, trace_basis, ks_basis, default_radix})
+        if (b < 2 || (b & (b - 1))) throw std::invalid_argument("toothpaste_b200: bases and radix must be powers of two");
+    if (restart_period == 0) throw std::invalid_argument("toothpaste_b200: restart period must be positive");
+}
+
+std::unique_ptr<GpuSAPDecomposer> SAPDecompositionContext::ConstructOperator(
+    const std::vector<std::vector<uint64_t>>& keys) const {
+    if (keys.size() < 2 || keys[0].size() < m_rot.lwe_dim || keys[1].size() < m_rot.ring_dim)
+        throw std::invalid_argument("toothpaste_b200: keys = {LWE key (n), RLWE key (N)}");
+    uint64_t weight = 0;
+    for (uint32_t i = 0; i < m_rot.lwe_dim; ++i) weight += keys[0][i] != 0;
+    Sampler rng(m_seed);
+    auto k = keygen::SAPKeys(rng, m_rot.variant, m_rot.ring_dim, m_rot.lwe_dim, log2_of(m_rot.basis), m_rot.digits,
+                             log2_of(m_tr_basis), (uint32_t)m_tr_digits, log2_of(m_ks_basis), (uint32_t)m_ks_digits,
+                             m_std, keys[0], keys[1]);
+    return std::make_unique<GpuSAPDecomposer>(m_rot, m_tr_basis, (uint32_t)m_tr_digits, m_ks_basis,
+                                              (uint32_t)m_ks_digits, k.rotation, k.trace, k.lwe_switch, weight,
+                                              m_restart, 64, m_device);
 }
 
 }  // namespace toothpaste_b200

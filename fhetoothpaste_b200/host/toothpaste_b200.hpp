@@ -61,6 +61,20 @@ std::vector<uint64_t> AutomorphismKey(Sampler& rng, uint32_t N, uint32_t basis_l
                                       uint32_t index, const std::vector<uint64_t>& key);
 std::vector<uint64_t> PackingKeys(Sampler& rng, uint32_t N, uint32_t basis_log2, uint32_t digits, double std_dev,
                                   const std::vector<uint64_t>& key);
+// LWEtoLWEConverter::KeyGen (lib/src/operators/lwe_conversion.cpp:174-203) on the Goldilocks
+// modulus: row (i, j) encrypts source_i * 2^(64 - beta (j + 1)) under the target key.
+std::vector<uint64_t> LWESwitchingKey(Sampler& rng, uint32_t n_in, uint32_t n_out, uint32_t basis_log2,
+                                      uint32_t digits, double std_dev, const std::vector<uint64_t>& source_key,
+                                      const std::vector<uint64_t>& target_key);
+// SAPDecompositionContext::ConstructOperator (lib/src/operators/sap_decomposer.cpp:166-186)
+// from one sampler stream: the rotation key, the trace keys, then the LWE key switch from the
+// RLWE key's coefficients (N) to the LWE key (n).
+struct SAPKeySet {
+    std::vector<uint64_t> rotation, trace, lwe_switch;
+};
+SAPKeySet SAPKeys(Sampler& rng, int variant, uint32_t N, uint32_t n, uint32_t br_basis_log2, uint32_t br_digits,
+                  uint32_t tr_basis_log2, uint32_t tr_digits, uint32_t ks_basis_log2, uint32_t ks_digits,
+                  double std_dev, const std::vector<uint64_t>& lwe_key, const std::vector<uint64_t>& rlwe_key);
 // SchemeSwitchingContext::ConstructOperator (lib/src/operators/lwe_to_rgsw_conversion.cpp:72-108)
 // from one sampler stream: the rotation key, the trace's automorphism keys (indices 3, 5, .., N+1),
 // then the key switch from s^2 to s.
@@ -270,6 +284,57 @@ private:
     tp_br_params m_rot;
     uint64_t m_tr_basis, m_tr_digits, m_sq_basis, m_sq_digits, m_out_digits, m_out_basis;
     double m_std;
+    int m_device;
+    uint64_t m_seed;
+};
+
+// SAPDecomposer (lib/src/operators/sap_decomposer.cpp:353-512). Decompose writes one LWE of
+// dimension N per radix digit at output + d (N + 1); like the reference it stops at the digit
+// count the input's words imply. The reference writes only the nonzero words of each digit
+// into a caller-zeroed output; here every word of a digit is written.
+class GpuSAPDecomposer {
+public:
+    GpuSAPDecomposer(const tp_br_params& rotation, uint64_t trace_basis, uint32_t trace_digits, uint64_t ks_basis,
+                     uint32_t ks_digits, const std::vector<uint64_t>& brk, const std::vector<uint64_t>& trace_keys,
+                     const std::vector<uint64_t>& lwe_ksk, uint64_t hamming_weight, uint64_t restart_period,
+                     uint64_t max_digits = 64, int device = 0);
+    ~GpuSAPDecomposer();
+    GpuSAPDecomposer(const GpuSAPDecomposer&) = delete;
+    GpuSAPDecomposer& operator=(const GpuSAPDecomposer&) = delete;
+    void Decompose(uint64_t* output, const uint64_t* input, uint64_t radix);
+    void Decompose(std::vector<uint64_t>& output, const std::vector<uint64_t>& input, uint64_t radix);
+    // Many at once on host buffers: lwes rows of n+1 words; outputs rows of out_digits x (N+1)
+    // words. Returns each LWE's digit count.
+    std::vector<uint32_t> DecomposeBatch(uint64_t batch, uint64_t* outputs, uint64_t out_digits, const uint64_t* lwes,
+                                         uint64_t radix);
+
+private:
+    tp_sap_ctx* m_ctx = nullptr;
+    uint32_t m_N, m_n;
+    uint64_t m_beta, m_restart, m_max_digits;
+};
+
+// SAPDecompositionContext(rotation, trace, LWE conversion N -> n, default_radix)
+// (lib/src/operators/sap_decomposer.cpp:15-186). The reference derives the restart period from
+// its floating-point variance models (ComputeRestartIterationForRadix, lines 78-145); those are
+// not part of this path, so the period is given here (SAPDecompositionContext's
+// GetRestartIteration(); UINT64_MAX: never).
+class SAPDecompositionContext {
+public:
+    SAPDecompositionContext(const tp_br_params& rotation, uint64_t trace_basis, uint64_t trace_digits,
+                            uint64_t ks_basis, uint64_t ks_digits, uint64_t default_radix, double std_dev,
+                            uint64_t restart_period = ~0ull, int device = 0, uint64_t seed = 1);
+    // keys = {LWE key (n words), RLWE key (N words, coefficients)}; the Hamming weight is the
+    // LWE key's nonzero count, as in the reference (lines 170-174).
+    std::unique_ptr<GpuSAPDecomposer> ConstructOperator(const std::vector<std::vector<uint64_t>>& keys) const;
+    uint64_t GetDefaultRadix() const { return m_radix; }
+    uint64_t GetRestartIteration() const { return m_restart; }
+
+private:
+    tp_br_params m_rot;
+    uint64_t m_tr_basis, m_tr_digits, m_ks_basis, m_ks_digits, m_radix;
+    double m_std;
+    uint64_t m_restart;
     int m_device;
     uint64_t m_seed;
 };

@@ -193,6 +193,23 @@ def case_lwe_to_rgsw_n2048(torch):
     conv.close()
 
 
+def case_sap_n4096(torch):
+    """SAP digit decomposition, 16 LWEs (CGGI binary n=10, N=4096, gadgets 2^16 l=4, radix 32,
+    inputs mod 2^40: 8 digits): br_kernel, ks_kernel (trace and split modes), ntt_batch_kernel,
+    lwe_ks_kernel and the element-wise SAP kernels, per decomposition call."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuSAPDecomposer
+    N, n, l, batch = 4096, 10, 4, 16
+    words = BlindRotationContext(0, N, n, 1 << 16, l).key_words()
+    dec = GpuSAPDecomposer((0, N, n, 1 << 16, l), (1 << 16, l), (1 << 16, l), _u64(71, words),
+                           _u64(72, 12 * 2 * N * l), _u64(73, N * l * (n + 1)), hamming_weight=5)
+    lw = _dev(torch, _u64(74, (batch, n + 1), 1 << 40))
+    out = torch.zeros((batch, 9, N + 1), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        dec.decompose_batch(batch, out.data_ptr(), 9, lw.data_ptr(), 32)
+    torch.cuda.synchronize()
+    dec.close()
+
+
 CASES = {name[5:]: fn for name, fn in globals().items() if name.startswith("case_")}
 
 

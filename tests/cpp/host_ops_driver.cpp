@@ -11,6 +11,9 @@
 //   keygen-ss   variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed lwe_key rlwe_key out
 //   ss          variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed out_digits out_beta
 //               lwe_key rlwe_key lwes count out
+//   keygen-sap  variant N n br_beta br_digits tr_beta tr_digits ks_beta ks_digits std seed lwe_key rlwe_key out
+//   sap         variant N n br_beta br_digits tr_beta tr_digits ks_beta ks_digits std seed radix restart
+//               lwe_key rlwe_key lwes count out_digits out
 //   errors
 #include <algorithm>
 #include <cstdio>
@@ -157,6 +160,42 @@ static int run(int argc, char** argv) {
         save(argv[19], batch.data(), batch.size());
         return 0;
     }
+    if (mode == "keygen-sap" && argc == 16) {
+        Sampler rng(u(argv[12]));
+        const auto k = keygen::SAPKeys(rng, (int)u(argv[2]), (uint32_t)u(argv[3]), (uint32_t)u(argv[4]),
+                                       (uint32_t)u(argv[5]), (uint32_t)u(argv[6]), (uint32_t)u(argv[7]),
+                                       (uint32_t)u(argv[8]), (uint32_t)u(argv[9]), (uint32_t)u(argv[10]),
+                                       std::atof(argv[11]), load(argv[13]), load(argv[14]));
+        std::vector<uint64_t> all(k.rotation);
+        all.insert(all.end(), k.trace.begin(), k.trace.end());
+        all.insert(all.end(), k.lwe_switch.begin(), k.lwe_switch.end());
+        save(argv[15], all.data(), all.size());
+        return 0;
+    }
+    if (mode == "sap" && argc == 21) {
+        // SAPDecompositionContext -> ConstructOperator -> DecomposeBatch, then Decompose one by one;
+        // both must agree. Output: the batch result (count x out_digits x (N+1), zero-initialised).
+        const tp_br_params rot{(int32_t)u(argv[2]), kGoldilocks, (uint32_t)u(argv[3]), (uint32_t)u(argv[4]),
+                               1ull << u(argv[5]), (uint32_t)u(argv[6])};
+        const uint64_t radix = u(argv[13]);
+        SAPDecompositionContext ctx(rot, 1ull << u(argv[7]), u(argv[8]), 1ull << u(argv[9]), u(argv[10]), radix,
+                                    std::atof(argv[11]), u(argv[14]), 0, u(argv[12]));
+        auto dec = ctx.ConstructOperator({load(argv[15]), load(argv[16])});
+        const auto lwes = load(argv[17]);
+        const uint64_t count = u(argv[18]), od = u(argv[19]), N = rot.ring_dim, n = rot.lwe_dim;
+        std::vector<uint64_t> batch(count * od * (N + 1), 0);
+        const auto digits = dec->DecomposeBatch(count, batch.data(), od, lwes.data(), radix);
+        for (uint64_t i = 0; i < count; ++i) {
+            std::vector<uint64_t> one;
+            dec->Decompose(one, std::vector<uint64_t>(lwes.begin() + i * (n + 1), lwes.begin() + (i + 1) * (n + 1)),
+                           radix);
+            if (one.size() != digits[i] * (N + 1) ||
+                !std::equal(one.begin(), one.end(), batch.begin() + i * od * (N + 1)))
+                throw std::runtime_error("Decompose and DecomposeBatch differ");
+        }
+        save(argv[20], batch.data(), batch.size());
+        return 0;
+    }
     if (mode == "errors") {
         // parameter checks that the reference asserts (bmmp_blind_rotation.cpp:16-24) and
         // C-ABI refusals surfacing as exceptions; none of these reaches a device
@@ -179,6 +218,8 @@ static int run(int argc, char** argv) {
             c.ConstructOperator({{1, 0}, {}});
         });
         bad += !throws([&] { GpuLWEtoRGSWConverter(rot, 1ull << 16, 4, 1ull << 16, 4, 3, 1ull << 16, {}, {}, {}); });
+        bad += !throws([&] { SAPDecompositionContext(rot, 1ull << 16, 4, 1ull << 16, 4, 6, 3.2); });
+        bad += !throws([&] { SAPDecompositionContext(rot, 1ull << 16, 4, 1ull << 16, 4, 4, 3.2, 0); });
         std::cout << (bad ? "FAIL " : "ok ") << bad << "\n";
         return bad ? 1 : 0;
     }

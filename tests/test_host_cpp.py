@@ -153,3 +153,35 @@ def test_cpp_scheme_switch_like_oracle(driver, oracle, cuda, tmp_path, variant):
     for j in range(count):
         want = oracle.lwe_to_rgsw(variant, N, n, br, keys[0], tr, keys[1], sq, keys[2], D, ob, lwes[j])
         np.testing.assert_array_equal(got.reshape(count, -1)[j], want, err_msg=f"input {j}")
+
+
+SAP_CASE = (CGGI_BINARY, 256, 10, (16, 4), (14, 4), (12, 5), 3.2)
+
+
+def test_sap_keygen_equals_oracle(driver, oracle, tmp_path):
+    """keygen::SAPKeys: rotation key, trace keys and the LWE key switch N -> n from one stream."""
+    variant, N, n, br, tr, ks, std = SAP_CASE
+    sk = lwe_secret(variant, n, N, seed=101)
+    z = rlwe_secret(N, seed=102)
+    got = run(driver, tmp_path, "keygen-sap", variant, N, n, *br, *tr, *ks, std, 31, sk, z)
+    want = np.concatenate(oracle.sap_keygen(variant, N, n, br, tr, ks, std, sk, z, 31))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_cpp_sap_like_oracle(driver, oracle, cuda, tmp_path):
+    variant, N, n, br, tr, ks, std = SAP_CASE
+    radix, restart, count, od = 4, 3, 3, 10
+    sk = lwe_secret(variant, n, N, seed=111)
+    z = rlwe_secret(N, seed=112)
+    rng = np.random.default_rng(113)
+    lwes = rng.integers(0, 1 << 16, (count, n + 1), dtype=np.uint64)
+    lwes[1] &= np.uint64(0xFF)
+    got = run(driver, tmp_path, "sap", variant, N, n, *br, *tr, *ks, std, 37, radix, restart, sk, z, lwes, count,
+              od).reshape(count, od, N + 1)
+    keys = oracle.sap_keygen(variant, N, n, br, tr, ks, std, sk, z, 37)
+    beta = int(np.count_nonzero(sk))
+    for j in range(count):
+        _, want = oracle.sap_decompose(variant, N, n, br, keys[0], tr, keys[1], ks, keys[2], radix, beta, restart,
+                                       lwes[j], od)
+        np.testing.assert_array_equal(got[j], want, err_msg=f"input {j}")
