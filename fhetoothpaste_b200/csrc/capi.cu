@@ -1255,6 +1255,16 @@ tp_status tp_ntt_backward(uint32_t ring_dim, uint64_t count, uint64_t* out, cons
     return ntt_launch(ring_dim, count, out, in, stream, false);
 }
 
+// A rotation launch inside a composite operator: two blocks per rotation when the
+// whole batch fits the two-block kernel's resident grid (small batches finish in
+// about half the time), else one, as the serving loop chooses.
+static tp_status br_rotate_auto(tp_br_ctx* br, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
+                                void* stream) {
+    const int split = batch <= tp::br_concurrency(br, 2) ? 2 : 1;
+    return tp::br_batch_launch(br, batch, results, lwes, lwe_stride, accs, acc_stride, out_coef, stream, split);
+}
+
 // ---------------------------------------------------------------------------
 // LWE -> RGSW scheme switching (lib/src/operators/lwe_to_rgsw_conversion.cpp)
 // ---------------------------------------------------------------------------
@@ -1396,7 +1406,7 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     const uint64_t total = rowsn * 2 * N;
     const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 65535);
     // 1. rotation of [0 | -tp] with coefficient output (line 178)
-    tp_status s = tp_br_blind_rotate_batch(c->br, batch, c->rot, lwes, (uint64_t)c->n + 1, c->acc, 0, 1, stream);
+    tp_status s = br_rotate_auto(c->br, batch, c->rot, lwes, (uint64_t)c->n + 1, c->acc, 0, 1, stream);
     if (s != TP_OK) return s;
     // 2. + (0, tp), Lev rows, times N^-1 (lines 180-200; trace_evaluation.cpp:143)
     tp::ss_rows_kernel<<<blocks, 256, 0, st>>>(c->rows, c->rot, c->acc + 2 * N, batch, (uint32_t)D, (uint32_t)N,
@@ -1602,7 +1612,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
             restart_period);
         TP_CUDA(cudaGetLastError());
         // rotation of the coefficient-domain accumulator in place, NTT output (lines 432-434)
-        s = tp_br_blind_rotate_batch(c->br, batch, c->acc, c->sub, n + 1, c->acc, 2 * N, 0, stream);
+        s = br_rotate_auto(c->br, batch, c->acc, c->sub, n + 1, c->acc, 2 * N, 0, stream);
         if (s != TP_OK) return s;
         // digit d = SampleExtract(INTT(acc (.) extract poly)) (lines 438-445)
         tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, xpoly, 1, batch,
@@ -1621,7 +1631,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
             TP_CUDA(cudaGetLastError());
             s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
             if (s == TP_OK) s = tp_pbs_epilogue_batch(c->lks, batch, c->lw, c->ext, 2 * N, stream);
-            if (s == TP_OK) s = tp_br_blind_rotate_batch(c->br, batch, c->ext, c->lw, n + 1, c->fresh, 0, 0, stream);
+            if (s == TP_OK) s = br_rotate_auto(c->br, batch, c->ext, c->lw, n + 1, c->fresh, 0, 0, stream);
             if (s != TP_OK) return s;
             tp::sap_select_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->ext, c->flags, batch,
                                                                            (uint32_t)N);
