@@ -1580,8 +1580,10 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
     const uint64_t* ovf = c->consts + 2 * N;
 
     // input moduli and digit counts (lines 409-416); one read-back to plan the steps
-    tp::sap_init_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(c->copy, c->modulus, c->acc, lwes, batch,
-                                                                       (uint32_t)n, (uint32_t)N);
+    tp::sap_init_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(c->copy, c->modulus, lwes, batch,
+                                                                       (uint32_t)n);
+    TP_CUDA(cudaGetLastError());
+    tp::sap_acc_init_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, batch, (uint32_t)N);
     TP_CUDA(cudaGetLastError());
     std::vector<uint64_t> M(batch);
     TP_CUDA(cudaMemcpyAsync(M.data(), c->modulus, batch * 8, cudaMemcpyDeviceToHost, st));

@@ -11,12 +11,11 @@ namespace tp {
 // The reference's IntLog2 (math_utils.cpp:11-25): ceil(log2 x), 0 for x <= 1.
 __device__ __forceinline__ uint32_t ref_int_log2(uint64_t x) { return x <= 1 ? 0u : 64u - __clzll(x - 1); }
 
-// Per LWE: copy of the input, the input modulus read from the words themselves
-// (lines 409-416: 2^IntLog2(a_0), doubled once for each later word it does not
-// exceed), and the starting accumulator (0, Q/2N) in coefficients.
+// Per LWE: copy of the input and the input modulus read from the words
+// themselves (lines 409-416: 2^IntLog2(a_0), doubled once for each later word it
+// does not exceed).
 __global__ void sap_init_kernel(uint64_t* __restrict__ copy, uint64_t* __restrict__ modulus,
-                                uint64_t* __restrict__ acc, const uint64_t* __restrict__ in, uint64_t batch,
-                                uint32_t n, uint32_t N) {
+                                const uint64_t* __restrict__ in, uint64_t batch, uint32_t n) {
     const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (b >= batch) return;
     const uint64_t* x = in + b * (n + 1ull);
@@ -29,9 +28,14 @@ __global__ void sap_init_kernel(uint64_t* __restrict__ copy, uint64_t* __restric
         c[i] = v;
     }
     modulus[b] = M;
-    uint64_t* a = acc + b * 2ull * N;
-    for (uint32_t k = 0; k < 2 * N; ++k) a[k] = 0;
-    a[N] = kP / (2ull * N);
+}
+
+// The starting accumulators (0, Q/2N) in coefficients (lines 389-392).
+__global__ void sap_acc_init_kernel(uint64_t* __restrict__ acc, uint64_t batch, uint32_t N) {
+    const uint64_t total = batch * 2ull * N;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
+         w += (uint64_t)gridDim.x * blockDim.x)
+        acc[w] = (w % (2ull * N)) == N ? kP / (2ull * N) : 0;
 }
 
 // One digit step on every LWE (lines 421-430): sub = copy mod radix, copy >>=

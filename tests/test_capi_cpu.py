@@ -72,3 +72,12 @@ def test_scheme_switch_rejects_bad_output_gadget(native):
         assert native.tp_ss_create(ctypes.byref(prm), 1 << 16, 4, 1 << 16, 4, digits, basis, 0,
                                    ctypes.byref(h)) == _native.TP_ERR_PARAM
         assert not h.value
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No fallback: without the built CUDA library the package refuses to run."""
+    from fhetoothpaste_b200 import _native
+    monkeypatch.setattr(_native, "LIB_PATH", tmp_path / "libtoothpaste_gpu.so")
+    monkeypatch.setattr(_native, "_lib", None)
+    with pytest.raises(ImportError):
+        _native.lib()
