@@ -76,6 +76,8 @@ def lib() -> ctypes.CDLL:
         "tp_ks_destroy": (ctypes.c_int, [VP]),
         "tp_ks_key_words": (U64, [VP]),
         "tp_ks_upload_key": (ctypes.c_int, [VP, U64P, U64]),
+        "tp_ks_set_tile": (ctypes.c_int, [VP, ctypes.c_uint32]),
+        "tp_ks_get_tile": (ctypes.c_uint32, [VP]),
         "tp_rlwe_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
         "tp_auto_eval_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
         "tp_pack_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),

@@ -724,7 +724,8 @@ struct tp_ks_ctx {
     bool key_ready = false;
     tp::KsKernelParams kp{};
     size_t smem = 0;
-    int per_sm[tp::kKsModes] = {};
+    int loge = 2;                 // log2 coefficients per thread: 2 (4) or 3 (8)
+    int per_sm[2][tp::kKsModes] = {};
     uint64_t* work = nullptr;     // packing tree nodes
     uint64_t work_words = 0;
     std::mutex mu;
@@ -753,6 +754,7 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     c->digits = digits;
     c->index = index;
     c->nkeys = kind == 2 ? c->logn : 1;
+    c->loge = 2;  // 4 per thread: faster than 8 in every mode and ring size measured
     c->key_words = (uint64_t)c->nkeys * digits * 2 * ring_dim;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
@@ -771,14 +773,17 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     kp.n_inv = c->tab->n_inv;
     signed_digit_consts(beta, digits, kp.corr, kp.dshift, kp.dmask, kp.ddelta);
     c->smem = tp::ks_smem_words(ring_dim) * 8;
-    for (int mode = 0; mode < tp::kKsModes; ++mode) {
-        const void* k = tp::ks_kernel_lookup(c->logn, mode);
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->per_sm[mode], k, ring_dim / 8, c->smem);
-        if (e != cudaSuccess || c->per_sm[mode] < 1) {
-            delete c;
-            return fail(TP_ERR_CUDA, "key-switch kernel set-up: %s", cudaGetErrorString(e));
+    for (int loge = 2; loge <= 3; ++loge) {
+        for (int mode = 0; mode < tp::kKsModes; ++mode) {
+            const void* k = tp::ks_kernel_lookup(c->logn, mode, loge);
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->per_sm[loge - 2][mode], k, ring_dim >> loge,
+                                                                  c->smem);
+            if (e != cudaSuccess || c->per_sm[loge - 2][mode] < 1) {
+                delete c;
+                return fail(TP_ERR_CUDA, "key-switch kernel set-up: %s", cudaGetErrorString(e));
+            }
         }
     }
     *out = c;
@@ -824,7 +829,8 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
         // each key: l rows of [A | B] (the reference's m_ksk) -> [row][c][jp][t][2]
         const uint64_t total = c->key_words;
         const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 65535);
-        tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn, 3);
+        tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn,
+                                                            c->loge);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -835,13 +841,41 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
 }
 
 static tp_status ks_launch(tp_ks_ctx* c, int mode, const tp::KsKernelParams& kp, cudaStream_t st) {
-    const uint64_t grid = std::min<uint64_t>(kp.items, (uint64_t)c->per_sm[mode] * sm_count(c->device));
+    const uint64_t grid =
+        std::min<uint64_t>(kp.items, (uint64_t)c->per_sm[c->loge - 2][mode] * sm_count(c->device));
     tp::KsKernelParams p = kp;
     void* args[] = {&p};
-    TP_CUDA(cudaLaunchKernel(tp::ks_kernel_lookup(c->logn, mode), dim3((unsigned)grid), dim3(c->N / 8), args, c->smem,
-                             st));
+    TP_CUDA(cudaLaunchKernel(tp::ks_kernel_lookup(c->logn, mode, c->loge), dim3((unsigned)grid),
+                             dim3(c->N >> c->loge), args, c->smem, st));
     return TP_OK;
 }
+
+tp_status tp_ks_set_tile(tp_ks_ctx* c, uint32_t coef_per_thread) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (coef_per_thread != 4 && coef_per_thread != 8) return fail(TP_ERR_PARAM, "tile must be 4 or 8");
+    const int loge = coef_per_thread == 4 ? 2 : 3;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (loge == c->loge) return TP_OK;
+    TP_CUDA(cudaSetDevice(c->device));
+    if (c->key_ready) {
+        uint64_t* nk = nullptr;
+        TP_CUDA(cudaMalloc(&nk, c->key_words * 8));
+        const uint64_t blocks = std::min<uint64_t>((c->key_words + 255) / 256, 65535);
+        tp::key_retile_kernel<<<(unsigned)blocks, 256>>>(nk, c->key, c->nkeys, 1, c->digits, c->logn, c->loge, loge);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            cudaFree(nk);
+            return fail(TP_ERR_CUDA, "key re-tiling: %s", cudaGetErrorString(e));
+        }
+        cudaFree(c->key);
+        c->key = nk;
+    }
+    c->loge = loge;
+    return TP_OK;
+}
+
+uint32_t tp_ks_get_tile(const tp_ks_ctx* c) { return c ? 1u << c->loge : 0; }
 
 tp_status tp_rlwe_ks_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
     if (!c || c->kind != 0) return fail(TP_ERR_PARAM, "not an RLWE key-switching context");

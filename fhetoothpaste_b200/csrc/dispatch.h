@@ -21,12 +21,12 @@ const void* br_pair_kernel_ptr_9(int variant);
 const void* br_pair_kernel_ptr_10(int variant);
 const void* br_pair_kernel_ptr_11(int variant);
 const void* br_pair_kernel_ptr_12(int variant);
-const void* ks_kernel_ptr_7(int mode);
-const void* ks_kernel_ptr_8(int mode);
-const void* ks_kernel_ptr_9(int mode);
-const void* ks_kernel_ptr_10(int mode);
-const void* ks_kernel_ptr_11(int mode);
-const void* ks_kernel_ptr_12(int mode);
+const void* ks_kernel_ptr_7(int mode, int loge);
+const void* ks_kernel_ptr_8(int mode, int loge);
+const void* ks_kernel_ptr_9(int mode, int loge);
+const void* ks_kernel_ptr_10(int mode, int loge);
+const void* ks_kernel_ptr_11(int mode, int loge);
+const void* ks_kernel_ptr_12(int mode, int loge);
 
 inline const void* br_kernel_lookup(int logn, int variant, int loge) {
     switch (logn) {
@@ -65,14 +65,14 @@ inline const void* ntt_kernel_lookup(int logn, bool forward) {
     }
 }
 
-inline const void* ks_kernel_lookup(int logn, int mode) {
+inline const void* ks_kernel_lookup(int logn, int mode, int loge) {
     switch (logn) {
-        case 7: return ks_kernel_ptr_7(mode);
-        case 8: return ks_kernel_ptr_8(mode);
-        case 9: return ks_kernel_ptr_9(mode);
-        case 10: return ks_kernel_ptr_10(mode);
-        case 11: return ks_kernel_ptr_11(mode);
-        case 12: return ks_kernel_ptr_12(mode);
+        case 7: return ks_kernel_ptr_7(mode, loge);
+        case 8: return ks_kernel_ptr_8(mode, loge);
+        case 9: return ks_kernel_ptr_9(mode, loge);
+        case 10: return ks_kernel_ptr_10(mode, loge);
+        case 11: return ks_kernel_ptr_11(mode, loge);
+        case 12: return ks_kernel_ptr_12(mode, loge);
         default: return nullptr;
     }
 }

@@ -35,13 +35,22 @@ const void* ntt_kernel_ptr_10(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<10, true> : (const void*)ntt_batch_kernel<10, false>;
 }
 
-const void* ks_kernel_ptr_10(int mode) {
+const void* ks_kernel_ptr_10(int mode, int loge) {
+    if (loge == 2) {
+        switch (mode) {
+            case kKsRlwe: return (const void*)ks_kernel<10, kKsRlwe, 2>;
+            case kKsAuto: return (const void*)ks_kernel<10, kKsAuto, 2>;
+            case kKsMerge: return (const void*)ks_kernel<10, kKsMerge, 2>;
+            case kKsTrace: return (const void*)ks_kernel<10, kKsTrace, 2>;
+            default: return (const void*)ks_kernel<10, kKsSplit, 2>;
+        }
+    }
     switch (mode) {
-        case kKsRlwe: return (const void*)ks_kernel<10, kKsRlwe>;
-        case kKsAuto: return (const void*)ks_kernel<10, kKsAuto>;
-        case kKsMerge: return (const void*)ks_kernel<10, kKsMerge>;
-        case kKsTrace: return (const void*)ks_kernel<10, kKsTrace>;
-        default: return (const void*)ks_kernel<10, kKsSplit>;
+        case kKsRlwe: return (const void*)ks_kernel<10, kKsRlwe, 3>;
+        case kKsAuto: return (const void*)ks_kernel<10, kKsAuto, 3>;
+        case kKsMerge: return (const void*)ks_kernel<10, kKsMerge, 3>;
+        case kKsTrace: return (const void*)ks_kernel<10, kKsTrace, 3>;
+        default: return (const void*)ks_kernel<10, kKsSplit, 3>;
     }
 }
 

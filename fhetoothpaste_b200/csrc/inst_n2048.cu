@@ -35,13 +35,22 @@ const void* ntt_kernel_ptr_11(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<11, true> : (const void*)ntt_batch_kernel<11, false>;
 }
 
-const void* ks_kernel_ptr_11(int mode) {
+const void* ks_kernel_ptr_11(int mode, int loge) {
+    if (loge == 2) {
+        switch (mode) {
+            case kKsRlwe: return (const void*)ks_kernel<11, kKsRlwe, 2>;
+            case kKsAuto: return (const void*)ks_kernel<11, kKsAuto, 2>;
+            case kKsMerge: return (const void*)ks_kernel<11, kKsMerge, 2>;
+            case kKsTrace: return (const void*)ks_kernel<11, kKsTrace, 2>;
+            default: return (const void*)ks_kernel<11, kKsSplit, 2>;
+        }
+    }
     switch (mode) {
-        case kKsRlwe: return (const void*)ks_kernel<11, kKsRlwe>;
-        case kKsAuto: return (const void*)ks_kernel<11, kKsAuto>;
-        case kKsMerge: return (const void*)ks_kernel<11, kKsMerge>;
-        case kKsTrace: return (const void*)ks_kernel<11, kKsTrace>;
-        default: return (const void*)ks_kernel<11, kKsSplit>;
+        case kKsRlwe: return (const void*)ks_kernel<11, kKsRlwe, 3>;
+        case kKsAuto: return (const void*)ks_kernel<11, kKsAuto, 3>;
+        case kKsMerge: return (const void*)ks_kernel<11, kKsMerge, 3>;
+        case kKsTrace: return (const void*)ks_kernel<11, kKsTrace, 3>;
+        default: return (const void*)ks_kernel<11, kKsSplit, 3>;
     }
 }
 

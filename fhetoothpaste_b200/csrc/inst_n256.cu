@@ -35,13 +35,22 @@ const void* ntt_kernel_ptr_8(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<8, true> : (const void*)ntt_batch_kernel<8, false>;
 }
 
-const void* ks_kernel_ptr_8(int mode) {
+const void* ks_kernel_ptr_8(int mode, int loge) {
+    if (loge == 2) {
+        switch (mode) {
+            case kKsRlwe: return (const void*)ks_kernel<8, kKsRlwe, 2>;
+            case kKsAuto: return (const void*)ks_kernel<8, kKsAuto, 2>;
+            case kKsMerge: return (const void*)ks_kernel<8, kKsMerge, 2>;
+            case kKsTrace: return (const void*)ks_kernel<8, kKsTrace, 2>;
+            default: return (const void*)ks_kernel<8, kKsSplit, 2>;
+        }
+    }
     switch (mode) {
-        case kKsRlwe: return (const void*)ks_kernel<8, kKsRlwe>;
-        case kKsAuto: return (const void*)ks_kernel<8, kKsAuto>;
-        case kKsMerge: return (const void*)ks_kernel<8, kKsMerge>;
-        case kKsTrace: return (const void*)ks_kernel<8, kKsTrace>;
-        default: return (const void*)ks_kernel<8, kKsSplit>;
+        case kKsRlwe: return (const void*)ks_kernel<8, kKsRlwe, 3>;
+        case kKsAuto: return (const void*)ks_kernel<8, kKsAuto, 3>;
+        case kKsMerge: return (const void*)ks_kernel<8, kKsMerge, 3>;
+        case kKsTrace: return (const void*)ks_kernel<8, kKsTrace, 3>;
+        default: return (const void*)ks_kernel<8, kKsSplit, 3>;
     }
 }
 

@@ -35,13 +35,22 @@ const void* ntt_kernel_ptr_12(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<12, true> : (const void*)ntt_batch_kernel<12, false>;
 }
 
-const void* ks_kernel_ptr_12(int mode) {
+const void* ks_kernel_ptr_12(int mode, int loge) {
+    if (loge == 2) {
+        switch (mode) {
+            case kKsRlwe: return (const void*)ks_kernel<12, kKsRlwe, 2>;
+            case kKsAuto: return (const void*)ks_kernel<12, kKsAuto, 2>;
+            case kKsMerge: return (const void*)ks_kernel<12, kKsMerge, 2>;
+            case kKsTrace: return (const void*)ks_kernel<12, kKsTrace, 2>;
+            default: return (const void*)ks_kernel<12, kKsSplit, 2>;
+        }
+    }
     switch (mode) {
-        case kKsRlwe: return (const void*)ks_kernel<12, kKsRlwe>;
-        case kKsAuto: return (const void*)ks_kernel<12, kKsAuto>;
-        case kKsMerge: return (const void*)ks_kernel<12, kKsMerge>;
-        case kKsTrace: return (const void*)ks_kernel<12, kKsTrace>;
-        default: return (const void*)ks_kernel<12, kKsSplit>;
+        case kKsRlwe: return (const void*)ks_kernel<12, kKsRlwe, 3>;
+        case kKsAuto: return (const void*)ks_kernel<12, kKsAuto, 3>;
+        case kKsMerge: return (const void*)ks_kernel<12, kKsMerge, 3>;
+        case kKsTrace: return (const void*)ks_kernel<12, kKsTrace, 3>;
+        default: return (const void*)ks_kernel<12, kKsSplit, 3>;
     }
 }
 

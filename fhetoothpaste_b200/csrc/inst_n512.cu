@@ -35,13 +35,22 @@ const void* ntt_kernel_ptr_9(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<9, true> : (const void*)ntt_batch_kernel<9, false>;
 }
 
-const void* ks_kernel_ptr_9(int mode) {
+const void* ks_kernel_ptr_9(int mode, int loge) {
+    if (loge == 2) {
+        switch (mode) {
+            case kKsRlwe: return (const void*)ks_kernel<9, kKsRlwe, 2>;
+            case kKsAuto: return (const void*)ks_kernel<9, kKsAuto, 2>;
+            case kKsMerge: return (const void*)ks_kernel<9, kKsMerge, 2>;
+            case kKsTrace: return (const void*)ks_kernel<9, kKsTrace, 2>;
+            default: return (const void*)ks_kernel<9, kKsSplit, 2>;
+        }
+    }
     switch (mode) {
-        case kKsRlwe: return (const void*)ks_kernel<9, kKsRlwe>;
-        case kKsAuto: return (const void*)ks_kernel<9, kKsAuto>;
-        case kKsMerge: return (const void*)ks_kernel<9, kKsMerge>;
-        case kKsTrace: return (const void*)ks_kernel<9, kKsTrace>;
-        default: return (const void*)ks_kernel<9, kKsSplit>;
+        case kKsRlwe: return (const void*)ks_kernel<9, kKsRlwe, 3>;
+        case kKsAuto: return (const void*)ks_kernel<9, kKsAuto, 3>;
+        case kKsMerge: return (const void*)ks_kernel<9, kKsMerge, 3>;
+        case kKsTrace: return (const void*)ks_kernel<9, kKsTrace, 3>;
+        default: return (const void*)ks_kernel<9, kKsSplit, 3>;
     }
 }
 

@@ -2,11 +2,12 @@
 // the merge/trace steps of n-LWE -> RLWE packing, and LWE -> LWE key switch.
 //
 // The RLWE kernels share one core with the blind rotation: a block of
-// T = N/8 threads takes the coefficient-domain A part of one ciphertext, forms
-// its signed gadget digits (lib/include/static/gadget_decomp.h:156-205), runs a
-// forward NTT per digit and multiply-accumulates against the key rows
-// (lib/src/operators/rlwe_conversion.cpp:224-249). Key rows are laid out like
-// the blind-rotation key (C = 2 components, A and B, per slot).
+// T = N/E threads (E = 2^LOGE = 4 or 8 coefficients per thread) takes the
+// coefficient-domain A part of one ciphertext, forms its signed gadget digits
+// (lib/include/static/gadget_decomp.h:156-205), runs a forward NTT per digit and
+// multiply-accumulates against the key rows (lib/src/operators/rlwe_conversion.cpp:
+// 224-249). Key rows are laid out like the blind-rotation key of the same tile
+// (C = 2 components, A and B, per slot).
 #pragma once
 
 #include "gl_arith.cuh"
@@ -24,7 +25,7 @@ enum KsMode : int {
 constexpr int kKsModes = 5;
 
 struct KsKernelParams {
-    const uint64_t* key;      // device layout: [digit][c][jp][t][2], C = 2
+    const uint64_t* key;      // device layout: [digit][c][jp][t][2], C = 2, jp < E/2
     const uint64_t* tw_fwd;
     const uint64_t* tw_inv;
     const uint64_t* in;       // per item: 2N words (kKsRlwe/kKsAuto), node pairs (kKsMerge), node (kKsTrace)
@@ -67,13 +68,14 @@ __device__ __forceinline__ uint64_t rot_coeff(const uint64_t* x, uint32_t m, uin
 
 // sum_d NTT(digit_d(a)) * key_d for both components (lazy residues), a in the
 // coefficient layout and canonical.
-template <int LOGN>
-__device__ __forceinline__ void ks_mac(uint64_t a[8], const KsKernelParams& prm, int t, uint64_t* buf0,
-                                       uint64_t* buf1, int& sel, const uint64_t* tw_f, uint64_t o[2][8]) {
+template <int LOGN, int LOGE>
+__device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelParams& prm, int t, uint64_t* buf0,
+                                       uint64_t* buf1, int& sel, const uint64_t* tw_f, uint64_t (&o)[2][1 << LOGE]) {
     constexpr int N = 1 << LOGN;
-    constexpr int T = N / 8;
+    constexpr int E = 1 << LOGE;
+    constexpr int T = N / E;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < E; ++j) {
         a[j] = gl_add(a[j], prm.corr);
         o[0][j] = 0;
         o[1][j] = 0;
@@ -83,28 +85,46 @@ __device__ __forceinline__ void ks_mac(uint64_t a[8], const KsKernelParams& prm,
         const uint32_t sh = prm.dshift[d];
         const uint64_t mk = prm.dmask[d];
         const uint64_t dl = prm.ddelta[d];
-        uint64_t x[8];
+        uint64_t x[1][E];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = gl_sub((a[j] >> sh) & mk, dl);
-        ntt_forward<LOGN>(x, t, sel ? buf1 : buf0, tw_f);
-        sel ^= 1;
+        for (int j = 0; j < E; ++j) x[0][j] = gl_sub((a[j] >> sh) & mk, dl);
         const uint64_t* kr = prm.key + (uint64_t)d * (2 * N);
+        // with 4 coefficients per thread the digit's key words (8 registers) are
+        // requested before its NTT, which hides their L2 latency; with 8 they
+        // would not fit next to the NTT's registers and are read after it
+        ulonglong2 kv[2][E / 2];
+        if constexpr (LOGE == 2) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int jp = 0; jp < E / 2; ++jp)
+                    kv[c][jp] = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
+        }
+        ntt_forward_k<LOGN, 1, LOGE>(x, t, sel ? buf1 : buf0, tw_f);
+        sel ^= 1;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
 #pragma unroll
-            for (int jp = 0; jp < 4; ++jp) {
-                const ulonglong2 kv = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * 4 + jp) * T + t) * 2));
-                o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[2 * jp], kv.x);
-                o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[2 * jp + 1], kv.y);
+            for (int jp = 0; jp < E / 2; ++jp) {
+                if constexpr (LOGE != 2)
+                    kv[c][jp] = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
+                o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[0][2 * jp], kv[c][jp].x);
+                o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[0][2 * jp + 1], kv[c][jp].y);
             }
         }
     }
 }
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelParams prm) {
+// Blocks per SM the kernel is compiled for: two where two blocks of N/E threads
+// still leave 128 registers per thread (N/E <= 256), else one.
+template <int LOGN, int LOGE>
+constexpr int ks_min_blocks() { return ((1 << LOGN) >> LOGE) <= 256 ? 2 : 1; }
+
+template <int LOGN, int MODE, int LOGE>
+__global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>()) ks_kernel(const KsKernelParams prm) {
     constexpr int N = 1 << LOGN;
-    constexpr int T = N / 8;
+    constexpr int E = 1 << LOGE;
+    constexpr int T = N / E;
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* tw_f = smem;
     uint64_t* tw_i = smem + N;
@@ -120,15 +140,15 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
         __syncthreads();
         const uint64_t* in = prm.in + it * prm.in_stride;
         uint64_t* out = prm.out + it * prm.out_stride;
-        uint64_t a[8], bb[8], base[2][8];
+        uint64_t a[E], bb[E], base[2][E];
         // ---- gather inputs (every global read precedes the first barrier below,
         //      so kKsMerge/kKsTrace may write their result in place) ----
         if constexpr (MODE == kKsRlwe) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) a[j] = in[t + j * T];
+            for (int j = 0; j < E; ++j) a[j] = in[t + j * T];
         } else if constexpr (MODE == kKsAuto) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
+            for (int j = 0; j < E; ++j) {
                 a[j] = aut_coeff<LOGN>(in, t + j * T, prm.auto_index_inv);
                 bb[j] = aut_coeff<LOGN>(in + N, t + j * T, prm.auto_index_inv);
             }
@@ -139,7 +159,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
+                for (int j = 0; j < E; ++j) {
                     const uint32_t m = t + j * T;
                     // diff = right - X^s left at the automorphism's source index
                     const uint32_t i = (m * prm.auto_index_inv) & (2 * N - 1);
@@ -158,37 +178,37 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
             }
         }
         // ---- key switch of the A part ----
-        uint64_t o[2][8];
-        ks_mac<LOGN>(a, prm, t, buf0, buf1, sel, tw_f, o);
+        uint64_t o[2][E];
+        ks_mac<LOGN, LOGE>(a, prm, t, buf0, buf1, sel, tw_f, o);
         if constexpr (MODE == kKsRlwe) {
-            // out -= KS; out.B += in.B (rlwe_conversion.cpp:243-248); slots 8t..8t+7
+            // out -= KS; out.B += in.B (rlwe_conversion.cpp:243-248); slots E t .. E t + E - 1
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int k = 8 * t + j;
+            for (int j = 0; j < E; ++j) {
+                const int k = E * t + j;
                 out[k] = gl_sub(out[k], gl_canon(o[0][j]));
                 out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), in[N + k]);
             }
         } else {
             // NTT of the automorphism's B part (automorphism_evaluation.cpp:156)
-            ntt_forward<LOGN>(bb, t, sel ? buf1 : buf0, tw_f);
+            ntt_forward_k<LOGN, 1, LOGE>(reinterpret_cast<uint64_t(&)[1][E]>(bb), t, sel ? buf1 : buf0, tw_f);
             sel ^= 1;
             if constexpr (MODE == kKsAuto) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int k = 8 * t + j;
+                for (int j = 0; j < E; ++j) {
+                    const int k = E * t + j;
                     out[k] = gl_sub(out[k], gl_canon(o[0][j]));
                     out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), bb[j]);
                 }
             } else {
                 // Auto eval output (NTT) -> coefficients, added to the sum half
                 // (lwe_to_rlwe_packing.cpp:205-210, 228-233)
-                uint64_t r[8];
+                uint64_t r[1][E];
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) r[j] = h == 0 ? gl_neg(gl_canon(o[0][j]))
-                                                              : gl_sub(bb[j], gl_canon(o[1][j]));
-                    ntt_backward_unscaled<LOGN>(r, t, sel ? buf1 : buf0, tw_i);
+                    for (int j = 0; j < E; ++j) r[0][j] = h == 0 ? gl_neg(gl_canon(o[0][j]))
+                                                                 : gl_sub(bb[j], gl_canon(o[1][j]));
+                    ntt_backward_unscaled_k<LOGN, 1, LOGE>(r, t, sel ? buf1 : buf0, tw_i);
                     sel ^= 1;
                     if constexpr (MODE == kKsSplit) {
                         // children of a truncation-tree node (sap_decomposer.cpp:266-284, in the
@@ -196,9 +216,9 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
                         uint64_t* out1 = out + prm.right_offset + h * N;
                         const uint32_t s = prm.shift;
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
+                        for (int j = 0; j < E; ++j) {
                             const uint32_t m = t + j * T;
-                            const uint64_t y = gl_mul(r[j], prm.n_inv);
+                            const uint64_t y = gl_mul(r[0][j], prm.n_inv);
                             out[h * N + m] = gl_add(base[h][j], y);
                             const uint64_t z = gl_sub(base[h][j], y);
                             if (m >= s) out1[m - s] = z;
@@ -206,8 +226,8 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) ks_kernel(const KsKernelPa
                         }
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 8; ++j)
-                            out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[j], prm.n_inv));
+                        for (int j = 0; j < E; ++j)
+                            out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[0][j], prm.n_inv));
                     }
                 }
             }

@@ -29,6 +29,14 @@ class _KsBase:
         key = np.ascontiguousarray(key, dtype=np.uint64)
         nat.check(nat.lib().tp_ks_upload_key(self._h, nat.ptr(key), key.size))
 
+    def set_tile(self, coef_per_thread: int) -> None:
+        """4 or 8 coefficients per thread for this context's kernels (same results)."""
+        nat.check(nat.lib().tp_ks_set_tile(self._h, coef_per_thread))
+
+    @property
+    def tile(self) -> int:
+        return int(nat.lib().tp_ks_get_tile(self._h))
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             nat.lib().tp_ks_destroy(self._h)

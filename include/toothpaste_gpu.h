@@ -190,6 +190,12 @@ uint64_t tp_ks_key_words(const tp_ks_ctx* ctx);
 /* Host key in the reference layout above; re-laid out on the device. Synchronous. */
 tp_status tp_ks_upload_key(tp_ks_ctx* ctx, const uint64_t* key_host, uint64_t words);
 
+/* Coefficients per thread of the key-switching kernels (4 or 8; default 4):
+ * N/4 or N/8 threads per ciphertext. The resident key is re-laid out for the
+ * new tile. Results do not depend on it. */
+tp_status tp_ks_set_tile(tp_ks_ctx* ctx, uint32_t coef_per_thread);
+uint32_t tp_ks_get_tile(const tp_ks_ctx* ctx);
+
 /* Batched RLWEtoRLWEConverter::Convert(out, in) (rlwe_conversion.cpp:224-249),
  * device buffers of 2N words per ciphertext: in = [A coefficients | B NTT];
  * out -= KS(in.A) and out.B += in.B, like the reference (which expects a

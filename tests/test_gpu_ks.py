@@ -13,11 +13,14 @@ def case(golden, name):
     return golden[0]["ks"][name], golden[1][f"ks_{name}"]
 
 
+@pytest.mark.parametrize("tile", [4, 8])
 @pytest.mark.parametrize("name", ["rlwe_ks_n2048", "rlwe_ks_n256_b12"])
-def test_rlwe_ks_matches_reference(native, oracle, golden, name):
+def test_rlwe_ks_matches_reference(native, oracle, golden, name, tile):
     from fhetoothpaste_b200 import GpuRLWEtoRLWEConverter
     c, expect = case(golden, name)
     conv = GpuRLWEtoRLWEConverter(c["N"], 1 << c["basis_log2"], c["digits"], ks_key(oracle, name, c))
+    conv.set_tile(tile)
+    assert conv.tile == tile
     x = ks_inputs(c)
     out = np.zeros((2, 2 * c["N"]), np.uint64)
     conv.Convert(out, x)
@@ -40,22 +43,26 @@ def test_rlwe_ks_batch_accumulates_into_output(native, oracle, golden):
         np.testing.assert_array_equal(out[b], exp)
 
 
+@pytest.mark.parametrize("tile", [4, 8])
 @pytest.mark.parametrize("name", ["auto5_n2048", "auto2049_n2048", "auto33_n128"])
-def test_automorphism_matches_reference(native, oracle, golden, name):
+def test_automorphism_matches_reference(native, oracle, golden, name, tile):
     from fhetoothpaste_b200 import GpuAutomorphismEvaluator
     c, expect = case(golden, name)
     ev = GpuAutomorphismEvaluator(c["N"], 1 << c["basis_log2"], c["digits"], c["index"], ks_key(oracle, name, c))
+    ev.set_tile(tile)
     x = ks_inputs(c)
     out = np.zeros((2, 2 * c["N"]), np.uint64)
     ev.Eval(out, x)
     np.testing.assert_array_equal(out, expect)
 
 
+@pytest.mark.parametrize("tile", [4, 8])
 @pytest.mark.parametrize("name", ["pack2_n128", "pack32_n256", "pack2048_n2048"])
-def test_pack_matches_reference(native, oracle, golden, name):
+def test_pack_matches_reference(native, oracle, golden, name, tile):
     from fhetoothpaste_b200 import GpuLWEtoRLWEPacker
     c, expect = case(golden, name)
     pk = GpuLWEtoRLWEPacker(c["N"], 1 << c["basis_log2"], c["digits"], ks_key(oracle, name, c))
+    pk.set_tile(tile)
     got = pk.Pack(ks_inputs(c), c["len"])
     np.testing.assert_array_equal(got[0], expect[0])
 
