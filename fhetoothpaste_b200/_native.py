@@ -111,6 +111,8 @@ def lib() -> ctypes.CDLL:
         "tp_sap_upload_keys": (ctypes.c_int, [VP, U64P, U64, U64P, U64, U64P, U64]),
         "tp_sap_decompose_batch": (ctypes.c_int, [VP, U64, VP, U64, VP, U64, U64, U64,
                                                   ctypes.POINTER(ctypes.c_uint32), VP]),
+        "tp_sap_homtrunc_batch": (ctypes.c_int, [VP, U64, VP, VP, U64, VP]),
+        "tp_sap_reset_batch": (ctypes.c_int, [VP, U64, VP, U64, VP]),
         "tp_server_create": (ctypes.c_int, [ctypes.c_int, U64, ctypes.POINTER(VP)]),
         "tp_server_add_set": (ctypes.c_int, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),

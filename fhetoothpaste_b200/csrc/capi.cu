@@ -1521,7 +1521,7 @@ tp_status tp_sap_create(const tp_br_params* rotation, uint64_t trace_basis, uint
     fresh[c->N] = kP / (2ull * c->N);
     cudaError_t e = cudaMalloc(&c->fresh, fresh.size() * 8);
     if (e == cudaSuccess) e = cudaMemcpy(c->fresh, fresh.data(), fresh.size() * 8, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&c->consts, 3ull * c->N * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&c->consts, 4ull * c->N * 8);
     if (e != cudaSuccess) {
         tp_sap_destroy(c);
         return fail(TP_ERR_CUDA, "SAP constants: %s", cudaGetErrorString(e));
@@ -1551,18 +1551,21 @@ tp_status tp_sap_upload_keys(tp_sap_ctx* c, const uint64_t* brk, uint64_t brk_wo
 
 // Constants for `radix` (NTT domain): the extraction polynomial x -> x mod radix,
 // reversed (lines 394-399), the truncation pad sum_{i<radix} X^(i-(radix-1))
-// (lines 212-217) and the reset's overflow polynomial (lines 320-324, radix 0 as
-// Decompose passes it, so IntLog2(0) = 0: -(N - i) at X^i).
+// (lines 212-217), and the reset's overflow polynomial -((N-i) >> r << r) at X^i
+// (lines 320-324) for r = IntLog2(0) = 0, as Decompose passes radix 0, and for
+// r = IntLog2(radix).
 static tp_status sap_constants(tp_sap_ctx* c, uint64_t radix, cudaStream_t st) {
     if (c->radix == radix) return TP_OK;
     const uint64_t N = c->N;
-    std::vector<uint64_t> h(3 * N, 0);
+    const int r = ilog2(radix);
+    std::vector<uint64_t> h(4 * N, 0);
     for (uint64_t i = 1; i < N; ++i) h[N - i] = (kP - (i & (radix - 1))) % kP;
     for (uint64_t i = N - (radix - 1); i < N; ++i) h[N + i] = kP - 1;
     h[N] = 1;
     for (uint64_t i = 1; i < N; ++i) h[2 * N + i] = kP - (N - i);
+    for (uint64_t i = 1; i < N; ++i) h[3 * N + i] = (kP - (((N - i) >> r) << r)) % kP;
     TP_CUDA(cudaMemcpyAsync(c->consts, h.data(), h.size() * 8, cudaMemcpyHostToDevice, st));
-    tp_status s = ntt_launch((uint32_t)N, 3, c->consts, c->consts, st, true);
+    tp_status s = ntt_launch((uint32_t)N, 4, c->consts, c->consts, st, true);
     if (s != TP_OK) return s;
     TP_CUDA(cudaStreamSynchronize(st));
     c->radix = radix;
@@ -1570,6 +1573,80 @@ static tp_status sap_constants(tp_sap_ctx* c, uint64_t radix, cudaStream_t st) {
 }
 
 static unsigned sap_blocks(uint64_t work) { return (unsigned)std::min<uint64_t>((work + 255) / 256, 65535); }
+
+// Scratch for `batch` LWEs and trees of `leaves` leaves.
+static tp_status sap_reserve(tp_sap_ctx* c, uint64_t batch, uint64_t leaves) {
+    if (c->cap >= batch && c->leaves >= leaves) return TP_OK;
+    const uint64_t N = c->N, n = c->n;
+    const uint64_t B = std::max(batch, c->cap), Lv = std::max(leaves, c->leaves);
+    for (void* p : {(void*)c->copy, (void*)c->sub, (void*)c->modulus, (void*)c->acc, (void*)c->ext, (void*)c->lw,
+                    (void*)c->tree, (void*)c->flags})
+        cudaFree(p);
+    c->copy = c->sub = c->modulus = c->acc = c->ext = c->lw = c->tree = nullptr;
+    c->flags = nullptr;
+    c->cap = c->leaves = 0;
+    TP_CUDA(cudaMalloc(&c->copy, B * (n + 1) * 8));
+    TP_CUDA(cudaMalloc(&c->sub, B * (n + 1) * 8));
+    TP_CUDA(cudaMalloc(&c->lw, B * (n + 1) * 8));
+    TP_CUDA(cudaMalloc(&c->modulus, B * 8));
+    TP_CUDA(cudaMalloc(&c->flags, B));
+    TP_CUDA(cudaMalloc(&c->acc, B * 2 * N * 8));
+    TP_CUDA(cudaMalloc(&c->ext, B * 2 * N * 8));
+    TP_CUDA(cudaMalloc(&c->tree, B * Lv * 2 * N * 8));
+    c->cap = B;
+    c->leaves = Lv;
+    return TP_OK;
+}
+
+// HomTrunc (lines 189-291) of `batch` NTT-domain RLWEs into coefficient-domain
+// results: N^-1 and the pad, INTT, the partial trace over N+1 .. 2^(L+1)+1, the
+// truncation tree level by level (kKsSplit), the leaf sum. Uses c->tree.
+static tp_status sap_trunc(tp_sap_ctx* c, uint64_t batch, const uint64_t* in_ntt, uint64_t* out_coef, uint64_t radix,
+                           cudaStream_t st) {
+    const uint64_t N = c->N;
+    const uint32_t L = c->logn - (uint32_t)ilog2(radix);
+    const uint64_t S = (2 * N) << L;  // words of one LWE's tree
+    tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->tree, S, in_ntt, c->consts + N,
+                                                                     c->br->tab->n_inv, batch, (uint32_t)N);
+    TP_CUDA(cudaGetLastError());
+    tp_status s = ntt_launch((uint32_t)N, batch, c->tree, c->tree, st, false, S, S);
+    if (s == TP_OK) s = ntt_launch((uint32_t)N, batch, c->tree + N, c->tree + N, st, false, S, S);
+    if (s == TP_OK) s = ks_trace_steps(c->trace, batch, c->tree, S, (int)c->logn, (int)(L + 1), st);
+    if (s != TP_OK) return s;
+    for (uint32_t l = L; l >= 1; --l) {
+        tp::KsKernelParams kp = c->trace->kp;
+        kp.key = c->trace->key + (uint64_t)(l - 1) * c->trace->digits * 2 * N;
+        kp.in = c->tree;
+        kp.out = c->tree;
+        kp.items = batch << (L - l);
+        kp.in_stride = kp.out_stride = (2 * N) << l;
+        kp.right_offset = (2 * N) << (l - 1);
+        kp.auto_index = (1u << l) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = (uint32_t)(N >> l);
+        s = ks_launch(c->trace, tp::kKsSplit, kp, st);
+        if (s != TP_OK) return s;
+    }
+    tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(out_coef, c->tree, batch, (uint32_t)N, L);
+    TP_CUDA(cudaGetLastError());
+    return TP_OK;
+}
+
+// ResetAccumulator (lines 293-351) of `batch` NTT-domain accumulators into fresh
+// NTT-domain ones: overflow extraction (polynomial `ovf`), INTT, the fused
+// SampleExtract -> LWE key switch -> FLOOR switch to 2N, a rotation of (0, Q/2N).
+// Uses c->ext and c->lw; `fresh` may be c->ext.
+static tp_status sap_reset_into(tp_sap_ctx* c, uint64_t batch, const uint64_t* acc_ntt, const uint64_t* ovf,
+                                uint64_t* fresh, cudaStream_t st) {
+    const uint64_t N = c->N, n = c->n;
+    tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, acc_ntt, ovf, 1, batch,
+                                                                     (uint32_t)N);
+    TP_CUDA(cudaGetLastError());
+    tp_status s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, st, false);
+    if (s == TP_OK) s = tp_pbs_epilogue_batch(c->lks, batch, c->lw, c->ext, 2 * N, st);
+    if (s == TP_OK) s = br_rotate_auto(c->br, batch, fresh, c->lw, n + 1, c->fresh, 0, 0, st);
+    return s;
+}
 
 tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, uint64_t out_digits,
                                  const uint64_t* lwes, uint64_t radix, uint64_t hamming_weight,
@@ -1586,32 +1663,9 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
     TP_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t logr = (uint32_t)ilog2(radix);
-    const uint32_t L = c->logn - logr;
-    const uint64_t leaves = 1ull << L;
-    if (c->cap < batch || c->leaves < leaves) {
-        for (void* p : {(void*)c->copy, (void*)c->sub, (void*)c->modulus, (void*)c->acc, (void*)c->ext,
-                        (void*)c->lw, (void*)c->tree, (void*)c->flags})
-            cudaFree(p);
-        c->copy = c->sub = c->modulus = c->acc = c->ext = c->lw = c->tree = nullptr;
-        c->flags = nullptr;
-        c->cap = c->leaves = 0;
-        const uint64_t B = std::max(batch, c->cap);
-        TP_CUDA(cudaMalloc(&c->copy, B * (n + 1) * 8));
-        TP_CUDA(cudaMalloc(&c->sub, B * (n + 1) * 8));
-        TP_CUDA(cudaMalloc(&c->lw, B * (n + 1) * 8));
-        TP_CUDA(cudaMalloc(&c->modulus, B * 8));
-        TP_CUDA(cudaMalloc(&c->flags, B));
-        TP_CUDA(cudaMalloc(&c->acc, B * 2 * N * 8));
-        TP_CUDA(cudaMalloc(&c->ext, B * 2 * N * 8));
-        TP_CUDA(cudaMalloc(&c->tree, B * leaves * 2 * N * 8));
-        c->cap = B;
-        c->leaves = leaves;
-    }
-    tp_status s = sap_constants(c, radix, st);
+    tp_status s = sap_reserve(c, batch, 1ull << (c->logn - logr));
+    if (s == TP_OK) s = sap_constants(c, radix, st);
     if (s != TP_OK) return s;
-    const uint64_t* xpoly = c->consts;
-    const uint64_t* pad = c->consts + N;
-    const uint64_t* ovf = c->consts + 2 * N;
 
     // input moduli and digit counts (lines 409-416); one read-back to plan the steps
     tp::sap_init_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(c->copy, c->modulus, lwes, batch,
@@ -1635,7 +1689,6 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
                         digits[b], (unsigned long long)out_digits);
 
     const uint64_t out_stride = out_digits * (N + 1);
-    const uint64_t S = leaves * 2 * N;  // words of one LWE's tree
     for (uint32_t d = 0; d < steps; ++d) {
         bool any_reset = false, more = false;
         for (uint64_t b = 0; b < batch; ++b) {
@@ -1651,8 +1704,8 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
         s = br_rotate_auto(c->br, batch, c->acc, c->sub, n + 1, c->acc, 2 * N, 0, stream);
         if (s != TP_OK) return s;
         // digit d = SampleExtract(INTT(acc (.) extract poly)) (lines 438-445)
-        tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, xpoly, 1, batch,
-                                                                         (uint32_t)N);
+        tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, c->consts, 1,
+                                                                         batch, (uint32_t)N);
         TP_CUDA(cudaGetLastError());
         s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
         if (s != TP_OK) return s;
@@ -1660,47 +1713,60 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
                                                                           batch, (uint32_t)N);
         TP_CUDA(cudaGetLastError());
         if (any_reset) {
-            // ResetAccumulator (lines 293-351): overflow extraction, SampleExtract, LWE key
-            // switch, FLOOR switch to 2N, rotation of (0, Q/2N); taken where flagged
-            tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, ovf, 1, batch,
-                                                                             (uint32_t)N);
-            TP_CUDA(cudaGetLastError());
-            s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
-            if (s == TP_OK) s = tp_pbs_epilogue_batch(c->lks, batch, c->lw, c->ext, 2 * N, stream);
-            if (s == TP_OK) s = br_rotate_auto(c->br, batch, c->ext, c->lw, n + 1, c->fresh, 0, 0, stream);
+            // ResetAccumulator(acc, 0) (line 452), taken where flagged
+            s = sap_reset_into(c, batch, c->acc, c->consts + 2 * N, c->ext, st);
             if (s != TP_OK) return s;
             tp::sap_select_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->ext, c->flags, batch,
                                                                            (uint32_t)N);
             TP_CUDA(cudaGetLastError());
         }
         if (!more) break;
-        // HomTrunc (lines 189-291) in coefficients: N^-1 and the pad, INTT, partial trace
-        // over N+1 .. 2^(L+1)+1, the truncation tree level by level, the leaf sum
-        tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->tree, S, c->acc, pad,
-                                                                         c->br->tab->n_inv, batch, (uint32_t)N);
-        TP_CUDA(cudaGetLastError());
-        s = ntt_launch((uint32_t)N, batch, c->tree, c->tree, stream, false, S, S);
-        if (s == TP_OK) s = ntt_launch((uint32_t)N, batch, c->tree + N, c->tree + N, stream, false, S, S);
-        if (s == TP_OK) s = ks_trace_steps(c->trace, batch, c->tree, S, (int)c->logn, (int)(L + 1), st);
+        // HomTrunc (line 457); its coefficient-domain result is the next rotation's accumulator
+        s = sap_trunc(c, batch, c->acc, c->acc, radix, st);
         if (s != TP_OK) return s;
-        for (uint32_t l = L; l >= 1; --l) {
-            tp::KsKernelParams kp = c->trace->kp;
-            kp.key = c->trace->key + (uint64_t)(l - 1) * c->trace->digits * 2 * N;
-            kp.in = c->tree;
-            kp.out = c->tree;
-            kp.items = batch << (L - l);
-            kp.in_stride = kp.out_stride = (2 * N) << l;
-            kp.right_offset = (2 * N) << (l - 1);
-            kp.auto_index = (1u << l) + 1;
-            kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
-            kp.shift = (uint32_t)(N >> l);
-            s = ks_launch(c->trace, tp::kKsSplit, kp, st);
-            if (s != TP_OK) return s;
-        }
-        tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->tree, batch, (uint32_t)N, L);
-        TP_CUDA(cudaGetLastError());
     }
     return TP_OK;
+}
+
+tp_status tp_sap_homtrunc_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, uint64_t radix,
+                                void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->ready) return fail(TP_ERR_STATE, "keys not uploaded");
+    if (radix < 2 || radix > c->N || (radix & (radix - 1)))
+        return fail(TP_ERR_PARAM, "radix must be a power of two in [2, N]");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    tp_status s = sap_reserve(c, batch, 1ull << (c->logn - ilog2(radix)));
+    if (s == TP_OK) s = sap_constants(c, radix, st);
+    if (s == TP_OK) s = sap_trunc(c, batch, in, out, radix, st);
+    // the reference's HomTrunc output is in the NTT domain
+    if (s == TP_OK) s = ntt_launch(c->N, 2 * batch, out, out, stream, true);
+    return s;
+}
+
+tp_status tp_sap_reset_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* acc, uint64_t radix, void* stream) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (!c->ready) return fail(TP_ERR_STATE, "keys not uploaded");
+    if (radix > c->N || (radix & (radix - 1))) return fail(TP_ERR_PARAM, "radix must be 0 or a power of two <= N");
+    if (batch == 0) return TP_OK;
+    if (!acc) return fail(TP_ERR_PARAM, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    // radix 0 and 1 give the same polynomial (IntLog2 of both is 0); keep the
+    // extraction and pad constants of a real radix if they are loaded
+    const uint64_t key = radix >= 2 ? radix : (c->radix ? c->radix : 2);
+    tp_status s = sap_reserve(c, batch, 1);
+    if (s == TP_OK) s = sap_constants(c, key, st);
+    if (s != TP_OK) return s;
+    const uint64_t* ovf = radix >= 2 ? c->consts + 3 * c->N : c->consts + 2 * c->N;
+    s = sap_reset_into(c, batch, acc, ovf, c->ext, st);
+    if (s == TP_OK)
+        TP_CUDA(cudaMemcpyAsync(acc, c->ext, batch * 2 * c->N * 8, cudaMemcpyDeviceToDevice, st));
+    return s;
 }
 
 }  // extern "C"

@@ -601,6 +601,24 @@ std::vector<uint32_t> GpuSAPDecomposer::DecomposeBatch(uint64_t batch, uint64_t*
     return digits;
 }
 
+void GpuSAPDecomposer::HomTrunc(uint64_t* output, uint64_t* input, uint64_t radix) {
+    DevBuf din(2ull * m_N), dout(2ull * m_N);
+    if (cudaMemcpy(din.p, input, 2ull * m_N * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_sap_homtrunc_batch(m_ctx, 1, dout.p, din.p, radix, nullptr));
+    if (cudaMemcpy(output, dout.p, 2ull * m_N * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
+void GpuSAPDecomposer::ResetAccumulator(uint64_t* acc, uint64_t radix) {
+    DevBuf d(2ull * m_N);
+    if (cudaMemcpy(d.p, acc, 2ull * m_N * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_sap_reset_batch(m_ctx, 1, d.p, radix, nullptr));
+    if (cudaMemcpy(acc, d.p, 2ull * m_N * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
 void GpuSAPDecomposer::Decompose(uint64_t* output, const uint64_t* input, uint64_t radix) {
     // the output holds as many digits as the input implies; stage through a buffer of the
     // context's maximum and copy those back

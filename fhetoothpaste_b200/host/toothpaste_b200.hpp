@@ -307,6 +307,10 @@ public:
     // words. Returns each LWE's digit count.
     std::vector<uint32_t> DecomposeBatch(uint64_t batch, uint64_t* outputs, uint64_t out_digits, const uint64_t* lwes,
                                          uint64_t radix);
+    // HomTrunc (lines 189-291) and ResetAccumulator (lines 293-351), reference signatures;
+    // 2N-word RLWEs in the NTT domain.
+    void HomTrunc(uint64_t* output, uint64_t* input, uint64_t radix);
+    void ResetAccumulator(uint64_t* acc, uint64_t radix);
 
 private:
     tp_sap_ctx* m_ctx = nullptr;

@@ -66,6 +66,29 @@ class GpuSAPDecomposer:
                                                    digits.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), stream))
         return digits
 
+    def homtrunc_batch(self, batch: int, out_ptr: int, in_ptr: int, radix: int, stream=None) -> None:
+        """HomTrunc of `batch` NTT-domain RLWEs (device, 2N words each) into out (NTT domain)."""
+        nat.check(nat.lib().tp_sap_homtrunc_batch(self._h, batch, out_ptr, in_ptr, radix, stream))
+
+    def reset_batch(self, batch: int, acc_ptr: int, radix: int = 0, stream=None) -> None:
+        """ResetAccumulator of `batch` NTT-domain accumulators in place (radix 0 as Decompose passes it)."""
+        nat.check(nat.lib().tp_sap_reset_batch(self._h, batch, acc_ptr, radix, stream))
+
+    def HomTrunc(self, rlwes: np.ndarray, radix: int) -> np.ndarray:
+        import torch
+        x = np.ascontiguousarray(rlwes, dtype=np.uint64).reshape(-1, 2 * self.N)
+        d_in = torch.from_numpy(x.view(np.int64)).cuda()
+        d_out = torch.empty_like(d_in)
+        self.homtrunc_batch(x.shape[0], d_out.data_ptr(), d_in.data_ptr(), radix)
+        return d_out.cpu().numpy().view(np.uint64)
+
+    def ResetAccumulator(self, accs: np.ndarray, radix: int = 0) -> np.ndarray:
+        import torch
+        x = np.ascontiguousarray(accs, dtype=np.uint64).reshape(-1, 2 * self.N)
+        d = torch.from_numpy(x.copy().view(np.int64)).cuda()
+        self.reset_batch(x.shape[0], d.data_ptr(), radix)
+        return d.cpu().numpy().view(np.uint64)
+
     def Decompose(self, lwes: np.ndarray, radix: int, out_digits: int) -> tuple[np.ndarray, np.ndarray]:
         """Decomposes rows of n+1 words; returns (digit counts, batch x out_digits x (N+1) words, zero-initialised)."""
         import torch

@@ -401,6 +401,14 @@ tp_status tp_sap_upload_keys(tp_sap_ctx* ctx, const uint64_t* brk, uint64_t brk_
 tp_status tp_sap_decompose_batch(tp_sap_ctx* ctx, uint64_t batch, uint64_t* out_dev, uint64_t out_digits,
                                  const uint64_t* lwes_dev, uint64_t radix, uint64_t hamming_weight,
                                  uint64_t restart_period, uint32_t* digits_host, void* stream);
+/* SAPDecomposer::HomTrunc(output, input, radix) (lines 189-291) on `batch` RLWEs
+ * (device, 2N words each, NTT domain in and out); radix a power of two in [2, N]. */
+tp_status tp_sap_homtrunc_batch(tp_sap_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev,
+                                uint64_t radix, void* stream);
+/* SAPDecomposer::ResetAccumulator(acc, radix) (lines 293-351) on `batch` RLWEs in
+ * place (device, NTT domain); radix 0 (as Decompose passes it) or a power of two.
+ * The LWE key switch runs as on a fresh converter. */
+tp_status tp_sap_reset_batch(tp_sap_ctx* ctx, uint64_t batch, uint64_t* acc_dev, uint64_t radix, void* stream);
 
 /* ---- Key files ------------------------------------------------------------
  * The reference keeps keys only in memory (no serialization). A key file holds

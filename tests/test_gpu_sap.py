@@ -50,6 +50,51 @@ def test_matches_reference_outputs(native, oracle, cuda, name):
         assert not nz or max(nz) < digits[j]
 
 
+@pytest.mark.parametrize("name", sorted(k for k, c in MANIFEST.items() if c["N"] <= 1024))
+def test_homtrunc_and_reset_match_reference(native, oracle, cuda, name):
+    """HomTrunc and ResetAccumulator as their own calls, on the recorded random inputs; then a batch
+    of both against the oracle, with ResetAccumulator at a nonzero radix too."""
+    from oracle.oracle import random_acc
+    c = MANIFEST[name]
+    N, n = c["N"], c["n"]
+    sk = lwe_secret(c["variant"], n, N, seed=c["sk_seed"])
+    z = rlwe_secret(N, seed=c["sk_seed"] + 1)
+    keys = oracle.sap_keygen(c["variant"], N, n, tuple(c["rotation"]), tuple(c["trace"]), tuple(c["ks"]), c["std"],
+                             sk, z, c["key_seed"])
+    dec = decomposer(c, keys, c["beta"], c["restart"])
+    x = random_acc(N, 2, c["in_seed"] + 1)
+    assert sha256(dec.HomTrunc(x[0], c["radix"])[0]) == c["homtrunc_sha256"]
+    assert sha256(dec.ResetAccumulator(x[1], 0)[0]) == c["reset_sha256"]
+    y = random_acc(N, 5, c["in_seed"] + 7)
+    ht = dec.HomTrunc(y, c["radix"])
+    rs = dec.ResetAccumulator(y, c["radix"])
+    for j in (0, 4):
+        np.testing.assert_array_equal(ht[j], oracle.sap_homtrunc(N, tuple(c["trace"]), keys[1], c["radix"], y[j]))
+        np.testing.assert_array_equal(rs[j], oracle.sap_reset(c["variant"], N, n, tuple(c["rotation"]), keys[0],
+                                                              tuple(c["ks"]), keys[2], c["radix"], y[j]))
+
+
+def test_radix_extremes_against_oracle(native, oracle, cuda):
+    """Radix 2 (the deepest tree; the reference's own buffer is too small for it) and radix N
+    (no tree: the whole trace) against the oracle restatement."""
+    N, n = 256, 10
+    c = {"variant": CGGI_BINARY, "N": N, "n": n, "rotation": (16, 4), "trace": (16, 4), "ks": (16, 4)}
+    sk = lwe_secret(CGGI_BINARY, n, N, seed=1501)
+    z = rlwe_secret(N, seed=1502)
+    keys = oracle.sap_keygen(CGGI_BINARY, N, n, (16, 4), (16, 4), (16, 4), 3.2, sk, z, 1503)
+    beta = int(np.count_nonzero(sk))
+    dec = decomposer(c, keys, beta, 4)
+    rng = np.random.default_rng(1504)
+    lwes = rng.integers(0, 1 << 12, (2, n + 1), dtype=np.uint64)
+    for radix, od in ((2, 13), (N, 3)):
+        digits, got = dec.Decompose(lwes, radix, od)
+        for j in range(2):
+            d, want = oracle.sap_decompose(CGGI_BINARY, N, n, (16, 4), keys[0], (16, 4), keys[1], (16, 4), keys[2],
+                                           radix, beta, 4, lwes[j], od)
+            assert digits[j] == d
+            np.testing.assert_array_equal(got[j], want, err_msg=f"radix {radix} lwe {j}")
+
+
 def test_batch_order_and_single_calls_agree(native, oracle, cuda):
     c = MANIFEST["bmmp_n256_r8_reset"]
     N, n = c["N"], c["n"]
@@ -116,6 +161,10 @@ def test_errors(native, cuda):
     for radix, restart in ((6, 5), (512, 5), (1, 5), (4, 0)):
         assert L.tp_sap_decompose_batch(h, 1, y.data_ptr(), 10, x.data_ptr(), radix, 3, restart, None,
                                         None) == nat.TP_ERR_PARAM
+    r = cuda.zeros(2 * 256, dtype=cuda.int64, device="cuda")
+    for radix in (1, 3, 512):
+        assert L.tp_sap_homtrunc_batch(h, 1, r.data_ptr(), r.data_ptr(), radix, None) == nat.TP_ERR_PARAM
+    assert L.tp_sap_reset_batch(h, 1, r.data_ptr(), 6, None) == nat.TP_ERR_PARAM
     x.fill_(1 << 40)                                  # 2^41 needs 21 base-4 digits
     assert L.tp_sap_decompose_batch(h, 1, y.data_ptr(), 10, x.data_ptr(), 4, 3, 5, None, None) == nat.TP_ERR_PARAM
     assert L.tp_sap_destroy(h) == nat.TP_OK
