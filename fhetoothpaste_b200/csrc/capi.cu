@@ -728,6 +728,12 @@ struct tp_ks_ctx {
     int per_sm[2][tp::kKsModes] = {};
     uint64_t* work = nullptr;     // packing tree nodes
     uint64_t work_words = 0;
+    // PackConsecutively plan for consec_len inputs: leaf inputs, then each level's node pairs
+    uint64_t consec_len = 0;
+    uint32_t* consec_plan = nullptr;
+    std::vector<uint64_t> consec_off;  // per level: offset into the plan (words)
+    std::vector<uint32_t> consec_cnt;  // per level: nodes of one pack
+    uint64_t* zero = nullptr;          // 2N zero words
     std::mutex mu;
 };
 
@@ -808,6 +814,8 @@ tp_status tp_ks_destroy(tp_ks_ctx* c) {
     cudaSetDevice(c->device);
     cudaFree(c->key);
     cudaFree(c->work);
+    cudaFree(c->consec_plan);
+    cudaFree(c->zero);
     delete c;
     return TP_OK;
 }
@@ -930,6 +938,109 @@ static tp_status ks_trace_steps(tp_ks_ctx* c, uint64_t items, uint64_t* data, ui
         kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
         kp.shift = 0;
         tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+        if (s != TP_OK) return s;
+    }
+    return TP_OK;
+}
+
+// The compacted tree of LWEtoRLWEPacker::PackConsecutively (lwe_to_rlwe_packing.cpp:
+// 260-393): a full tree over N leaves, leaf e holding input (N-1) ^ brv(e) when that is
+// below len and an empty subtree otherwise; only nodes with an input below them are kept,
+// a level's nodes in tree order. Level 0 lists the leaves' inputs, level l >= 1 one
+// (left, right) pair of previous-level nodes per node (kNoNode: an empty subtree, zero).
+static tp_status consec_plan(tp_ks_ctx* c, uint64_t len) {
+    if (c->consec_len == len) return TP_OK;
+    const uint64_t N = c->N;
+    const int logn = c->logn;
+    std::vector<uint32_t> plan;
+    std::vector<uint64_t> off(logn + 1);
+    std::vector<uint32_t> cnt(logn + 1);
+    std::vector<int64_t> rank(N), next(N);
+    off[0] = 0;
+    for (uint64_t e = 0; e < N; ++e) {
+        uint64_t r = 0;
+        for (int b = 0; b < logn; ++b) r |= ((e >> b) & 1) << (logn - 1 - b);
+        const uint64_t src = (N - 1) ^ r;
+        rank[e] = src < len ? (int64_t)plan.size() : -1;
+        if (src < len) plan.push_back((uint32_t)src);
+    }
+    cnt[0] = (uint32_t)plan.size();
+    for (int l = 1; l <= logn; ++l) {
+        off[l] = plan.size();
+        uint32_t k = 0;
+        for (uint64_t u = 0; u < (N >> l); ++u) {
+            const int64_t a = rank[2 * u], b = rank[2 * u + 1];
+            if (a < 0 && b < 0) {
+                next[u] = -1;
+                continue;
+            }
+            plan.push_back(a < 0 ? tp::kNoNode : (uint32_t)a);
+            plan.push_back(b < 0 ? tp::kNoNode : (uint32_t)b);
+            next[u] = k++;
+        }
+        cnt[l] = k;
+        for (uint64_t u = 0; u < (N >> l); ++u) rank[u] = next[u];
+    }
+    cudaFree(c->consec_plan);
+    c->consec_plan = nullptr;
+    c->consec_len = 0;
+    TP_CUDA(cudaMalloc(&c->consec_plan, plan.size() * 4));
+    TP_CUDA(cudaMemcpy(c->consec_plan, plan.data(), plan.size() * 4, cudaMemcpyHostToDevice));
+    if (!c->zero) {
+        TP_CUDA(cudaMalloc(&c->zero, 2 * N * 8));
+        TP_CUDA(cudaMemset(c->zero, 0, 2 * N * 8));
+    }
+    c->consec_off = off;
+    c->consec_cnt = cnt;
+    c->consec_len = len;
+    return TP_OK;
+}
+
+tp_status tp_pack_consecutive_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out, const uint64_t* in,
+                                    void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (packs == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->N;
+    if (len < 2 || len > N) return fail(TP_ERR_PARAM, "len must be in [2, N]");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    tp_status s = consec_plan(c, len);
+    if (s != TP_OK) return s;
+    const uint64_t half = packs * len * 2 * N;  // each level's nodes fit one half (at most len per pack)
+    if (c->work_words < 2 * half) {
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_words = 0;
+        TP_CUDA(cudaMalloc(&c->work, 2 * half * 8));
+        c->work_words = 2 * half;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t* buf[2] = {c->work, c->work + half};
+    {
+        const uint64_t total = packs * c->consec_cnt[0] * 2 * N;
+        tp::pack_l0_idx_kernel<<<(unsigned)std::min<uint64_t>((total + 255) / 256, 65535), 256, 0, st>>>(
+            buf[0], in, c->consec_plan, packs, c->consec_cnt[0], (uint32_t)len, (uint32_t)c->logn, c->tab->n_inv);
+        TP_CUDA(cudaGetLastError());
+    }
+    const uint64_t kw = (uint64_t)c->digits * 2 * N;
+    tp::KsKernelParams kp = c->kp;
+    for (int l = 1; l <= c->logn; ++l) {
+        kp.key = c->key + (uint64_t)(l - 1) * kw;
+        kp.in = buf[(l - 1) & 1];
+        kp.out = l == c->logn ? out : buf[l & 1];
+        kp.items = packs * c->consec_cnt[l];
+        kp.in_stride = kp.out_stride = 2 * N;
+        kp.right_offset = 0;
+        kp.pairs = c->consec_plan + c->consec_off[l];
+        kp.zero = c->zero;
+        kp.pair_count = c->consec_cnt[l];
+        kp.prev_count = c->consec_cnt[l - 1];
+        kp.auto_index = (1u << l) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = (uint32_t)(N >> l);
+        s = ks_launch(c, tp::kKsMerge, kp, st);
         if (s != TP_OK) return s;
     }
     return TP_OK;

@@ -23,6 +23,7 @@ enum KsMode : int {
     kKsSplit = 4   // SAP truncation tree node: y = INTT(AutoKS(x)); x <- x + y; out1 <- X^-s (x - y)
 };
 constexpr int kKsModes = 5;
+constexpr uint32_t kNoNode = 0xFFFFFFFFu;
 
 struct KsKernelParams {
     const uint64_t* key;      // device layout: [digit][c][jp][t][2], C = 2, jp < E/2
@@ -39,6 +40,14 @@ struct KsKernelParams {
     uint32_t auto_index_inv;  // t^-1 mod 2N
     uint32_t shift;           // kKsMerge: X^shift rotation of the left node; kKsSplit: X^-shift of the difference
     uint64_t n_inv;
+    // kKsMerge over a compacted tree (PackConsecutively): item it of pack p = it / pair_count
+    // merges nodes pairs[2q] (left) and pairs[2q+1] (right) of the pack's previous level,
+    // q = it % pair_count, each node at in + (p * prev_count + slot) * in_stride; a slot of
+    // kNoNode stands for an empty subtree, read as `zero` (2N zero words)
+    const uint32_t* pairs;
+    const uint64_t* zero;
+    uint32_t pair_count;
+    uint32_t prev_count;
     uint64_t corr;
     uint32_t dshift[8];
     uint64_t dmask[8];
@@ -155,6 +164,15 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
         } else {
             const uint64_t* left = in;
             const uint64_t* right = in + (MODE == kKsMerge ? prm.right_offset : 0);
+            if constexpr (MODE == kKsMerge) {
+                if (prm.pairs) {
+                    const uint64_t pk = it / prm.pair_count, q = it % prm.pair_count;
+                    const uint32_t ls = prm.pairs[2 * q], rs = prm.pairs[2 * q + 1];
+                    const uint64_t* base = prm.in + pk * prm.prev_count * prm.in_stride;
+                    left = ls == kNoNode ? prm.zero : base + ls * prm.in_stride;
+                    right = rs == kNoNode ? prm.zero : base + rs * prm.in_stride;
+                }
+            }
             const uint32_t s = prm.shift;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {

@@ -28,6 +28,28 @@ __global__ void pack_l0_kernel(uint64_t* __restrict__ nodes, const uint64_t* __r
     }
 }
 
+// L0Setup of the inputs of a consecutive packing (lwe_to_rlwe_packing.cpp:260-393):
+// node s of pack p is the tree leaf whose input index is src[s] < len.
+__global__ void pack_l0_idx_kernel(uint64_t* __restrict__ nodes, const uint64_t* __restrict__ in,
+                                   const uint32_t* __restrict__ src, uint64_t packs, uint32_t count, uint32_t len,
+                                   uint32_t logn, uint64_t n_inv) {
+    const uint64_t N = 1ull << logn;
+    const uint64_t total = packs * count * 2 * N;
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
+         w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = w % (2 * N);
+        const uint64_t c = (w / (2 * N)) % count;
+        const uint64_t p = w / (2 * N * count);
+        const uint64_t* lwe = in + (p * len + src[c]) * (N + 1);
+        uint64_t v;
+        if (k == 0) v = lwe[0];
+        else if (k < N) v = gl_neg(lwe[N - k]);
+        else if (k == N) v = lwe[N];
+        else v = 0;
+        nodes[w] = gl_mul(v, n_inv);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // LWE -> LWE key switching (lib/src/operators/lwe_conversion.cpp:205-239), q = p:
 //   out[n_out] = in[n_in]; out[k] -= sum_{i,j} digit_j(in[i]) * ksk[i][j][k]

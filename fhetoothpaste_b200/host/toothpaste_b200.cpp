@@ -482,6 +482,15 @@ void GpuLWEtoRLWEPacker::Pack(uint64_t* output, const uint64_t* input, uint64_t 
         throw std::runtime_error("toothpaste_b200: copy back failed");
 }
 
+void GpuLWEtoRLWEPacker::PackConsecutively(uint64_t* output, const uint64_t* input, uint64_t len) {
+    DevBuf din(len * (m_N + 1ull)), dout(2ull * m_N);
+    if (cudaMemcpy(din.p, input, len * (m_N + 1ull) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_pack_consecutive_batch(m_ctx, 1, len, dout.p, din.p, nullptr));
+    if (cudaMemcpy(output, dout.p, 16ull * m_N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
 GpuLWEtoLWEConverter::GpuLWEtoLWEConverter(uint32_t n_in, uint32_t n_out, uint64_t basis, uint32_t digits,
                                            const std::vector<uint64_t>& ksk, int device)
     : m_n_in(n_in), m_n_out(n_out) {

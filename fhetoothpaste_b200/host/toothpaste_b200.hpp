@@ -222,6 +222,8 @@ public:
                        int device = 0);
     ~GpuLWEtoRLWEPacker();
     void Pack(uint64_t* output, const uint64_t* input, uint64_t len);
+    // lwe_to_rlwe_packing.cpp:260-393: the inputs on the first len coefficients, any 2 <= len <= N
+    void PackConsecutively(uint64_t* output, const uint64_t* input, uint64_t len);
 
 private:
     tp_ks_ctx* m_ctx = nullptr;

@@ -94,6 +94,18 @@ class GpuLWEtoRLWEPacker(_KsBase):
     def pack_batch(self, packs: int, length: int, out_ptr: int, in_ptr: int, stream=None) -> None:
         nat.check(nat.lib().tp_pack_batch(self._h, packs, length, out_ptr, in_ptr, stream))
 
+    def pack_consecutive_batch(self, packs: int, length: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_pack_consecutive_batch(self._h, packs, length, out_ptr, in_ptr, stream))
+
+    def PackConsecutively(self, lwes: np.ndarray, length: int) -> np.ndarray:
+        """PackConsecutively of `lwes` (packs*length rows of N+1 words); packs x 2N coefficients."""
+        import torch
+        d_in = _dev(torch, lwes)
+        packs = d_in.numel() // (length * (self.N + 1))
+        d_out = torch.empty((packs, 2 * self.N), dtype=torch.int64, device="cuda")
+        self.pack_consecutive_batch(packs, length, d_out.data_ptr(), d_in.data_ptr())
+        return d_out.cpu().numpy().view(np.uint64)
+
     def Pack(self, lwes: np.ndarray, length: int) -> np.ndarray:
         """Packs `lwes` (packs*length rows of N+1 words); returns packs x 2N coefficients."""
         import torch

@@ -215,6 +215,14 @@ tp_status tp_auto_eval_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, 
  * per level, in a context-owned work area of packs*len*2N words. Asynchronous. */
 tp_status tp_pack_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev, const uint64_t* in_dev,
                         void* stream);
+/* LWEtoRLWEPacker::PackConsecutively(out, in, len) (lwe_to_rlwe_packing.cpp:260-393)
+ * for `packs` packings of len inputs each (2 <= len <= N, any length): the inputs
+ * land on the first len coefficients. Runs the reference's full N-leaf tree with
+ * the empty subtrees cut away: per level one launch over the nodes that have an
+ * input below them (an empty sibling reads as zero). Device buffers as for
+ * tp_pack_batch; scratch 2 x packs x len x 2N words. Asynchronous. */
+tp_status tp_pack_consecutive_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev,
+                                    const uint64_t* in_dev, void* stream);
 
 /* tp_pack_batch for callers that cannot allocate device memory when they call:
  * a process whose HBM is owned by another allocator's pool, or a latency-bound

@@ -215,6 +215,10 @@ void* ref_pack_create(uint64_t N, uint64_t basis_log2, uint64_t digits, double s
 
 void ref_pack(void* hp, uint64_t* out, const uint64_t* in, uint64_t len) { ((LWEtoRLWEPacker*)hp)->Pack(out, in, len); }
 
+void ref_pack_consecutive(void* hp, uint64_t* out, const uint64_t* in, uint64_t len) {
+    ((LWEtoRLWEPacker*)hp)->PackConsecutively(out, in, len);
+}
+
 // The packer's automorphism keys (index 2^j + 1, j = 1..logN), concatenated.
 void ref_pack_key_copy(void* hp, uint64_t* out) {
     for (auto& ev : ((LWEtoRLWEPacker*)hp)->m_auto_evaluators) {

@@ -824,6 +824,54 @@ int tpo_pack(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* k
     return 0;
 }
 
+int tpo_pack_consecutive(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* keys,
+                         uint64_t* out, const uint64_t* in, uint64_t len) {
+    const uint64_t logn = int_log2(N);
+    if (!get_tables(N) || len < 2 || len > N) return -1;
+    uint64_t* slots = (uint64_t*)calloc((logn + 2) * 2 * N, 8);
+    uint64_t* rot = (uint64_t*)malloc(2 * N * 8);
+    uint64_t level[72], fake[72];
+    uint64_t head = 0, elem = 0;
+    /* element e is real when its input index (N-1) ^ brv(e) is below len (line 276) */
+#define CONSEC_PUSH(slot)                                                      \
+    do {                                                                       \
+        const uint64_t src = (N - 1) ^ rev_bits(elem, (unsigned)logn);          \
+        uint64_t* dst = slots + (slot) * 2 * N;                                 \
+        memset(dst, 0, 2 * N * 8);                                              \
+        if (src < len) l0_setup(N, dst, in + src * (N + 1));                    \
+        level[slot] = 0;                                                        \
+        fake[slot] = src >= len;                                                \
+        ++elem;                                                                 \
+    } while (0)
+    CONSEC_PUSH(0);
+    head = 1;
+    CONSEC_PUSH(1);
+    while (level[0] != logn) {
+        const uint64_t hl = head > 0 ? level[head] : UINT64_MAX;
+        const uint64_t nl = head > 0 ? level[head - 1] : 0;
+        if (hl == nl) {
+            if (fake[head] && fake[head - 1]) { /* two empty subtrees: no work (lines 327-331) */
+                --head;
+                level[head] = hl + 1;
+                fake[head] = 1;
+                continue;
+            }
+            pack_merge(N, basis_log2, digits, keys, hl + 1, slots + (head - 1) * 2 * N, slots + head * 2 * N, rot);
+            --head;
+            level[head] = hl + 1;
+            fake[head] = 0;
+        } else {
+            ++head;
+            CONSEC_PUSH(head);
+        }
+    }
+#undef CONSEC_PUSH
+    memcpy(out, slots, 2 * N * 8);
+    free(slots);
+    free(rot);
+    return 0;
+}
+
 void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index, uint64_t N) {
     for (uint64_t i = 0; i <= index; ++i) out_lwe[i] = rlwe[index - i];
     for (uint64_t i = index + 1; i < N; ++i) {

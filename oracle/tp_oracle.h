@@ -121,6 +121,13 @@ void tpo_pack_keygen(tpo_rng* r, uint64_t N, uint64_t basis_log2, uint64_t digit
 int tpo_pack(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* keys,
              uint64_t* out, const uint64_t* in, uint64_t len);
 
+/* PackConsecutively (lwe_to_rlwe_packing.cpp:260-393): len LWEs (2 <= len <= N) into the
+ * first len coefficients of one RLWE [A|B] (coefficient domain), by the reference's stack
+ * walk over a full N-leaf tree whose leaves without an input are zero and whose merges of
+ * two such leaves are skipped. */
+int tpo_pack_consecutive(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* keys,
+                         uint64_t* out, const uint64_t* in, uint64_t len);
+
 /* SampleExtract (lib/include/static/sample_extraction.h:20-36): writes nothing
  * where the source coefficient is zero (the caller pre-zeroes). */
 void tpo_sample_extract(uint64_t* out_lwe, const uint64_t* rlwe, uint64_t index, uint64_t N);

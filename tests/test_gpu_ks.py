@@ -1,10 +1,13 @@
 """Key switching, automorphisms, packing and LWE key switching on the GPU, bit-exact
 against the reference's golden vectors and the C oracle."""
+import json
+from pathlib import Path
+
 import numpy as np
 import pytest
 
 from kscases import ks_inputs, ks_key
-from oracle.oracle import P, random_acc, rlwe_secret, uniform_mod
+from oracle.oracle import P, random_acc, rlwe_secret, sha256, sm64, uniform_mod
 
 pytestmark = pytest.mark.gpu
 
@@ -128,3 +131,52 @@ def test_lwe_ks_large_batch_against_oracle(native, oracle, golden):
     for b in (0, 17, 999):
         np.testing.assert_array_equal(out[b], oracle.lwe_ks(P, c["n_in"], c["n_out"], c["basis_log2"], c["digits"],
                                                             k, x[b]))
+
+
+CONSEC = json.loads((Path(__file__).resolve().parent / "golden" / "consec.json").read_text())
+
+
+@pytest.mark.parametrize("name", sorted(CONSEC))
+def test_pack_consecutive_matches_reference(native, oracle, name):
+    """PackConsecutively (lwe_to_rlwe_packing.cpp:260-393) on the GPU against the reference's outputs,
+    lengths 2 to N including non-powers of two; tile 8 on one case too."""
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker
+    from test_consec_cpu import consec_case
+    c = CONSEC[name]
+    keys, lwes = consec_case(oracle, c)
+    pk = GpuLWEtoRLWEPacker(c["N"], 1 << c["basis_log2"], c["digits"], keys)
+    got = pk.PackConsecutively(lwes, c["len"])[0]
+    assert sha256(got) == c["output_sha256"]
+    if name == "consec100_n256":
+        pk.set_tile(8)
+        assert sha256(pk.PackConsecutively(lwes, c["len"])[0]) == c["output_sha256"]
+
+
+def test_pack_consecutive_many_packs_and_decryption(native, oracle):
+    """Several packings per call equal one-by-one oracle packings; with noise-free keys the packed
+    phase holds message i at coefficient i and zeros after (packing_tests.cpp TestConsecutivePacking)."""
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker
+    N, bl, dg, length, packs = 256, 16, 4, 24, 3
+    z = (sm64(801, N) & np.uint64(1))
+    keys = oracle.pack_keygen(N, bl, dg, 0.0, z, 802)
+    rng = np.random.default_rng(803)
+    lwes = np.zeros((packs * length, N + 1), np.uint64)
+    zo = [int(v) for v in z]
+    for r in range(packs * length):
+        a = [int(v) for v in rng.integers(0, P, N, dtype=np.uint64)]
+        lwes[r, :N] = a
+        lwes[r, N] = (sum(x * s for x, s in zip(a, zo)) + (r % length) + 1000 * (r // length)) % P
+    pk = GpuLWEtoRLWEPacker(N, 1 << bl, dg, keys)
+    got = pk.PackConsecutively(lwes, length)
+    for p in range(packs):
+        want = oracle.pack_consecutive(N, bl, dg, keys, lwes[p * length:(p + 1) * length], length)
+        np.testing.assert_array_equal(got[p], want, err_msg=f"pack {p}")
+        phase = oracle.phase_rlwe(oracle_ntt_pair(oracle, got[p]), z)
+        expect = np.zeros(N, np.uint64)
+        expect[:length] = np.arange(length, dtype=np.uint64) + np.uint64(1000 * p)
+        np.testing.assert_array_equal(phase, expect)
+
+
+def oracle_ntt_pair(oracle, rlwe_coef):
+    N = rlwe_coef.size // 2
+    return np.concatenate([oracle.ntt_forward(rlwe_coef[:N]), oracle.ntt_forward(rlwe_coef[N:])])
