@@ -7,7 +7,7 @@ from ._native import GOLDILOCKS, TP_BR_BMMP_BINARY, TP_BR_CGGI_BINARY, TP_BR_CGG
 from .blind_rotation import (BatchGraph, BlindRotationContext, GpuBlindRotator, NegacyclicFunctionEvaluator,  # noqa: F401
                              ntt_backward, ntt_forward, sample_extract_batch)
 from .key_switching import (GpuAutomorphismEvaluator, GpuLWEtoLWEConverter, GpuLWEtoRLWEPacker,  # noqa: F401,E402
-                            GpuRLWEtoRLWEConverter, modulus_switch_batch)
+                            GpuRLWEtoRLWEConverter, GpuTraceEvaluator, modulus_switch_batch)
 from .sap import GpuSAPDecomposer  # noqa: F401,E402
 from .scheme_switching import GpuLWEtoRGSWConverter  # noqa: F401,E402
 from .serving import BootstrapServer  # noqa: F401,E402

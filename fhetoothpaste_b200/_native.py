@@ -83,6 +83,8 @@ def lib() -> ctypes.CDLL:
         "tp_pack_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
         "tp_pack_batch_noalloc": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
         "tp_pack_consecutive_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
+        "tp_trace_eval_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_trace_eval_auto_batch": (ctypes.c_int, [VP, U64, VP, VP, ctypes.c_uint32, VP]),
         "tp_lwe_ks_create": (ctypes.c_int, [U64, ctypes.c_uint32, ctypes.c_uint32, U64, ctypes.c_uint32, ctypes.c_int,
                                             ctypes.POINTER(VP)]),
         "tp_lwe_ks_destroy": (ctypes.c_int, [VP]),

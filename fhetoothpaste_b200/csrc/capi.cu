@@ -943,6 +943,51 @@ static tp_status ks_trace_steps(tp_ks_ctx* c, uint64_t items, uint64_t* data, ui
     return TP_OK;
 }
 
+static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
+                            bool fwd, uint64_t in_stride, uint64_t out_stride);
+
+tp_status tp_trace_eval_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing (trace) context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t N = c->N, words = batch * 2 * N;
+    // output = input * N^-1, then x += INTT(Auto_{2^j+1}(x)) for j = log2 N .. 1, then NTT of
+    // both halves (trace_evaluation.cpp:135-158)
+    tp::scale_kernel<<<(unsigned)std::min<uint64_t>((words + 255) / 256, 65535), 256, 0, st>>>(out, in, words,
+                                                                                            c->tab->n_inv);
+    TP_CUDA(cudaGetLastError());
+    tp_status s = ks_trace_steps(c, batch, out, 2 * N, c->logn, 1, st);
+    if (s == TP_OK) s = ntt_launch((uint32_t)N, 2 * batch, out, out, stream, true, 0, 0);
+    return s;
+}
+
+tp_status tp_trace_eval_auto_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const uint64_t* in,
+                                   uint32_t auto_index, void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing (trace) context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    int j = 0;
+    while (j <= c->logn && (1u << j) + 1 != auto_index) ++j;
+    if (j < 1 || j > c->logn) return fail(TP_ERR_PARAM, "automorphism index must be 2^j + 1, 1 <= j <= log2 N");
+    if (batch == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    if (out == in) return fail(TP_ERR_PARAM, "automorphism output must not alias its input");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    tp::KsKernelParams kp = c->kp;
+    kp.key = c->key + (uint64_t)(j - 1) * c->digits * 2 * c->N;
+    kp.in = in;
+    kp.out = out;
+    kp.items = batch;
+    kp.in_stride = kp.out_stride = 2ull * c->N;
+    kp.auto_index = auto_index;
+    kp.auto_index_inv = inv_mod_2n(auto_index, 2 * c->N);
+    return ks_launch(c, tp::kKsAuto, kp, (cudaStream_t)stream);
+}
+
 // The compacted tree of LWEtoRLWEPacker::PackConsecutively (lwe_to_rlwe_packing.cpp:
 // 260-393): a full tree over N leaves, leaf e holding input (N-1) ^ brv(e) when that is
 // below len and an empty subtree otherwise; only nodes with an input below them are kept,

@@ -50,6 +50,14 @@ __global__ void pack_l0_idx_kernel(uint64_t* __restrict__ nodes, const uint64_t*
     }
 }
 
+// out = in * factor (mod p), element-wise (out may equal in).
+__global__ void scale_kernel(uint64_t* __restrict__ out, const uint64_t* __restrict__ in, uint64_t count,
+                             uint64_t factor) {
+    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < count;
+         w += (uint64_t)gridDim.x * blockDim.x)
+        out[w] = gl_mul(in[w], factor);
+}
+
 // ---------------------------------------------------------------------------
 // LWE -> LWE key switching (lib/src/operators/lwe_conversion.cpp:205-239), q = p:
 //   out[n_out] = in[n_in]; out[k] -= sum_{i,j} digit_j(in[i]) * ksk[i][j][k]

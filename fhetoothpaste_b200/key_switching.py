@@ -4,6 +4,7 @@
   GpuAutomorphismEvaluator AutomorphismEvaluator::Eval  (lib/src/operators/automorphism_evaluation.cpp:150-159)
   GpuLWEtoRLWEPacker      LWEtoRLWEPacker::Pack          (lib/src/operators/lwe_to_rlwe_packing.cpp:129-236)
   GpuLWEtoLWEConverter    LWEtoLWEConverter::Convert     (lib/src/operators/lwe_conversion.cpp:205-239)
+  GpuTraceEvaluator       TraceEvaluator::Eval / EvalAuto (lib/src/operators/trace_evaluation.cpp:135-179)
 
 Each takes its key in the reference layout (the operator's m_ksk; for the
 packer the automorphism keys for indices 2^j + 1, j = 1..log2 N, concatenated).
@@ -114,6 +115,39 @@ class GpuLWEtoRLWEPacker(_KsBase):
         d_out = torch.empty((packs, 2 * self.N), dtype=torch.int64, device="cuda")
         self.pack_batch(packs, length, d_out.data_ptr(), d_in.data_ptr())
         return d_out.cpu().numpy().view(np.uint64)
+
+
+class GpuTraceEvaluator(_KsBase):
+    """TraceEvaluator (lib/src/operators/trace_evaluation.cpp:135-186) with its automorphism keys
+    for indices 2^j + 1, j = 1..log2 N, concatenated (the packer's key layout)."""
+
+    def __init__(self, ring_dim: int, basis: int, digits: int, keys: np.ndarray, device: int = 0):
+        h = ctypes.c_void_p()
+        nat.check(nat.lib().tp_pack_create(ring_dim, basis, digits, device, ctypes.byref(h)))
+        self.N = ring_dim
+        super().__init__(h, keys)
+
+    def eval_batch(self, batch: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        nat.check(nat.lib().tp_trace_eval_batch(self._h, batch, out_ptr, in_ptr, stream))
+
+    def eval_auto_batch(self, batch: int, out_ptr: int, in_ptr: int, auto_index: int, stream=None) -> None:
+        nat.check(nat.lib().tp_trace_eval_auto_batch(self._h, batch, out_ptr, in_ptr, auto_index, stream))
+
+    def Eval(self, inp: np.ndarray) -> np.ndarray:
+        """Rows of 2N coefficient words -> the trace, NTT domain."""
+        import torch
+        d = _dev(torch, inp)
+        out = torch.empty_like(d)
+        self.eval_batch(d.numel() // (2 * self.N), out.data_ptr(), d.data_ptr())
+        return out.cpu().numpy().view(np.uint64)
+
+    def EvalAuto(self, inp: np.ndarray, auto_index: int) -> np.ndarray:
+        """AutomorphismEvaluator::Eval with the trace's key for auto_index = 2^j + 1 (fresh output)."""
+        import torch
+        d = _dev(torch, inp)
+        out = torch.zeros_like(d)
+        self.eval_auto_batch(d.numel() // (2 * self.N), out.data_ptr(), d.data_ptr(), auto_index)
+        return out.cpu().numpy().view(np.uint64)
 
 
 class GpuLWEtoLWEConverter:

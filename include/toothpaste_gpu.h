@@ -223,6 +223,17 @@ tp_status tp_pack_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* 
  * tp_pack_batch; scratch 2 x packs x len x 2N words. Asynchronous. */
 tp_status tp_pack_consecutive_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev,
                                     const uint64_t* in_dev, void* stream);
+/* TraceEvaluator::Eval(out, in) (lib/src/operators/trace_evaluation.cpp:135-158) on a
+ * packing context (its keys are the trace's, indices 3, 5, .., N+1): in = [A | B]
+ * coefficients; out = NTT of both halves of N^-1 Tr(in), the key-switched trace the
+ * reference computes. out may equal in. Asynchronous. */
+tp_status tp_trace_eval_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev,
+                              void* stream);
+/* TraceEvaluator::EvalAuto(out, in, auto_index) (lines 172-179, the pointer overload):
+ * the automorphism X -> X^auto_index, auto_index = 2^j + 1, with the trace's key for it;
+ * AutomorphismEvaluator::Eval semantics (out -= ..., NTT domain; out zeroed by the caller). */
+tp_status tp_trace_eval_auto_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev,
+                                   uint32_t auto_index, void* stream);
 
 /* tp_pack_batch for callers that cannot allocate device memory when they call:
  * a process whose HBM is owned by another allocator's pool, or a latency-bound

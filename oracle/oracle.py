@@ -150,6 +150,7 @@ class Oracle:
             "tpo_pack": (I, [U64, U64, U64, U64P, U64P, U64P, U64]),
             "tpo_sample_extract": (None, [U64P, U64P, U64, U64]),
             "tpo_pack_consecutive": (I, [U64, U64, U64, U64P, U64P, U64P, U64]),
+            "tpo_trace_eval": (None, [U64, U64, U64, U64P, U64P, U64P]),
             "tpo_modulus_switch": (I, [U64P, U64, U64, U64, I]),
             "tpo_ss_test_poly": (I, [U64, U64, U64, U64P]),
             "tpo_ss_keygen": (None, [R, I, U64, U64, U64, U64, U64, U64, U64, U64, D, U64P, U64P, U64P, U64P,
@@ -270,6 +271,12 @@ class Oracle:
         out = np.empty(2 * N, np.uint64)
         assert self.L.tpo_pack_consecutive(N, bl, dg, ptr(keys), ptr(out),
                                            ptr(np.ascontiguousarray(lwes, np.uint64)), length) == 0
+        return out
+
+    def trace_eval(self, N, bl, dg, keys, rlwe_coef):
+        """TraceEvaluator::Eval: NTT-domain result."""
+        out = np.empty(2 * N, np.uint64)
+        self.L.tpo_trace_eval(N, bl, dg, ptr(keys), ptr(out), ptr(np.ascontiguousarray(rlwe_coef, np.uint64)))
         return out
 
     def lwe_ks_keygen(self, q, n_in, n_out, bl, dg, std, src, tgt, seed):
@@ -413,6 +420,11 @@ class Reference:
             "ref_pack": (None, [VP, U64P, U64P, U64]),
             "ref_pack_key_copy": (None, [VP, U64P]),
             "ref_pack_consecutive": (None, [VP, U64P, U64P, U64]),
+            "ref_trace_create": (VP, [U64, U64, U64, D, U64P]),
+            "ref_trace_key_copy": (None, [VP, U64P]),
+            "ref_trace_eval": (None, [VP, U64P, U64P]),
+            "ref_trace_eval_auto": (None, [VP, U64P, U64P, U64]),
+            "ref_trace_destroy": (None, [VP]),
             "ref_pack_destroy": (None, [VP]),
             "ref_sample_extract": (None, [U64P, U64P, U64, U64]),
             "ref_modulus_switch": (None, [U64P, U64, U64, U64, I]),

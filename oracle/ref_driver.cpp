@@ -229,6 +229,28 @@ void ref_pack_key_copy(void* hp, uint64_t* out) {
 
 void ref_pack_destroy(void* hp) { delete (LWEtoRLWEPacker*)hp; }
 
+// TraceEvaluationContext(BINARY, modulus, N, basis, digits, std) and its operator.
+void* ref_trace_create(uint64_t N, uint64_t basis_log2, uint64_t digits, double std_dev, const uint64_t* key) {
+    auto ctx = std::make_shared<TraceEvaluationContext>(BINARY, kQ, N, 1ULL << basis_log2, digits, std_dev);
+    std::vector<GenericKey> keys = {{"KEY", key, N}};
+    return ctx->ConstructOperator(keys).release();
+}
+
+void ref_trace_key_copy(void* hp, uint64_t* out) {
+    for (auto& ev : ((TraceEvaluator*)hp)->m_trace_evaluators) {
+        const auto& k = ev->m_converter->m_ksk;
+        out = std::copy(k.begin(), k.end(), out);
+    }
+}
+
+void ref_trace_eval(void* hp, uint64_t* out, const uint64_t* in) { ((TraceEvaluator*)hp)->Eval(out, in); }
+
+void ref_trace_eval_auto(void* hp, uint64_t* out, const uint64_t* in, uint64_t index) {
+    ((TraceEvaluator*)hp)->EvalAuto(out, in, index);
+}
+
+void ref_trace_destroy(void* hp) { delete (TraceEvaluator*)hp; }
+
 void ref_sample_extract(uint64_t* out_lwe, uint64_t* rlwe, uint64_t index, uint64_t N) {
     SampleExtract<uint64_t>(out_lwe, rlwe, index, N, kQ);
 }

@@ -953,6 +953,13 @@ static void trace_eval(uint64_t N, uint64_t bl, uint64_t dg, const uint64_t* key
     tpo_ntt_forward(N, x + N, x + N);
 }
 
+void tpo_trace_eval(uint64_t N, uint64_t bl, uint64_t dg, const uint64_t* keys, uint64_t* out, const uint64_t* in) {
+    uint64_t* tmp = (uint64_t*)malloc(2 * N * 8);
+    memmove(out, in, 2 * N * 8);
+    trace_eval(N, bl, dg, keys, out, tmp);
+    free(tmp);
+}
+
 int tpo_lwe_to_rgsw(int variant, uint64_t N, uint64_t n, uint64_t br_bl, uint64_t br_dg, const uint64_t* brk,
                     uint64_t tr_bl, uint64_t tr_dg, const uint64_t* trace_keys, uint64_t sq_bl, uint64_t sq_dg,
                     const uint64_t* sq_key, uint64_t D, uint64_t out_bl, const uint64_t* lwe, uint64_t* out) {

@@ -141,6 +141,10 @@ int tpo_modulus_switch(uint64_t* vec, uint64_t n, uint64_t source, uint64_t targ
  * Returns -1 where the reference's first scale (an int shift) would overflow
  * or out_digits does not split N into even blocks. */
 int tpo_ss_test_poly(uint64_t N, uint64_t out_digits, uint64_t out_basis_log2, uint64_t* acc);
+/* TraceEvaluator::Eval (trace_evaluation.cpp:135-158): out = NTT of both halves of the
+ * key-switched N^-1 Tr(in); in = [A | B] coefficients; keys for indices 2^j + 1. */
+void tpo_trace_eval(uint64_t N, uint64_t basis_log2, uint64_t digits, const uint64_t* keys, uint64_t* out,
+                    const uint64_t* in);
 /* Convert (lines 168-225) of one LWE (n+1 words mod 2N) into 4 N out_digits
  * words [lev_left | lev_right], NTT domain. trace_keys: automorphism keys for
  * indices 2^j + 1, j = 1..logN, concatenated; sq_key: RLWE key switch s^2 -> s. */

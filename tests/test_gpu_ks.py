@@ -180,3 +180,19 @@ def test_pack_consecutive_many_packs_and_decryption(native, oracle):
 def oracle_ntt_pair(oracle, rlwe_coef):
     N = rlwe_coef.size // 2
     return np.concatenate([oracle.ntt_forward(rlwe_coef[:N]), oracle.ntt_forward(rlwe_coef[N:])])
+
+
+TRACE = json.loads((Path(__file__).resolve().parent / "golden" / "trace.json").read_text())
+
+
+@pytest.mark.parametrize("name", sorted(TRACE))
+def test_trace_evaluator_matches_reference(native, oracle, name):
+    """TraceEvaluator::Eval and EvalAuto (trace_evaluation.cpp:135-179) against the reference's outputs."""
+    from fhetoothpaste_b200 import GpuTraceEvaluator
+    from test_trace_cpu import trace_case
+    c = TRACE[name]
+    keys, x = trace_case(oracle, c)
+    tr = GpuTraceEvaluator(c["N"], 1 << c["basis_log2"], c["digits"], keys)
+    assert [sha256(r) for r in tr.Eval(x)] == c["eval_sha256"]
+    for t, want in zip(c["auto_index"], c["auto_sha256"]):
+        assert sha256(tr.EvalAuto(x[:1], t)[0]) == want, f"index {t}"
