@@ -181,8 +181,19 @@ def cpu_reference_sample(variant, N, n, bl, l, lwes, accs, seconds_target=15.0):
     res = np.empty((count, 2 * N), np.uint64)
     secs = L.ref_br_rotate_many(h, ptr(res), ptr(np.ascontiguousarray(lwes[:count])),
                                 ptr(np.ascontiguousarray(accs[:count])), count, 0, threads)
+    key = np.empty(L.ref_br_key_words(h), np.uint64)
+    L.ref_br_key_copy(h, ptr(key))
     L.ref_br_destroy(h)
-    return count / secs, threads, count, secs
+    return count / secs, threads, count, secs, key, res
+
+
+def gpu_matches_reference(variant, N, n, bl, l, key, lwes, accs, ref_out, device) -> bool:
+    """Rotates the CPU sample on the GPU with the reference's own key and compares every word."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    rot = GpuBlindRotator(BlindRotationContext(variant, N, n, 1 << bl, l), key, device=device)
+    got = rot.blind_rotate_batch_host(np.ascontiguousarray(lwes), np.ascontiguousarray(accs), out_coef=False)
+    rot.close()
+    return bool(np.array_equal(got, ref_out))
 
 
 def run_reference(args, wl):
@@ -193,7 +204,7 @@ def run_reference(args, wl):
     vals = []
     for s in range(args.warmup + args.steps):
         v, threads, count, secs = cpu_reference_sample(variant, N, n, bl, l, lwes, accs,
-                                                       seconds_target=args.ref_seconds)
+                                                       seconds_target=args.ref_seconds)[:4]
         if s >= args.warmup:
             vals.append((v, threads, count, secs))
     v = statistics.median([x[0] for x in vals])
@@ -612,11 +623,16 @@ def main():
         line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, threads, count, secs = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
-                                                           seconds_target=args.ref_seconds)
+            v, threads, count, secs, ref_key, ref_out = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
+                                                                             seconds_target=args.ref_seconds)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "BR/s", "cores": threads, "kind": "reference",
                                     "sample": f"{count} rotations on {threads} threads in {secs:.1f}s "
-                                              "(reference library, one rotator per thread)"}
+                                              "(reference library, one rotator per thread)",
+                                    "gpu_outputs_match": gpu_matches_reference(variant, N, n, bl, l, ref_key,
+                                                                               lwes_h[:count], accs_h[:count],
+                                                                               ref_out, local)}
+            launches += 2  # the key re-layout and the comparison's rotation launch
+            line["gpu_launches"] = launches
         except Exception as exc:  # the baseline is reported, not required
             line["cpu_baseline"] = {"value": None, "unit": "BR/s", "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {exc}"}
