@@ -259,25 +259,19 @@ def bmmp_batch_sweep(device: int) -> dict:
     ident = np.zeros(2 * N, np.uint64)
     ident[N:] = np.arange(N, dtype=np.uint64)
     out = {"workload": "BMMP n=768 (384 pairs), N=2048, base 2^16 l=4, identity LUT", "unit": "BR/s"}
-    launches = 0
     lw_all = torch.from_numpy(lwe_inputs(N, n, max(BMMP_BATCHES), 33).view(np.int64)).cuda()
     ac = torch.from_numpy(ident.view(np.int64)).cuda()
     res = torch.empty((max(BMMP_BATCHES), 2 * N), dtype=torch.int64, device="cuda")
     for b in BMMP_BATCHES:
-        prev = rot.tile
         coef, _ = rot.autotune(b)
-        # three candidates x three launches, plus the key re-tilings between them
-        launches += 9 + (prev != 8) + 1 + (coef == 8)
         g = rot.capture_batch(res.data_ptr(), lw_all.data_ptr(), n + 1, ac.data_ptr(), 0, b)
         reps = 3 if b >= 512 else 5
         ms = _timed(torch, lambda: g.launch(stream), 2, reps, stream)
-        launches += 2 + reps
         g.close()
         out[str(b)] = {"BR_per_s": round(b / (ms * 1e-3), 1), "ms_per_launch": round(ms, 3),
                        "tile": {"coef_per_thread": coef, "blocks_per_rotation": rot.split}}
     rot.check(stream)
     rot.close()
-    out["launches"] = launches
     return out
 
 
@@ -302,14 +296,11 @@ def packing_run(device: int) -> dict:
     co = torch.zeros((cts, 2 * N), dtype=torch.int64, device="cuda")
     ks_ms = _timed(torch, lambda: conv.convert_batch(cts, co.data_ptr(), ci.data_ptr(), stream), 2, 5, stream)
     conv.close()
-    levels = L.bit_length() - 1
-    per_pack_launch = 1 + levels + (N.bit_length() - 1 - levels)  # L0 setup, one launch per tree level, traces
     return {"workload": "pack 2048 LWE (n=2048) -> RLWE N=2048, base 2^16 l=4; RLWE KS x1024",
             "packs_per_launch": packs, "ms_per_pack_launch": round(pack_ms, 3),
             "packs_per_s": round(packs / (pack_ms * 1e-3), 2),
             "lwe_packed_per_s": round(packs * L / (pack_ms * 1e-3), 1),
-            "rlwe_ks_per_s": round(cts / (ks_ms * 1e-3), 1), "ms_per_ks_launch": round(ks_ms, 3),
-            "launches": 3 * per_pack_launch + 7}
+            "rlwe_ks_per_s": round(cts / (ks_ms * 1e-3), 1), "ms_per_ks_launch": round(ks_ms, 3)}
 
 
 def bootstrap_run(device: int) -> dict:
@@ -340,7 +331,7 @@ def bootstrap_run(device: int) -> dict:
     conv.close()
     return {"workload": "bootstrap: CGGI binary n=500 N=1024 2^16 l=4 + extract + LWE KS 1024->500 + switch to 2N",
             "batch": batch, "bootstraps_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
-            "epilogue_ms": round(ep, 3), "launches": 2 * 5 + 4 + 1}  # graphs x 2 kernels, epilogues, key upload
+            "epilogue_ms": round(ep, 3)}
 
 
 def scheme_switch_run(device: int) -> dict:
@@ -361,10 +352,8 @@ def scheme_switch_run(device: int) -> dict:
     out = torch.empty((batch, 4 * N * D), dtype=torch.int64, device="cuda")
     ms = _timed(torch, lambda: conv.convert_batch(batch, out.data_ptr(), lw.data_ptr(), stream), 1, 3, stream)
     conv.close()
-    per_call = 1 + 1 + 11 + 1 + 1 + 1 + 1  # rotation, rows, 11 traces, NTT, INTT, key switch, assembly
     return {"workload": "LWE->RGSW: CGGI binary n=100 N=2048, gadgets 2^14 l=4, out 4 digits 2^14",
-            "batch": batch, "conversions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
-            "launches": per_call * 4 + 3}  # + the three key re-layouts
+            "batch": batch, "conversions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3)}
 
 
 def sap_run(device: int) -> dict:
@@ -386,12 +375,8 @@ def sap_run(device: int) -> dict:
     ms = _timed(torch, lambda: dec.decompose_batch(batch, out.data_ptr(), 9, lw.data_ptr(), radix, stream), 1, 3,
                 stream)
     dec.close()
-    # per digit: digit, rotation, multiply, NTT, extract; per truncation (7 of them): multiply, 2 NTT,
-    # 5 trace steps, 7 tree levels, leaf sum; once: the two init kernels
-    per_call = 2 + 8 * 5 + 7 * (1 + 2 + 5 + 7 + 1)
     return {"workload": "SAP: CGGI binary n=10 N=4096, gadgets 2^16 l=4, radix 32, inputs mod 2^40 (8 digits)",
-            "batch": batch, "decompositions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3),
-            "launches": per_call * 4 + 3 + 1 + 3}  # + constants, key re-layouts
+            "batch": batch, "decompositions_per_s": round(batch / (ms * 1e-3), 1), "ms_per_batch": round(ms, 3)}
 
 
 SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l = 3
@@ -502,11 +487,14 @@ def main():
         step()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib = _native.lib()
     with ClockSampler(local) as clk:
+        c0 = lib.tp_kernel_launches()
         e0.record()
         for _ in range(args.steps):
             step()
         e1.record()
+        c1 = lib.tp_kernel_launches()
         barrier()
     rot.check(stream)
     ms = e0.elapsed_time(e1) / args.steps
@@ -521,7 +509,7 @@ def main():
         return
     ms = max_over_ranks(ms, dist, "cuda")
     value = aggregate_rate(batch, world, ms * 1e-3)
-    launches = args.steps
+    timed_launches = c1 - c0
 
     # end-to-end through the host-buffer call: pinned host inputs, copies inside
     lw_p = torch.from_numpy(lwes_h.view(np.int64)).pin_memory()
@@ -541,14 +529,15 @@ def main():
     barrier()
     # CUDA events on the launching stream: the call's host->device copies, the
     # launch and the device->host copy of the results are all on this stream
+    c2 = L.tp_kernel_launches()
     e0.record()
     for _ in range(e2e_steps):
         e2e_step()
     e1.record()
+    e2e_launches = L.tp_kernel_launches() - c2
     barrier()
     e2e_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3 / e2e_steps, dist, "cuda")
     e2e_val = aggregate_rate(batch, world, e2e_s)
-    launches += e2e_steps + 1
     h2d = lwes_h.nbytes + accs_h.nbytes
     d2h = batch * 2 * N * 8
 
@@ -572,7 +561,6 @@ def main():
     rot.set_split(2)
     plain2_ms = plain_time()
     rot.set_split(1)
-    launches += 2 * (plain_reps + 1)
 
     # roofline: algorithmic modmuls per launch over the kernel's launch time,
     # against the measured 64x64->128 product rate of this GPU
@@ -598,7 +586,9 @@ def main():
                   "batched_over_plain": round(value / world / (1e3 / plain_ms), 1),
                   "two_blocks": {"value": round(1e3 / plain2_ms, 3), "ms_per_rotation": round(plain2_ms, 3),
                                  "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)}},
-        "gpu_launches": launches,
+        "gpu_launches": int(timed_launches),
+        "gpu_launches_detail": {"timed_region": int(timed_launches), "e2e_timed_region": int(e2e_launches),
+                                "counted_by": "tp_kernel_launches() deltas (graph replays count their kernels)"},
         "roofline": {"bound": "int32", "achieved": round(achieved / 1e9, 1), "peak": round(prod.value / 1e9, 1),
                      "unit": "Gmodmul/s", "frac": round(achieved / prod.value, 4), "traffic": traffic,
                      "traffic_source": tsrc,
@@ -617,10 +607,6 @@ def main():
         line["bootstrap"] = bootstrap_run(local)
         line["scheme_switch"] = scheme_switch_run(local)
         line["sap"] = sap_run(local)
-        launches += (line["bmmp_batches"].pop("launches") + line["packing"].pop("launches") +
-                     line["bootstrap"].pop("launches") + line["scheme_switch"].pop("launches") +
-                     line["sap"].pop("launches"))
-        line["gpu_launches"] = launches
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, threads, count, secs, ref_key, ref_out = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
@@ -631,12 +617,11 @@ def main():
                                     "gpu_outputs_match": gpu_matches_reference(variant, N, n, bl, l, ref_key,
                                                                                lwes_h[:count], accs_h[:count],
                                                                                ref_out, local)}
-            launches += 2  # the key re-layout and the comparison's rotation launch
-            line["gpu_launches"] = launches
         except Exception as exc:  # the baseline is reported, not required
             line["cpu_baseline"] = {"value": None, "unit": "BR/s", "cores": 0, "kind": "reference",
                                     "sample": f"unavailable: {exc}"}
     rot.close()
+    line["gpu_launches_detail"]["whole_run"] = int(_native.lib().tp_kernel_launches())
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

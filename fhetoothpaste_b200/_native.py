@@ -134,6 +134,7 @@ def lib() -> ctypes.CDLL:
         "tp_measure_int_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]),
         "tp_last_error": (ctypes.c_char_p, []),
+        "tp_kernel_launches": (U64, []),
         "tp_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():

@@ -22,6 +22,21 @@
 #include "sap_kernels.cuh"
 #include "ss_kernels.cuh"
 
+#include <atomic>
+
+// Kernels this library has launched in the process (tp_kernel_launches). Launches
+// made while a stream is being captured into one of the library's graphs are not
+// executed then; they are counted when the graph is replayed instead.
+namespace tp {
+static std::atomic<uint64_t> g_launches{0};
+static thread_local int t_capturing = 0;
+static void note_launch() {
+    if (!t_capturing) g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+}  // namespace tp
+
+extern "C" uint64_t tp_kernel_launches(void) { return tp::g_launches.load(std::memory_order_relaxed); }
+
 namespace {
 
 using u128 = unsigned __int128;
@@ -383,6 +398,7 @@ tp_status tp_br_upload_key(tp_br_ctx* c, const uint64_t* brk, uint64_t words) {
             const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
             tp::key_relayout_kernel<<<(unsigned)blocks, threads>>>(c->key + g0 * per_group, stage, ng, c->G,
                                                                     2 * c->prm.digits, c->logn, c->loge);
+            tp::note_launch();
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -408,6 +424,7 @@ static tp_status br_retile(tp_br_ctx* c, int loge) {
         const uint64_t blocks = std::min<uint64_t>((c->key_words + 255) / 256, 65535);
         tp::key_retile_kernel<<<(unsigned)blocks, 256>>>(nk, c->key, c->groups, c->G, 2 * c->prm.digits, c->logn,
                                                           c->loge, loge);
+        tp::note_launch();
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
@@ -601,6 +618,7 @@ tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* o
     const int threads = 256;
     const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
     tp::sample_extract0_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(out, rlwe, batch, ring_dim);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -608,7 +626,21 @@ tp_status tp_sample_extract_batch(uint32_t ring_dim, uint64_t batch, uint64_t* o
 struct tp_graph {
     cudaGraphExec_t exec = nullptr;
     int device = 0;
+    uint64_t kernels = 0;  // kernel nodes of the graph: launches per replay
 };
+
+static uint64_t graph_kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    uint64_t k = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
 
 tp_status tp_br_batch_graph_create(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
                                    uint64_t lwe_stride, const uint64_t* accs, uint64_t acc_stride, int out_coef,
@@ -625,8 +657,10 @@ tp_status tp_br_batch_graph_create(tp_br_ctx* c, uint64_t batch, uint64_t* resul
         cudaStreamDestroy(s);
         return fail(TP_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
     }
+    ++tp::t_capturing;
     tp_status st = tp_br_blind_rotate_batch(c, batch, results, lwes, lwe_stride, accs, acc_stride, out_coef, s);
     if (st == TP_OK && extract_out) st = tp_sample_extract_batch(c->prm.ring_dim, batch, extract_out, results, s);
+    --tp::t_capturing;
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(s, &g);  // always ends the capture, also after a failed launch
     cudaStreamDestroy(s);
@@ -637,6 +671,7 @@ tp_status tp_br_batch_graph_create(tp_br_ctx* c, uint64_t batch, uint64_t* resul
     if (e != cudaSuccess) return fail(TP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
     auto* gr = new tp_graph();
     gr->device = c->device;
+    gr->kernels = graph_kernel_nodes(g);
     e = cudaGraphInstantiate(&gr->exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
@@ -651,6 +686,7 @@ tp_status tp_graph_launch(tp_graph* g, void* stream) {
     if (!g) return fail(TP_ERR_PARAM, "null graph");
     TP_CUDA(cudaSetDevice(g->device));
     TP_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    if (!tp::t_capturing) tp::g_launches.fetch_add(g->kernels, std::memory_order_relaxed);
     return TP_OK;
 }
 
@@ -670,6 +706,7 @@ tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out, const uint64_t* 
     const int threads = 256;
     const uint64_t blocks = std::min<uint64_t>((count + threads - 1) / threads, 65535);
     tp::debug_arith_kernel<<<(unsigned)blocks, threads, 0, (cudaStream_t)stream>>>(op, count, out, a, b, c);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -690,6 +727,7 @@ tp_status tp_measure_int_peak(int device, double* products_per_s, double* imad_p
             cudaEventRecord(e0);
             if (mode == 0) tp::int_peak_kernel<0><<<blocks, threads>>>(out, 12345, iters);
             else tp::int_peak_kernel<1><<<blocks, threads>>>(out, 12345, iters);
+            tp::note_launch();
             cudaEventRecord(e1);
             cudaEventSynchronize(e1);
             cudaEventElapsedTime(&ms[mode], e0, e1);
@@ -839,6 +877,7 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
         const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 65535);
         tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn,
                                                             c->loge);
+        tp::note_launch();
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -855,6 +894,7 @@ static tp_status ks_launch(tp_ks_ctx* c, int mode, const tp::KsKernelParams& kp,
     void* args[] = {&p};
     TP_CUDA(cudaLaunchKernel(tp::ks_kernel_lookup(c->logn, mode, c->loge), dim3((unsigned)grid),
                              dim3(c->N >> c->loge), args, c->smem, st));
+    tp::note_launch();
     return TP_OK;
 }
 
@@ -870,6 +910,7 @@ tp_status tp_ks_set_tile(tp_ks_ctx* c, uint32_t coef_per_thread) {
         TP_CUDA(cudaMalloc(&nk, c->key_words * 8));
         const uint64_t blocks = std::min<uint64_t>((c->key_words + 255) / 256, 65535);
         tp::key_retile_kernel<<<(unsigned)blocks, 256>>>(nk, c->key, c->nkeys, 1, c->digits, c->logn, c->loge, loge);
+        tp::note_launch();
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
@@ -959,6 +1000,7 @@ tp_status tp_trace_eval_batch(tp_ks_ctx* c, uint64_t batch, uint64_t* out, const
     // both halves (trace_evaluation.cpp:135-158)
     tp::scale_kernel<<<(unsigned)std::min<uint64_t>((words + 255) / 256, 65535), 256, 0, st>>>(out, in, words,
                                                                                             c->tab->n_inv);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp_status s = ks_trace_steps(c, batch, out, 2 * N, c->logn, 1, st);
     if (s == TP_OK) s = ntt_launch((uint32_t)N, 2 * batch, out, out, stream, true, 0, 0);
@@ -1067,6 +1109,7 @@ tp_status tp_pack_consecutive_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, 
         const uint64_t total = packs * c->consec_cnt[0] * 2 * N;
         tp::pack_l0_idx_kernel<<<(unsigned)std::min<uint64_t>((total + 255) / 256, 65535), 256, 0, st>>>(
             buf[0], in, c->consec_plan, packs, c->consec_cnt[0], (uint32_t)len, (uint32_t)c->logn, c->tab->n_inv);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
     }
     const uint64_t kw = (uint64_t)c->digits * 2 * N;
@@ -1114,6 +1157,7 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
         const uint64_t blocks = std::min<uint64_t>((need + 255) / 256, 65535 * 4ull);
         tp::pack_l0_kernel<<<(unsigned)std::min<uint64_t>(blocks, 65535), 256, 0, st>>>(
             c->work, in, packs, (uint32_t)len, (uint32_t)log_len, (uint32_t)c->logn, c->tab->n_inv);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
     }
     const uint64_t kw = (uint64_t)c->digits * 2 * N;
@@ -1225,6 +1269,7 @@ tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* c, const uint64_t* ksk, uint64_t w
     kp.ksk = c->key;
     const unsigned blocks = (c->n_out + 1 + 127) / 128;
     tp::lwe_ks_cterm_kernel<<<blocks, 128>>>(c->cterm, kp);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     TP_CUDA(cudaDeviceSynchronize());
     c->kp.cterm = c->cterm;
@@ -1247,6 +1292,7 @@ tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* c, uint64_t batch, uint64_t* out, const
     dim3 grid((c->n_out + 1 + tp::kLweKsCols - 1) / tp::kLweKsCols,
               (unsigned)((batch + tp::kLweKsRows - 1) / tp::kLweKsRows));
     tp::lwe_ks_kernel<<<grid, tp::kLweKsCols, 0, (cudaStream_t)stream>>>(kp);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -1270,6 +1316,7 @@ tp_status tp_modulus_switch_batch(uint64_t count, uint64_t* vec, uint64_t source
     if (!vec) return fail(TP_ERR_PARAM, "null buffer");
     const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 65535);
     tp::ms_floor_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vec, count, (uint32_t)k);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -1296,6 +1343,7 @@ tp_status tp_pbs_epilogue_batch(tp_lwe_ks_ctx* c, uint64_t batch, uint64_t* out_
     dim3 grid((c->n_out + 1 + tp::kLweKsCols - 1) / tp::kLweKsCols,
               (unsigned)((batch + tp::kLweKsRows - 1) / tp::kLweKsRows));
     tp::lwe_ks_kernel<<<grid, tp::kLweKsCols, 0, (cudaStream_t)stream>>>(kp);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -1318,9 +1366,11 @@ tp_status tp_pbs_graph_create(tp_br_ctx* br, tp_lwe_ks_ctx* ks, uint64_t batch, 
         cudaStreamDestroy(s);
         return fail(TP_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
     }
+    ++tp::t_capturing;
     tp_status st = tp_br_blind_rotate_batch(br, batch, rlwe_scratch, lwes, (uint64_t)br->prm.lwe_dim + 1, accs,
                                             acc_stride, 1, s);
     if (st == TP_OK) st = tp_pbs_epilogue_batch(ks, batch, out_lwe, rlwe_scratch, 2ull * br->prm.ring_dim, s);
+    --tp::t_capturing;
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(s, &g);
     cudaStreamDestroy(s);
@@ -1331,6 +1381,7 @@ tp_status tp_pbs_graph_create(tp_br_ctx* br, tp_lwe_ks_ctx* ks, uint64_t batch, 
     if (e != cudaSuccess) return fail(TP_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
     auto* gr = new tp_graph();
     gr->device = br->device;
+    gr->kernels = graph_kernel_nodes(g);
     e = cudaGraphInstantiate(&gr->exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
@@ -1434,6 +1485,7 @@ static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, co
     if (!out_stride) out_stride = ring_dim;
     void* args[] = {&out, &in, &count, &tw, &n_inv, &in_stride, &out_stride};
     TP_CUDA(cudaLaunchKernel(k, dim3((unsigned)grid), dim3(ring_dim / 8), args, smem, (cudaStream_t)stream));
+    tp::note_launch();
     return TP_OK;
 }
 
@@ -1601,6 +1653,7 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     // 2. + (0, tp), Lev rows, times N^-1 (lines 180-200; trace_evaluation.cpp:143)
     tp::ss_rows_kernel<<<blocks, 256, 0, st>>>(c->rows, c->rot, c->acc + 2 * N, batch, (uint32_t)D, (uint32_t)N,
                                                  (uint32_t)(N / D), c->br->tab->n_inv);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     // 3. trace: automorphisms N+1 down to 3 (trace_evaluation.cpp:145-153), then NTT of both halves
     s = ks_trace_steps(c->trace, rowsn, c->rows, 2 * N, (int)c->logn, 1, st);
@@ -1616,6 +1669,7 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     if (s != TP_OK) return s;
     // 5. RGSW = [lev_left | lev_right] (lines 218-224)
     tp::ss_assemble_kernel<<<blocks, 256, 0, st>>>(out, c->rows, c->sqout, batch, (uint32_t)D, (uint32_t)N);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -1764,6 +1818,7 @@ static tp_status sap_trunc(tp_sap_ctx* c, uint64_t batch, const uint64_t* in_ntt
     const uint64_t S = (2 * N) << L;  // words of one LWE's tree
     tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->tree, S, in_ntt, c->consts + N,
                                                                      c->br->tab->n_inv, batch, (uint32_t)N);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp_status s = ntt_launch((uint32_t)N, batch, c->tree, c->tree, st, false, S, S);
     if (s == TP_OK) s = ntt_launch((uint32_t)N, batch, c->tree + N, c->tree + N, st, false, S, S);
@@ -1784,6 +1839,7 @@ static tp_status sap_trunc(tp_sap_ctx* c, uint64_t batch, const uint64_t* in_ntt
         if (s != TP_OK) return s;
     }
     tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(out_coef, c->tree, batch, (uint32_t)N, L);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
 }
@@ -1797,6 +1853,7 @@ static tp_status sap_reset_into(tp_sap_ctx* c, uint64_t batch, const uint64_t* a
     const uint64_t N = c->N, n = c->n;
     tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, acc_ntt, ovf, 1, batch,
                                                                      (uint32_t)N);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp_status s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, st, false);
     if (s == TP_OK) s = tp_pbs_epilogue_batch(c->lks, batch, c->lw, c->ext, 2 * N, st);
@@ -1826,8 +1883,10 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
     // input moduli and digit counts (lines 409-416); one read-back to plan the steps
     tp::sap_init_kernel<<<(unsigned)((batch + 127) / 128), 128, 0, st>>>(c->copy, c->modulus, lwes, batch,
                                                                        (uint32_t)n);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp::sap_acc_init_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, batch, (uint32_t)N);
+    tp::note_launch();
     TP_CUDA(cudaGetLastError());
     std::vector<uint64_t> M(batch);
     TP_CUDA(cudaMemcpyAsync(M.data(), c->modulus, batch * 8, cudaMemcpyDeviceToHost, st));
@@ -1855,6 +1914,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
         tp::sap_digit_kernel<<<sap_blocks(batch * (n + 1)), 256, 0, st>>>(
             c->copy, c->sub, c->modulus, c->flags, batch, (uint32_t)n, (uint32_t)N, logr, hamming_weight, d,
             restart_period);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
         // rotation of the coefficient-domain accumulator in place, NTT output (lines 432-434)
         s = br_rotate_auto(c->br, batch, c->acc, c->sub, n + 1, c->acc, 2 * N, 0, stream);
@@ -1862,11 +1922,13 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
         // digit d = SampleExtract(INTT(acc (.) extract poly)) (lines 438-445)
         tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, c->consts, 1,
                                                                          batch, (uint32_t)N);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
         s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
         if (s != TP_OK) return s;
         tp::sap_extract_kernel<<<sap_blocks(batch * (N + 1)), 256, 0, st>>>(out, out_stride, d, c->ext, c->flags,
                                                                           batch, (uint32_t)N);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
         if (any_reset) {
             // ResetAccumulator(acc, 0) (line 452), taken where flagged
@@ -1874,6 +1936,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
             if (s != TP_OK) return s;
             tp::sap_select_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->ext, c->flags, batch,
                                                                            (uint32_t)N);
+            tp::note_launch();
             TP_CUDA(cudaGetLastError());
         }
         if (!more) break;
@@ -1989,6 +2052,7 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
         const uint64_t blocks = std::min<uint64_t>((need + 255) / 256, 65535);
         tp::pack_l0_kernel<<<(unsigned)blocks, 256, 0, st>>>(work, in, packs, (uint32_t)len, (uint32_t)log_len,
                                                             (uint32_t)c->logn, c->tab->n_inv);
+        tp::note_launch();
         TP_CUDA(cudaGetLastError());
     }
     const uint64_t kw = (uint64_t)c->digits * 2 * N;
@@ -2070,11 +2134,13 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
         const unsigned pairs = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->pair_cap);
         TP_CUDA(cudaLaunchKernel(c->pair_kernel, dim3(2 * pairs), dim3(c->prm.ring_dim >> 2), args, c->pair_smem,
                                  (cudaStream_t)stream));
+        tp::note_launch();
         return TP_OK;
     }
     const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
     TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args,
                              c->smem[c->loge], (cudaStream_t)stream));
+    tp::note_launch();
     return TP_OK;
 }
 

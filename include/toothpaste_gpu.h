@@ -459,6 +459,11 @@ tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* ctx, const char* path);
 
 /* Message for the last failing call on this thread ("" if none). */
 const char* tp_last_error(void);
+/* Kernels this library has launched in this process so far (a replay of a
+ * graph made by tp_*_graph_create counts its kernels; launches recorded into
+ * such a graph count when it is replayed). For accounting in benchmarks. No
+ * reference counterpart. */
+uint64_t tp_kernel_launches(void);
 
 /* Library version string. */
 const char* tp_version(void);

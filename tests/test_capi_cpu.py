@@ -81,3 +81,8 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_native, "_lib", None)
     with pytest.raises(ImportError):
         _native.lib()
+
+
+def test_launch_counter_starts_without_launches(native):
+    """No kernel has run in a process without a GPU; the counter is exported and readable."""
+    assert native.tp_kernel_launches() == 0

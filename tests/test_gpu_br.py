@@ -148,6 +148,32 @@ def test_graph_replays_read_fresh_inputs(native, oracle, golden, cuda, name):
     graph.close()
 
 
+def test_launch_counter(native, oracle, golden, cuda):
+    """tp_kernel_launches: a batch launch counts one kernel; recording a graph counts nothing;
+    each replay counts the graph's kernels (rotation + SampleExtract = 2)."""
+    torch = cuda
+    case, rot = rotator(oracle, golden, "small_binary_n256")
+    N, n = case["N"], case["n"]
+    batch = 8
+    d_lwe = torch.zeros((batch, n + 1), dtype=torch.int64, device="cuda")
+    d_acc = torch.zeros((batch, 2 * N), dtype=torch.int64, device="cuda")
+    d_res = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    d_ext = torch.empty((batch, N + 1), dtype=torch.int64, device="cuda")
+    count = native.tp_kernel_launches
+    c0 = count()
+    rot.blind_rotate_batch(d_res.data_ptr(), d_lwe.data_ptr(), n + 1, d_acc.data_ptr(), 2 * N, batch)
+    assert count() - c0 == 1
+    c1 = count()
+    graph = rot.capture_batch(d_res.data_ptr(), d_lwe.data_ptr(), n + 1, d_acc.data_ptr(), 2 * N, batch,
+                              out_coef=True, extract_ptr=d_ext.data_ptr())
+    assert count() == c1
+    graph.launch()
+    graph.launch()
+    torch.cuda.synchronize()
+    assert count() - c1 == 4
+    graph.close()
+
+
 def test_graph_refuses_extract_without_coefficients(native, oracle, golden, cuda):
     from fhetoothpaste_b200 import TpError
     torch = cuda
