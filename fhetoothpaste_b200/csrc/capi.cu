@@ -1310,12 +1310,12 @@ tp_status tp_modulus_switch_batch(uint64_t count, uint64_t* vec, uint64_t source
     if (source_modulus != kP) return fail(TP_ERR_PARAM, "the GPU modulus switch takes the Goldilocks modulus as source");
     const int k = pow2_log2(target_modulus);
     if (!k) return fail(TP_ERR_PARAM, "target modulus must be a power of two in [2, 2^32]");
-    if (type != TP_MS_FLOOR)
-        return fail(TP_ERR_PARAM, "only FLOOR is computed on the GPU (the type the bootstrap path uses)");
+    if (type != TP_MS_ROUND && type != TP_MS_FLOOR && type != TP_MS_CEIL)
+        return fail(TP_ERR_PARAM, "type must be TP_MS_ROUND, TP_MS_FLOOR or TP_MS_CEIL");
     if (count == 0) return TP_OK;
     if (!vec) return fail(TP_ERR_PARAM, "null buffer");
     const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 65535);
-    tp::ms_floor_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vec, count, (uint32_t)k);
+    tp::ms_pow2_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(vec, count, (uint32_t)k, type);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;

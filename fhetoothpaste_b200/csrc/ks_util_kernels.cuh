@@ -96,9 +96,46 @@ __device__ __forceinline__ uint64_t ms_floor_pow2(uint64_t v, uint32_t k) {
     return hi + ((r < lo || r >= kP) ? 1u : 0u);
 }
 
-__global__ void ms_floor_kernel(uint64_t* __restrict__ vec, uint64_t count, uint32_t k) {
+// ModulusSwitch from p to 2^k, 1 <= k <= 32, of any 64-bit word, with the
+// reference's result (modulus_switching.cpp:36-93): x = RN64(v 2^k / p) in x87
+// long double (64-bit significand, ties to even), then floorl / ceill / roundl,
+// then minus 2^k where that reaches 2^k. Computed exactly with integers: with
+// v 2^k = a p + r (0 <= r < p, a <= 2^k) and b the bit length of a, x lies in a's
+// binade, so x = a + F 2^-s with s = 64 - b and F = RN(r 2^s / p) (no ties: p is
+// odd and prime). Then
+//   FLOOR: a (F never reaches 2^s: p = 1 mod 2^k keeps p - r >= a + 1);
+//   CEIL:  a when r = 0 or F = 0 (a >= 1 and r <= p >> (s+1)), else a + 1;
+//   ROUND: a + 1 when F >= 2^(s-1), i.e. r >= ceil((p - (p >> s)) / 2); for a = 0
+//          the binade below 1/2 has half-ulp 2^-66 and the test is 2r >= p (s = 65).
+// type: 0 ROUND, 1 FLOOR, 2 CEIL.
+__device__ __forceinline__ uint64_t ms_pow2(uint64_t v, uint32_t k, int type) {
+    const uint64_t hi = v >> (64 - k), lo = v << k;
+    const uint64_t t = lo + ((hi << 32) - hi);  // lo + hi (2^32 - 1), 65 bits
+    const bool carry = t < lo;
+    uint64_t a = hi, r = t;
+    if (carry || t >= kP) {
+        a = hi + 1;
+        r = t - kP;  // mod 2^64: the 65-bit t minus p, below p
+    }
+    uint64_t res = a;
+    if (r != 0 && type != 1) {
+        const int b = a ? 64 - __clzll((long long)a) : 0;
+        const int sh = a ? 64 - b : 65;
+        if (type == 2) {
+            const uint64_t lim = sh + 1 >= 64 ? 0 : (kP >> (sh + 1));
+            res = (a && r <= lim) ? a : a + 1;
+        } else {
+            const uint64_t tail = sh >= 64 ? 0 : (kP >> sh);
+            res = r >= (kP - tail + 1) / 2 ? a + 1 : a;
+        }
+    }
+    const uint64_t top = 1ull << k;
+    return res >= top ? res - top : res;
+}
+
+__global__ void ms_pow2_kernel(uint64_t* __restrict__ vec, uint64_t count, uint32_t k, int type) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
-        vec[i] = ms_floor_pow2(vec[i], k);
+        vec[i] = ms_pow2(vec[i], k, type);
 }
 
 // Input word i (< n_in) and the body word of ciphertext row `row`: an LWE row, or

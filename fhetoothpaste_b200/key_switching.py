@@ -188,7 +188,8 @@ class GpuLWEtoLWEConverter:
         out[...] = d_out.cpu().numpy().view(np.uint64).reshape(out.shape)
 
 
-def modulus_switch_batch(count: int, vec_ptr: int, target_modulus: int, stream=None) -> None:
-    """In-place FLOOR modulus switch of `count` device words from p to a power of two."""
-    nat.check(nat.lib().tp_modulus_switch_batch(count, vec_ptr, nat.GOLDILOCKS, target_modulus, nat.TP_MS_FLOOR,
-                                                stream))
+def modulus_switch_batch(count: int, vec_ptr: int, target_modulus: int, stream=None, kind: str = "floor") -> None:
+    """In-place modulus switch of `count` device words from p to a power of two; kind 'round' | 'floor' |
+    'ceil', each word as the reference's long-double ModulusSwitch gives it."""
+    code = {"round": nat.TP_MS_ROUND, "floor": nat.TP_MS_FLOOR, "ceil": nat.TP_MS_CEIL}[kind]
+    nat.check(nat.lib().tp_modulus_switch_batch(count, vec_ptr, nat.GOLDILOCKS, target_modulus, code, stream))

@@ -273,9 +273,10 @@ tp_status tp_lwe_ks_batch(tp_lwe_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev,
 
 /* ModulusSwitch (lib/src/static/modulus_switching.cpp:36-93) in place on a
  * device vector: source must be the Goldilocks prime p, target a power of two
- * up to 2^32 (2N), type TP_MS_FLOOR. The result equals the reference's 80-bit
- * long-double floorl((target * v) / p) word for word; ROUND and CEIL are not
- * computed here (TP_ERR_PARAM). */
+ * up to 2^32 (2N), type ROUND, FLOOR or CEIL (RANDOM, which draws from an
+ * unseeded generator, is not offered). Each word equals the reference's 80-bit
+ * long-double result (roundl / floorl / ceill of (target * v) / p, then minus
+ * target where it reaches target), computed exactly with integers. */
 #define TP_MS_ROUND 0
 #define TP_MS_FLOOR 1
 #define TP_MS_CEIL 2

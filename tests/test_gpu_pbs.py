@@ -25,17 +25,37 @@ def test_modulus_switch_matches_reference(native, cuda):
     from fhetoothpaste_b200 import modulus_switch_batch
     d = np.load(GOLD / "modswitch.npz")
     for t in (256, 2048, 4096, 8192):
-        x = dev(cuda, d[f"in_{t}"])
-        modulus_switch_batch(x.numel(), x.data_ptr(), t)
-        np.testing.assert_array_equal(host(x), d[f"floor_{t}"], err_msg=f"target {t}")
+        for kind in ("round", "floor", "ceil"):
+            x = dev(cuda, d[f"in_{t}"])
+            modulus_switch_batch(x.numel(), x.data_ptr(), t, kind=kind)
+            np.testing.assert_array_equal(host(x), d[f"{kind}_{t}"], err_msg=f"{kind} to {t}")
 
 
-def test_modulus_switch_refuses_other_types(native, cuda):
+def test_modulus_switch_any_word_any_target(native, oracle, cuda):
+    """Random words (some above p) and the neighbours of the rounding boundaries, targets 2 to 2^32,
+    against the oracle's long-double switch."""
+    from fhetoothpaste_b200 import modulus_switch_batch
+    rng = np.random.default_rng(12)
+    for k in (1, 5, 13, 20, 32):
+        T = 1 << k
+        xs = [int(v) for v in rng.integers(0, 2**64 - 1, 4000, dtype=np.uint64)] + [0, 1, P - 1, P, 2**64 - 1]
+        for m in np.linspace(0, T - 1, 100).astype(np.int64).tolist():
+            for base in ((m * P) // T, ((2 * m + 1) * P) // (2 * T)):
+                xs += [base + d for d in range(-3, 4) if 0 <= base + d < 2**64]
+        arr = np.array(xs, dtype=np.uint64)
+        for kind in ("round", "floor", "ceil"):
+            x = dev(cuda, arr)
+            modulus_switch_batch(x.numel(), x.data_ptr(), T, kind=kind)
+            np.testing.assert_array_equal(host(x), oracle.modulus_switch(arr, P, T, kind), err_msg=f"{kind} 2^{k}")
+
+
+def test_modulus_switch_refuses_bad_arguments(native, cuda):
     from fhetoothpaste_b200 import _native
     x = cuda.zeros(4, dtype=cuda.int64, device="cuda")
     L = _native.lib()
-    assert L.tp_modulus_switch_batch(4, x.data_ptr(), P, 2048, _native.TP_MS_ROUND, None) == _native.TP_ERR_PARAM
+    assert L.tp_modulus_switch_batch(4, x.data_ptr(), P, 2048, 3, None) == _native.TP_ERR_PARAM
     assert L.tp_modulus_switch_batch(4, x.data_ptr(), P, 3000, _native.TP_MS_FLOOR, None) == _native.TP_ERR_PARAM
+    assert L.tp_modulus_switch_batch(4, x.data_ptr(), P - 2, 2048, _native.TP_MS_ROUND, None) == _native.TP_ERR_PARAM
 
 
 def lut_value(f, k):
