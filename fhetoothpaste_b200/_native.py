@@ -135,6 +135,13 @@ def lib() -> ctypes.CDLL:
                                                 ctypes.POINTER(ctypes.c_double)]),
         "tp_last_error": (ctypes.c_char_p, []),
         "tp_kernel_launches": (U64, []),
+        "tp_ctx_create": (ctypes.c_int, [ctypes.POINTER(BrParams), ctypes.POINTER(VP)]),
+        "tp_ctx_destroy": (ctypes.c_int, [VP]),
+        "tp_brk_upload": (ctypes.c_int, [VP, U64P, U64, ctypes.c_int]),
+        "tp_blind_rotate": (ctypes.c_int, [VP, U64P, U64P, U64P, ctypes.c_int]),
+        "tp_blind_rotate_batch": (ctypes.c_int, [VP, U64, VP, VP, VP, U64, ctypes.c_int, VP]),
+        "tp_auto_ks_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
+        "tp_last_error_string": (ctypes.c_char_p, []),
         "tp_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():

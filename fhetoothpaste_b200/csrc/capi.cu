@@ -2145,3 +2145,38 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
 }
 
 }  // namespace tp
+
+// ---------------------------------------------------------------------------
+// Short names (the same calls)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+tp_status tp_ctx_create(const tp_params* params, tp_ctx** out) { return tp_br_create(params, 0, out); }
+
+tp_status tp_ctx_destroy(tp_ctx* ctx) { return tp_br_destroy(ctx); }
+
+tp_status tp_brk_upload(tp_ctx* ctx, const uint64_t* brk, uint64_t words, int layout_tag) {
+    if (layout_tag != TP_LAYOUT_REFERENCE)
+        return fail(TP_ERR_LAYOUT, "key layout tag %d: only the reference's m_brk layout (0) is accepted",
+                    layout_tag);
+    return tp_br_upload_key(ctx, brk, words);
+}
+
+tp_status tp_blind_rotate(tp_ctx* ctx, uint64_t* result, const uint64_t* lwe, const uint64_t* acc, int out_coef) {
+    return tp_br_blind_rotate(ctx, result, lwe, acc, out_coef);
+}
+
+tp_status tp_blind_rotate_batch(tp_ctx* ctx, uint64_t batch, uint64_t* results, const uint64_t* lwes,
+                                const uint64_t* accs, uint64_t acc_stride, int out_coef, void* stream) {
+    if (!ctx) return fail(TP_ERR_PARAM, "null context");
+    return tp_br_blind_rotate_batch(ctx, batch, results, lwes, (uint64_t)ctx->prm.lwe_dim + 1, accs, acc_stride,
+                                    out_coef, stream);
+}
+
+tp_status tp_auto_ks_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out, const uint64_t* in, void* stream) {
+    return tp_auto_eval_batch(ctx, batch, out, in, stream);
+}
+
+const char* tp_last_error_string(void) { return tp_last_error(); }
+
+}  // extern "C"

@@ -469,6 +469,22 @@ uint64_t tp_kernel_launches(void);
 /* Library version string. */
 const char* tp_version(void);
 
+/* ---- Short names for the blind-rotation calls ------------------------------
+ * The same functions under the short names: a context is a blind-rotation
+ * context, its key the rotator's m_brk (layout_tag TP_LAYOUT_REFERENCE, the
+ * only layout accepted), batch rows of n+1 LWE words. */
+typedef tp_br_params tp_params;
+typedef tp_br_ctx tp_ctx;
+#define TP_LAYOUT_REFERENCE 0
+tp_status tp_ctx_create(const tp_params* params, tp_ctx** out);  /* device 0; tp_br_create for others */
+tp_status tp_ctx_destroy(tp_ctx* ctx);
+tp_status tp_brk_upload(tp_ctx* ctx, const uint64_t* brk, uint64_t words, int layout_tag);
+tp_status tp_blind_rotate(tp_ctx* ctx, uint64_t* result, const uint64_t* lwe, const uint64_t* acc, int out_coef);
+tp_status tp_blind_rotate_batch(tp_ctx* ctx, uint64_t batch, uint64_t* results_dev, const uint64_t* lwes_dev,
+                                const uint64_t* accs_dev, uint64_t acc_stride, int out_coef, void* stream);
+tp_status tp_auto_ks_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, const uint64_t* in_dev, void* stream);
+const char* tp_last_error_string(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,3 +86,13 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
 def test_launch_counter_starts_without_launches(native):
     """No kernel has run in a process without a GPU; the counter is exported and readable."""
     assert native.tp_kernel_launches() == 0
+
+
+def test_short_names_check_their_arguments(native):
+    from fhetoothpaste_b200 import _native
+    assert native.tp_ctx_create(None, None) == _native.TP_ERR_PARAM
+    assert native.tp_brk_upload(None, None, 0, 1) == _native.TP_ERR_LAYOUT
+    assert native.tp_brk_upload(None, None, 0, 0) == _native.TP_ERR_PARAM
+    assert native.tp_blind_rotate_batch(None, 1, None, None, None, 0, 0, None) == _native.TP_ERR_PARAM
+    assert native.tp_ctx_destroy(None) == _native.TP_OK
+    assert native.tp_last_error_string() == native.tp_last_error()

@@ -174,6 +174,38 @@ def test_launch_counter(native, oracle, golden, cuda):
     graph.close()
 
 
+def test_short_names_rotate_like_the_oracle(native, oracle, golden, cuda):
+    """tp_ctx_create / tp_brk_upload / tp_blind_rotate(_batch): the same calls under the short names."""
+    import ctypes
+    from fhetoothpaste_b200 import _native as nat
+    torch = cuda
+    name = "small_binary_n256"
+    case = golden[0]["br"][name]
+    _, _, brk = case_key(oracle, name, case)
+    N, n = case["N"], case["n"]
+    p = nat.BrParams(case["variant"], nat.GOLDILOCKS, N, n, 1 << case["basis_log2"], case["digits"])
+    h = ctypes.c_void_p()
+    assert native.tp_ctx_create(ctypes.byref(p), ctypes.byref(h)) == nat.TP_OK
+    assert native.tp_brk_upload(h, nat.ptr(brk), brk.size, 1) == nat.TP_ERR_LAYOUT
+    assert native.tp_brk_upload(h, nat.ptr(brk), brk.size, 0) == nat.TP_OK
+    lwes = lwe_inputs(N, n, 5, 91)
+    accs = random_acc(N, 5, 92)
+    d_l = torch.from_numpy(lwes.view(np.int64)).cuda()
+    d_a = torch.from_numpy(accs.view(np.int64)).cuda()
+    d_r = torch.empty((5, 2 * N), dtype=torch.int64, device="cuda")
+    assert native.tp_blind_rotate_batch(h, 5, d_r.data_ptr(), d_l.data_ptr(), d_a.data_ptr(), 2 * N, 1,
+                                        None) == nat.TP_OK
+    got = d_r.cpu().numpy().view(np.uint64)
+    one = np.empty(2 * N, np.uint64)
+    assert native.tp_blind_rotate(h, nat.ptr(one), nat.ptr(np.ascontiguousarray(lwes[2])),
+                                  nat.ptr(np.ascontiguousarray(accs[2])), 1) == nat.TP_OK
+    for b in range(5):
+        want = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], accs[b], 1)
+        np.testing.assert_array_equal(got[b], want)
+    np.testing.assert_array_equal(one, got[2])
+    assert native.tp_ctx_destroy(h) == nat.TP_OK
+
+
 def test_graph_refuses_extract_without_coefficients(native, oracle, golden, cuda):
     from fhetoothpaste_b200 import TpError
     torch = cuda
