@@ -612,6 +612,7 @@ def main():
             v, threads, count, secs, ref_key, ref_out = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
                                                                              seconds_target=args.ref_seconds)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "BR/s", "cores": threads, "kind": "reference",
+                                    "ms_per_rotation_per_core": round(1e3 * threads / v, 1),
                                     "sample": f"{count} rotations on {threads} threads in {secs:.1f}s "
                                               "(reference library, one rotator per thread)",
                                     "gpu_outputs_match": gpu_matches_reference(variant, N, n, bl, l, ref_key,
