@@ -1,6 +1,7 @@
 // Key files: a versioned, self-describing container for the keys this library
 // consumes (blind-rotation keys, RLWE/automorphism/packing key-switching keys,
-// LWE key-switching keys), in the reference's own in-memory layouts. The
+// LWE key-switching keys), in the reference's own in-memory layouts, and for
+// batches of LWE / RLWE ciphertexts. The
 // reference keeps keys only in memory; this lets a key be generated once on a
 // host, stored, shipped and uploaded to a GPU context with its parameters and
 // integrity checked. Host code only.
@@ -9,13 +10,15 @@
 //   0   char[8]  magic "TPKEYv1\0"
 //   8   u32      header bytes (128)
 //   12  u32      kind (tp_key_kind)
-//   16  u32      variant (blind rotation: tp_br_variant; else 0)
+//   16  u32      variant (blind rotation: tp_br_variant; RLWE batch: 0 coefficients,
+//                1 NTT domain; else 0)
 //   20  u32      ring dimension N (LWE key switch: n_in)
 //   24  u32      LWE dimension (blind rotation: n; LWE key switch: n_out; else 0)
 //   28  u32      gadget digits
 //   32  u64      modulus
 //   40  u64      gadget basis
-//   48  u32      automorphism index (kind TP_KEY_AUTOMORPHISM; else 0)
+//   48  u32      automorphism index (kind TP_KEY_AUTOMORPHISM), ciphertext count (TP_CT_*);
+//                else 0
 //   52  u32      layout tag (1: the reference's layout, NTT-domain words in
 //                Solinas bit-reversed slot order)
 //   56  u64      payload words
@@ -180,6 +183,14 @@ extern "C" {
 
 tp_status tp_key_file_write(const char* path, const tp_key_info* info, const uint64_t* words) {
     if (!path || !info || (!words && info->words)) return tp::set_error(TP_ERR_PARAM, "null argument");
+    if (info->kind == TP_CT_LWE || info->kind == TP_CT_RLWE) {
+        const uint64_t row = info->kind == TP_CT_LWE ? info->lwe_dim + 1ull : 2ull * info->ring_dim;
+        if (info->kind == TP_CT_RLWE && info->variant > 1)
+            return tp::set_error(TP_ERR_PARAM, "RLWE batch domain must be 0 (coefficients) or 1 (NTT)");
+        if ((uint64_t)info->index * row != info->words)
+            return tp::set_error(TP_ERR_PARAM, "ciphertext batch: %llu words are not %u rows of %llu words",
+                                 (unsigned long long)info->words, info->index, (unsigned long long)row);
+    }
     uint8_t h[kHeaderBytes] = {};
     std::memcpy(h, kMagic, 8);
     put<uint32_t>(h, 8, kHeaderBytes);

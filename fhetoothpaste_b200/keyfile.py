@@ -1,5 +1,6 @@
 """Key files: one key in the reference's layout behind a checked header (format in
-include/toothpaste_gpu.h and csrc/keyfile.cu). Host-only; no device needed."""
+include/toothpaste_gpu.h and csrc/keyfile.cu), and batches of LWE / RLWE ciphertexts in
+the same container. Host-only; no device needed."""
 from __future__ import annotations
 
 import ctypes
@@ -8,7 +9,8 @@ import numpy as np
 
 from . import _native as nat
 
-KINDS = {"blind_rotation": 1, "rlwe_switch": 2, "automorphism": 3, "packing": 4, "lwe_switch": 5}
+KINDS = {"blind_rotation": 1, "rlwe_switch": 2, "automorphism": 3, "packing": 4, "lwe_switch": 5,
+         "lwe_batch": 16, "rlwe_batch": 17}
 
 
 class KeyInfo(ctypes.Structure):
@@ -39,3 +41,27 @@ def read_key_file(path) -> tuple[dict, np.ndarray]:
     info = KeyInfo()
     nat.check(nat.lib().tp_key_file_read(str(path).encode(), ctypes.byref(info), nat.ptr(words), words.size))
     return info.as_dict(), words
+
+
+def write_lwe_batch(path, lwes: np.ndarray, modulus: int) -> None:
+    """count x (n+1) LWE words mod `modulus` (2N for rotation inputs, p after a key switch)."""
+    lwes = np.ascontiguousarray(lwes, dtype=np.uint64)
+    count, row = lwes.shape
+    write_key_file(path, "lwe_batch", lwes, ring_dim=0, digits=0, basis=0, lwe_dim=row - 1, index=count,
+                   modulus=modulus)
+
+
+def write_rlwe_batch(path, rlwes: np.ndarray, ntt_domain: bool) -> None:
+    """count x 2N RLWE words [A | B] mod p, coefficients or NTT domain."""
+    rlwes = np.ascontiguousarray(rlwes, dtype=np.uint64)
+    count, row = rlwes.shape
+    write_key_file(path, "rlwe_batch", rlwes, ring_dim=row // 2, digits=0, basis=0, variant=int(ntt_domain),
+                   index=count)
+
+
+def read_ciphertext_batch(path) -> tuple[dict, np.ndarray]:
+    """(header fields, count x row words) of an LWE or RLWE batch file."""
+    info, words = read_key_file(path)
+    if info["kind"] not in (KINDS["lwe_batch"], KINDS["rlwe_batch"]):
+        raise ValueError(f"{path}: not a ciphertext batch (kind {info['kind']})")
+    return info, words.reshape(info["index"], -1)

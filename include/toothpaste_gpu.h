@@ -437,13 +437,17 @@ tp_status tp_sap_reset_batch(tp_sap_ctx* ctx, uint64_t batch, uint64_t* acc_dev,
  * the SHA-256 of the payload; all fields little-endian. Reading checks the
  * magic, the layout tag and the hash (TP_ERR_LAYOUT on a mismatch); the
  * *_upload_key_file calls also check the header against the context's
- * parameters before uploading. Host-only, no device needed to read or write. */
+ * parameters before uploading. Writing a ciphertext batch checks that the word
+ * count is count x row words. Host-only, no device needed to read or write. */
 typedef enum {
     TP_KEY_BLIND_ROTATION = 1, /* m_brk: variant, ring_dim N, lwe_dim n */
     TP_KEY_RLWE_SWITCH = 2,    /* RLWEtoRLWEConverter m_ksk: ring_dim */
     TP_KEY_AUTOMORPHISM = 3,   /* AutomorphismEvaluator key: ring_dim, index */
     TP_KEY_PACKING = 4,        /* LWEtoRLWEPacker: log2 N automorphism keys, ring_dim */
-    TP_KEY_LWE_SWITCH = 5      /* LWEtoLWEConverter m_ksk: ring_dim = n_in, lwe_dim = n_out */
+    TP_KEY_LWE_SWITCH = 5,     /* LWEtoLWEConverter m_ksk: ring_dim = n_in, lwe_dim = n_out */
+    /* Ciphertext batches in the same container (index = number of ciphertexts): */
+    TP_CT_LWE = 16,            /* rows of lwe_dim+1 words [a | b] mod `modulus` (2N before a rotation) */
+    TP_CT_RLWE = 17            /* rows of 2N words [A | B]; variant 0: coefficients, 1: NTT domain */
 } tp_key_kind;
 
 typedef struct {

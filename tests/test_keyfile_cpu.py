@@ -52,3 +52,28 @@ def test_refusals(native, tmp_path):
     assert nat.lib().tp_key_file_read(str(good).encode(), ctypes.byref(KeyInfo()), nat.ptr(small), 10) == \
         nat.TP_ERR_PARAM
     assert nat.lib().tp_key_file_info(b"/nonexistent/x.tpkey", ctypes.byref(KeyInfo())) == nat.TP_ERR_PARAM
+
+
+def test_ciphertext_batches(native, tmp_path):
+    """LWE and RLWE batches in the same container: round trip, header fields, shape checks."""
+    from fhetoothpaste_b200 import TpError
+    from fhetoothpaste_b200.keyfile import (read_ciphertext_batch, write_key_file, write_lwe_batch,
+                                            write_rlwe_batch)
+    from oracle.oracle import P, lwe_inputs, random_acc
+    lwes = lwe_inputs(2048, 630, 17, 3)
+    write_lwe_batch(tmp_path / "l.tpct", lwes, modulus=4096)
+    info, back = read_ciphertext_batch(tmp_path / "l.tpct")
+    np.testing.assert_array_equal(back, lwes)
+    assert (info["kind"], info["lwe_dim"], info["index"], info["modulus"]) == (16, 630, 17, 4096)
+    rl = random_acc(256, 5, 4)
+    write_rlwe_batch(tmp_path / "r.tpct", rl, ntt_domain=True)
+    info, back = read_ciphertext_batch(tmp_path / "r.tpct")
+    np.testing.assert_array_equal(back, rl)
+    assert (info["kind"], info["ring_dim"], info["variant"], info["index"], info["modulus"]) == (17, 256, 1, 5, P)
+    with pytest.raises(TpError):   # 5 rows of 2N words claimed, 4 given
+        write_key_file(tmp_path / "x.tpct", "rlwe_batch", rl[:4], ring_dim=256, digits=0, basis=0, index=5)
+    with pytest.raises(TpError):   # domain tag other than coefficients / NTT
+        write_key_file(tmp_path / "x.tpct", "rlwe_batch", rl, ring_dim=256, digits=0, basis=0, index=5, variant=2)
+    with pytest.raises(ValueError):
+        write_key_file(tmp_path / "k.tpkey", "packing", rl, ring_dim=256, digits=4, basis=1 << 16)
+        read_ciphertext_batch(tmp_path / "k.tpkey")
