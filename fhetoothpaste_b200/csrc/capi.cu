@@ -1651,8 +1651,8 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     tp_status s = br_rotate_auto(c->br, batch, c->rot, lwes, (uint64_t)c->n + 1, c->acc, 0, 1, stream);
     if (s != TP_OK) return s;
     // 2. + (0, tp), Lev rows, times N^-1 (lines 180-200; trace_evaluation.cpp:143)
-    tp::ss_rows_kernel<<<blocks, 256, 0, st>>>(c->rows, c->rot, c->acc + 2 * N, batch, (uint32_t)D, (uint32_t)N,
-                                                 (uint32_t)(N / D), c->br->tab->n_inv);
+    tp::ss_rows_kernel<<<blocks, 256, 0, st>>>(c->rows, c->rot, c->acc + 2 * N, batch, (uint32_t)ilog2(D),
+                                                 c->logn, (uint32_t)(N / D), c->br->tab->n_inv);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     // 3. trace: automorphisms N+1 down to 3 (trace_evaluation.cpp:145-153), then NTT of both halves
@@ -1668,7 +1668,7 @@ tp_status tp_lwe_to_rgsw_batch(tp_ss_ctx* c, uint64_t batch, uint64_t* out, cons
     s = tp_rlwe_ks_batch(c->sq, rowsn, c->sqout, c->sqin, stream);
     if (s != TP_OK) return s;
     // 5. RGSW = [lev_left | lev_right] (lines 218-224)
-    tp::ss_assemble_kernel<<<blocks, 256, 0, st>>>(out, c->rows, c->sqout, batch, (uint32_t)D, (uint32_t)N);
+    tp::ss_assemble_kernel<<<blocks, 256, 0, st>>>(out, c->rows, c->sqout, batch, (uint32_t)ilog2(D), c->logn);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
@@ -1817,7 +1817,7 @@ static tp_status sap_trunc(tp_sap_ctx* c, uint64_t batch, const uint64_t* in_ntt
     const uint32_t L = c->logn - (uint32_t)ilog2(radix);
     const uint64_t S = (2 * N) << L;  // words of one LWE's tree
     tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->tree, S, in_ntt, c->consts + N,
-                                                                     c->br->tab->n_inv, batch, (uint32_t)N);
+                                                                     c->br->tab->n_inv, batch, c->logn);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp_status s = ntt_launch((uint32_t)N, batch, c->tree, c->tree, st, false, S, S);
@@ -1838,7 +1838,7 @@ static tp_status sap_trunc(tp_sap_ctx* c, uint64_t batch, const uint64_t* in_ntt
         s = ks_launch(c->trace, tp::kKsSplit, kp, st);
         if (s != TP_OK) return s;
     }
-    tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(out_coef, c->tree, batch, (uint32_t)N, L);
+    tp::sap_leaf_sum_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(out_coef, c->tree, batch, c->logn, L);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     return TP_OK;
@@ -1852,7 +1852,7 @@ static tp_status sap_reset_into(tp_sap_ctx* c, uint64_t batch, const uint64_t* a
                                 uint64_t* fresh, cudaStream_t st) {
     const uint64_t N = c->N, n = c->n;
     tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, acc_ntt, ovf, 1, batch,
-                                                                     (uint32_t)N);
+                                                                     c->logn);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     tp_status s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, st, false);
@@ -1885,7 +1885,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
                                                                        (uint32_t)n);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
-    tp::sap_acc_init_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, batch, (uint32_t)N);
+    tp::sap_acc_init_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, batch, c->logn);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     std::vector<uint64_t> M(batch);
@@ -1921,7 +1921,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
         if (s != TP_OK) return s;
         // digit d = SampleExtract(INTT(acc (.) extract poly)) (lines 438-445)
         tp::sap_mul_poly_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->ext, 2 * N, c->acc, c->consts, 1,
-                                                                         batch, (uint32_t)N);
+                                                                         batch, c->logn);
         tp::note_launch();
         TP_CUDA(cudaGetLastError());
         s = ntt_launch((uint32_t)N, 2 * batch, c->ext, c->ext, stream, false);
@@ -1935,7 +1935,7 @@ tp_status tp_sap_decompose_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* out, u
             s = sap_reset_into(c, batch, c->acc, c->consts + 2 * N, c->ext, st);
             if (s != TP_OK) return s;
             tp::sap_select_kernel<<<sap_blocks(batch * 2 * N), 256, 0, st>>>(c->acc, c->ext, c->flags, batch,
-                                                                           (uint32_t)N);
+                                                                           c->logn);
             tp::note_launch();
             TP_CUDA(cudaGetLastError());
         }

@@ -34,12 +34,12 @@ __global__ void pack_l0_idx_kernel(uint64_t* __restrict__ nodes, const uint64_t*
                                    const uint32_t* __restrict__ src, uint64_t packs, uint32_t count, uint32_t len,
                                    uint32_t logn, uint64_t n_inv) {
     const uint64_t N = 1ull << logn;
-    const uint64_t total = packs * count * 2 * N;
+    const uint64_t total = (packs * count) << (logn + 1);
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = w % (2 * N);
-        const uint64_t c = (w / (2 * N)) % count;
-        const uint64_t p = w / (2 * N * count);
+        const uint64_t k = w & (2 * N - 1);
+        const uint64_t node = w >> (logn + 1);
+        const uint64_t p = node / count, c = node - p * count;
         const uint64_t* lwe = in + (p * len + src[c]) * (N + 1);
         uint64_t v;
         if (k == 0) v = lwe[0];

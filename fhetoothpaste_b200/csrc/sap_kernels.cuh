@@ -31,11 +31,11 @@ __global__ void sap_init_kernel(uint64_t* __restrict__ copy, uint64_t* __restric
 }
 
 // The starting accumulators (0, Q/2N) in coefficients (lines 389-392).
-__global__ void sap_acc_init_kernel(uint64_t* __restrict__ acc, uint64_t batch, uint32_t N) {
-    const uint64_t total = batch * 2ull * N;
+__global__ void sap_acc_init_kernel(uint64_t* __restrict__ acc, uint64_t batch, uint32_t logn) {
+    const uint64_t N = 1ull << logn, total = batch << (logn + 1);
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x)
-        acc[w] = (w % (2ull * N)) == N ? kP / (2ull * N) : 0;
+        acc[w] = (w & (2 * N - 1)) == N ? kP / (2 * N) : 0;
 }
 
 // One digit step on every LWE (lines 421-430): sub = copy mod radix, copy >>=
@@ -71,11 +71,11 @@ __global__ void sap_digit_kernel(uint64_t* __restrict__ copy, uint64_t* __restri
 
 // dst = src (.) poly * scale over both halves of every RLWE (NTT domain).
 __global__ void sap_mul_poly_kernel(uint64_t* __restrict__ dst, uint64_t dst_stride, const uint64_t* __restrict__ src,
-                                    const uint64_t* __restrict__ poly, uint64_t scale, uint64_t batch, uint32_t N) {
-    const uint64_t total = batch * 2ull * N;
+                                    const uint64_t* __restrict__ poly, uint64_t scale, uint64_t batch, uint32_t logn) {
+    const uint64_t N = 1ull << logn, total = batch << (logn + 1);
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = w / (2ull * N), k = w % (2ull * N);
+        const uint64_t b = w >> (logn + 1), k = w & (2 * N - 1);
         dst[b * dst_stride + k] = gl_mul(gl_mul(src[w], poly[k & (N - 1)]), scale);
     }
 }
@@ -99,25 +99,26 @@ __global__ void sap_extract_kernel(uint64_t* __restrict__ out, uint64_t out_stri
 
 // acc_b <- fresh_b where LWE b is reset at this step.
 __global__ void sap_select_kernel(uint64_t* __restrict__ acc, const uint64_t* __restrict__ fresh,
-                                  const uint8_t* __restrict__ flags, uint64_t batch, uint32_t N) {
-    const uint64_t total = batch * 2ull * N;
+                                  const uint8_t* __restrict__ flags, uint64_t batch, uint32_t logn) {
+    const uint64_t total = batch << (logn + 1);
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        if (flags[w / (2ull * N)] & 2) acc[w] = fresh[w];
+        if (flags[w >> (logn + 1)] & 2) acc[w] = fresh[w];
     }
 }
 
 // End of HomTrunc (lines 253-263), in coefficients: acc_b = sum_e X^brev(e) * leaf_{b,e}
 // over the 2^L leaves of LWE b's tree (leaf e at words e*2N of its tree).
 __global__ void sap_leaf_sum_kernel(uint64_t* __restrict__ acc, const uint64_t* __restrict__ tree, uint64_t batch,
-                                    uint32_t N, uint32_t L) {
-    const uint64_t total = batch * 2ull * N;
+                                    uint32_t logn, uint32_t L) {
+    const uint32_t N = 1u << logn;
+    const uint64_t total = batch << (logn + 1);
     const uint32_t leaves = 1u << L;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = w / (2ull * N);
-        const uint32_t k = (uint32_t)(w % (2ull * N));
-        const uint32_t h = k / N, m = k % N;
+        const uint64_t b = w >> (logn + 1);
+        const uint32_t k = (uint32_t)(w & (2ull * N - 1));
+        const uint32_t h = k >> logn, m = k & (N - 1);
         const uint64_t* t = tree + b * (uint64_t)leaves * 2 * N + (uint64_t)h * N;
         uint64_t sum = 0;
         for (uint32_t e = 0; e < leaves; ++e) {

@@ -210,6 +210,56 @@ def case_sap_n4096(torch):
     dec.close()
 
 
+def case_lwe_to_rgsw_n2048_b1024(torch):
+    """As lwe_to_rgsw_n2048 with 1024 LWEs, so the element-wise kernels' rows (134 MB) exceed L2."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuLWEtoRGSWConverter
+    N, n, beta, l, D, batch = 2048, 100, 14, 4, 4, 1024
+    words = BlindRotationContext(0, N, n, 1 << beta, l).key_words()
+    conv = GpuLWEtoRGSWConverter((0, N, n, 1 << beta, l), (1 << beta, l), (1 << beta, l), D, 1 << beta,
+                                 _u64(61, words), _u64(62, 11 * 2 * N * l), _u64(63, 2 * N * l))
+    lw = _dev(torch, _u64(64, (batch, n + 1), 2 * N))
+    out = torch.empty((batch, 4 * N * D), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        conv.convert_batch(batch, out.data_ptr(), lw.data_ptr())
+    torch.cuda.synchronize()
+    conv.close()
+
+
+def case_modswitch_round(torch):
+    """ms_pow2_kernel: ROUND switch of 64 M words (512 MB) from p to 2^12, twice."""
+    from fhetoothpaste_b200 import modulus_switch_batch
+    x = _dev(torch, _u64(81, 1 << 26))
+    for _ in range(2):
+        modulus_switch_batch(x.numel(), x.data_ptr(), 1 << 12, kind="round")
+    torch.cuda.synchronize()
+
+
+def case_pack_consecutive_n2048(torch):
+    """pack_l0_idx_kernel + compacted merges: 64 consecutive packings of 64 LWEs (n = N = 2048)."""
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker
+    N, L, packs, l = 2048, 64, 64, 4
+    pk = GpuLWEtoRLWEPacker(N, 1 << 16, l, _u64(82, 11 * 2 * N * l))
+    lw = _dev(torch, _u64(83, (packs * L, N + 1)))
+    out = torch.empty((packs, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        pk.pack_consecutive_batch(packs, L, out.data_ptr(), lw.data_ptr())
+    torch.cuda.synchronize()
+    pk.close()
+
+
+def case_trace_n2048(torch):
+    """scale_kernel + trace steps + NTT: TraceEvaluator::Eval of 4096 RLWEs (N = 2048, l = 4)."""
+    from fhetoothpaste_b200 import GpuTraceEvaluator
+    N, l, batch = 2048, 4, 4096
+    tr = GpuTraceEvaluator(N, 1 << 16, l, _u64(84, 11 * 2 * N * l))
+    x = _dev(torch, _u64(85, (batch, 2 * N)))
+    y = torch.empty_like(x)
+    for _ in range(2):
+        tr.eval_batch(batch, y.data_ptr(), x.data_ptr())
+    torch.cuda.synchronize()
+    tr.close()
+
+
 CASES = {name[5:]: fn for name, fn in globals().items() if name.startswith("case_")}
 
 
