@@ -78,7 +78,9 @@ __host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
 // after, so the L2 latency of the key stream hides behind the NTTs. The stage
 // needs C*N words and is used where it fits (not for ternary and BMMP at
 // N = 4096). Keeping the accumulator in registers there to make room measured
-// slower (ternary N = 4096: 1856 vs 1977 rotations/s; the spills cost more).
+// slower (ternary N = 4096: 1856 vs 1977 rotations/s; the spills cost more), and
+// so did staging part of each row there (two components, the rest read from L2
+// at use: ternary 1918 vs 1978; BMMP 2939 vs 2889, within run-to-run spread).
 __host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge) {
     return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
            (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
