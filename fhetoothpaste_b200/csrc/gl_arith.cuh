@@ -17,18 +17,20 @@ __device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
 __device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
 __device__ __forceinline__ uint64_t pack64(uint32_t lo, uint32_t hi) { return ((uint64_t)hi << 32) | lo; }
 
-// a + b mod p.  a + (b + eps) carries out iff a + b >= p; without the carry the
-// eps is taken back.
+// a + b mod p.  a + (b + eps) carries out iff a + b >= p, and then its low 64
+// bits are a + b - p; without the carry the eps is taken back. The carry picks
+// the correction directly: 0xFFFFFFFF + carry is 0 with it and eps without.
+// (b < p keeps b + eps below 2^64; for any 64-bit a the result is still a
+// 64-bit value congruent to a + b.)
 __device__ __forceinline__ uint64_t gl_add(uint64_t a, uint64_t b) {
     uint32_t sl, sh;
     asm("{\n\t"
-        ".reg .u32 bl, bh, c, m;\n\t"
+        ".reg .u32 bl, bh, m;\n\t"
         "add.cc.u32 bl, %2, 0xFFFFFFFF;\n\t"
         "addc.u32 bh, %3, 0;\n\t"
         "add.cc.u32 %0, %4, bl;\n\t"
         "addc.cc.u32 %1, %5, bh;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "sub.u32 m, c, 1;\n\t"
+        "addc.u32 m, 0xFFFFFFFF, 0;\n\t"
         "sub.cc.u32 %0, %0, m;\n\t"
         "subc.u32 %1, %1, 0;\n\t"
         "}"
@@ -78,33 +80,28 @@ __device__ __forceinline__ void mul_wide(uint64_t a, uint64_t b, uint32_t& r0, u
 }
 
 // Reduces x = r0 + r1 2^32 + r2 2^64 + r3 2^96 (any 128-bit value) to [0, p).
-//   t = (r1:r0) - r3            (a borrow takes eps off: t stays >= 2^64 - 2^32)
-//   s = t + r2 (2^32 - 1)       (65 bits: carry c)
-//   result = s + eps (mod 2^64) if c or s >= p, else s
-// With a carry the wrapped s is below r2 (2^32 - 1) <= 2^64 - 2^33 + 1, so
-// s + eps neither overflows nor reaches p; without one, s >= p exactly when
-// s + eps carries, and then s + eps (mod 2^64) = s - p.
+//   t = (r1:r0) - r3            (a borrow takes eps off: t stays >= 2^64 - 2^33 + 2)
+//   S = t + r2 (2^32 - 1)       (the value to reduce, below 2^65 - 2^33)
+// S + eps = t + (r2 2^32 + (2^32 - 1 - r2)), i.e. t plus the word pair
+// (r2, ~r2): no multiply. If that sum carries out, S >= p and its low 64 bits
+// are S - p, which is below p; otherwise S < p and the result is the sum minus
+// eps (no underflow: the sum is at least eps). As in gl_add, 0xFFFFFFFF +
+// carry gives the correction.
 __device__ __forceinline__ uint64_t gl_reduce128(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
     uint32_t s0, s1;
     asm("{\n\t"
-        ".reg .u32 t0, t1, b, u0, u1, c, x0, x1;\n\t"
-        ".reg .pred pc;\n\t"
+        ".reg .u32 t0, t1, b, n, m;\n\t"
         "sub.cc.u32 t0, %2, %5;\n\t"
         "subc.cc.u32 t1, %3, 0;\n\t"
         "subc.u32 b, 0, 0;\n\t"
         "sub.cc.u32 t0, t0, b;\n\t"
         "subc.u32 t1, t1, 0;\n\t"
-        "sub.cc.u32 u0, 0, %4;\n\t"
-        "subc.u32 u1, %4, 0;\n\t"
-        "add.cc.u32 %0, t0, u0;\n\t"
-        "addc.cc.u32 %1, t1, u1;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "add.cc.u32 x0, %0, 0xFFFFFFFF;\n\t"
-        "addc.cc.u32 x1, %1, 0;\n\t"
-        "addc.u32 c, c, 0;\n\t"
-        "setp.ne.u32 pc, c, 0;\n\t"
-        "selp.b32 %0, x0, %0, pc;\n\t"
-        "selp.b32 %1, x1, %1, pc;\n\t"
+        "not.b32 n, %4;\n\t"
+        "add.cc.u32 %0, t0, n;\n\t"
+        "addc.cc.u32 %1, t1, %4;\n\t"
+        "addc.u32 m, 0xFFFFFFFF, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
         "}"
         : "=r"(s0), "=r"(s1)
         : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
