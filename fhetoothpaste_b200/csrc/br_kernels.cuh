@@ -221,7 +221,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
-                ntt_forward_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
@@ -313,7 +313,7 @@ br_kernel(const BrKernelParams prm) {
                         x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
                     }
                 }
-                ntt_forward_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
                 if constexpr (PF && K == 1) cp_async_wait_all();
 #pragma unroll
                 for (int p = 0; p < K; ++p) {

@@ -119,7 +119,7 @@ br_pair_kernel(const BrKernelParams prm) {
             uint64_t x[1][E];
 #pragma unroll
             for (int j = 0; j < E; ++j) x[0][j] = ain[t + j * T];
-            ntt_forward_k<LOGN, 1, LOGE, R4>(x, t, xb(), tw_f);
+            ntt_forward_k<LOGN, 1, LOGE, R4, true>(x, t, xb(), tw_f);
 #pragma unroll
             for (int j = 0; j < E; ++j)
                 acc[j * T + t] = gl_mul(x[0][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j), bb));
@@ -180,7 +180,7 @@ br_pair_kernel(const BrKernelParams prm) {
                     const uint64_t raw = (cx[0][j] >> sh) & mk;
                     x[0][j] = SIGNED ? gl_sub(raw, dl) : raw;
                 }
-                ntt_forward_k<LOGN, 1, LOGE, R4>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGN, 1, LOGE, R4, true>(x, t, xb(), tw_f);
                 if constexpr (PF) cp_async_wait_all();
 #pragma unroll
                 for (int c = 0; c < C; ++c)

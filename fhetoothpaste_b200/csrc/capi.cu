@@ -700,7 +700,7 @@ tp_status tp_graph_destroy(tp_graph* g) {
 
 tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out, const uint64_t* a, const uint64_t* b,
                          const uint64_t* c, void* stream) {
-    if (op < 0 || op > 5) return fail(TP_ERR_PARAM, "unknown op %d", op);
+    if (op < 0 || op > 9) return fail(TP_ERR_PARAM, "unknown op %d", op);
     if (count == 0) return TP_OK;
     if (!out || !a || !b || !c) return fail(TP_ERR_PARAM, "null buffer");
     const int threads = 256;

@@ -109,7 +109,7 @@ __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelP
                 for (int jp = 0; jp < E / 2; ++jp)
                     kv[c][jp] = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
         }
-        ntt_forward_k<LOGN, 1, LOGE>(x, t, sel ? buf1 : buf0, tw_f);
+        ntt_forward_k<LOGN, 1, LOGE, false, true>(x, t, sel ? buf1 : buf0, tw_f);
         sel ^= 1;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {

@@ -102,7 +102,7 @@ __device__ __forceinline__ void ntt_sync(bool block_wide) {
 // 2^48, 2^120, 2^168 and every product is a shift. This trades IMADs (FMA
 // pipe) for shifts and adds (ALU pipe); it measured faster only where the FMA
 // pipe is the busier one (BMMP, whose key MAC is 1.5x CGGI ternary's).
-template <int LOGN, int P, int K>
+template <int LOGN, int P, int K, bool LAZY>
 __device__ __forceinline__ void fwd_radix4(uint64_t (&x)[K][4], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, 2>;
     constexpr int TMIN = SH::N >> (SH::L0(P) + 2);
@@ -126,11 +126,12 @@ __device__ __forceinline__ void fwd_radix4(uint64_t (&x)[K][4], int t, const uin
             t2 = gl_mul(x[p][1], w2);
             t3 = gl_mul(x[p][3], w12);
         }
-        const uint64_t a = gl_add(x[p][0], t1), bb = gl_sub(x[p][0], t1);
+        // with LAZY, x0 may be any 64-bit value; t1, c and d are canonical
+        const uint64_t a = LAZY ? gl_add_lazy(x[p][0], t1) : gl_add(x[p][0], t1), bb = gl_sub(x[p][0], t1);
         const uint64_t c = gl_add(t2, t3), d = gl_mul_pow2<48>(gl_sub(t2, t3));
-        x[p][0] = gl_add(a, c);
+        x[p][0] = LAZY ? gl_add_lazy(a, c) : gl_add(a, c);
         x[p][1] = gl_sub(a, c);
-        x[p][2] = gl_add(bb, d);
+        x[p][2] = LAZY ? gl_add_lazy(bb, d) : gl_add(bb, d);
         x[p][3] = gl_sub(bb, d);
     }
 }
@@ -169,13 +170,13 @@ __device__ __forceinline__ void inv_radix4(uint64_t (&x)[K][4], int t, const uin
 }
 
 // Forward butterflies of pass P on the thread's registers (R4: use the fused
-// radix-4 form for radix-4 passes).
-template <int LOGN, int P, int K, int LOGE, bool R4>
+// radix-4 form for radix-4 passes; LAZY: see ntt_forward_k).
+template <int LOGN, int P, int K, int LOGE, bool R4, bool LAZY>
 __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
     if constexpr (R4 && LOGE == 2 && S == 2) {
-        fwd_radix4<LOGN, P, K>(x, t, tw);
+        fwd_radix4<LOGN, P, K, LAZY>(x, t, tw);
     } else {
         constexpr int G = 1 << S;
         constexpr int PER = SH::E / G;
@@ -195,7 +196,7 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t
                     for (int p = 0; p < K; ++p) {
                         const uint64_t u = x[p][q * G + j];
                         const uint64_t v = gl_mul(x[p][q * G + j + half], w);
-                        x[p][q * G + j] = gl_add(u, v);
+                        x[p][q * G + j] = LAZY ? gl_add_lazy(u, v) : gl_add(u, v);
                         x[p][q * G + j + half] = gl_sub(u, v);
                     }
                 }
@@ -280,16 +281,16 @@ __device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][1 <<
     }
 }
 
-template <int LOGN, int P, int K, int LOGE, bool R4>
+template <int LOGN, int P, int K, int LOGE, bool R4, bool LAZY>
 __device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                 const uint64_t* tw) {
     using SH = NttShape<LOGN, LOGE>;
-    fwd_pass_math<LOGN, P, K, LOGE, R4>(x, t, tw);
+    fwd_pass_math<LOGN, P, K, LOGE, R4, LAZY>(x, t, tw);
     if constexpr (P + 1 < SH::NPASS) {
         xstore<LOGN, P, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P));
         xload<LOGN, P + 1, K, LOGE>(buf, x, t);
-        fwd_passes_from<LOGN, P + 1, K, LOGE, R4>(x, t, buf, tw);
+        fwd_passes_from<LOGN, P + 1, K, LOGE, R4, LAZY>(x, t, buf, tw);
     }
 }
 
@@ -309,10 +310,16 @@ __device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][1 << LOGE], int
 // Forward NTT of K polynomials: coefficient layout -> slot layout. buf holds K*N words.
 // R4 (4 coefficients per thread only) selects the fused radix-4 butterflies,
 // whose twiddle products sit at tw_fwd + N.
-template <int LOGN, int K, int LOGE = 3, bool R4 = false>
+// LAZY: the outputs are 64-bit values congruent to the evaluations but not
+// necessarily below p, for callers that only multiply them (gl_mul,
+// gl_fma_lazy take any 64-bit operand). Each butterfly's sum then skips the
+// canonical step (gl_add_lazy: its right operand, the twiddle product, is
+// canonical; the left may be any 64-bit value, and gl_sub takes that too). The
+// inputs must be canonical (the radix-4 form's first pass shifts them).
+template <int LOGN, int K, int LOGE = 3, bool R4 = false, bool LAZY = false>
 __device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                               const uint64_t* tw_fwd) {
-    fwd_passes_from<LOGN, 0, K, LOGE, R4>(x, t, buf, tw_fwd);
+    fwd_passes_from<LOGN, 0, K, LOGE, R4, LAZY>(x, t, buf, tw_fwd);
 }
 
 // Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.

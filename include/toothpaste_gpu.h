@@ -351,7 +351,9 @@ tp_status tp_server_run_poisson(tp_server* srv, double rate, double seconds, con
 /* Diagnostic: element-wise Goldilocks primitives of the kernels on device
  * buffers, for testing them against exact integer arithmetic. op: 0 a+b,
  * 1 a-b, 2 a*b (a, b canonical); 3 c + a*b (any 64-bit a, b, c); 4 reduction
- * of the 128-bit value a + 2^64 b; 5 canonical form of a. Results canonical.
+ * of the 128-bit value a + 2^64 b; 5 canonical form of a; 6 op 4 through the
+ * canonical reduction (its own output, not re-canonicalised); 7 lazy a+b,
+ * 8 a+b, 9 a-b (any 64-bit a, b canonical). Results canonical.
  * No reference counterpart (internal arithmetic check). */
 tp_status tp_debug_arith(int op, uint64_t count, uint64_t* out_dev, const uint64_t* a_dev, const uint64_t* b_dev,
                          const uint64_t* c_dev, void* stream);

@@ -63,3 +63,25 @@ def test_reduce128_any_value(native, cuda):
     got = run(native, cuda, 4, lo, hi)
     exp = np.array([(int(x) + (int(y) << 64)) % P for x, y in zip(lo, hi)], dtype=np.uint64)
     np.testing.assert_array_equal(got, exp)
+
+
+def test_canonical_reduction_any_value(native, cuda):
+    # the canonical reduction's own output must already be below p
+    lo, hi = grid(EDGE_ANY)
+    lo = np.concatenate([lo, sm64(8, 20000), np.zeros(4, np.uint64)])
+    hi = np.concatenate([hi, sm64(9, 20000), np.array([1 << 32, 2**32 - 1, 2**64 - 2**32, 2**64 - 1], np.uint64)])
+    got = run(native, cuda, 6, lo, hi)
+    exp = np.array([(int(x) + (int(y) << 64)) % P for x, y in zip(lo, hi)], dtype=np.uint64)
+    np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("op,fn", [(7, lambda a, b: (a + b) % P), (8, lambda a, b: (a + b) % P),
+                                   (9, lambda a, b: (a - b) % P)])
+def test_add_sub_any_left_operand(native, cuda, op, fn):
+    # left operand any 64-bit value (a lazily reduced butterfly input), right canonical
+    a, b = np.meshgrid(np.array(EDGE_ANY, dtype=np.uint64), np.array(EDGE, dtype=np.uint64))
+    a = np.concatenate([a.ravel(), sm64(10, 20000)])
+    b = np.concatenate([b.ravel(), canon_rand(11, 20000)])
+    got = run(native, cuda, op, a, b)
+    exp = np.array([fn(int(x), int(y)) for x, y in zip(a, b)], dtype=np.uint64)
+    np.testing.assert_array_equal(got, exp)
