@@ -243,7 +243,7 @@ br_kernel(const BrKernelParams prm) {
             }
             const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
 
-            // MAC accumulators (lazy residues, any 64-bit value)
+            // MAC accumulators (canonical: every update is a gl_fma)
             uint64_t o[C][E];
 #pragma unroll
             for (int c = 0; c < C; ++c)
@@ -266,7 +266,7 @@ br_kernel(const BrKernelParams prm) {
             // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
             auto finish_half = [&](uint64_t (&v)[E]) {
 #pragma unroll
-                for (int j = 0; j < E; ++j) v[j] = gl_canon(gl_fma_lazy(prm.corr, v[j], prm.n_inv));
+                for (int j = 0; j < E; ++j) v[j] = gl_fma(prm.corr, v[j], prm.n_inv);
             };
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
@@ -326,8 +326,8 @@ br_kernel(const BrKernelParams prm) {
                             const ulonglong2 kv = (PF && K == 1)
                                                       ? *reinterpret_cast<const ulonglong2*>(kst + ko)
                                                       : __ldg(reinterpret_cast<const ulonglong2*>(kr + ko));
-                            o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[p][2 * jp], kv.x);
-                            o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
+                            o[c][2 * jp] = gl_fma(o[c][2 * jp], x[p][2 * jp], kv.x);
+                            o[c][2 * jp + 1] = gl_fma(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
                         }
                     }
                 }
@@ -341,14 +341,14 @@ br_kernel(const BrKernelParams prm) {
                 uint64_t ub = acc_ld(1, j);
                 if constexpr (VARIANT == kCggiBinary) {
                     // acc += ExtProd (mux_operator.cpp:151)
-                    ua = gl_add(ua, gl_canon(o[0][j]));
-                    ub = gl_add(ub, gl_canon(o[1][j]));
+                    ua = gl_add(ua, o[0][j]);
+                    ub = gl_add(ub, o[1][j]);
                 } else if constexpr (VARIANT == kCggiTernary) {
                     // acc += (X^{-a}-1) ExtProd(lo) + (X^{a}-1) ExtProd(hi) (mux_operator.cpp:188-200)
                     const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek, 2u * N - a0), 1);
                     const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek, a0), 1);
-                    ua = gl_canon(gl_fma_lazy(gl_fma_lazy(ua, o[0][j], mp), o[2][j], mn));
-                    ub = gl_canon(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], mp), o[3][j], mn));
+                    ua = gl_fma(gl_fma(ua, o[0][j], mp), o[2][j], mn);
+                    ub = gl_fma(gl_fma(ub, o[1][j], mp), o[3][j], mn);
                 } else {
                     // weights X^{a0}-1, X^{a1}-1, X^{a0+a1}-X^{a0}-X^{a1}+1
                     // (bmmp_blind_rotation.cpp:280-323; MultiMux mux_operator.cpp:274-291)
@@ -358,8 +358,8 @@ br_kernel(const BrKernelParams prm) {
                     const uint64_t w0 = gl_sub(m0, 1);
                     const uint64_t w1 = gl_sub(m1, 1);
                     const uint64_t w2 = gl_add(gl_sub(gl_sub(m2, m0), m1), 1);
-                    ua = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ua, o[0][j], w0), o[2][j], w1), o[4][j], w2));
-                    ub = gl_canon(gl_fma_lazy(gl_fma_lazy(gl_fma_lazy(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2));
+                    ua = gl_fma(gl_fma(gl_fma(ua, o[0][j], w0), o[2][j], w1), o[4][j], w2);
+                    ub = gl_fma(gl_fma(gl_fma(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2);
                 }
                 acc_st(0, j, ua);
                 acc_st(1, j, ub);

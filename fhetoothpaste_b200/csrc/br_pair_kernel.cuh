@@ -169,7 +169,7 @@ br_pair_kernel(const BrKernelParams prm) {
                 if (d == 0) {
                     ntt_backward_unscaled_k<LOGN, 1, LOGE, R4>(cx, t, xb(), tw_i);
 #pragma unroll
-                    for (int j = 0; j < E; ++j) cx[0][j] = gl_canon(gl_fma_lazy(prm.corr, cx[0][j], prm.n_inv));
+                    for (int j = 0; j < E; ++j) cx[0][j] = gl_fma(prm.corr, cx[0][j], prm.n_inv);
                 }
                 uint64_t x[1][E];
                 const uint32_t sh = prm.dshift[d];
@@ -189,8 +189,8 @@ br_pair_kernel(const BrKernelParams prm) {
                         const int ko = ((c * (E / 2) + jp) * T + t) * 2;
                         const ulonglong2 kv = PF ? *reinterpret_cast<const ulonglong2*>(kst + ko)
                                                  : __ldg(reinterpret_cast<const ulonglong2*>(kr + ko));
-                        o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[0][2 * jp], kv.x);
-                        o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[0][2 * jp + 1], kv.y);
+                        o[c][2 * jp] = gl_fma(o[c][2 * jp], x[0][2 * jp], kv.x);
+                        o[c][2 * jp + 1] = gl_fma(o[c][2 * jp + 1], x[0][2 * jp + 1], kv.y);
                     }
             }
 
@@ -225,12 +225,12 @@ br_pair_kernel(const BrKernelParams prm) {
                     const uint32_t ek = slot_exponent<LOGN>(E * t + j);
                     uint64_t u = acc[j * T + t];
                     if constexpr (VARIANT == kCggiBinary) {
-                        u = gl_add(gl_add(u, gl_canon(mine(0, j))), gl_canon(pr[0][e]));
+                        u = gl_add(gl_add(u, mine(0, j)), pr[0][e]);
                     } else if constexpr (VARIANT == kCggiTernary) {
                         const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek, 2u * N - a0), 1);
                         const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek, a0), 1);
-                        u = gl_fma_lazy(gl_fma_lazy(u, mine(0, j), mp), pr[0][e], mp);
-                        u = gl_canon(gl_fma_lazy(gl_fma_lazy(u, mine(1, j), mn), pr[1][e], mn));
+                        u = gl_fma(gl_fma(u, mine(0, j), mp), pr[0][e], mp);
+                        u = gl_fma(gl_fma(u, mine(1, j), mn), pr[1][e], mn);
                     } else {
                         const uint64_t m0 = mono<LOGN>(prm.psi_pow, ek, a0);
                         const uint64_t m1 = mono<LOGN>(prm.psi_pow, ek, a1);
@@ -238,9 +238,9 @@ br_pair_kernel(const BrKernelParams prm) {
                         const uint64_t w0 = gl_sub(m0, 1);
                         const uint64_t w1 = gl_sub(m1, 1);
                         const uint64_t w2 = gl_add(gl_sub(gl_sub(m2, m0), m1), 1);
-                        u = gl_fma_lazy(gl_fma_lazy(u, mine(0, j), w0), pr[0][e], w0);
-                        u = gl_fma_lazy(gl_fma_lazy(u, mine(1, j), w1), pr[1][e], w1);
-                        u = gl_canon(gl_fma_lazy(gl_fma_lazy(u, mine(2, j), w2), pr[2][e], w2));
+                        u = gl_fma(gl_fma(u, mine(0, j), w0), pr[0][e], w0);
+                        u = gl_fma(gl_fma(u, mine(1, j), w1), pr[1][e], w1);
+                        u = gl_fma(gl_fma(u, mine(2, j), w2), pr[2][e], w2);
                     }
                     acc[j * T + t] = u;
                 }

@@ -139,32 +139,6 @@ __device__ __forceinline__ uint64_t gl_mul(uint64_t a, uint64_t b) {
     return gl_reduce128(r0, r1, r2, r3);
 }
 
-// Reduces any 128-bit x = (r3 r2 r1 r0) to a 64-bit value congruent to x mod p
-// (not necessarily below p):  s = (r1:r0) + r2*eps  (its carry folds back as
-// another eps, which cannot overflow), then s - r3 (a borrow takes eps off,
-// which cannot underflow).
-__device__ __forceinline__ uint64_t gl_reduce128_lazy(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
-    uint32_t d0, d1;
-    asm("{\n\t"
-        ".reg .u32 s0, s1, c, b;\n\t"
-        ".reg .u64 s;\n\t"
-        "mad.lo.cc.u32 s0, %4, 0xFFFFFFFF, %2;\n\t"
-        "madc.hi.cc.u32 s1, %4, 0xFFFFFFFF, %3;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
-        "mov.b64 s, {s0, s1};\n\t"
-        "mad.wide.u32 s, c, 0xFFFFFFFF, s;\n\t"
-        "mov.b64 {s0, s1}, s;\n\t"
-        "sub.cc.u32 %0, s0, %5;\n\t"
-        "subc.cc.u32 %1, s1, 0;\n\t"
-        "subc.u32 b, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, b;\n\t"
-        "subc.u32 %1, %1, 0;\n\t"
-        "}"
-        : "=r"(d0), "=r"(d1)
-        : "r"(r0), "r"(r1), "r"(r2), "r"(r3));
-    return pack64(d0, d1);
-}
-
 // acc + a*b as an exact 128-bit value (acc, a, b any 64-bit: the sum stays
 // below 2^128), accumulated inside the multiply's carry chain.
 __device__ __forceinline__ void mad_wide(uint64_t acc, uint64_t a, uint64_t b, uint32_t& r0, uint32_t& r1,
@@ -185,11 +159,14 @@ __device__ __forceinline__ void mad_wide(uint64_t acc, uint64_t a, uint64_t b, u
         : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)), "r"(lo32(acc)), "r"(hi32(acc)));
 }
 
-// acc + a*b mod p, as a 64-bit value congruent to it (any 64-bit inputs).
-__device__ __forceinline__ uint64_t gl_fma_lazy(uint64_t acc, uint64_t a, uint64_t b) {
+// acc + a*b mod p, canonical (any 64-bit inputs). The accumulate rides in the
+// product's carry chain; the carry-form reduction needs no IMAD, which the
+// product's own chain keeps busy (measured: +2% CGGI, +4% BMMP over a
+// reduction that folds r2 (2^32 - 1) with mad.hi/mad.wide).
+__device__ __forceinline__ uint64_t gl_fma(uint64_t acc, uint64_t a, uint64_t b) {
     uint32_t r0, r1, r2, r3;
     mad_wide(acc, a, b, r0, r1, r2, r3);
-    return gl_reduce128_lazy(r0, r1, r2, r3);
+    return gl_reduce128(r0, r1, r2, r3);
 }
 
 // hi * 2^64 + lo mod p as a 64-bit representative (not necessarily below p),

@@ -75,7 +75,7 @@ __device__ __forceinline__ uint64_t rot_coeff(const uint64_t* x, uint32_t m, uin
     return m >= s ? x[m - s] : gl_neg(x[N + m - s]);
 }
 
-// sum_d NTT(digit_d(a)) * key_d for both components (lazy residues), a in the
+// sum_d NTT(digit_d(a)) * key_d for both components (canonical), a in the
 // coefficient layout and canonical.
 template <int LOGN, int LOGE>
 __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelParams& prm, int t, uint64_t* buf0,
@@ -117,8 +117,8 @@ __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelP
             for (int jp = 0; jp < E / 2; ++jp) {
                 if constexpr (LOGE != 2)
                     kv[c][jp] = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
-                o[c][2 * jp] = gl_fma_lazy(o[c][2 * jp], x[0][2 * jp], kv[c][jp].x);
-                o[c][2 * jp + 1] = gl_fma_lazy(o[c][2 * jp + 1], x[0][2 * jp + 1], kv[c][jp].y);
+                o[c][2 * jp] = gl_fma(o[c][2 * jp], x[0][2 * jp], kv[c][jp].x);
+                o[c][2 * jp + 1] = gl_fma(o[c][2 * jp + 1], x[0][2 * jp + 1], kv[c][jp].y);
             }
         }
     }
@@ -203,8 +203,8 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
 #pragma unroll
             for (int j = 0; j < E; ++j) {
                 const int k = E * t + j;
-                out[k] = gl_sub(out[k], gl_canon(o[0][j]));
-                out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), in[N + k]);
+                out[k] = gl_sub(out[k], o[0][j]);
+                out[N + k] = gl_add(gl_sub(out[N + k], o[1][j]), in[N + k]);
             }
         } else {
             // NTT of the automorphism's B part (automorphism_evaluation.cpp:156)
@@ -214,8 +214,8 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
                     const int k = E * t + j;
-                    out[k] = gl_sub(out[k], gl_canon(o[0][j]));
-                    out[N + k] = gl_add(gl_sub(out[N + k], gl_canon(o[1][j])), bb[j]);
+                    out[k] = gl_sub(out[k], o[0][j]);
+                    out[N + k] = gl_add(gl_sub(out[N + k], o[1][j]), bb[j]);
                 }
             } else {
                 // Auto eval output (NTT) -> coefficients, added to the sum half
@@ -224,8 +224,8 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
 #pragma unroll
-                    for (int j = 0; j < E; ++j) r[0][j] = h == 0 ? gl_neg(gl_canon(o[0][j]))
-                                                                 : gl_sub(bb[j], gl_canon(o[1][j]));
+                    for (int j = 0; j < E; ++j) r[0][j] = h == 0 ? gl_neg(o[0][j])
+                                                                 : gl_sub(bb[j], o[1][j]);
                     ntt_backward_unscaled_k<LOGN, 1, LOGE>(r, t, sel ? buf1 : buf0, tw_i);
                     sel ^= 1;
                     if constexpr (MODE == kKsSplit) {

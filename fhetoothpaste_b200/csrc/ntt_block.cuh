@@ -312,7 +312,7 @@ __device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][1 << LOGE], int
 // whose twiddle products sit at tw_fwd + N.
 // LAZY: the outputs are 64-bit values congruent to the evaluations but not
 // necessarily below p, for callers that only multiply them (gl_mul,
-// gl_fma_lazy take any 64-bit operand). Each butterfly's sum then skips the
+// gl_fma take any 64-bit operand). Each butterfly's sum then skips the
 // canonical step (gl_add_lazy: its right operand, the twiddle product, is
 // canonical; the left may be any 64-bit value, and gl_sub takes that too). The
 // inputs must be canonical (the radix-4 form's first pass shifts them).

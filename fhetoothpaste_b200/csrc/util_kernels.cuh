@@ -77,8 +77,8 @@ __global__ void debug_arith_kernel(int op, uint64_t count, uint64_t* __restrict_
             case 0: r = gl_add(a[i], b[i]); break;
             case 1: r = gl_sub(a[i], b[i]); break;
             case 2: r = gl_mul(a[i], b[i]); break;
-            case 3: r = gl_canon(gl_fma_lazy(c[i], a[i], b[i])); break;
-            case 4: r = gl_canon(gl_reduce128_lazy(lo32(a[i]), hi32(a[i]), lo32(b[i]), hi32(b[i]))); break;
+            case 3: r = gl_fma(c[i], a[i], b[i]); break;
+            case 4: r = gl_canon(gl_reduce128(lo32(a[i]), hi32(a[i]), lo32(b[i]), hi32(b[i]))); break;
             case 6: r = gl_reduce128(lo32(a[i]), hi32(a[i]), lo32(b[i]), hi32(b[i])); break;
             case 7: r = gl_canon(gl_add_lazy(a[i], b[i])); break;
             case 8: r = gl_canon(gl_add(a[i], b[i])); break;
