@@ -10,7 +10,8 @@ step = one persistent launch over the whole batch.
   e2e    the same through the host-buffer C-ABI call (tp_br_blind_rotate_batch_host):
          host->device copy of the step's LWEs and test polynomials, the launch,
          device->host copy of the results, all inside the timed region
-  plain  the one-rotation-per-launch form (batch 1) for the batched/plain ratio
+  plain  the one-rotation-per-launch form (batch 1) for the batched/plain ratio, also
+         with the rotation split over two and four SMs (cluster kernels)
 
 `--impl reference` times the reference library's own CPU blind rotation (built
 from its sources into oracle/_ref/, one rotator per host thread) on a bounded
@@ -542,7 +543,7 @@ def main():
     d2h = batch * 2 * N * 8
 
     # plain form: one rotation per launch (one thread block, as the batched kernel
-    # runs it), and the same with the rotation split over two SMs
+    # runs it), and the same with the rotation split over two and four SMs
     one_out = torch.empty((1, 2 * N), dtype=torch.int64, device="cuda")
     plain_reps = 3
 
@@ -560,6 +561,12 @@ def main():
     plain_ms = plain_time()
     rot.set_split(2)
     plain2_ms = plain_time()
+    plain4_ms = None
+    try:
+        rot.set_split(4)
+        plain4_ms = plain_time()
+    except _native.TpError:  # the four-block kernel does not fit this parameter set
+        pass
     rot.set_split(1)
 
     # roofline: algorithmic modmuls per launch over the kernel's launch time,
@@ -585,7 +592,10 @@ def main():
         "plain": {"value": round(1e3 / plain_ms, 3), "unit": "BR/s", "ms_per_rotation": round(plain_ms, 3),
                   "batched_over_plain": round(value / world / (1e3 / plain_ms), 1),
                   "two_blocks": {"value": round(1e3 / plain2_ms, 3), "ms_per_rotation": round(plain2_ms, 3),
-                                 "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)}},
+                                 "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)},
+                  "four_blocks": None if plain4_ms is None else {
+                      "value": round(1e3 / plain4_ms, 3), "ms_per_rotation": round(plain4_ms, 3),
+                      "batched_over_plain": round(value / world / (1e3 / plain4_ms), 1)}},
         "gpu_launches": int(timed_launches),
         "gpu_launches_detail": {"timed_region": int(timed_launches), "e2e_timed_region": int(e2e_launches),
                                 "counted_by": "tp_kernel_launches() deltas (graph replays count their kernels)"},

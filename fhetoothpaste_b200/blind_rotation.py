@@ -123,14 +123,15 @@ class GpuBlindRotator:
 
     @property
     def split(self) -> int:
-        """Thread blocks per rotation (1, or 2 for the two-SM cluster kernel)."""
+        """Thread blocks per rotation (1, or 2 / 4 for the cluster kernels)."""
         return int(nat.lib().tp_br_get_split(self._h))
 
     def set_split(self, blocks_per_rotation: int) -> None:
         nat.check(nat.lib().tp_br_set_split(self._h, blocks_per_rotation))
 
     def autotune(self, batch: int) -> tuple[int, float]:
-        """Times every tile (and the two-block split) on `batch` synthetic rotations and keeps the fastest."""
+        """Times every tile (and the two- and four-block splits) on `batch` synthetic rotations and keeps
+        the fastest."""
         coef, rate = ctypes.c_uint32(), ctypes.c_double()
         nat.check(nat.lib().tp_br_autotune(self._h, batch, ctypes.byref(coef), ctypes.byref(rate)))
         return int(coef.value), float(rate.value)

@@ -214,10 +214,13 @@ struct tp_br_ctx {
     const void* kernels[4] = {};  // by loge (2, 3)
     int grid_caps[4] = {};        // resident blocks on the device, by loge
     size_t smem[4] = {};          // dynamic shared memory bytes, by loge
-    int split = 1;                // thread blocks per rotation (2: cluster kernel, tile 4 only)
+    int split = 1;                // thread blocks per rotation (2, 4: cluster kernels, tile 4 only)
     const void* pair_kernel = nullptr;
     size_t pair_smem = 0;
     int pair_cap = 0;             // resident two-CTA clusters on the device (0: unavailable)
+    const void* quad_kernel = nullptr;
+    size_t quad_smem = 0;
+    int quad_cap = 0;             // resident four-CTA clusters on the device (0: unavailable)
     // workspace for host-pointer calls
     uint64_t* ws = nullptr;
     uint64_t ws_words = 0;
@@ -335,24 +338,25 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         c->grid_caps[lg] = per_sm * sm_count(device);
     }
     c->loge = tp::br_default_loge(c->logn, p->variant);
-    {
-        // two-CTA cluster kernel; optional: a parameter set it does not fit keeps pair_cap = 0
-        const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant);
-        const size_t smem = tp::br_pair_smem_words(c->logn, p->variant, p->lwe_dim, 2) * 8;
-        cudaError_t pe = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (int split = 2; split <= 4; split += 2) {
+        // two- and four-CTA cluster kernels; optional: a parameter set one does not fit keeps its cap 0
+        const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant, split);
+        const size_t smem = tp::br_pair_smem_words(c->logn, p->variant, p->lwe_dim, 2, split) * 8;
         int clusters = 0;
+        cudaError_t pe = k ? cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaErrorInvalidValue;
         if (pe == cudaSuccess) {
             cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(2 * (unsigned)sm_count(device));
+            cfg.gridDim = dim3((unsigned)split * (unsigned)sm_count(device));
             cfg.blockDim = dim3((unsigned)(N >> 2));
             cfg.dynamicSmemBytes = smem;
             pe = cudaOccupancyMaxActiveClusters(&clusters, k, &cfg);
         }
         if (pe == cudaSuccess && clusters > 0) {
-            c->pair_kernel = k;
-            c->pair_smem = smem;
-            c->pair_cap = clusters;
-        } else {
+            (split == 2 ? c->pair_kernel : c->quad_kernel) = k;
+            (split == 2 ? c->pair_smem : c->quad_smem) = smem;
+            (split == 2 ? c->pair_cap : c->quad_cap) = clusters;
+        } else if (k) {
             cudaGetLastError();  // clear the optional probe's error
         }
     }
@@ -442,8 +446,9 @@ tp_status tp_br_set_tile(tp_br_ctx* c, uint32_t coef_per_thread) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
     if (coef_per_thread != 4 && coef_per_thread != 8) return fail(TP_ERR_PARAM, "coefficients per thread must be 4 or 8");
     std::lock_guard<std::mutex> lk(c->mu);
-    if (coef_per_thread == 8 && c->split == 2)
-        return fail(TP_ERR_STATE, "the two-block kernel runs with 4 coefficients per thread; set the split to 1 first");
+    if (coef_per_thread == 8 && c->split > 1)
+        return fail(TP_ERR_STATE, "the %d-block kernel runs with 4 coefficients per thread; set the split to 1 first",
+                    c->split);
     TP_CUDA(cudaSetDevice(c->device));
     return br_retile(c, coef_per_thread == 4 ? 2 : 3);
 }
@@ -452,14 +457,16 @@ uint32_t tp_br_get_tile(const tp_br_ctx* c) { return c ? 1u << c->loge : 0u; }
 
 tp_status tp_br_set_split(tp_br_ctx* c, uint32_t blocks_per_rotation) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
-    if (blocks_per_rotation != 1 && blocks_per_rotation != 2)
-        return fail(TP_ERR_PARAM, "blocks per rotation must be 1 or 2");
+    if (blocks_per_rotation != 1 && blocks_per_rotation != 2 && blocks_per_rotation != 4)
+        return fail(TP_ERR_PARAM, "blocks per rotation must be 1, 2 or 4");
     std::lock_guard<std::mutex> lk(c->mu);
-    if (blocks_per_rotation == 2) {
-        if (c->pair_cap == 0)
-            return fail(TP_ERR_PARAM, "the two-block kernel does not fit this parameter set on this device");
+    if (blocks_per_rotation > 1) {
+        if ((blocks_per_rotation == 2 ? c->pair_cap : c->quad_cap) == 0)
+            return fail(TP_ERR_PARAM, "the %u-block kernel does not fit this parameter set on this device",
+                        blocks_per_rotation);
         if (c->loge != 2)
-            return fail(TP_ERR_STATE, "the two-block kernel runs with 4 coefficients per thread; set the tile first");
+            return fail(TP_ERR_STATE, "the %u-block kernel runs with 4 coefficients per thread; set the tile first",
+                        blocks_per_rotation);
     }
     c->split = (int)blocks_per_rotation;
     return TP_OK;
@@ -472,7 +479,7 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
     if (batch == 0) return fail(TP_ERR_PARAM, "empty batch");
     const uint64_t N = c->prm.ring_dim, n = c->prm.lwe_dim;
-    const uint64_t cap = (uint64_t)std::max(std::max(c->grid_caps[2], c->grid_caps[3]), c->pair_cap);
+    const uint64_t cap = (uint64_t)std::max(std::max(c->grid_caps[2], c->grid_caps[3]), c->pair_cap);  // >= quad_cap
     const uint64_t tb = std::min<uint64_t>(batch, 2 * cap);  // at most two waves per trial
     std::vector<uint64_t> lw(tb * (n + 1));
     uint64_t z = 0x5eedull;
@@ -512,9 +519,9 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     std::lock_guard<std::mutex> lk(c->mu);
     int best_split = c->split;
     struct Cand { int loge, split; };
-    const Cand cands[] = {{3, 1}, {2, 1}, {2, 2}};
+    const Cand cands[] = {{3, 1}, {2, 1}, {2, 2}, {2, 4}};
     for (const Cand& cd : cands) {
-        if (cd.split == 2 && c->pair_cap == 0) continue;
+        if ((cd.split == 2 && c->pair_cap == 0) || (cd.split == 4 && c->quad_cap == 0)) continue;
         s = br_retile(c, cd.loge);
         if (s != TP_OK) break;
         c->split = cd.split;
@@ -2103,6 +2110,7 @@ tp_status set_error(tp_status s, const char* fmt, ...) {
 uint64_t br_concurrency(const tp_br_ctx* c, int split) {
     if (!c) return 0;
     if (split == 2) return c->loge == 2 ? (uint64_t)c->pair_cap : 0;
+    if (split == 4) return c->loge == 2 ? (uint64_t)c->quad_cap : 0;
     return (uint64_t)c->grid_caps[c->loge];
 }
 
@@ -2118,6 +2126,7 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
     if (((uintptr_t)results & 15) || ((uintptr_t)accs & 7) || ((uintptr_t)lwes & 7))
         return fail(TP_ERR_PARAM, "results must be 16-byte aligned, lwes/accs 8-byte aligned");
     if (split == 0) split = c->split;
+    if (split == 4 && br_concurrency(c, 4) == 0) split = 2;
     if (split == 2 && br_concurrency(c, 2) == 0) split = 1;
     TP_CUDA(cudaSetDevice(c->device));
     BrKernelParams kp = c->kp;
@@ -2130,9 +2139,10 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
     kp.batch = batch;
     kp.out_coef = out_coef ? 1u : 0u;
     void* args[] = {&kp};
-    if (split == 2) {
-        const unsigned pairs = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->pair_cap);
-        TP_CUDA(cudaLaunchKernel(c->pair_kernel, dim3(2 * pairs), dim3(c->prm.ring_dim >> 2), args, c->pair_smem,
+    if (split == 2 || split == 4) {
+        const unsigned clusters = (unsigned)std::min<uint64_t>(batch, br_concurrency(c, split));
+        TP_CUDA(cudaLaunchKernel(split == 2 ? c->pair_kernel : c->quad_kernel, dim3((unsigned)split * clusters),
+                                 dim3(c->prm.ring_dim >> 2), args, split == 2 ? c->pair_smem : c->quad_smem,
                                  (cudaStream_t)stream));
         tp::note_launch();
         return TP_OK;

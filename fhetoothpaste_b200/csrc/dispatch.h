@@ -15,12 +15,12 @@ const void* br_kernel_ptr_11(int variant, int loge);
 const void* ntt_kernel_ptr_11(bool forward);
 const void* br_kernel_ptr_12(int variant, int loge);
 const void* ntt_kernel_ptr_12(bool forward);
-const void* br_pair_kernel_ptr_7(int variant);
-const void* br_pair_kernel_ptr_8(int variant);
-const void* br_pair_kernel_ptr_9(int variant);
-const void* br_pair_kernel_ptr_10(int variant);
-const void* br_pair_kernel_ptr_11(int variant);
-const void* br_pair_kernel_ptr_12(int variant);
+const void* br_pair_kernel_ptr_7(int variant, int split);
+const void* br_pair_kernel_ptr_8(int variant, int split);
+const void* br_pair_kernel_ptr_9(int variant, int split);
+const void* br_pair_kernel_ptr_10(int variant, int split);
+const void* br_pair_kernel_ptr_11(int variant, int split);
+const void* br_pair_kernel_ptr_12(int variant, int split);
 const void* ks_kernel_ptr_7(int mode, int loge);
 const void* ks_kernel_ptr_8(int mode, int loge);
 const void* ks_kernel_ptr_9(int mode, int loge);
@@ -40,15 +40,16 @@ inline const void* br_kernel_lookup(int logn, int variant, int loge) {
     }
 }
 
-// Two-CTA (cluster) rotation kernel, 4 coefficients per thread.
-inline const void* br_pair_kernel_lookup(int logn, int variant) {
+// Two- or four-CTA (cluster) rotation kernel, 4 coefficients per thread
+// (nullptr for four where it does not fit).
+inline const void* br_pair_kernel_lookup(int logn, int variant, int split) {
     switch (logn) {
-        case 7: return br_pair_kernel_ptr_7(variant);
-        case 8: return br_pair_kernel_ptr_8(variant);
-        case 9: return br_pair_kernel_ptr_9(variant);
-        case 10: return br_pair_kernel_ptr_10(variant);
-        case 11: return br_pair_kernel_ptr_11(variant);
-        case 12: return br_pair_kernel_ptr_12(variant);
+        case 7: return br_pair_kernel_ptr_7(variant, split);
+        case 8: return br_pair_kernel_ptr_8(variant, split);
+        case 9: return br_pair_kernel_ptr_9(variant, split);
+        case 10: return br_pair_kernel_ptr_10(variant, split);
+        case 11: return br_pair_kernel_ptr_11(variant, split);
+        case 12: return br_pair_kernel_ptr_12(variant, split);
         default: return nullptr;
     }
 }

@@ -23,13 +23,7 @@ const void* br_kernel_ptr_10(int variant, int loge) {
     }
 }
 
-const void* br_pair_kernel_ptr_10(int variant) {
-    switch (variant) {
-        case kCggiBinary: return (const void*)br_pair_kernel<10, kCggiBinary, 2>;
-        case kCggiTernary: return (const void*)br_pair_kernel<10, kCggiTernary, 2>;
-        default: return (const void*)br_pair_kernel<10, kBmmpBinary, 2>;
-    }
-}
+const void* br_pair_kernel_ptr_10(int variant, int split) { return br_split_kernel_ptr<10>(variant, split); }
 
 const void* ntt_kernel_ptr_10(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<10, true> : (const void*)ntt_batch_kernel<10, false>;

@@ -23,13 +23,7 @@ const void* br_kernel_ptr_12(int variant, int loge) {
     }
 }
 
-const void* br_pair_kernel_ptr_12(int variant) {
-    switch (variant) {
-        case kCggiBinary: return (const void*)br_pair_kernel<12, kCggiBinary, 2>;
-        case kCggiTernary: return (const void*)br_pair_kernel<12, kCggiTernary, 2>;
-        default: return (const void*)br_pair_kernel<12, kBmmpBinary, 2>;
-    }
-}
+const void* br_pair_kernel_ptr_12(int variant, int split) { return br_split_kernel_ptr<12>(variant, split); }
 
 const void* ntt_kernel_ptr_12(bool forward) {
     return forward ? (const void*)ntt_batch_kernel<12, true> : (const void*)ntt_batch_kernel<12, false>;

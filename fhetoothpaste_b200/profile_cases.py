@@ -78,6 +78,23 @@ def case_br_pair_ternary_n2048(torch):
     rot.close()
 
 
+def case_br_quad_ternary_n2048(torch):
+    """br_quad_kernel (four blocks per rotation), CGGI ternary N=2048 l=3, n reduced to 64, batch 16."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    N, n, batch = 2048, 64, 16
+    ctx = BlindRotationContext(1, N, n, 1 << 12, 3)
+    rot = GpuBlindRotator(ctx, _u64(1, ctx.key_words()))
+    rot.set_tile(4)
+    rot.set_split(4)
+    lw = _dev(torch, _u64(2, (batch, n + 1), 2 * N))
+    ac = _dev(torch, _u64(3, (batch, 2 * N)))
+    out = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        rot.blind_rotate_batch(out.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(), 2 * N, batch)
+    rot.check()
+    rot.close()
+
+
 def case_pbs_epilogue_n1024(torch):
     """lwe_ks_kernel as the bootstrap epilogue: 4096 RLWEs N=1024 -> extract -> KS to n=500
     (base 2^16, l=4, 16 MB key) -> FLOOR switch to 2N."""

@@ -108,19 +108,23 @@ tp_status tp_br_blind_rotate_batch_host(tp_br_ctx* ctx, uint64_t batch, uint64_t
 tp_status tp_br_set_tile(tp_br_ctx* ctx, uint32_t coef_per_thread);
 uint32_t tp_br_get_tile(const tp_br_ctx* ctx);
 
-/* Thread blocks per rotation: 1 (default) or 2. With 2, a cluster of two
+/* Thread blocks per rotation: 1 (default), 2 or 4. With 2, a cluster of two
  * blocks on two SMs rotates each ciphertext, each block owning one accumulator
  * half and its gadget rows and exchanging partial sums with the other through
- * distributed shared memory: half the latency per rotation, for batches smaller
- * than the number of SMs (large batches run faster with 1). Needs the tile of
- * 4 coefficients per thread; TP_ERR_PARAM if the parameter set does not fit the
- * two-block kernel on this device. Same output words either way. No reference
+ * distributed shared memory: about half the latency per rotation, for batches
+ * smaller than the number of SMs (large batches run faster with 1). With 4, two
+ * blocks per half split that half's gadget digits between them and combine
+ * their sums in a second exchange (for batches up to a quarter of the SMs).
+ * Needs the tile of 4 coefficients per thread; TP_ERR_PARAM if the parameter
+ * set does not fit the chosen kernel on this device (the four-block kernel
+ * needs (3 + 2G) N + 1024 words of shared memory, G = RGSWs per iteration: not
+ * at N = 4096 for ternary or BMMP). Same output words either way. No reference
  * counterpart. */
 tp_status tp_br_set_split(tp_br_ctx* ctx, uint32_t blocks_per_rotation);
 uint32_t tp_br_get_split(const tp_br_ctx* ctx);
 
-/* Times every tile (8 or 4 coefficients per thread, and 4 with two blocks per
- * rotation) on up to two waves of `batch` synthetic rotations with the uploaded
+/* Times every tile (8 or 4 coefficients per thread, and 4 with two or four
+ * blocks per rotation) on up to two waves of `batch` synthetic rotations with the uploaded
  * key, keeps the fastest and reports it (either output may be NULL; the split
  * is read back with tp_br_get_split). Blocks until done; the context must be
  * idle. */

@@ -283,18 +283,87 @@ def test_two_block_batches_of_any_size(native, oracle, golden, name):
             np.testing.assert_array_equal(got[b], exp, err_msg=f"batch {batch}, ciphertext {b}")
 
 
-def test_two_block_split_needs_tile_of_four(native, oracle, golden):
+@pytest.mark.parametrize("split", [2, 4])
+def test_split_needs_tile_of_four(native, oracle, golden, split):
     from fhetoothpaste_b200 import TpError
     case, rot = rotator(oracle, golden, "small_binary_n256")
     rot.set_tile(8)
     with pytest.raises(TpError):
-        rot.set_split(2)
+        rot.set_split(split)
     rot.set_tile(4)
-    rot.set_split(2)
+    rot.set_split(split)
     with pytest.raises(TpError):
         rot.set_tile(8)
+    with pytest.raises(TpError):
+        rot.set_split(3)
     rot.set_split(1)
     rot.set_tile(8)
+
+
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_four_block_rotation_matches_reference(native, oracle, golden, name):
+    """Four thread blocks per ciphertext (two per accumulator half, the half's gadget
+    digits split between them): same words as the reference. A parameter set whose
+    shared-memory plan does not fit one SM refuses the split."""
+    from fhetoothpaste_b200 import TpError
+    case, rot = rotator(oracle, golden, name)
+    rot.set_tile(4)
+    try:
+        rot.set_split(4)
+    except TpError:
+        assert case["N"] == 4096 and case["variant"] != 0, "only N = 4096 ternary / BMMP sets may refuse"
+        pytest.skip("the four-block kernel does not fit this parameter set")
+    assert rot.split == 4
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for oc in (0, 1):
+        idx = [i for i, c in enumerate(coefs) if c == oc]
+        got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+        np.testing.assert_array_equal(got, expect[idx], err_msg="four blocks per rotation")
+    res = np.ascontiguousarray(accs[0])
+    rot.BlindRotate(res, np.ascontiguousarray(lwes[0]), res, bool(coefs[0]))
+    np.testing.assert_array_equal(res, expect[0])
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_four_block_batches_of_any_size(native, oracle, golden, name):
+    """Batch 1, 37 and more clusters than fit on the device (clusters loop over ciphertexts)."""
+    case, rot = rotator(oracle, golden, name)
+    N, n = case["N"], case["n"]
+    _, _, brk = case_key(oracle, name, case)
+    rot.set_split(4)
+    for batch in (1, 37, 4 * 148 + 3):
+        lwes = lwe_inputs(N, n, batch, 700 + batch)
+        accs = random_acc(N, batch, 800 + batch)
+        got = rot.blind_rotate_batch_host(lwes, accs, out_coef=False)
+        for b in sorted({0, batch // 2, batch - 1}):
+            exp = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b],
+                                      accs[b], 0)
+            np.testing.assert_array_equal(got[b], exp, err_msg=f"batch {batch}, ciphertext {b}")
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("digits", [1, 2])
+def test_four_block_uneven_digit_split(native, oracle, variant, digits):
+    """One or two gadget digits: the second digit subset's CTAs hold one digit or none and
+    only relay partial sums. Words equal the oracle's and the one-block kernel's."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    from oracle.oracle import lwe_secret, rlwe_secret
+    N, n, beta = 256, 8, 16
+    lk = lwe_secret(variant, n, N, seed=71)
+    rk = rlwe_secret(N, seed=72)
+    brk = oracle.br_keygen(variant, N, n, beta, digits, 3.2, lk, rk, seed=73)
+    rot = GpuBlindRotator(BlindRotationContext(variant, N, n, 1 << beta, digits), brk)
+    rot.set_tile(4)
+    lwes = lwe_inputs(N, n, 5, 74)
+    accs = random_acc(N, 5, 75)
+    one = rot.blind_rotate_batch_host(lwes, accs)
+    rot.set_split(4)
+    four = rot.blind_rotate_batch_host(lwes, accs)
+    np.testing.assert_array_equal(four, one)
+    for b in range(5):
+        exp = oracle.blind_rotate(variant, N, n, beta, digits, brk, lwes[b], accs[b], 0)
+        np.testing.assert_array_equal(four[b], exp, err_msg=f"ciphertext {b}")
 
 
 def test_function_evaluator_like_oracle(native, oracle, golden):
