@@ -121,11 +121,15 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
 }
 
 // Fused radix-4 NTT passes (three products and a shift per two levels, see
-// ntt_block.cuh) for 4 coefficients per thread. Measured against plain radix-2
-// butterflies, rotations/s: BMMP N = 2048 5570 vs 5438; CGGI ternary N = 2048
-// 6247 vs 6443, binary N = 1024 15675 vs 16249, ternary N = 1024 and 4096 equal.
-__host__ __device__ constexpr bool br_fused_radix4(int loge, int variant) {
-    return loge == 2 && variant == kBmmpBinary;
+// ntt_block.cuh) for 4 coefficients per thread, by blocks per rotation. They
+// trade IMAD work for ALU work. With the carry-form reduction (both integer
+// pipes level) plain radix-2 butterflies are faster everywhere but in the BMMP
+// four-block kernel, rotations/s: BMMP N = 2048 7808 vs 7615 (one block), 81.0
+// vs 79.0 (two blocks, batch 1), 100.7 vs 102.4 (four blocks, batch 1); CGGI
+// ternary N = 2048 7275 vs 6885, binary N = 1024 18.8k vs 17.5k. (With the
+// earlier 16-instruction reduction radix-4 was faster for BMMP: 5570 vs 5438.)
+__host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int blocks) {
+    return loge == 2 && variant == kBmmpBinary && blocks == 4;
 }
 
 // Coefficients per thread (log2) a context starts with; tp_br_set_tile and
@@ -161,7 +165,7 @@ br_kernel(const BrKernelParams prm) {
     constexpr bool TW_SMEM = br_smem_twiddles(LOGN);
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
-    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT);
+    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT, 1);
     constexpr bool PF = br_key_prefetch(LOGN, VARIANT, LOGE);
 
     extern __shared__ __align__(16) uint64_t smem[];

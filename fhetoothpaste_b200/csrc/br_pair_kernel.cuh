@@ -83,7 +83,7 @@ __device__ __forceinline__ void br_split_body(const BrKernelParams& prm) {
     constexpr int C = 2 * G;
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
-    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT);
+    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT, S);
     constexpr bool PF = br_pair_key_prefetch(LOGN, VARIANT, S);
     constexpr bool TW_SMEM = br_pair_smem_twiddles(LOGN, VARIANT, LOGE, S);
 
