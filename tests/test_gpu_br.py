@@ -391,3 +391,29 @@ def test_function_evaluator_like_oracle(native, oracle, golden):
     for b in range(3):
         rl = oracle.blind_rotate(case["variant"], N, n, case["basis_log2"], case["digits"], brk, lwes[b], luts[b], 1)
         np.testing.assert_array_equal(batch[b], oracle.sample_extract(rl))
+
+
+def test_four_block_binary_n4096(native, oracle):
+    """Binary N = 4096 is the one N = 4096 set whose four-block plan fits (one RGSW per
+    iteration); ternary and BMMP refuse the split there."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator, TpError
+    from oracle.oracle import lwe_secret, rlwe_secret
+    N, n, beta, digits = 4096, 6, 16, 4
+    lk = lwe_secret(0, n, N, seed=81)
+    rk = rlwe_secret(N, seed=82)
+    brk = oracle.br_keygen(0, N, n, beta, digits, 3.2, lk, rk, seed=83)
+    rot = GpuBlindRotator(BlindRotationContext(0, N, n, 1 << beta, digits), brk)
+    rot.set_tile(4)
+    lwes = lwe_inputs(N, n, 3, 84)
+    accs = random_acc(N, 3, 85)
+    rot.set_split(4)
+    for oc in (False, True):
+        got = rot.blind_rotate_batch_host(lwes, accs, out_coef=oc)
+        for b in range(3):
+            exp = oracle.blind_rotate(0, N, n, beta, digits, brk, lwes[b], accs[b], int(oc))
+            np.testing.assert_array_equal(got[b], exp, err_msg=f"ciphertext {b}, out_coef {oc}")
+    tctx = BlindRotationContext(1, N, n, 1 << 12, 3)
+    trot = GpuBlindRotator(tctx, np.zeros(tctx.key_words(), np.uint64))
+    trot.set_tile(4)
+    with pytest.raises(TpError):
+        trot.set_split(4)
