@@ -1274,8 +1274,8 @@ tp_status tp_lwe_ks_upload_key(tp_lwe_ks_ctx* c, const uint64_t* ksk, uint64_t w
     TP_CUDA(cudaMemcpy(c->key, ksk, c->key_words * 8, cudaMemcpyHostToDevice));
     tp::LweKsParams kp = c->kp;
     kp.ksk = c->key;
-    const unsigned blocks = (c->n_out + 1 + 127) / 128;
-    tp::lwe_ks_cterm_kernel<<<blocks, 128>>>(c->cterm, kp);
+    const unsigned blocks = (c->n_out + 1 + 31) / 32;
+    tp::lwe_ks_cterm_kernel<<<blocks, dim3(32, tp::kCtermSlices)>>>(c->cterm, kp);
     tp::note_launch();
     TP_CUDA(cudaGetLastError());
     TP_CUDA(cudaDeviceSynchronize());

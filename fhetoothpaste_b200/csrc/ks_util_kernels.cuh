@@ -218,18 +218,32 @@ __global__ void __launch_bounds__(kLweKsCols) lwe_ks_kernel(const LweKsParams pr
     }
 }
 
-// cterm[col] = sum_j ddelta[j] * (sum_i ksk[i][j][col]) mod p, one thread per output word.
-__global__ void lwe_ks_cterm_kernel(uint64_t* __restrict__ cterm, const LweKsParams prm) {
+// cterm[col] = sum_j ddelta[j] * (sum_i ksk[i][j][col]) mod p. Block (32, Y): threadIdx.x
+// picks the column of a 32-column tile (coalesced key reads), threadIdx.y a slice of the
+// input index i; each thread forms sum_j ddelta[j] * (its slice's sum) and the Y partials
+// are added in shared memory (the constant is linear in the sums, so the words equal a
+// serial sum's).
+constexpr int kCtermSlices = 16;
+__global__ void __launch_bounds__(32 * kCtermSlices) lwe_ks_cterm_kernel(uint64_t* __restrict__ cterm,
+                                                                         const LweKsParams prm) {
+    __shared__ uint64_t part[kCtermSlices][32];
     const uint32_t width = prm.n_out + 1;
-    for (uint32_t col = blockIdx.x * blockDim.x + threadIdx.x; col < width; col += gridDim.x * blockDim.x) {
-        uint64_t total = 0;
+    const uint32_t col = blockIdx.x * 32 + threadIdx.x;
+    uint64_t total = 0;
+    if (col < width) {
         for (uint32_t j = 0; j < prm.digits; ++j) {
             uint64_t s = 0;
-            for (uint32_t i = 0; i < prm.n_in; ++i)
+            for (uint32_t i = threadIdx.y; i < prm.n_in; i += kCtermSlices)
                 s = gl_add(s, gl_canon(prm.ksk[((uint64_t)i * prm.digits + j) * width + col]));
             total = gl_add(total, gl_mul(s, gl_canon(prm.ddelta[j])));
         }
-        cterm[col] = total;
+    }
+    part[threadIdx.y][threadIdx.x] = total;
+    __syncthreads();
+    if (threadIdx.y == 0 && col < width) {
+        uint64_t sum = part[0][threadIdx.x];
+        for (int y = 1; y < kCtermSlices; ++y) sum = gl_add(sum, part[y][threadIdx.x]);
+        cterm[col] = sum;
     }
 }
 

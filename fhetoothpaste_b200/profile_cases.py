@@ -227,6 +227,23 @@ def case_sap_n4096(torch):
     dec.close()
 
 
+def case_sap_reset_n4096(torch):
+    """The SAP case above with an accumulator reset every 2 digits (restart period 2), so the
+    reset path (epilogue, fresh rotation, sap_select_kernel) runs too."""
+    from fhetoothpaste_b200 import BlindRotationContext, GpuSAPDecomposer
+    N, n, l, batch = 4096, 10, 4, 16
+    words = BlindRotationContext(0, N, n, 1 << 16, l).key_words()
+    dec = GpuSAPDecomposer((0, N, n, 1 << 16, l), (1 << 16, l), (1 << 16, l), _u64(71, words),
+                           _u64(72, 12 * 2 * N * l), _u64(73, N * l * (n + 1)), hamming_weight=5,
+                           restart_period=2)
+    lw = _dev(torch, _u64(74, (batch, n + 1), 1 << 40))
+    out = torch.zeros((batch, 9, N + 1), dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        dec.decompose_batch(batch, out.data_ptr(), 9, lw.data_ptr(), 32)
+    torch.cuda.synchronize()
+    dec.close()
+
+
 def case_lwe_to_rgsw_n2048_b1024(torch):
     """As lwe_to_rgsw_n2048 with 1024 LWEs, so the element-wise kernels' rows (134 MB) exceed L2."""
     from fhetoothpaste_b200 import BlindRotationContext, GpuLWEtoRGSWConverter
