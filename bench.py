@@ -384,9 +384,14 @@ SERVING_SETS = [(1024, 500), (2048, 630), (4096, 900)]  # ternary, base 2^12, l 
 SERVING_MIX = [0.5, 0.35, 0.15]
 
 
+SERVING_LIGHT_RATE = 300.0  # requests/s of the light-load point (launches of a few requests)
+
+
 def serving_run(device: int, rate: float, seconds: float) -> dict:
     """Config-5 serving loop: Poisson single-bootstrap requests over three resident
-    ternary parameter sets, continuous batching in the native scheduler."""
+    ternary parameter sets, continuous batching in the native scheduler. Three load
+    points: the offered rate (overload), 80% of what that achieved (sustainable), and
+    a light load whose latency is one small launch."""
     from fhetoothpaste_b200 import BlindRotationContext, BootstrapServer, GpuBlindRotator
     from oracle.oracle import lwe_inputs
     rots, pools = [], []
@@ -400,7 +405,7 @@ def serving_run(device: int, rate: float, seconds: float) -> dict:
         pools.append((lwe_inputs(N, n, 256, 900 + i), lut_polys(N, 256, 950 + i)))
     out = {"sets": [f"N={N} n={n}" for N, n in SERVING_SETS], "mix": SERVING_MIX,
            "key_bytes_resident": sum(r.ctx.key_words() * 8 for r in rots), "duration_s": seconds}
-    for label, r in (("offered", rate), ("sustainable", None)):
+    for label, r in (("offered", rate), ("sustainable", None), ("light", SERVING_LIGHT_RATE)):
         srv = BootstrapServer(device=device, max_queue=2500)
         for rot, mb in zip(rots, (296, 148, 148)):
             srv.add_set(rot, max_batch=mb, buffers=2)
