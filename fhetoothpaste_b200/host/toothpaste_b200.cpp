@@ -311,6 +311,20 @@ void GpuBlindRotator::BlindRotateBatch(uint64_t batch, uint64_t* results, const 
     check(tp_br_check(m_ctx, nullptr));
 }
 
+void GpuBlindRotator::SetTile(uint32_t coef_per_thread) { check(tp_br_set_tile(m_ctx, coef_per_thread)); }
+
+void GpuBlindRotator::SetSplit(uint32_t blocks_per_rotation) { check(tp_br_set_split(m_ctx, blocks_per_rotation)); }
+
+uint32_t GpuBlindRotator::Tile() const { return tp_br_get_tile(m_ctx); }
+
+uint32_t GpuBlindRotator::Split() const { return tp_br_get_split(m_ctx); }
+
+uint32_t GpuBlindRotator::Autotune(uint64_t batch, double* rotations_per_s) {
+    uint32_t coef = 0;
+    check(tp_br_autotune(m_ctx, batch, &coef, rotations_per_s));
+    return coef;
+}
+
 // ---- contexts ----
 
 CGGIBlindRotationContext::CGGIBlindRotationContext(KeyDistribution distr, uint64_t modulus, uint64_t ring_dim,

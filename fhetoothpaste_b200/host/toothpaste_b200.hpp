@@ -113,6 +113,15 @@ public:
     // or one shared row when acc_stride == 0).
     void BlindRotateBatch(uint64_t batch, uint64_t* results, const uint64_t* lwes, const uint64_t* accs,
                           uint64_t acc_stride, bool output_as_coefficients = false);
+    // GPU launch form (no reference counterpart; same output words in every form):
+    // coefficients per thread (4 or 8), thread blocks per rotation (1, 2 or 4; 2 and 4
+    // need 4 per thread), or both chosen by timing `batch` synthetic rotations.
+    void SetTile(uint32_t coef_per_thread);
+    void SetSplit(uint32_t blocks_per_rotation);
+    uint32_t Tile() const;
+    uint32_t Split() const;
+    // returns the chosen coefficients per thread (the split is read back with Split())
+    uint32_t Autotune(uint64_t batch, double* rotations_per_s = nullptr);
     tp_br_ctx* Handle() const { return m_ctx; }
     uint32_t RingDimension() const { return m_N; }
     uint32_t LWEDimension() const { return m_n; }

@@ -98,6 +98,22 @@ static int run(int argc, char** argv) {
         if (count > 1)
             op->BlindRotateBatch(count - 1, out.data() + 2 * N, lwes.data() + (n + 1), accs.data() + 2 * N, 2 * N,
                                  false);
+        // the same batch with two and four blocks per rotation (where the kernel fits) gives the same words
+        op->SetTile(4);
+        for (uint32_t split : {2u, 4u}) {
+            try {
+                op->SetSplit(split);
+            } catch (const std::exception&) {
+                if (split == 2) throw;
+                continue;  // the four-block kernel does not fit this parameter set
+            }
+            if (op->Split() != split || op->Tile() != 4) throw std::runtime_error("launch form not kept");
+            std::vector<uint64_t> again(count * 2 * N);
+            op->BlindRotateBatch(count, again.data(), lwes.data(), accs.data(), 2 * N, false);
+            if (std::memcmp(again.data(), out.data(), again.size() * 8) != 0)
+                throw std::runtime_error("blocks per rotation changed the words");
+        }
+        op->SetSplit(1);
         save(argv[14], out.data(), out.size());
         return 0;
     }
