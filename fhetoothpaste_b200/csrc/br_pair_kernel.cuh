@@ -47,9 +47,20 @@ namespace tp {
 // Shared-memory plan of the S-block kernel, in words (LWE area budgeted at 1024
 // words; the host adds the real size and checks the total). The key row stage
 // is kept when it fits, then the twiddles.
+// Exchange buffers of the NTTs: two (transforms alternate between them), or one
+// where two do not fit beside the four-block kernel's receive areas (then every
+// transform starts after a block barrier instead).
+__host__ __device__ constexpr int br_split_xbufs(int logn, int variant, int s) {
+    return ((size_t)(1 << logn) * (2 + 1 + (s == 4 ? 2 : 1) * br_rgsw_per_group(variant)) + 1024) * 8 <=
+                   227u * 1024u
+               ? 2
+               : 1;
+}
 __host__ __device__ constexpr size_t br_pair_core_words(int logn, int variant, int s = 2) {
     // xbufs, acc half, receive area(s)
-    return (size_t)(1 << logn) * (2 + 1 + (s == 4 ? 2 : 1) * br_rgsw_per_group(variant)) + 1024;
+    return (size_t)(1 << logn) *
+               (br_split_xbufs(logn, variant, s) + 1 + (s == 4 ? 2 : 1) * br_rgsw_per_group(variant)) +
+           1024;
 }
 __host__ __device__ constexpr bool br_pair_key_prefetch(int logn, int variant, int s = 2) {
     return (br_pair_core_words(logn, variant, s) + (size_t)(1 << logn) * 2 * br_rgsw_per_group(variant)) * 8 <=
@@ -106,9 +117,10 @@ __device__ __forceinline__ void br_split_body(const BrKernelParams& prm) {
         tw_i = base + TWW;
         base += 2 * TWW;
     }
+    constexpr int XB = br_split_xbufs(LOGN, VARIANT, S);
     uint64_t* xbuf0 = base;
-    uint64_t* xbuf1 = base + N;
-    uint64_t* acc = base + 2 * N;        // this CTA's half, [j*T + t], canonical, NTT domain
+    uint64_t* xbuf1 = base + (XB - 1) * N;
+    uint64_t* acc = base + XB * N;       // this CTA's half, [j*T + t], canonical, NTT domain
     uint64_t* recv = acc + N;            // area 1: partial sums for this half, [(g*E/2 + jp)*T + t] x 16 bytes
     uint64_t* recv2 = recv + G * N;      // area 2 (S = 4): the other digit subset's sums, same layout
     uint64_t* kst = recv + (S == 4 ? 2 : 1) * G * N;  // key row stage (C*N words)
@@ -124,7 +136,10 @@ __device__ __forceinline__ void br_split_body(const BrKernelParams& prm) {
     const uint32_t d_end = S == 4 && !q ? (L + 1) / 2 : L;
 
     int sel = 0;
+    // exchange buffer of the next transform; with one buffer, a block barrier first
+    // (every warp has finished reading the previous transform's last exchange)
     auto xb = [&]() -> uint64_t* {
+        if constexpr (XB == 1) __syncthreads();
         uint64_t* b = sel ? xbuf1 : xbuf0;
         sel ^= 1;
         return b;

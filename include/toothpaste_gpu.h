@@ -117,9 +117,9 @@ uint32_t tp_br_get_tile(const tp_br_ctx* ctx);
  * their sums in a second exchange (for batches up to a quarter of the SMs).
  * Needs the tile of 4 coefficients per thread; TP_ERR_PARAM if the parameter
  * set does not fit the chosen kernel on this device (the four-block kernel
- * needs (3 + 2G) N + 1024 words of shared memory, G = RGSWs per iteration: not
- * at N = 4096 for ternary or BMMP). Same output words either way. No reference
- * counterpart. */
+ * needs (2 + 2G) N + 1024 words of shared memory with one NTT exchange buffer,
+ * G = RGSWs per iteration: not for BMMP at N = 4096). Same output words either
+ * way. No reference counterpart. */
 tp_status tp_br_set_split(tp_br_ctx* ctx, uint32_t blocks_per_rotation);
 uint32_t tp_br_get_split(const tp_br_ctx* ctx);
 

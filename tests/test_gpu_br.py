@@ -311,7 +311,7 @@ def test_four_block_rotation_matches_reference(native, oracle, golden, name):
     try:
         rot.set_split(4)
     except TpError:
-        assert case["N"] == 4096 and case["variant"] != 0, "only N = 4096 ternary / BMMP sets may refuse"
+        assert case["N"] == 4096 and case["variant"] == 2, "only N = 4096 BMMP sets may refuse"
         pytest.skip("the four-block kernel does not fit this parameter set")
     assert rot.split == 4
     lwes, accs, coefs = case_inputs(name, case)
@@ -394,8 +394,8 @@ def test_function_evaluator_like_oracle(native, oracle, golden):
 
 
 def test_four_block_binary_n4096(native, oracle):
-    """Binary N = 4096 is the one N = 4096 set whose four-block plan fits (one RGSW per
-    iteration); ternary and BMMP refuse the split there."""
+    """Binary N = 4096 fits the four-block plan with two exchange buffers (one RGSW per
+    iteration); BMMP (three RGSWs per pair) refuses the split there."""
     from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator, TpError
     from oracle.oracle import lwe_secret, rlwe_secret
     N, n, beta, digits = 4096, 6, 16, 4
@@ -412,8 +412,8 @@ def test_four_block_binary_n4096(native, oracle):
         for b in range(3):
             exp = oracle.blind_rotate(0, N, n, beta, digits, brk, lwes[b], accs[b], int(oc))
             np.testing.assert_array_equal(got[b], exp, err_msg=f"ciphertext {b}, out_coef {oc}")
-    tctx = BlindRotationContext(1, N, n, 1 << 12, 3)
-    trot = GpuBlindRotator(tctx, np.zeros(tctx.key_words(), np.uint64))
-    trot.set_tile(4)
+    bctx = BlindRotationContext(2, N, n, 1 << 16, 4)
+    brot = GpuBlindRotator(bctx, np.zeros(bctx.key_words(), np.uint64))
+    brot.set_tile(4)
     with pytest.raises(TpError):
-        trot.set_split(4)
+        brot.set_split(4)
