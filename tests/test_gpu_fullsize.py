@@ -1,8 +1,8 @@
 """Full-size checks on the benchmark's own workload (CGGI ternary n=630, N=2048, base 2^12
 l=3, 4096 ciphertexts with their own test polynomials): ciphertexts sampled across the
 persistent grid's waves equal the oracle; the batch is order-independent (a permuted batch
-gives the permuted results, word for word); the two-block kernel and a graph replay give the
-one-block kernel's words."""
+gives the permuted results, word for word); the two- and four-block kernels and a graph
+replay give the one-block kernel's words."""
 import numpy as np
 import pytest
 
@@ -40,11 +40,13 @@ def test_batch_order_does_not_matter(native, cuda, setup):
 def test_two_blocks_and_graph_give_the_same_words(native, cuda, setup):
     torch = cuda
     rot, _, lwes, accs, out = setup
-    rot.set_split(2)
-    try:
-        np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[:300], accs[:300]), out[:300])
-    finally:
-        rot.set_split(1)
+    for split, count in ((2, 300), (4, 100)):
+        rot.set_split(split)
+        try:
+            np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[:count], accs[:count]), out[:count],
+                                          err_msg=f"{split} blocks per rotation")
+        finally:
+            rot.set_split(1)
     d_lwe = torch.from_numpy(lwes.view(np.int64)).cuda()
     d_acc = torch.from_numpy(accs.view(np.int64)).cuda()
     d_out = torch.empty((BATCH, 2 * N), dtype=torch.int64, device="cuda")
