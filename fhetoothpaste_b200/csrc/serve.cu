@@ -29,13 +29,11 @@
 
 #include "toothpaste_gpu.h"
 #include "br_launch.h"
+#include "serve_policy.h"
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
-
-// Largest launch the scheduler runs with four blocks per rotation.
-constexpr uint32_t kServeFourBlockMax = 8;
 
 struct Request {
     uint64_t ticket;
@@ -148,12 +146,9 @@ void launch_pending(tp_server* srv, uint32_t si) {
         // four-block kernel fits (15-30% less latency again); under load the
         // four-block form's extra SM-time (1.7x the two-block form's) would slow the
         // other launches, so it is not used.
-        const bool room = busy + 4ull * take <= srv->sm_count;
-        const int split = room && take <= kServeFourBlockMax && take <= tp::br_concurrency(s.ctx, 4) ? 4
-                          : take <= tp::br_concurrency(s.ctx, 2)                                     ? 2
-                                                                                                      : 1;
-        b.blocks = (uint32_t)std::min<uint64_t>((uint64_t)split * take, (uint64_t)split *
-                                                std::max<uint64_t>(tp::br_concurrency(s.ctx, split), 1));
+        const int split = tp::serve_split(take, busy, srv->sm_count, tp::br_concurrency(s.ctx, 4),
+                                          tp::br_concurrency(s.ctx, 2));
+        b.blocks = (uint32_t)tp::serve_blocks(split, take, tp::br_concurrency(s.ctx, split));
         tp_status st = e == cudaSuccess ? tp::br_batch_launch(s.ctx, take, b.d_res, b.d_lwe, lw, b.d_acc, aw,
                                                                s.out_coef, b.stream, split)
                                         : TP_ERR_CUDA;
