@@ -10,8 +10,10 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 @pytest.fixture(scope="module")
-def policy(tmp_path_factory):
-    exe = tmp_path_factory.mktemp("serve_policy") / "serve_policy_driver"
+def policy():
+    out_dir = ROOT / "tests" / "_build"  # git-ignored build folder
+    out_dir.mkdir(exist_ok=True)
+    exe = out_dir / "serve_policy_driver"
     subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'fhetoothpaste_b200' / 'csrc'}",
                     str(ROOT / "tests" / "cpp" / "serve_policy_driver.cpp"), "-o", str(exe)], check=True)
 
