@@ -134,9 +134,9 @@ __host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int bl
 
 // Coefficients per thread (log2) a context starts with; tp_br_set_tile and
 // tp_br_autotune change it. 4 per thread measured faster than 8 for every
-// variant and ring size (rotations/s, full waves: ternary N = 2048 6361 vs
-// 6039, BMMP N = 2048 5317 vs 3893, ternary N = 1024 16437 vs 13729, ternary
-// N = 4096 1941 vs 1644): twice the warps per SM hide the integer pipes'
+// variant and ring size (rotations/s, full waves: ternary N = 2048 7286 vs
+// 6798, BMMP N = 2048 7658 vs 7099, binary N = 1024 18786 vs 17168, ternary
+// N = 4096 2188 vs 1874): twice the warps per SM hide the integer pipes'
 // dependency latency that 8 per thread left exposed.
 __host__ __device__ constexpr int br_default_loge(int logn, int variant) {
     return (void)logn, (void)variant, 2;
