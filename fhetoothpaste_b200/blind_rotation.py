@@ -1,7 +1,7 @@
 """Python mirror of the reference's blind-rotation operator API over the C ABI.
 
 Mirrors CGGIBlindRotationContext / BMMPBlindRotationContext and
-BlindRotator::BlindRotate (lib/include/interfaces/blindrotation_operator.h:183-212
+BlindRotator::BlindRotate (lib/include/interfaces/blindrotation_operator.h:20-49
 of the reference) for tests, the benchmark and the serving loop. Key
 generation stays with the caller (the C++ adapters in fhetoothpaste_b200/host/
 run it on the host); this class takes the generated key words.

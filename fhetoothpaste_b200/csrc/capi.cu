@@ -1098,6 +1098,9 @@ tp_status tp_pack_consecutive_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, 
     if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
     const uint64_t N = c->N;
     if (len < 2 || len > N) return fail(TP_ERR_PARAM, "len must be in [2, N]");
+    if (packs > (UINT64_MAX / 16) / (len * 2 * N))  // two halves of packs * len * 2N words must not wrap
+        return fail(TP_ERR_PARAM, "packs * len * 2N words overflow (%llu packs of length %llu)",
+                    (unsigned long long)packs, (unsigned long long)len);
     std::lock_guard<std::mutex> lk(c->mu);
     TP_CUDA(cudaSetDevice(c->device));
     tp_status s = consec_plan(c, len);
@@ -1148,6 +1151,9 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
     if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
     const uint64_t N = c->N;
     if (len < 2 || len > N || (len & (len - 1))) return fail(TP_ERR_PARAM, "len must be a power of two in [2, N]");
+    if (packs > (UINT64_MAX / 8) / (len * 2 * N))  // packs * len * 2N * 8 bytes must not wrap
+        return fail(TP_ERR_PARAM, "packs * len * 2N words overflow (%llu packs of length %llu)",
+                    (unsigned long long)packs, (unsigned long long)len);
     std::lock_guard<std::mutex> lk(c->mu);
     TP_CUDA(cudaSetDevice(c->device));
     const uint64_t need = packs * len * 2 * N;
@@ -2012,7 +2018,10 @@ tp_status tp_sap_reset_batch(tp_sap_ctx* c, uint64_t batch, uint64_t* acc, uint6
 // library reserves its kPackScratchWords * 8 bytes (16 MiB) until the process
 // exits. In host code the name `g_pack_scratch` only stands in for the
 // variable, it is not a device address; the device address is fetched once
-// per device with cudaGetSymbolAddress and cached.
+// per device with cudaGetSymbolAddress and cached. The cache assumes the
+// device's primary context lives until the process exits: after a
+// cudaDeviceReset the module may load at another address, so a process that
+// resets a device must not call this entry point on it again.
 
 namespace {
 constexpr uint64_t kPackScratchWords = 2ull << 20;  // 16 MiB of packing-tree nodes
@@ -2031,13 +2040,18 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
     if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
     const uint64_t N = c->N;
     if (len < 2 || len > N || (len & (len - 1))) return fail(TP_ERR_PARAM, "len must be a power of two in [2, N]");
-    const uint64_t need = packs * len * 2 * N;
-    if (need > kPackScratchWords)
+    // compared by division: packs * len * 2N itself can wrap around 64 bits
+    const uint64_t per_pack = len * 2 * N;
+    if (packs > kPackScratchWords / per_pack)
         return fail(TP_ERR_PARAM,
-                    "packs * len * 2N = %llu words exceeds the fixed scratch of %llu words (16 MiB); "
+                    "packs * len * 2N (%llu packs of %llu words) exceeds the fixed scratch of %llu words (16 MiB); "
                     "use fewer packs per call or tp_pack_batch",
-                    (unsigned long long)need, (unsigned long long)kPackScratchWords);
+                    (unsigned long long)packs, (unsigned long long)per_pack, (unsigned long long)kPackScratchWords);
+    const uint64_t need = packs * per_pack;
     if (c->device < 0 || c->device >= kMaxDevices) return fail(TP_ERR_PARAM, "device index out of range");
+    // The context's key, tile and tables are read under its lock, as in tp_pack_batch:
+    // tp_ks_set_tile or tp_ks_upload_key on another thread cannot swap them mid-call.
+    std::lock_guard<std::mutex> ctx_lock(c->mu);
     TP_CUDA(cudaSetDevice(c->device));
     uint64_t* work = nullptr;
     {
@@ -2078,18 +2092,8 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
         tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
         if (s != TP_OK) return s;
     }
-    for (int i = 0; i < c->logn - log_len; ++i) {
-        const int j = c->logn - i;
-        kp.key = c->key + (uint64_t)(j - 1) * kw;
-        kp.in = work;
-        kp.out = work;
-        kp.items = packs;
-        kp.in_stride = kp.out_stride = len * 2 * N;
-        kp.right_offset = 0;
-        kp.auto_index = (1u << j) + 1;
-        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
-        kp.shift = 0;
-        tp_status s = ks_launch(c, tp::kKsTrace, kp, st);
+    {
+        tp_status s = ks_trace_steps(c, packs, work, len * 2 * N, c->logn, log_len + 1, st);
         if (s != TP_OK) return s;
     }
     TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));

@@ -1,7 +1,7 @@
 // C++ drop-in operators over the B200 C ABI (include/toothpaste_gpu.h).
 //
 // These classes carry the reference's operator names, constructor parameters
-// and call signatures (lib/include/interfaces/blindrotation_operator.h:183-212,
+// and call signatures (lib/include/interfaces/blindrotation_operator.h:20-49,
 // lib/include/operators/cggi_blind_rotation.h:19-161,
 // lib/include/operators/bmmp_blind_rotation.h:18-176,
 // lib/include/operators/endo_glwe_conversion.h, automorphism_evaluation.h,
@@ -87,7 +87,7 @@ SchemeSwitchingKeySet SchemeSwitchingKeys(Sampler& rng, int variant, uint32_t N,
                                           const std::vector<uint64_t>& lwe_key, const std::vector<uint64_t>& rlwe_key);
 }  // namespace keygen
 
-// BlindRotator (lib/include/interfaces/blindrotation_operator.h:183-212).
+// BlindRotator (lib/include/interfaces/blindrotation_operator.h:20-49).
 struct BlindRotator {
     virtual void BlindRotate(std::vector<uint64_t>& result, const std::vector<uint64_t>& lwe_ciphertext,
                              std::vector<uint64_t>& accumulator, bool output_as_coefficients = false) = 0;

@@ -30,7 +30,7 @@ typedef enum {
     TP_ERR_PARAM = 1,   /* invalid argument or unsupported parameter set */
     TP_ERR_OOM = 2,     /* device allocation failed */
     TP_ERR_CUDA = 3,    /* a CUDA call failed (message in tp_last_error) */
-    TP_ERR_TIMEOUT = 4, /* a bounded device-side wait ran out */
+    TP_ERR_TIMEOUT = 4, /* a bounded host-side wait ran out (serving: a result or a drain) */
     TP_ERR_LAYOUT = 5,  /* key size or layout does not match the context */
     TP_ERR_STATE = 6    /* call order: e.g. rotate before a key was uploaded */
 } tp_status;
@@ -74,7 +74,7 @@ uint64_t tp_br_key_words(const tp_br_ctx* ctx);
 tp_status tp_br_upload_key(tp_br_ctx* ctx, const uint64_t* brk_host, uint64_t words);
 
 /* Drop-in for BlindRotator::BlindRotate(result, lwe, acc, output_as_coefficients)
- * (lib/include/interfaces/blindrotation_operator.h:202-203; CGGI body
+ * (lib/include/interfaces/blindrotation_operator.h:39-40; CGGI body
  * cggi_blind_rotation.cpp:236-262, BMMP body bmmp_blind_rotation.cpp:325-335).
  * Host pointers: lwe has n+1 words [a_0..a_{n-1}, b], each in [0, 2N); acc is
  * 2N words [A | B] in the coefficient domain; result receives 2N words in the
@@ -247,7 +247,10 @@ tp_status tp_trace_eval_auto_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out
  * packs * len * 2N above 2^21 words fail with TP_ERR_PARAM. The call itself
  * allocates nothing. Its first call on a device looks up the array's device
  * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture. Every GPU that loads the library holds the
+ * call before any stream capture; that address stays valid while the device's
+ * primary context lives (do not call it again on a device after cudaDeviceReset).
+ * Like every call on a context it holds the context's lock while it reads the
+ * key and enqueues its launches. Every GPU that loads the library holds the
  * array until the process exits. All calls on a device share the one array:
  * calls whose work overlaps on the GPU (different streams, or different
  * contexts on the same device) race and corrupt each other, so order them.

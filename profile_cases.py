@@ -1,6 +1,6 @@
 """Runs each GPU kernel of the library on one small case, for profiler captures.
 
-    python -m fhetoothpaste_b200.profile_cases CASE [CASE ...]   (or: all)
+    python profile_cases.py CASE [CASE ...]   (or: all)
 
 Every case launches its kernel(s) twice: one warm-up launch, then the launch to
 capture (so `ncu -s <launches per warm-up> -c <launches>` selects the second).
