@@ -169,37 +169,161 @@ __device__ __forceinline__ uint64_t gl_fma(uint64_t acc, uint64_t a, uint64_t b)
     return gl_reduce128(r0, r1, r2, r3);
 }
 
-// hi * 2^64 + lo mod p as a 64-bit representative (not necessarily below p),
-// for any hi, lo: hi 2^64 = h0 2^64 + h1 2^96 = h0 (2^32 - 1) - h1.
-__device__ __forceinline__ uint64_t gl_fold(uint64_t hi, uint64_t lo) {
-    const uint64_t h0 = hi & 0xFFFFFFFFull, h1 = hi >> 32;
-    uint64_t t = lo - h1;
-    if (lo < h1) t -= kEps;              // t was >= 2^64 - 2^32: no underflow
-    const uint64_t u = (h0 << 32) - h0;  // h0 (2^32 - 1) < 2^64
-    uint64_t s = t + u;
-    if (s < u) s += kEps;                // wrapped s < u <= 2^64 - 2^33 + 1: no overflow
-    return s;
+// Exact sum of many 64x64-bit products, reduced once at the end. D holds the
+// sum of x0 k0 + x1 k1 2^64 in five words (d4 counts carries out of 2^128), M
+// the cross products x0 k1 + x1 k0 in three words weighted 2^32; a term costs
+// the product's eight IMADs and three carry adds, against a product chain plus
+// an eleven-instruction reduction per term for a running canonical sum. Up to
+// 2^32 terms fit (the carry words cannot wrap).
+struct WideAcc {
+    uint32_t d0, d1, d2, d3, d4, m0, m1, m2;
+};
+
+__device__ __forceinline__ void wide_zero(WideAcc& a) { a = WideAcc{0, 0, 0, 0, 0, 0, 0, 0}; }
+
+// a += x * k (x, k any 64-bit values).
+__device__ __forceinline__ void wide_mad(WideAcc& a, uint64_t x, uint64_t k) {
+    asm("{\n\t"
+        "mad.lo.cc.u32 %0, %8, %10, %0;\n\t"
+        "madc.hi.cc.u32 %1, %8, %10, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
+        "addc.u32 %4, %4, 0;\n\t"
+        "mad.lo.cc.u32 %5, %8, %11, %5;\n\t"
+        "madc.hi.cc.u32 %6, %8, %11, %6;\n\t"
+        "addc.u32 %7, %7, 0;\n\t"
+        "mad.lo.cc.u32 %5, %9, %10, %5;\n\t"
+        "madc.hi.cc.u32 %6, %9, %10, %6;\n\t"
+        "addc.u32 %7, %7, 0;\n\t"
+        "}"
+        : "+r"(a.d0), "+r"(a.d1), "+r"(a.d2), "+r"(a.d3), "+r"(a.d4), "+r"(a.m0), "+r"(a.m1), "+r"(a.m2)
+        : "r"(lo32(x)), "r"(hi32(x)), "r"(lo32(k)), "r"(hi32(k)));
 }
 
-// x * 2^K mod p for a compile-time K (canonical in and out), with shifts and
-// adds only. Every root of unity of order dividing 64 is a power of two in this
-// field (2 has order 192), so the twiddles of the first NTT levels are such
-// shifts.
+// The accumulated value mod p, canonical. V = s0 + s1 2^32 + s2 2^64 + s3 2^96
+// + s4 2^128 with s = D + M 2^32; 2^128 = -2^32 and 2^96 = -1 make
+// V = (s1:s0) - (s4:s3) + s2 (2^32 - 1): gl_reduce128 with a two-word
+// subtrahend ((s4:s3) is far below p, so adding p after a borrow keeps t >= 0).
+__device__ __forceinline__ uint64_t wide_reduce(const WideAcc& a) {
+    uint32_t s0, s1;
+    asm("{\n\t"
+        ".reg .u32 w1, w2, w3, w4, t0, t1, b, n, m;\n\t"
+        "add.cc.u32 w1, %3, %7;\n\t"
+        "addc.cc.u32 w2, %4, %8;\n\t"
+        "addc.cc.u32 w3, %5, %9;\n\t"
+        "addc.u32 w4, %6, 0;\n\t"
+        "sub.cc.u32 t0, %2, w3;\n\t"
+        "subc.cc.u32 t1, w1, w4;\n\t"
+        "subc.u32 b, 0, 0;\n\t"
+        "sub.cc.u32 t0, t0, b;\n\t"
+        "subc.u32 t1, t1, 0;\n\t"
+        "not.b32 n, w2;\n\t"
+        "add.cc.u32 %0, t0, n;\n\t"
+        "addc.cc.u32 %1, t1, w2;\n\t"
+        "addc.u32 m, 0xFFFFFFFF, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(s0), "=r"(s1)
+        : "r"(a.d0), "r"(a.d1), "r"(a.d2), "r"(a.d3), "r"(a.d4), "r"(a.m0), "r"(a.m1), "r"(a.m2));
+    return pack64(s0, s1);
+}
+
+// Multiplication by powers of two. 2 has order 192 in this field (2^96 = -1),
+// and every root of unity of order dividing 64 is a power of two, so the
+// twiddles of the first NTT levels are such multiplications. Each form below
+// takes any 64-bit x and returns a canonical residue, with shifts and adds
+// only (no IMAD).
+
+// (W1:W0) + W2 2^64 = (W1:W0) + W2 (2^32 - 1) mod p, canonical: the tail of
+// gl_reduce128 (t + the word pair (W2, ~W2), the carry picks the correction).
+__device__ __forceinline__ uint64_t gl_reduce96(uint32_t w0, uint32_t w1, uint32_t w2) {
+    uint32_t s0, s1;
+    asm("{\n\t"
+        ".reg .u32 n, m;\n\t"
+        "not.b32 n, %4;\n\t"
+        "add.cc.u32 %0, %2, n;\n\t"
+        "addc.cc.u32 %1, %3, %4;\n\t"
+        "addc.u32 m, 0xFFFFFFFF, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        "}"
+        : "=r"(s0), "=r"(s1)
+        : "r"(w0), "r"(w1), "r"(w2));
+    return pack64(s0, s1);
+}
+
+// x 2^K mod p for a compile-time K in [0, 64). For K < 32, x 2^K is the three
+// words (x0 << K, funnel(x0, x1), x1 >> (32 - K)); for K >= 32 those words of
+// x 2^(K-32) sit one word higher and the four-word reduction folds them.
 template <int K>
-__device__ __forceinline__ uint64_t gl_mul_pow2(uint64_t x) {
-    static_assert(K >= 0 && K < 192, "exponent out of range");
-    if constexpr (K >= 96) {
-        return gl_neg(gl_mul_pow2<K - 96>(x));  // 2^96 = -1
-    } else if constexpr (K == 0) {
-        return x;
-    } else if constexpr (K < 64) {
-        return gl_canon(gl_fold(x >> (64 - K), x << K));
-    } else if constexpr (K == 64) {
-        return gl_canon(gl_fold(x, 0));
+__device__ __forceinline__ uint64_t gl_shl(uint64_t x) {
+    static_assert(K >= 0 && K < 64, "shift out of range");
+    constexpr int R = K & 31;
+    const uint32_t x0 = lo32(x), x1 = hi32(x);
+    const uint32_t w0 = R ? x0 << R : x0;
+    const uint32_t w1 = R ? __funnelshift_l(x0, x1, R) : x1;
+    const uint32_t w2 = R ? x1 >> ((32 - R) & 31) : 0u;
+    if constexpr (K == 0) {
+        return gl_canon(x);
+    } else if constexpr (K < 32) {
+        return gl_reduce96(w0, w1, w2);
     } else {
-        return gl_canon(gl_fold(gl_fold(x >> (128 - K), x << (K - 64)), 0));
+        return gl_reduce128(0u, w0, w1, w2);
     }
 }
 
+// x 2^-K mod p for a compile-time K in [1, 32]. With x = h 2^K + l (l < 2^K),
+// l 2^-K = l 2^(192-K) = -l 2^(96-K) = -y 2^64 = -y (2^32 - 1), y = l 2^(32-K)
+// below 2^32 (the low word of x shifted up). So x 2^-K = A - B with
+// A = h + y and B = y 2^32; on a borrow p is added (eps taken off modulo 2^64).
+// B - A <= y (2^32 - 1) < p, so the result is canonical.
+template <int K>
+__device__ __forceinline__ uint64_t gl_shr(uint64_t x) {
+    static_assert(K >= 1 && K <= 32, "shift out of range");
+    const uint32_t x0 = lo32(x), x1 = hi32(x);
+    const uint32_t h0 = K < 32 ? __funnelshift_r(x0, x1, K & 31) : x1;
+    const uint32_t h1 = K < 32 ? x1 >> (K & 31) : 0u;
+    const uint32_t y = K < 32 ? x0 << ((32 - K) & 31) : x0;
+    uint32_t r0, r1;
+    asm("{\n\t"
+        ".reg .u32 a0, a1, d1, m;\n\t"
+        "add.cc.u32 a0, %2, %4;\n\t"
+        "addc.u32 a1, %3, 0;\n\t"
+        "sub.cc.u32 d1, a1, %4;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, a0, m;\n\t"
+        "subc.u32 %1, d1, 0;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1)
+        : "r"(h0), "r"(h1), "r"(y));
+    return pack64(r0, r1);
+}
+
+// 2^E (E taken mod 192) as +-2^SHIFT with SHIFT in (-32, 64): exponents in
+// [64, 96) and [160, 192) become negative shifts (2^E = -2^(E-96), 2^(E-192)),
+// [96, 160) a sign and E - 96.
+template <int E>
+struct Pow2 {
+    static constexpr int e = ((E % 192) + 192) % 192;
+    static constexpr bool NEG = e >= 64 && e < 160;
+    static constexpr int SHIFT = e < 64 ? e : (e < 160 ? e - 96 : e - 192);
+};
+
+// |2^E| x: x 2^SHIFT of Pow2<E> (the sign is the caller's: butterflies swap
+// their add and subtract instead of negating).
+template <int E>
+__device__ __forceinline__ uint64_t gl_pow2_mag(uint64_t x) {
+    constexpr int S = Pow2<E>::SHIFT;
+    if constexpr (S >= 0) return gl_shl<(S >= 0 ? S : 0)>(x);
+    else return gl_shr<(S < 0 ? -S : 1)>(x);
+}
+
+// x * 2^K mod p for a compile-time K (canonical out, any 64-bit x in).
+template <int K>
+__device__ __forceinline__ uint64_t gl_mul_pow2(uint64_t x) {
+    const uint64_t t = gl_pow2_mag<K>(x);
+    return Pow2<K>::NEG ? gl_neg(t) : t;
+}
 
 }  // namespace tp

@@ -169,6 +169,77 @@ __device__ __forceinline__ void inv_radix4(uint64_t (&x)[K][4], int t, const uin
     }
 }
 
+// Exponent e of the power-of-two twiddle 2^e = psi^(+-brv(2^l + i)) of level
+// l < 5, block i (the same for every N: psi^(N/2^(l+1)) = 2^g_l with g = 48,
+// 120, 156, 78, 39, and block i uses 2^(g_l (2 brv_l(i) + 1))); the inverse
+// table holds the negated exponents.
+__host__ __device__ constexpr int pow2_twiddle_exp(int level, int block, bool inverse) {
+    constexpr int g[5] = {48, 120, 156, 78, 39};
+    int r = 0;
+    for (int b = 0; b < level; ++b) r |= ((block >> b) & 1) << (level - 1 - b);
+    const int e = (g[level] * (2 * r + 1)) % 192;
+    return inverse ? (192 - e) % 192 : e;
+}
+
+// Pass 0 (levels 0 .. S-1, block 0 only) with its power-of-two twiddles as
+// shifts (gl_pow2_mag): a sign of the twiddle swaps the butterfly's add and
+// subtract. Level LV pairs registers J and J + G/2^(LV+1) with twiddle block
+// J >> (S - LV), as the table path below does.
+template <int S, int LV, int J, int K, bool LAZY>
+__device__ __forceinline__ void fwd_pow2_level(uint64_t (&x)[K][1 << S]) {
+    constexpr int G = 1 << S;
+    if constexpr (J < G) {
+        constexpr int half = G >> (LV + 1);
+        if constexpr ((J & half) == 0) {
+            constexpr int EX = pow2_twiddle_exp(LV, J >> (S - LV), false);
+#pragma unroll
+            for (int p = 0; p < K; ++p) {
+                const uint64_t u = x[p][J];
+                const uint64_t t = gl_pow2_mag<EX>(x[p][J + half]);
+                const uint64_t sum = LAZY ? gl_add_lazy(u, t) : gl_add(u, t);
+                const uint64_t dif = gl_sub(u, t);
+                x[p][J] = Pow2<EX>::NEG ? dif : sum;
+                x[p][J + half] = Pow2<EX>::NEG ? sum : dif;
+            }
+        }
+        fwd_pow2_level<S, LV, J + 1, K, LAZY>(x);
+    }
+}
+template <int S, int LV, int K, bool LAZY>
+__device__ __forceinline__ void fwd_pow2_pass(uint64_t (&x)[K][1 << S]) {
+    if constexpr (LV < S) {
+        fwd_pow2_level<S, LV, 0, K, LAZY>(x);
+        fwd_pow2_pass<S, LV + 1, K, LAZY>(x);
+    }
+}
+// Inverse (Gentleman-Sande): (u, v) -> (u + v, (u - v) 2^e); a negative
+// twiddle multiplies v - u instead.
+template <int S, int LV, int J, int K>
+__device__ __forceinline__ void inv_pow2_level(uint64_t (&x)[K][1 << S]) {
+    constexpr int G = 1 << S;
+    if constexpr (J < G) {
+        constexpr int half = G >> (LV + 1);
+        if constexpr ((J & half) == 0) {
+            constexpr int EX = pow2_twiddle_exp(LV, J >> (S - LV), true);
+#pragma unroll
+            for (int p = 0; p < K; ++p) {
+                const uint64_t u = x[p][J];
+                const uint64_t v = x[p][J + half];
+                x[p][J] = gl_add(u, v);
+                x[p][J + half] = gl_pow2_mag<EX>(Pow2<EX>::NEG ? gl_sub(v, u) : gl_sub(u, v));
+            }
+        }
+        inv_pow2_level<S, LV, J + 1, K>(x);
+    }
+}
+template <int S, int LV, int K>
+__device__ __forceinline__ void inv_pow2_pass(uint64_t (&x)[K][1 << S]) {
+    if constexpr (LV >= 0) {
+        inv_pow2_level<S, LV, 0, K>(x);
+        inv_pow2_pass<S, LV - 1, K>(x);
+    }
+}
+
 // Forward butterflies of pass P on the thread's registers (R4: use the fused
 // radix-4 form for radix-4 passes; LAZY: see ntt_forward_k).
 template <int LOGN, int P, int K, int LOGE, bool R4, bool LAZY>
@@ -177,6 +248,8 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t
     constexpr int S = SH::S(P);
     if constexpr (R4 && LOGE == 2 && S == 2) {
         fwd_radix4<LOGN, P, K, LAZY>(x, t, tw);
+    } else if constexpr (P == 0 && S == LOGE) {
+        fwd_pow2_pass<LOGE, 0, K, LAZY>(x);
     } else {
         constexpr int G = 1 << S;
         constexpr int PER = SH::E / G;
@@ -212,6 +285,8 @@ __device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][1 << LOGE], int t
     constexpr int S = SH::S(P);
     if constexpr (R4 && LOGE == 2 && S == 2) {
         inv_radix4<LOGN, P, K>(x, t, tw);
+    } else if constexpr (P == 0 && S == LOGE) {
+        inv_pow2_pass<LOGE, LOGE - 1, K>(x);
     } else {
         constexpr int G = 1 << S;
         constexpr int PER = SH::E / G;
