@@ -129,6 +129,14 @@ class GpuBlindRotator:
     def set_split(self, blocks_per_rotation: int) -> None:
         nat.check(nat.lib().tp_br_set_split(self._h, blocks_per_rotation))
 
+    @property
+    def mac_form(self) -> int:
+        """Multiply-accumulate form of the one-block kernel at tile 4 (0 row by row, 1 digit-staged)."""
+        return int(nat.lib().tp_br_get_mac_form(self._h))
+
+    def set_mac_form(self, form: int) -> None:
+        nat.check(nat.lib().tp_br_set_mac_form(self._h, form))
+
     def autotune(self, batch: int) -> tuple[int, float]:
         """Times every tile (and the two- and four-block splits) on `batch` synthetic rotations and keeps
         the fastest."""

@@ -67,10 +67,22 @@ __host__ __device__ constexpr int br_ntt_width(int logn, int variant) {
 // transforms leave no room for them (then they are read through L1).
 __host__ __device__ constexpr bool br_smem_twiddles(int logn) { return logn <= 11; }
 
-// Twiddle words per direction: psi^(+-brv(k)) for k < N, plus for radix-4
-// passes the products tw[i] tw[2i] (i < N/2) at N + i.
-__host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
-    return loge == 2 ? (1 << logn) + (1 << (logn - 1)) : (1 << logn);
+// Twiddle words per direction: psi^(+-brv(k)) for k < N, plus for the fused
+// radix-4 passes the products tw[i] tw[2i] (i < N/2) at N + i.
+__host__ __device__ constexpr int br_twiddle_words(int logn, int loge, bool r4 = true) {
+    return loge == 2 && r4 ? (1 << logn) + (1 << (logn - 1)) : (1 << logn);
+}
+
+// Fused radix-4 NTT passes (three products and a shift per two levels, see
+// ntt_block.cuh) for 4 coefficients per thread, by blocks per rotation. They
+// trade IMAD work for ALU work. With the carry-form reduction (both integer
+// pipes level) plain radix-2 butterflies are faster everywhere but in the BMMP
+// four-block kernel, rotations/s: BMMP N = 2048 7808 vs 7615 (one block), 81.0
+// vs 79.0 (two blocks, batch 1), 100.7 vs 102.4 (four blocks, batch 1); CGGI
+// ternary N = 2048 7275 vs 6885, binary N = 1024 18.8k vs 17.5k. (With the
+// earlier 16-instruction reduction radix-4 was faster for BMMP: 5570 vs 5438.)
+__host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int blocks) {
+    return loge == 2 && variant == kBmmpBinary && blocks == 4;
 }
 
 // Key rows staged in shared memory: each thread copies its own slots of the
@@ -82,7 +94,7 @@ __host__ __device__ constexpr int br_twiddle_words(int logn, int loge) {
 // so did staging part of each row there (two components, the rest read from L2
 // at use: ternary 1918 vs 1978; BMMP 2939 vs 2889, within run-to-run spread).
 __host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge) {
-    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
+    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge, br_fused_radix4(loge, variant, 1)) : 0) +
            (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
            1024;  // LWE area budget for the plan; the host adds the real size
 }
@@ -93,13 +105,26 @@ __host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int lo
     return (br_base_words(logn, variant, loge) + br_stage_words(logn, variant)) * 8 <= 227u * 1024u;
 }
 
+// Digit-staged multiply-accumulate (template parameter DL = the digit count l,
+// 4 coefficients per thread): each iteration transforms all 2l gadget digits
+// first, keeping rows 0..2l-2 in shared memory (each thread its own slots) and
+// the last in registers, then sums every output word over the 2l rows exactly
+// (WideAcc) and reduces it once, reading the key words straight from L2. No
+// key row stage. A running canonical sum instead pays a reduction per row.
+__host__ __device__ constexpr size_t br_digit_stage_words(int logn, int dl) {
+    return dl > 0 ? (size_t)(2 * dl - 1) << logn : 0;
+}
+
 // Shared memory of one block, in words: twiddles (both directions, if kept
 // there), two exchange areas of width*N words, the accumulator (2N), the key
-// row stage (C*N, if used), the LWE vector (n+1, rounded up to an even count).
-__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge) {
-    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge) : 0) +
+// row stage (C*N, if used) or the digit stage (DL > 0), the LWE vector (n+1,
+// rounded up to an even count).
+__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge, int dl = 0) {
+    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge, br_fused_radix4(loge, variant, 1)) : 0) +
            (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
-           (br_key_prefetch(logn, variant, loge) ? br_stage_words(logn, variant) : 0) + ((n + 2) & ~1u);
+           (dl > 0 ? br_digit_stage_words(logn, dl)
+                   : (br_key_prefetch(logn, variant, loge) ? br_stage_words(logn, variant) : 0)) +
+           ((n + 2) & ~1u);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
@@ -120,17 +145,6 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
     return __ldg(psi_pow + ((ek * a) & (2u * (1u << LOGN) - 1u)));
 }
 
-// Fused radix-4 NTT passes (three products and a shift per two levels, see
-// ntt_block.cuh) for 4 coefficients per thread, by blocks per rotation. They
-// trade IMAD work for ALU work. With the carry-form reduction (both integer
-// pipes level) plain radix-2 butterflies are faster everywhere but in the BMMP
-// four-block kernel, rotations/s: BMMP N = 2048 7808 vs 7615 (one block), 81.0
-// vs 79.0 (two blocks, batch 1), 100.7 vs 102.4 (four blocks, batch 1); CGGI
-// ternary N = 2048 7275 vs 6885, binary N = 1024 18.8k vs 17.5k. (With the
-// earlier 16-instruction reduction radix-4 was faster for BMMP: 5570 vs 5438.)
-__host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int blocks) {
-    return loge == 2 && variant == kBmmpBinary && blocks == 4;
-}
 
 // Coefficients per thread (log2) a context starts with; tp_br_set_tile and
 // tp_br_autotune change it. 4 per thread measured faster than 8 for every
@@ -152,7 +166,7 @@ __host__ __device__ constexpr int br_min_blocks(int logn, int variant, int loge)
     return loge == 2 ? (logn <= 10 ? 2 : 1) : ((logn >= 11 || variant == kBmmpBinary) ? 1 : 2);
 }
 
-template <int LOGN, int VARIANT, int LOGE>
+template <int LOGN, int VARIANT, int LOGE, int DL = 0>
 __global__ void __launch_bounds__((1 << LOGN) >> LOGE, br_min_blocks(LOGN, VARIANT, LOGE))
 br_kernel(const BrKernelParams prm) {
     using SH = NttShape<LOGN, LOGE>;
@@ -166,14 +180,16 @@ br_kernel(const BrKernelParams prm) {
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
     constexpr bool R4 = br_fused_radix4(LOGE, VARIANT, 1);
-    constexpr bool PF = br_key_prefetch(LOGN, VARIANT, LOGE);
+    constexpr bool DS = DL > 0;              // digit-staged multiply-accumulate (prm.digits == DL)
+    constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE);
+    static_assert(!DS || (LOGE == 2 && K == 1), "the digit stage runs with 4 coefficients per thread");
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
     const uint64_t* tw_f = prm.tw_fwd;
     const uint64_t* tw_i = prm.tw_inv;
     if constexpr (TW_SMEM) {
-        constexpr int TWW = br_twiddle_words(LOGN, LOGE);
+        constexpr int TWW = br_twiddle_words(LOGN, LOGE, R4);
         for (int i = threadIdx.x; i < TWW; i += T) {
             base[i] = prm.tw_fwd[i];
             base[TWW + i] = prm.tw_inv[i];
@@ -186,7 +202,9 @@ br_kernel(const BrKernelParams prm) {
     uint64_t* xbuf1 = base + K * N;
     uint64_t* acc = base + 2 * K * N;        // [(h*E + j)*T + t], canonical, NTT domain
     uint64_t* kst = acc + 2 * N;             // key row stage, device layout of one row (C*N words)
-    uint64_t* lwe_s = kst + (PF ? C * N : 0);
+    // digit stage (DS): row r < 2L-1 of this thread's slot pair jp at xs + r*N + (jp*T + t)*2
+    uint64_t* xs = acc + 2 * N;
+    uint64_t* lwe_s = kst + (PF ? C * N : (DS ? (2 * DL - 1) * N : 0));
 
     const int t = threadIdx.x;
     const uint32_t n = prm.n;
@@ -247,12 +265,15 @@ br_kernel(const BrKernelParams prm) {
             }
             const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
 
-            // MAC accumulators (canonical: every update is a gl_fma)
-            uint64_t o[C][E];
+            // MAC accumulators (canonical: every update is a gl_fma); the digit-staged
+            // form sums per slot pair after the digit loop instead
+            uint64_t o[DS ? 1 : C][DS ? 1 : E];
+            if constexpr (!DS) {
 #pragma unroll
-            for (int c = 0; c < C; ++c)
+                for (int c = 0; c < C; ++c)
 #pragma unroll
-                for (int j = 0; j < E; ++j) o[c][j] = 0;
+                    for (int j = 0; j < E; ++j) o[c][j] = 0;
+            }
 
             // Backward NTT of an accumulator half into corrected coefficients. Binary
             // CGGI decomposes (X^{-a} - 1) * acc (mux_operator.cpp:144-150); the other
@@ -279,6 +300,18 @@ br_kernel(const BrKernelParams prm) {
                 finish_half(cx[0]);
                 finish_half(cx[1]);
             }
+            uint64_t x[K][E];  // digit transform of the row last processed
+            // digit-staged form: the key words of one (slot pair jp, component c) group, all
+            // 2L rows; each thread's 16 bytes at ((c*E/2 + jp)*T + t)*2 of row r
+            constexpr int R2 = 2 * (DL > 0 ? DL : 1);
+            constexpr int NG = C * (E / 2);
+            auto kload = [&](int jp, int c, ulonglong2 (&kv)[R2]) {
+#pragma unroll
+                for (int r = 0; r < R2; ++r)
+                    kv[r] = __ldg(reinterpret_cast<const ulonglong2*>(
+                        kit + (uint64_t)r * (N * C) + ((c * (E / 2) + jp) * T + t) * 2));
+            };
+            ulonglong2 kv[2][R2];
 #pragma unroll 1
             for (uint32_t r = 0; r < 2 * L; r += K) {
                 if constexpr (PF && K == 1) {
@@ -301,7 +334,6 @@ br_kernel(const BrKernelParams prm) {
                         finish_half(cx[0]);
                     }
                 }
-                uint64_t x[K][E];
 #pragma unroll
                 for (int p = 0; p < K; ++p) {
                     const uint32_t rr = r + p;
@@ -318,41 +350,50 @@ br_kernel(const BrKernelParams prm) {
                     }
                 }
                 ntt_forward_k<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
-                if constexpr (PF && K == 1) cp_async_wait_all();
+                if constexpr (DS) {
+                    // rows before the last wait in the stage (this thread's own slots: no barrier)
+                    if (r + 1 < 2 * L) {
 #pragma unroll
-                for (int p = 0; p < K; ++p) {
-                    const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
+                        for (int jp = 0; jp < E / 2; ++jp)
+                            *reinterpret_cast<ulonglong2*>(xs + r * N + (jp * T + t) * 2) =
+                                make_ulonglong2(x[0][2 * jp], x[0][2 * jp + 1]);
+                    }
+                } else {
+                    if constexpr (PF && K == 1) cp_async_wait_all();
 #pragma unroll
-                    for (int c = 0; c < C; ++c) {
+                    for (int p = 0; p < K; ++p) {
+                        const uint64_t* kr = kit + (uint64_t)(r + p) * (N * C);
 #pragma unroll
-                        for (int jp = 0; jp < E / 2; ++jp) {
-                            const int ko = ((c * (E / 2) + jp) * T + t) * 2;
-                            const ulonglong2 kv = (PF && K == 1)
-                                                      ? *reinterpret_cast<const ulonglong2*>(kst + ko)
-                                                      : __ldg(reinterpret_cast<const ulonglong2*>(kr + ko));
-                            o[c][2 * jp] = gl_fma(o[c][2 * jp], x[p][2 * jp], kv.x);
-                            o[c][2 * jp + 1] = gl_fma(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
+                        for (int c = 0; c < C; ++c) {
+#pragma unroll
+                            for (int jp = 0; jp < E / 2; ++jp) {
+                                const int ko = ((c * (E / 2) + jp) * T + t) * 2;
+                                const ulonglong2 kv = (PF && K == 1)
+                                                          ? *reinterpret_cast<const ulonglong2*>(kst + ko)
+                                                          : __ldg(reinterpret_cast<const ulonglong2*>(kr + ko));
+                                o[c][2 * jp] = gl_fma(o[c][2 * jp], x[p][2 * jp], kv.x);
+                                o[c][2 * jp + 1] = gl_fma(o[c][2 * jp + 1], x[p][2 * jp + 1], kv.y);
+                            }
                         }
                     }
                 }
             }
 
-            // Accumulator update.
-#pragma unroll
-            for (int j = 0; j < E; ++j) {
+            // Accumulator update of slot j from its C key-component sums oj[c].
+            auto update = [&](int j, const uint64_t* oj) {
                 const uint32_t ek = slot_exponent<LOGN>(E * t + j);
                 uint64_t ua = acc_ld(0, j);
                 uint64_t ub = acc_ld(1, j);
                 if constexpr (VARIANT == kCggiBinary) {
                     // acc += ExtProd (mux_operator.cpp:151)
-                    ua = gl_add(ua, o[0][j]);
-                    ub = gl_add(ub, o[1][j]);
+                    ua = gl_add(ua, oj[0]);
+                    ub = gl_add(ub, oj[1]);
                 } else if constexpr (VARIANT == kCggiTernary) {
                     // acc += (X^{-a}-1) ExtProd(lo) + (X^{a}-1) ExtProd(hi) (mux_operator.cpp:188-200)
                     const uint64_t mp = gl_sub(mono<LOGN>(prm.psi_pow, ek, 2u * N - a0), 1);
                     const uint64_t mn = gl_sub(mono<LOGN>(prm.psi_pow, ek, a0), 1);
-                    ua = gl_fma(gl_fma(ua, o[0][j], mp), o[2][j], mn);
-                    ub = gl_fma(gl_fma(ub, o[1][j], mp), o[3][j], mn);
+                    ua = gl_fma(gl_fma(ua, oj[0], mp), oj[2], mn);
+                    ub = gl_fma(gl_fma(ub, oj[1], mp), oj[3], mn);
                 } else {
                     // weights X^{a0}-1, X^{a1}-1, X^{a0+a1}-X^{a0}-X^{a1}+1
                     // (bmmp_blind_rotation.cpp:280-323; MultiMux mux_operator.cpp:274-291)
@@ -362,11 +403,52 @@ br_kernel(const BrKernelParams prm) {
                     const uint64_t w0 = gl_sub(m0, 1);
                     const uint64_t w1 = gl_sub(m1, 1);
                     const uint64_t w2 = gl_add(gl_sub(gl_sub(m2, m0), m1), 1);
-                    ua = gl_fma(gl_fma(gl_fma(ua, o[0][j], w0), o[2][j], w1), o[4][j], w2);
-                    ub = gl_fma(gl_fma(gl_fma(ub, o[1][j], w0), o[3][j], w1), o[5][j], w2);
+                    ua = gl_fma(gl_fma(gl_fma(ua, oj[0], w0), oj[2], w1), oj[4], w2);
+                    ub = gl_fma(gl_fma(gl_fma(ub, oj[1], w0), oj[3], w1), oj[5], w2);
                 }
                 acc_st(0, j, ua);
                 acc_st(1, j, ub);
+            };
+
+            if constexpr (DS) {
+                // Every slot's C sums over the 2L rows, exact, one reduction each. The key
+                // words of component c, slot pair jp, row r are the thread's 16 bytes at
+                // ((c*E/2 + jp)*T + t)*2 of row r; all 2L rows of one (jp, c) group are
+                // requested together, one group ahead of their use.
+                kload(0, 0, kv[0]);
+#pragma unroll
+                for (int jp = 0; jp < E / 2; ++jp) {
+                    uint64_t oj[2][C];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        const int g = jp * C + c;
+                        if (g + 1 < NG) kload((g + 1) / C, (g + 1) % C, kv[(g + 1) & 1]);
+                        const ulonglong2(&kc)[R2] = kv[g & 1];
+                        WideAcc s0, s1;
+                        wide_zero(s0);
+                        wide_zero(s1);
+#pragma unroll
+                        for (int r = 0; r < R2 - 1; ++r) {
+                            const ulonglong2 xv = *reinterpret_cast<const ulonglong2*>(xs + r * N + (jp * T + t) * 2);
+                            wide_mad(s0, xv.x, kc[r].x);
+                            wide_mad(s1, xv.y, kc[r].y);
+                        }
+                        wide_mad(s0, x[0][2 * jp], kc[R2 - 1].x);
+                        wide_mad(s1, x[0][2 * jp + 1], kc[R2 - 1].y);
+                        oj[0][c] = wide_reduce(s0);
+                        oj[1][c] = wide_reduce(s1);
+                    }
+                    update(2 * jp, oj[0]);
+                    update(2 * jp + 1, oj[1]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < E; ++j) {
+                    uint64_t oj[C];
+#pragma unroll
+                    for (int c = 0; c < C; ++c) oj[c] = o[c][j];
+                    update(j, oj);
+                }
             }
         }
 

@@ -215,6 +215,10 @@ struct tp_br_ctx {
     int grid_caps[4] = {};        // resident blocks on the device, by loge
     size_t smem[4] = {};          // dynamic shared memory bytes, by loge
     int split = 1;                // thread blocks per rotation (2, 4: cluster kernels, tile 4 only)
+    int mac = 0;                  // multiply-accumulate form of the one-block kernel at tile 4 (TP_MAC_*)
+    const void* ds_kernel = nullptr;  // digit-staged one-block kernel (digits 3 or 4, N <= 2048)
+    size_t ds_smem = 0;
+    int ds_cap = 0;               // its resident blocks on the device (0: unavailable)
     const void* pair_kernel = nullptr;
     size_t pair_smem = 0;
     int pair_cap = 0;             // resident two-CTA clusters on the device (0: unavailable)
@@ -338,6 +342,24 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         c->grid_caps[lg] = per_sm * sm_count(device);
     }
     c->loge = tp::br_default_loge(c->logn, p->variant);
+    if (p->digits == 3 || p->digits == 4) {
+        // digit-staged kernel: optional, a parameter set it does not fit keeps the row-by-row form
+        const void* k = tp::br_kernel_lookup(c->logn, p->variant, 2, (int)p->digits);
+        const size_t smem = tp::br_smem_words(c->logn, p->variant, p->lwe_dim, 2, (int)p->digits) * 8;
+        int per_sm = 0;
+        cudaError_t de = k && smem <= 227u * 1024u
+                             ? cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                             : cudaErrorInvalidValue;
+        if (de == cudaSuccess) de = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(N >> 2), smem);
+        if (de == cudaSuccess && per_sm > 0) {
+            c->ds_kernel = k;
+            c->ds_smem = smem;
+            c->ds_cap = per_sm * sm_count(device);
+            c->mac = TP_MAC_DIGIT_STAGED;
+        } else if (k) {
+            cudaGetLastError();  // clear the optional probe's error
+        }
+    }
     for (int split = 2; split <= 4; split += 2) {
         // two- and four-CTA cluster kernels; optional: a parameter set one does not fit keeps its cap 0
         const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant, split);
@@ -474,6 +496,20 @@ tp_status tp_br_set_split(tp_br_ctx* c, uint32_t blocks_per_rotation) {
 
 uint32_t tp_br_get_split(const tp_br_ctx* c) { return c ? (uint32_t)c->split : 0u; }
 
+tp_status tp_br_set_mac_form(tp_br_ctx* c, uint32_t form) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (form != TP_MAC_ROWWISE && form != TP_MAC_DIGIT_STAGED)
+        return fail(TP_ERR_PARAM, "unknown multiply-accumulate form %u", form);
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (form == TP_MAC_DIGIT_STAGED && !c->ds_kernel)
+        return fail(TP_ERR_PARAM, "the digit-staged kernel is not built for this parameter set on this device "
+                                  "(digits 3 or 4, N <= 2048, shared memory permitting)");
+    c->mac = (int)form;
+    return TP_OK;
+}
+
+uint32_t tp_br_get_mac_form(const tp_br_ctx* c) { return c ? (uint32_t)c->mac : 0u; }
+
 tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_thread, double* best_rotations_per_s) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
     if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
@@ -518,13 +554,18 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     }
     std::lock_guard<std::mutex> lk(c->mu);
     int best_split = c->split;
-    struct Cand { int loge, split; };
-    const Cand cands[] = {{3, 1}, {2, 1}, {2, 2}, {2, 4}};
+    int best_mac = c->mac;
+    // tile (coefficients per thread), blocks per rotation, multiply-accumulate form
+    struct Cand { int loge, split, mac; };
+    const Cand cands[] = {{3, 1, TP_MAC_ROWWISE}, {2, 1, TP_MAC_ROWWISE}, {2, 1, TP_MAC_DIGIT_STAGED},
+                          {2, 2, TP_MAC_ROWWISE}, {2, 4, TP_MAC_ROWWISE}};
     for (const Cand& cd : cands) {
         if ((cd.split == 2 && c->pair_cap == 0) || (cd.split == 4 && c->quad_cap == 0)) continue;
+        if (cd.mac == TP_MAC_DIGIT_STAGED && !c->ds_kernel) continue;
         s = br_retile(c, cd.loge);
         if (s != TP_OK) break;
         c->split = cd.split;
+        c->mac = cd.mac;
         for (int rep = 0; rep < 3 && s == TP_OK; ++rep) {  // one warm-up, two timed
             if (rep == 1) cudaEventRecord(e0, st);
             s = tp_br_blind_rotate_batch(c, tb, d_res, d_lwe, n + 1, d_acc, 0, 0, st);
@@ -543,11 +584,15 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
             best_rate = rate;
             best = cd.loge;
             best_split = cd.split;
+            best_mac = cd.mac;
         }
     }
     c->split = 1;
     if (s == TP_OK) s = br_retile(c, best);
-    if (s == TP_OK) c->split = best_split;
+    if (s == TP_OK) {
+        c->split = best_split;
+        c->mac = best_mac;
+    }
     cleanup();
     if (s != TP_OK) return s;
     if (best_coef_per_thread) *best_coef_per_thread = 1u << best;
@@ -2112,11 +2157,17 @@ tp_status set_error(tp_status s, const char* fmt, ...) {
     return s;
 }
 
+// The one-block kernel a launch uses: the digit-staged form when selected and
+// the tile is 4 coefficients per thread, else the row-by-row form of the tile.
+static bool br_uses_ds(const tp_br_ctx* c) {
+    return c->loge == 2 && c->mac == TP_MAC_DIGIT_STAGED && c->ds_kernel;
+}
+
 uint64_t br_concurrency(const tp_br_ctx* c, int split) {
     if (!c) return 0;
     if (split == 2) return c->loge == 2 ? (uint64_t)c->pair_cap : 0;
     if (split == 4) return c->loge == 2 ? (uint64_t)c->quad_cap : 0;
-    return (uint64_t)c->grid_caps[c->loge];
+    return br_uses_ds(c) ? (uint64_t)c->ds_cap : (uint64_t)c->grid_caps[c->loge];
 }
 
 tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
@@ -2152,9 +2203,10 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
         tp::note_launch();
         return TP_OK;
     }
-    const unsigned grid = (unsigned)std::min<uint64_t>(batch, (uint64_t)c->grid_caps[c->loge]);
-    TP_CUDA(cudaLaunchKernel(c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge), args,
-                             c->smem[c->loge], (cudaStream_t)stream));
+    const bool ds = br_uses_ds(c);
+    const unsigned grid = (unsigned)std::min<uint64_t>(batch, br_concurrency(c, 1));
+    TP_CUDA(cudaLaunchKernel(ds ? c->ds_kernel : c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge),
+                             args, ds ? c->ds_smem : c->smem[c->loge], (cudaStream_t)stream));
     tp::note_launch();
     return TP_OK;
 }

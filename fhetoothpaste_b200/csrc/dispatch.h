@@ -3,17 +3,17 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_7(int variant, int loge);
+const void* br_kernel_ptr_7(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_7(bool forward);
-const void* br_kernel_ptr_8(int variant, int loge);
+const void* br_kernel_ptr_8(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_8(bool forward);
-const void* br_kernel_ptr_9(int variant, int loge);
+const void* br_kernel_ptr_9(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_9(bool forward);
-const void* br_kernel_ptr_10(int variant, int loge);
+const void* br_kernel_ptr_10(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_10(bool forward);
-const void* br_kernel_ptr_11(int variant, int loge);
+const void* br_kernel_ptr_11(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_11(bool forward);
-const void* br_kernel_ptr_12(int variant, int loge);
+const void* br_kernel_ptr_12(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_12(bool forward);
 const void* br_pair_kernel_ptr_7(int variant, int split);
 const void* br_pair_kernel_ptr_8(int variant, int split);
@@ -28,14 +28,16 @@ const void* ks_kernel_ptr_10(int mode, int loge);
 const void* ks_kernel_ptr_11(int mode, int loge);
 const void* ks_kernel_ptr_12(int mode, int loge);
 
-inline const void* br_kernel_lookup(int logn, int variant, int loge) {
+// One-block rotation kernel; dl = 0: multiply-accumulate row by row, dl = 3 or
+// 4: the digit-staged form for that digit count (nullptr where not built).
+inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0) {
     switch (logn) {
-        case 7: return br_kernel_ptr_7(variant, loge);
-        case 8: return br_kernel_ptr_8(variant, loge);
-        case 9: return br_kernel_ptr_9(variant, loge);
-        case 10: return br_kernel_ptr_10(variant, loge);
-        case 11: return br_kernel_ptr_11(variant, loge);
-        case 12: return br_kernel_ptr_12(variant, loge);
+        case 7: return br_kernel_ptr_7(variant, loge, dl);
+        case 8: return br_kernel_ptr_8(variant, loge, dl);
+        case 9: return br_kernel_ptr_9(variant, loge, dl);
+        case 10: return br_kernel_ptr_10(variant, loge, dl);
+        case 11: return br_kernel_ptr_11(variant, loge, dl);
+        case 12: return br_kernel_ptr_12(variant, loge, dl);
         default: return nullptr;
     }
 }

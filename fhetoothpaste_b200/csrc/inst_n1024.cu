@@ -8,7 +8,19 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_10(int variant, int loge) {
+const void* br_kernel_ptr_10(int variant, int loge, int dl) {
+    if (dl == 3 || dl == 4) {  // digit-staged multiply-accumulate, 4 coefficients per thread
+        if (loge != 2) return nullptr;
+        switch (variant) {
+            case kCggiBinary: return dl == 3 ? (const void*)br_kernel<10, kCggiBinary, 2, 3>
+                                             : (const void*)br_kernel<10, kCggiBinary, 2, 4>;
+            case kCggiTernary: return dl == 3 ? (const void*)br_kernel<10, kCggiTernary, 2, 3>
+                                              : (const void*)br_kernel<10, kCggiTernary, 2, 4>;
+            default: return dl == 3 ? (const void*)br_kernel<10, kBmmpBinary, 2, 3>
+                                    : (const void*)br_kernel<10, kBmmpBinary, 2, 4>;
+        }
+    }
+    if (dl != 0) return nullptr;
     if (loge == 2) {
         switch (variant) {
             case kCggiBinary: return (const void*)br_kernel<10, kCggiBinary, 2>;

@@ -8,7 +8,8 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_12(int variant, int loge) {
+const void* br_kernel_ptr_12(int variant, int loge, int dl) {
+    if (dl != 0) return nullptr;  // the digit stage does not fit one SM's shared memory at this N
     if (loge == 2) {
         switch (variant) {
             case kCggiBinary: return (const void*)br_kernel<12, kCggiBinary, 2>;

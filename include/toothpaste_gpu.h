@@ -123,11 +123,23 @@ uint32_t tp_br_get_tile(const tp_br_ctx* ctx);
 tp_status tp_br_set_split(tp_br_ctx* ctx, uint32_t blocks_per_rotation);
 uint32_t tp_br_get_split(const tp_br_ctx* ctx);
 
-/* Times every tile (8 or 4 coefficients per thread, and 4 with two or four
- * blocks per rotation) on up to two waves of `batch` synthetic rotations with the uploaded
- * key, keeps the fastest and reports it (either output may be NULL; the split
- * is read back with tp_br_get_split). Blocks until done; the context must be
- * idle. */
+/* Multiply-accumulate form of the one-block kernel at 4 coefficients per thread.
+ * TP_MAC_ROWWISE keeps a canonical running sum per output word, one gadget row at
+ * a time (the next key row staged in shared memory while the digit is transformed);
+ * TP_MAC_DIGIT_STAGED transforms all 2l digits first and sums each output word over
+ * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048; the default
+ * where it is built). Both give the same words. Project-specific tuning (no
+ * reference counterpart); tp_br_autotune chooses between them. */
+enum { TP_MAC_ROWWISE = 0, TP_MAC_DIGIT_STAGED = 1 };
+tp_status tp_br_set_mac_form(tp_br_ctx* ctx, uint32_t form);
+uint32_t tp_br_get_mac_form(const tp_br_ctx* ctx);
+
+/* Times every launch form (8 or 4 coefficients per thread; at 4 also the
+ * digit-staged multiply-accumulate and two or four blocks per rotation) on up to
+ * two waves of `batch` synthetic rotations with the uploaded key, keeps the
+ * fastest and reports it (either output may be NULL; the split and form are read
+ * back with tp_br_get_split / tp_br_get_mac_form). Blocks until done; the context
+ * must be idle. */
 tp_status tp_br_autotune(tp_br_ctx* ctx, uint64_t batch, uint32_t* best_coef_per_thread,
                          double* best_rotations_per_s);
 

@@ -237,6 +237,30 @@ def test_tile_of_four_matches_reference(native, oracle, golden, name):
             np.testing.assert_array_equal(got, expect[idx], err_msg=f"tile {tile}")
 
 
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_both_accumulation_forms_match_reference(native, oracle, golden, name):
+    """Tile 4 with the row-by-row multiply-accumulate and, where it is built (3 or 4 digits,
+    N <= 2048), the digit-staged form that sums every output word over all rows before one
+    reduction."""
+    from fhetoothpaste_b200 import _native
+    case, rot = rotator(oracle, golden, name)
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    rot.set_tile(4)
+    staged = case["digits"] in (3, 4) and case["N"] <= 2048
+    assert rot.mac_form == (1 if staged else 0)  # the staged form is the default where it is built
+    for form in (0, 1):
+        if form == 1 and not staged:
+            with pytest.raises(_native.TpError):
+                rot.set_mac_form(1)
+            continue
+        rot.set_mac_form(form)
+        for oc in (0, 1):
+            idx = [i for i, c in enumerate(coefs) if c == oc]
+            got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+            np.testing.assert_array_equal(got, expect[idx], err_msg=f"form {form}")
+
+
 def test_autotune_picks_a_tile_and_keeps_results(native, oracle, golden):
     name = "small_bmmp_n512"
     case, rot = rotator(oracle, golden, name)

@@ -37,6 +37,16 @@ def test_batch_order_does_not_matter(native, cuda, setup):
     np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[perm], accs[perm]), out[perm])
 
 
+def test_row_by_row_form_gives_the_same_words(native, cuda, setup):
+    rot, _, lwes, accs, out = setup
+    assert rot.mac_form == 1
+    rot.set_mac_form(0)
+    try:
+        np.testing.assert_array_equal(rot.blind_rotate_batch_host(lwes[:600], accs[:600]), out[:600])
+    finally:
+        rot.set_mac_form(1)
+
+
 def test_two_blocks_and_graph_give_the_same_words(native, cuda, setup):
     torch = cuda
     rot, _, lwes, accs, out = setup
