@@ -153,6 +153,23 @@ def traffic_from_profiles(workload: str):
     return d.get("dram_bytes_per_launch"), d.get("source")
 
 
+def bench_config(wl: str, batch: int, n: int) -> dict:
+    """The `config` object of the JSON line, the same keys in both arms."""
+    variant, N, _, bl, l, _ = WORKLOADS[wl]
+    key_bytes = BlindRotationKeyWords(variant, N, n, l) * 8
+    return {"workload": DESCR[wl], "batch_per_gpu": batch, "ring_dim": N, "lwe_dim": n, "gadget": f"2^{bl} l={l}",
+            "output": "NTT domain",
+            "inputs": "seeded synthetic LWEs + per-ciphertext 16-entry LUT test polynomials",
+            "l2": f"inputs larger than L2: {key_bytes / 2**20:.0f} MiB key streamed per launch"}
+
+
+def BlindRotationKeyWords(variant: int, N: int, n: int, l: int) -> int:
+    """Words of the reference's m_brk: per iteration group 2l rows of G RGSWs x [A|B]."""
+    groups = n // 2 if variant == 2 else n
+    g = 1 if variant == 0 else (2 if variant == 1 else 3)
+    return groups * g * 4 * N * l
+
+
 def cpu_reference_sample(variant, N, n, bl, l, lwes, accs, seconds_target=15.0):
     """Times the reference library's CPU blind rotation on a bounded sample,
     one rotator per host thread. Returns (BR/s, threads, rotations, seconds)."""
@@ -210,8 +227,7 @@ def run_reference(args, wl):
             vals.append((v, threads, count, secs))
     v = statistics.median([x[0] for x in vals])
     threads, count = vals[-1][1], vals[-1][2]
-    cfg = {"workload": DESCR[wl], "batch": batch, "ring_dim": N, "lwe_dim": n, "gadget": f"2^{bl} l={l}",
-           "inputs": "seeded synthetic LWEs + per-ciphertext LUT test polynomials"}
+    cfg = bench_config(wl, batch, n)
     line = {"impl": "reference", "metric": "blind rotations/sec", "value": round(v, 3), "unit": "BR/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(statistics.median([x[3] for x in vals]) * 1e3, 3),
@@ -263,6 +279,8 @@ def bmmp_batch_sweep(device: int) -> dict:
     lw_all = torch.from_numpy(lwe_inputs(N, n, max(BMMP_BATCHES), 33).view(np.int64)).cuda()
     ac = torch.from_numpy(ident.view(np.int64)).cuda()
     res = torch.empty((max(BMMP_BATCHES), 2 * N), dtype=torch.int64, device="cuda")
+    key = _uniform_key(ctx.key_words(), 31)
+    lw_host = lwe_inputs(N, n, max(BMMP_BATCHES), 33)
     for b in BMMP_BATCHES:
         coef, _ = rot.autotune(b)
         g = rot.capture_batch(res.data_ptr(), lw_all.data_ptr(), n + 1, ac.data_ptr(), 0, b)
@@ -270,7 +288,16 @@ def bmmp_batch_sweep(device: int) -> dict:
         ms = _timed(torch, lambda: g.launch(stream), 2, reps, stream)
         g.close()
         out[str(b)] = {"BR_per_s": round(b / (ms * 1e-3), 1), "ms_per_launch": round(ms, 3),
-                       "tile": {"coef_per_thread": coef, "blocks_per_rotation": rot.split}}
+                       "tile": {"coef_per_thread": coef, "blocks_per_rotation": rot.split,
+                                "mac_form": rot.mac_form}}
+        if b >= 2048:
+            # sampled parity of the timed launch's results: the oracle with the same key words
+            from oracle.oracle import Oracle
+            idx = sorted({0, 147, 148, b // 2, b - 1})
+            got = res[idx].cpu().numpy().view(np.uint64)
+            want = Oracle().blind_rotate_many(2, N, n, 16, 4, key, lw_host[idx],
+                                              np.repeat(ident[None, :], len(idx), axis=0), False, 8)
+            out[str(b)]["sampled_parity"] = {"ciphertexts": idx, "equal_to_oracle": bool(np.array_equal(got, want))}
     rot.check(stream)
     rot.close()
     return out
@@ -529,7 +556,7 @@ def main():
             _native.ctypes.cast(lw_p.data_ptr(), _native.U64P), n + 1,
             _native.ctypes.cast(ac_p.data_ptr(), _native.U64P), 2 * N, 0, stream))
 
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = args.steps
     for _ in range(1):
         e2e_step()
     barrier()
@@ -584,35 +611,37 @@ def main():
     traffic, tsrc = traffic_from_profiles(wl)
     key_bytes = kw * 8
 
+    plain = {"value": round(1e3 / plain_ms, 3), "unit": "BR/s", "ms_per_rotation": round(plain_ms, 3),
+             "batched_over_plain": round(value / world / (1e3 / plain_ms), 1),
+             "two_blocks": {"value": round(1e3 / plain2_ms, 3), "ms_per_rotation": round(plain2_ms, 3),
+                            "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)},
+             "four_blocks": None if plain4_ms is None else {
+                 "value": round(1e3 / plain4_ms, 3), "ms_per_rotation": round(plain4_ms, 3),
+                 "batched_over_plain": round(value / world / (1e3 / plain4_ms), 1)}}
+    imad8 = imad.value / 8  # 8 IMAD issues per 64x64 modmul at the measured IMAD rate
     line = {
         "metric": "blind rotations/sec", "value": round(value, 2), "unit": "BR/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (mod p)", "data": "synthetic",
-        "config": {"workload": DESCR[wl], "batch_per_gpu": batch, "ring_dim": N, "lwe_dim": n,
-                   "gadget": f"2^{bl} l={l}", "output": "NTT domain", "launch": "CUDA graph, one kernel per step",
-                   "l2": f"inputs larger than L2: {key_bytes / 2**20:.0f} MiB key streamed per launch",
-                   "key": "uniform random key words (timing does not depend on key values)"},
-        "e2e": {"value": round(e2e_val, 2), "unit": "BR/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
-        "plain": {"value": round(1e3 / plain_ms, 3), "unit": "BR/s", "ms_per_rotation": round(plain_ms, 3),
-                  "batched_over_plain": round(value / world / (1e3 / plain_ms), 1),
-                  "two_blocks": {"value": round(1e3 / plain2_ms, 3), "ms_per_rotation": round(plain2_ms, 3),
-                                 "batched_over_plain": round(value / world / (1e3 / plain2_ms), 1)},
-                  "four_blocks": None if plain4_ms is None else {
-                      "value": round(1e3 / plain4_ms, 3), "ms_per_rotation": round(plain4_ms, 3),
-                      "batched_over_plain": round(value / world / (1e3 / plain4_ms), 1)}},
         "gpu_launches": int(timed_launches),
-        "gpu_launches_detail": {"timed_region": int(timed_launches), "e2e_timed_region": int(e2e_launches),
-                                "counted_by": "tp_kernel_launches() deltas (graph replays count their kernels)"},
+        "config": bench_config(wl, batch, n),
         "roofline": {"bound": "int32", "achieved": round(achieved / 1e9, 1), "peak": round(prod.value / 1e9, 1),
                      "unit": "Gmodmul/s", "frac": round(achieved / prod.value, 4), "traffic": traffic,
                      "traffic_source": tsrc,
                      "peak_source": "measured 64x64->128 IMAD-chain product rate of this GPU (tp_measure_int_peak)",
+                     "frac_imad8": round(achieved / imad8, 4),
+                     "peak_imad8": round(imad8 / 1e9, 1),
+                     "imad8_source": "measured mad.lo.u32 rate / 8 IMAD per modmul (the scope table's formula)",
                      "imad_per_s": round(imad.value / 1e12, 2),
                      "algorithmic_modmul_per_launch": mm,
                      "key_hbm": {"bytes_per_launch": key_bytes,
                                  "achieved_gbs": round(key_bytes / (ms * 1e-3) / 1e9, 1)}},
+        "e2e": {"value": round(e2e_val, 2), "unit": "BR/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "clocks": clk.summary(),
+        "launch": {"form": "CUDA graph, one kernel per step", "coef_per_thread": rot.tile,
+                   "blocks_per_rotation": rot.split, "mac_form": rot.mac_form,
+                   "key": "uniform random key words (timing does not depend on key values)"},
     }
     if rank == 0 and world == 1 and not args.no_serving:
         line["serving"] = serving_run(local, args.serve_rate, args.serve_seconds)
@@ -622,6 +651,8 @@ def main():
         line["bootstrap"] = bootstrap_run(local)
         line["scheme_switch"] = scheme_switch_run(local)
         line["sap"] = sap_run(local)
+    line["gpu_launches_detail"] = {"timed_region": int(timed_launches), "e2e_timed_region": int(e2e_launches),
+                                   "counted_by": "tp_kernel_launches() deltas (graph replays count their kernels)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             v, threads, count, secs, ref_key, ref_out = cpu_reference_sample(variant, N, n, bl, l, lwes_h, accs_h,
@@ -638,6 +669,8 @@ def main():
                                     "sample": f"unavailable: {exc}"}
     rot.close()
     line["gpu_launches_detail"]["whole_run"] = int(_native.lib().tp_kernel_launches())
+    # last, so that a reader keeping the end of the line sees the batched/plain ratio
+    line["plain"] = plain
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -54,6 +54,7 @@ struct BrKernelParams {
     uint64_t dmask[8];        // per-digit mask
     uint64_t ddelta[8];       // per-digit offset subtracted (signed) or 0 (unsigned)
     unsigned int* err;        // bit 0: an LWE word was outside [0, 2N)
+    uint32_t small_digits;    // every digit is at most 2^14 in magnitude: integer pass 0 (tile 4)
 };
 
 // Polynomials transformed together by the rotation kernel (the accumulator
@@ -111,6 +112,14 @@ __host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int lo
 // the last in registers, then sums every output word over the 2l rows exactly
 // (WideAcc) and reduces it once, reading the key words straight from L2. No
 // key row stage. A running canonical sum instead pays a reduction per row.
+// Key loads of the digit-staged multiply-accumulate run ahead of their use either
+// row by row, AH rows ahead through a ring of registers (AH > 0), or a whole
+// (slot pair, component) group of 2l rows at a time, one group ahead (AH = 0).
+// Measured (rotations/s, full waves, N = 2048): CGGI ternary 8185 (ring, 5 ahead),
+// 7850 (8), 7274 (11), 7911 (groups); BMMP 9212 (groups) against 6204 and 6020
+// for rings of 5 and 8; CGGI binary N = 1024 about equal (20.35k to 20.55k).
+__host__ __device__ constexpr int br_ds_ahead(int variant) { return variant == kBmmpBinary ? 0 : 5; }
+
 __host__ __device__ constexpr size_t br_digit_stage_words(int logn, int dl) {
     return dl > 0 ? (size_t)(2 * dl - 1) << logn : 0;
 }
@@ -288,10 +297,11 @@ br_kernel(const BrKernelParams prm) {
                                                                   2u * N - a0), 1));
                 }
             };
-            // times 1/N, plus the signed-digit corrector (gadget_decomp.h:169-173)
+            // times 1/N (a shift: N^-1 = 2^-log2 N), plus the signed-digit corrector
+            // (gadget_decomp.h:169-173)
             auto finish_half = [&](uint64_t (&v)[E]) {
 #pragma unroll
-                for (int j = 0; j < E; ++j) v[j] = gl_fma(prm.corr, v[j], prm.n_inv);
+                for (int j = 0; j < E; ++j) v[j] = gl_add(gl_div_pow2<LOGN>(v[j]), prm.corr);
             };
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
@@ -301,17 +311,6 @@ br_kernel(const BrKernelParams prm) {
                 finish_half(cx[1]);
             }
             uint64_t x[K][E];  // digit transform of the row last processed
-            // digit-staged form: the key words of one (slot pair jp, component c) group, all
-            // 2L rows; each thread's 16 bytes at ((c*E/2 + jp)*T + t)*2 of row r
-            constexpr int R2 = 2 * (DL > 0 ? DL : 1);
-            constexpr int NG = C * (E / 2);
-            auto kload = [&](int jp, int c, ulonglong2 (&kv)[R2]) {
-#pragma unroll
-                for (int r = 0; r < R2; ++r)
-                    kv[r] = __ldg(reinterpret_cast<const ulonglong2*>(
-                        kit + (uint64_t)r * (N * C) + ((c * (E / 2) + jp) * T + t) * 2));
-            };
-            ulonglong2 kv[2][R2];
 #pragma unroll 1
             for (uint32_t r = 0; r < 2 * L; r += K) {
                 if constexpr (PF && K == 1) {
@@ -334,22 +333,40 @@ br_kernel(const BrKernelParams prm) {
                         finish_half(cx[0]);
                     }
                 }
+                bool pass0_done = false;
+                if constexpr (LOGE == 2 && K == 1) {
+                    if (prm.small_digits) {
+                        // digits as small signed integers, levels 0 and 1 in integer arithmetic
+                        const uint32_t d = r < L ? r : r - L;
+                        const uint32_t sh = prm.dshift[d];
+                        const uint64_t mk = prm.dmask[d];
+                        const int64_t dl = SIGNED ? (int64_t)prm.ddelta[d] : 0;
+                        int64_t dv[4];
 #pragma unroll
-                for (int p = 0; p < K; ++p) {
-                    const uint32_t rr = r + p;
-                    const bool hb = K == 2 && rr >= L;          // digit of the B half
-                    const uint32_t d = rr < L ? rr : rr - L;
-                    const uint32_t sh = prm.dshift[d];
-                    const uint64_t mk = prm.dmask[d];
-                    const uint64_t dl = prm.ddelta[d];
-#pragma unroll
-                    for (int j = 0; j < E; ++j) {
-                        const uint64_t c = hb ? cx[K - 1][j] : cx[0][j];
-                        const uint64_t raw = (c >> sh) & mk;
-                        x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
+                        for (int j = 0; j < 4; ++j) dv[j] = (int64_t)((cx[0][j] >> sh) & mk) - dl;
+                        ntt_pass0_small(dv, reinterpret_cast<uint64_t(&)[4]>(x[0]));
+                        pass0_done = true;
                     }
                 }
-                ntt_forward_k<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                if (!pass0_done) {
+#pragma unroll
+                    for (int p = 0; p < K; ++p) {
+                        const uint32_t rr = r + p;
+                        const bool hb = K == 2 && rr >= L;          // digit of the B half
+                        const uint32_t d = rr < L ? rr : rr - L;
+                        const uint32_t sh = prm.dshift[d];
+                        const uint64_t mk = prm.dmask[d];
+                        const uint64_t dl = prm.ddelta[d];
+#pragma unroll
+                        for (int j = 0; j < E; ++j) {
+                            const uint64_t c = hb ? cx[K - 1][j] : cx[0][j];
+                            const uint64_t raw = (c >> sh) & mk;
+                            x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
+                        }
+                    }
+                    fwd_pass_math<LOGN, 0, K, LOGE, R4, true>(x, t, tw_f);
+                }
+                ntt_forward_after_pass0<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
                 if constexpr (DS) {
                     // rows before the last wait in the stage (this thread's own slots: no barrier)
                     if (r + 1 < 2 * L) {
@@ -411,35 +428,86 @@ br_kernel(const BrKernelParams prm) {
             };
 
             if constexpr (DS) {
-                // Every slot's C sums over the 2L rows, exact, one reduction each. The key
-                // words of component c, slot pair jp, row r are the thread's 16 bytes at
-                // ((c*E/2 + jp)*T + t)*2 of row r; all 2L rows of one (jp, c) group are
-                // requested together, one group ahead of their use.
-                kload(0, 0, kv[0]);
+                // Every slot's C sums over the 2L rows, exact, one reduction each: for slot
+                // pair jp and key component c, the thread's 16 bytes of row r sit at
+                // ((c*E/2 + jp)*T + t)*2 of that row. The loads run ahead of their use in one
+                // of two schedules (br_ds_ahead).
+                constexpr int R2 = 2 * (DL > 0 ? DL : 1);
+                constexpr int AH = br_ds_ahead(VARIANT);
+                auto kaddr = [&](int jp, int c, int r) {
+                    return reinterpret_cast<const ulonglong2*>(kit + (uint64_t)r * (N * C) +
+                                                               ((c * (E / 2) + jp) * T + t) * 2);
+                };
+                auto row_x = [&](int jp, int r) -> ulonglong2 {
+                    return r < R2 - 1 ? *reinterpret_cast<const ulonglong2*>(xs + r * N + (jp * T + t) * 2)
+                                      : make_ulonglong2(x[0][2 * jp], x[0][2 * jp + 1]);
+                };
+                if constexpr (AH > 0) {
+                    // steps st = (jp*C + c)*2L + r, each row's key requested AH steps ahead
+                    // through a ring of AH+1 register pairs
+                    constexpr int NS = (E / 2) * C * R2;
+                    ulonglong2 ring[AH + 1];
 #pragma unroll
-                for (int jp = 0; jp < E / 2; ++jp) {
+                    for (int st = 0; st < AH && st < NS; ++st)
+                        ring[st] = __ldg(kaddr(st / (C * R2), (st / R2) % C, st % R2));
+                    WideAcc s0, s1;
                     uint64_t oj[2][C];
 #pragma unroll
-                    for (int c = 0; c < C; ++c) {
-                        const int g = jp * C + c;
-                        if (g + 1 < NG) kload((g + 1) / C, (g + 1) % C, kv[(g + 1) & 1]);
-                        const ulonglong2(&kc)[R2] = kv[g & 1];
-                        WideAcc s0, s1;
-                        wide_zero(s0);
-                        wide_zero(s1);
-#pragma unroll
-                        for (int r = 0; r < R2 - 1; ++r) {
-                            const ulonglong2 xv = *reinterpret_cast<const ulonglong2*>(xs + r * N + (jp * T + t) * 2);
-                            wide_mad(s0, xv.x, kc[r].x);
-                            wide_mad(s1, xv.y, kc[r].y);
+                    for (int st = 0; st < NS; ++st) {
+                        if (st + AH < NS) {
+                            const int sa = st + AH;
+                            ring[sa % (AH + 1)] = __ldg(kaddr(sa / (C * R2), (sa / R2) % C, sa % R2));
                         }
-                        wide_mad(s0, x[0][2 * jp], kc[R2 - 1].x);
-                        wide_mad(s1, x[0][2 * jp + 1], kc[R2 - 1].y);
-                        oj[0][c] = wide_reduce(s0);
-                        oj[1][c] = wide_reduce(s1);
+                        const int jp = st / (C * R2), c = (st / R2) % C, r = st % R2;
+                        const ulonglong2 kv = ring[st % (AH + 1)];
+                        if (r == 0) {
+                            wide_zero(s0);
+                            wide_zero(s1);
+                        }
+                        const ulonglong2 xv = row_x(jp, r);
+                        wide_mad(s0, xv.x, kv.x);
+                        wide_mad(s1, xv.y, kv.y);
+                        if (r == R2 - 1) {
+                            oj[0][c] = wide_reduce(s0);
+                            oj[1][c] = wide_reduce(s1);
+                            if (c == C - 1) {
+                                update(2 * jp, oj[0]);
+                                update(2 * jp + 1, oj[1]);
+                            }
+                        }
                     }
-                    update(2 * jp, oj[0]);
-                    update(2 * jp + 1, oj[1]);
+                } else {
+                    // groups g = jp*C + c: all 2L rows of a group requested together, one group
+                    // ahead of their use
+                    constexpr int NG = C * (E / 2);
+                    ulonglong2 kv[2][R2];
+                    auto kload = [&](int g, ulonglong2 (&k)[R2]) {
+#pragma unroll
+                        for (int r = 0; r < R2; ++r) k[r] = __ldg(kaddr(g / C, g % C, r));
+                    };
+                    kload(0, kv[0]);
+#pragma unroll
+                    for (int jp = 0; jp < E / 2; ++jp) {
+                        uint64_t oj[2][C];
+#pragma unroll
+                        for (int c = 0; c < C; ++c) {
+                            const int g = jp * C + c;
+                            if (g + 1 < NG) kload(g + 1, kv[(g + 1) & 1]);
+                            WideAcc s0, s1;
+                            wide_zero(s0);
+                            wide_zero(s1);
+#pragma unroll
+                            for (int r = 0; r < R2; ++r) {
+                                const ulonglong2 xv = row_x(jp, r);
+                                wide_mad(s0, xv.x, kv[g & 1][r].x);
+                                wide_mad(s1, xv.y, kv[g & 1][r].y);
+                            }
+                            oj[0][c] = wide_reduce(s0);
+                            oj[1][c] = wide_reduce(s1);
+                        }
+                        update(2 * jp, oj[0]);
+                        update(2 * jp + 1, oj[1]);
+                    }
                 }
             } else {
 #pragma unroll
@@ -466,7 +534,7 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < E; ++j) res[(h0 + p) * N + t + j * T] = gl_mul(x[p][j], prm.n_inv);
+                    for (int j = 0; j < E; ++j) res[(h0 + p) * N + t + j * T] = gl_div_pow2<LOGN>(x[p][j]);
             } else {
 #pragma unroll
                 for (int p = 0; p < K; ++p)

@@ -215,7 +215,7 @@ __device__ __forceinline__ void br_split_body(const BrKernelParams& prm) {
                 if (d == d_begin) {
                     ntt_backward_unscaled_k<LOGN, 1, LOGE, R4>(cx, t, xb(), tw_i);
 #pragma unroll
-                    for (int j = 0; j < E; ++j) cx[0][j] = gl_fma(prm.corr, cx[0][j], prm.n_inv);
+                    for (int j = 0; j < E; ++j) cx[0][j] = gl_add(gl_div_pow2<LOGN>(cx[0][j]), prm.corr);
                 }
                 uint64_t x[1][E];
                 const uint32_t sh = prm.dshift[d];
@@ -336,7 +336,7 @@ __device__ __forceinline__ void br_split_body(const BrKernelParams& prm) {
         if (prm.out_coef) {
             ntt_backward_unscaled_k<LOGN, 1, LOGE, R4>(x, t, xb(), tw_i);
 #pragma unroll
-            for (int j = 0; j < E; ++j) res[t + j * T] = gl_mul(x[0][j], prm.n_inv);
+            for (int j = 0; j < E; ++j) res[t + j * T] = gl_div_pow2<LOGN>(x[0][j]);
         } else {
 #pragma unroll
             for (int c = 0; c < E / 2; ++c)

@@ -323,6 +323,9 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
         }
     }
 
+    // Digits small enough for the integer pass 0 of the digit transforms: signed digits lie in
+    // [-2^(beta-1), 2^(beta-1)), unsigned in [0, 2^beta); the pass is exact up to 2^14.
+    kp.small_digits = (p->variant == TP_BR_CGGI_BINARY ? beta <= 14 : beta <= 15) ? 1u : 0u;
     for (int lg = 2; lg <= 3; ++lg) {
         const void* k = tp::br_kernel_lookup(c->logn, p->variant, lg);
         const size_t smem = tp::br_smem_words(c->logn, p->variant, p->lwe_dim, lg) * 8;

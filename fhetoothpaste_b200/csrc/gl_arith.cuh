@@ -319,6 +319,12 @@ __device__ __forceinline__ uint64_t gl_pow2_mag(uint64_t x) {
     else return gl_shr<(S < 0 ? -S : 1)>(x);
 }
 
+// x * N^-1 mod p for N = 2^LOGN (N^-1 = 2^-LOGN): a shift multiply.
+template <int LOGN>
+__device__ __forceinline__ uint64_t gl_div_pow2(uint64_t x) {
+    return gl_shr<LOGN <= 32 ? LOGN : 32>(x);
+}
+
 // x * 2^K mod p for a compile-time K (canonical out, any 64-bit x in).
 template <int K>
 __device__ __forceinline__ uint64_t gl_mul_pow2(uint64_t x) {

@@ -257,7 +257,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
 #pragma unroll
                         for (int j = 0; j < E; ++j) {
                             const uint32_t m = t + j * T;
-                            const uint64_t y = gl_mul(r[0][j], prm.n_inv);
+                            const uint64_t y = gl_div_pow2<LOGN>(r[0][j]);
                             out[h * N + m] = gl_add(base[h][j], y);
                             const uint64_t z = gl_sub(base[h][j], y);
                             if (m >= s) out1[m - s] = z;
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
                     } else {
 #pragma unroll
                         for (int j = 0; j < E; ++j)
-                            out[h * N + t + j * T] = gl_add(base[h][j], gl_mul(r[0][j], prm.n_inv));
+                            out[h * N + t + j * T] = gl_add(base[h][j], gl_div_pow2<LOGN>(r[0][j]));
                     }
                 }
             }

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8) ntt_batch_kernel(uint64_t* ou
             ntt_backward_unscaled<LOGN>(x, t, buf[sel], tws);
             sel ^= 1;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) dst[t + j * T] = gl_mul(x[j], n_inv);
+            for (int j = 0; j < 8; ++j) dst[t + j * T] = gl_div_pow2<LOGN>(x[j]);
         }
     }
 }

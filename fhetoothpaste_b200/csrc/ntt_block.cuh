@@ -397,6 +397,41 @@ __device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][1 << LOGE], int t
     fwd_passes_from<LOGN, 0, K, LOGE, R4, LAZY>(x, t, buf, tw_fwd);
 }
 
+// The rest of a forward transform whose pass 0 the caller has already applied to x
+// (same layouts and LAZY rule as ntt_forward_k).
+template <int LOGN, int K, int LOGE, bool R4 = false, bool LAZY = false>
+__device__ __forceinline__ void ntt_forward_after_pass0(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
+                                                        const uint64_t* tw_fwd) {
+    using SH = NttShape<LOGN, LOGE>;
+    if constexpr (SH::NPASS > 1) {
+        xstore<LOGN, 0, K, LOGE>(buf, x, t);
+        ntt_sync<LOGN, LOGE>(!SH::WarpLocal(0));
+        xload<LOGN, 1, K, LOGE>(buf, x, t);
+        fwd_passes_from<LOGN, 1, K, LOGE, R4, LAZY>(x, t, buf, tw_fwd);
+    }
+}
+
+// Pass 0 of the forward transform (levels 0 and 1, 4 coefficients per thread) for
+// small signed inputs d_j (coefficients t + jT), in exact 64-bit integer arithmetic.
+// Its twiddles are 2^48 (level 0), 2^120 = -2^24 and 2^168 = 2^-24 (level 1); with
+// 2^72 = 2^40 - 2^8 and 2^88 = 2^56 - 2^24 (mod p) the four outputs are
+//   y0 = A - P, y1 = A + P, y2 = B - Q, y3 = B + Q,
+//   A = d0 + 2^48 d2, B = d0 - 2^48 d2,
+//   P = 2^24 d1 + (2^40 - 2^8) d3, Q = (2^40 - 2^8) d1 + 2^24 d3,
+// exact as long as |d_j| (1 + 2^8 + 2^24 + 2^40 + 2^48) < 2^63, i.e. |d_j| <= 2^14.
+// A negative y is its 64-bit pattern y + 2^64 = y + eps (mod p), so eps is taken off
+// (giving y + p); the outputs are canonical. Replaces two levels of butterflies.
+__device__ __forceinline__ int64_t shl_signed(int64_t v, int k) { return (int64_t)((uint64_t)v << k); }
+
+__device__ __forceinline__ void ntt_pass0_small(const int64_t (&d)[4], uint64_t (&y)[4]) {
+    const int64_t a = d[0] + shl_signed(d[2], 48), b = d[0] - shl_signed(d[2], 48);
+    const int64_t pp = shl_signed(d[1], 24) + shl_signed(d[3], 40) - shl_signed(d[3], 8);
+    const int64_t qq = shl_signed(d[1], 40) - shl_signed(d[1], 8) + shl_signed(d[3], 24);
+    const int64_t v[4] = {a - pp, a + pp, b - qq, b + qq};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) y[j] = (uint64_t)v[j] - (v[j] < 0 ? kEps : 0ull);
+}
+
 // Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.
 template <int LOGN, int K, int LOGE = 3, bool R4 = false>
 __device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,

@@ -199,3 +199,31 @@ def test_wide_accumulator_sums_exactly():
                 acc = wide_mad(acc, x, k)
             got = wide_reduce(acc)
             assert got == sum(x * k for x, k in pairs) % P, (terms, pairs)
+
+
+def test_integer_pass0_for_small_digits():
+    """ntt_pass0_small (csrc/ntt_block.cuh): levels 0 and 1 of the forward transform on small
+    signed digits as exact 64-bit integer sums, against the butterflies with the reference's
+    twiddles psi^brv(1), psi^brv(2), psi^brv(3), at the largest digits allowed (|d| <= 2^14)."""
+    rng = random.Random(6)
+    D = 1 << 14
+    for N in (1024, 2048, 4096):
+        logn = N.bit_length() - 1
+        psi = pow(7, (P - 1) // (2 * N), P)
+        w1, w2, w3 = (pow(psi, int(format(k, f"0{logn}b")[::-1], 2), P) for k in (1, 2, 3))
+        cases = [[D, D, D, D], [-D, -D, -D, -D], [D, -D, D, -D], [-D, D, -D, D], [0, 0, 0, 0]]
+        cases += [[rng.randint(-D, D) for _ in range(4)] for _ in range(3000)]
+        for d in cases:
+            x = [v % P for v in d]
+            a0, a2 = (x[0] + w1 * x[2]) % P, (x[0] - w1 * x[2]) % P
+            a1, a3 = (x[1] + w1 * x[3]) % P, (x[1] - w1 * x[3]) % P
+            want = [(a0 + w2 * a1) % P, (a0 - w2 * a1) % P, (a2 + w3 * a3) % P, (a2 - w3 * a3) % P]
+            a, b = d[0] + (d[2] << 48), d[0] - (d[2] << 48)
+            pp = (d[1] << 24) + (d[3] << 40) - (d[3] << 8)
+            qq = (d[1] << 40) - (d[1] << 8) + (d[3] << 24)
+            v = [a - pp, a + pp, b - qq, b + qq]
+            for j in range(4):
+                assert -2**63 <= v[j] < 2**63
+                u = v[j] & (2**64 - 1)           # the 64-bit pattern
+                got = u - (M32 if v[j] < 0 else 0)  # eps off for negative values
+                assert got == want[j] and 0 <= got < P, (N, d, j)
