@@ -42,19 +42,24 @@ __device__ __forceinline__ uint64_t gl_add(uint64_t a, uint64_t b) {
 
 // a + b as a 64-bit value congruent to it mod p (not necessarily below p), for
 // any 64-bit a and b < p: a + b < 2^64 + p, so after a carry out the sum's low
-// 64 bits plus eps stay below 2^64. Six instructions against gl_add's seven.
+// 64 bits plus eps stay below 2^64. Six instructions against gl_add's seven; the
+// five carry adds are written as multiply-adds by 1 so that they issue on the
+// IMAD pipe: the forward transforms that use this sum are otherwise ALU-bound
+// (their butterflies put 9 IMADs against 22 ALU instructions). Measured on the
+// rotation kernel: +2.0% CGGI ternary N = 2048, +1.2% binary N = 1024, +0.8%
+// BMMP; moving gl_add's or the reduction's adds as well measured slower.
 // (The carry is read with addc and negated with sub: a subc right after the
 // addc.cc, reading the add's carry as a borrow, gave wrong words here.)
 __device__ __forceinline__ uint64_t gl_add_lazy(uint64_t a, uint64_t b) {
     uint32_t sl, sh;
     asm("{\n\t"
         ".reg .u32 c, m;\n\t"
-        "add.cc.u32 %0, %2, %4;\n\t"
-        "addc.cc.u32 %1, %3, %5;\n\t"
-        "addc.u32 c, 0, 0;\n\t"
+        "mad.lo.cc.u32 %0, %2, 1, %4;\n\t"
+        "madc.lo.cc.u32 %1, %3, 1, %5;\n\t"
+        "madc.lo.u32 c, 0, 0, 0;\n\t"
         "sub.u32 m, 0, c;\n\t"
-        "add.cc.u32 %0, %0, m;\n\t"
-        "addc.u32 %1, %1, 0;\n\t"
+        "mad.lo.cc.u32 %0, m, 1, %0;\n\t"
+        "madc.lo.u32 %1, %1, 1, 0;\n\t"
         "}"
         : "=r"(sl), "=r"(sh)
         : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
