@@ -122,6 +122,8 @@ def lib() -> ctypes.CDLL:
         "tp_server_add_set": (ctypes.c_int, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                              ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_uint32)]),
         "tp_server_start": (ctypes.c_int, [VP]),
+        "tp_server_set_memory_budget": (ctypes.c_int, [VP, U64]),
+        "tp_server_memory": (ctypes.c_int, [VP, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]),
         "tp_server_submit": (ctypes.c_int, [VP, ctypes.c_uint32, U64P, U64P, U64P, ctypes.POINTER(U64)]),
         "tp_server_wait": (ctypes.c_int, [VP, U64, ctypes.c_uint32]),
         "tp_server_drain": (ctypes.c_int, [VP, ctypes.c_uint32]),

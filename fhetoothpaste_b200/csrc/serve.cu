@@ -38,6 +38,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     uint64_t ticket;
     uint32_t set;
+    uint64_t bytes;             // device bytes reserved for it until it completes
     const uint64_t* lwe;
     const uint64_t* acc;
     uint64_t* result;
@@ -62,6 +63,7 @@ struct Set {
     uint32_t N = 0, n = 0;
     uint32_t max_batch = 0;
     int out_coef = 0;
+    uint64_t req_bytes = 0;     // device bytes of one request: its LWE, test polynomial and result
     std::vector<LaunchBuffer> bufs;
     std::deque<Request> pending;
 };
@@ -83,6 +85,12 @@ struct tp_server {
     std::vector<uint8_t> done_flag;  // by ticket
     std::vector<double> latency_ms;  // completed requests, in completion order
     uint64_t completed = 0, rejected = 0, launches = 0;
+    // device-memory admission: requests reserve their device bytes from the budget when
+    // admitted and return them when their result is back in host memory
+    uint64_t mem_budget = 0;    // 0 until set: the free device memory at tp_server_start
+    bool mem_budget_set = false;
+    uint64_t mem_in_use = 0;
+    uint64_t rejected_memory = 0;
     tp_status worker_status = TP_OK;
     std::string worker_error;
     Clock::time_point t_first, t_last;
@@ -175,6 +183,7 @@ bool retire_done(tp_server* srv) {
                 const Request& r = b.reqs[i];
                 std::memcpy(r.result, b.h_res + i * aw, aw * 8);
                 srv->done_flag[r.ticket] = 1;
+                srv->mem_in_use -= r.bytes;
                 srv->latency_ms.push_back(std::chrono::duration<double, std::milli>(now - r.t_submit).count());
                 srv->completed++;
             }
@@ -238,6 +247,7 @@ tp_status tp_server_add_set(tp_server* srv, tp_br_ctx* ctx, uint32_t ring_dim, u
     s.max_batch = max_batch;
     s.out_coef = out_coef;
     const uint64_t lw = (uint64_t)lwe_dim + 1, aw = 2ull * ring_dim;
+    s.req_bytes = (lw + 2 * aw) * 8;
     const uint64_t per_buf = ((uint64_t)max_batch * lw + 2 * (uint64_t)max_batch * aw) * 8;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -263,9 +273,37 @@ tp_status tp_server_add_set(tp_server* srv, tp_br_ctx* ctx, uint32_t ring_dim, u
     return TP_OK;
 }
 
+tp_status tp_server_set_memory_budget(tp_server* srv, uint64_t bytes) {
+    if (!srv) return serr(TP_ERR_PARAM, "null argument");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->mem_budget = bytes;
+    srv->mem_budget_set = true;
+    return TP_OK;
+}
+
+tp_status tp_server_memory(tp_server* srv, uint64_t* budget, uint64_t* in_use, uint64_t* rejected_memory) {
+    if (!srv) return serr(TP_ERR_PARAM, "null argument");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (budget) *budget = srv->mem_budget;
+    if (in_use) *in_use = srv->mem_in_use;
+    if (rejected_memory) *rejected_memory = srv->rejected_memory;
+    return TP_OK;
+}
+
 tp_status tp_server_start(tp_server* srv) {
     if (!srv) return serr(TP_ERR_PARAM, "null argument");
     if (srv->worker.joinable()) return TP_OK;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        if (!srv->mem_budget_set) {
+            // by default the device memory still free once keys and launch buffers are resident
+            size_t free_b = 0, total_b = 0;
+            cudaSetDevice(srv->device);
+            if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return serr(TP_ERR_CUDA, "cudaMemGetInfo failed");
+            srv->mem_budget = free_b;
+            srv->mem_budget_set = true;
+        }
+    }
     srv->stop = false;
     srv->worker = std::thread(worker_loop, srv);
     return TP_OK;
@@ -281,9 +319,16 @@ tp_status tp_server_submit(tp_server* srv, uint32_t set_id, const uint64_t* lwe,
         srv->rejected++;
         return serr(TP_ERR_STATE, "queue full: request rejected by admission control");
     }
+    const uint64_t bytes = srv->sets[set_id].req_bytes;
+    if (srv->mem_budget_set && srv->mem_in_use + bytes > srv->mem_budget) {
+        srv->rejected++;
+        srv->rejected_memory++;
+        return serr(TP_ERR_OOM, "device memory budget exhausted: request rejected by admission control");
+    }
     const uint64_t t = srv->next_ticket++;
     if (srv->done_flag.size() <= t) srv->done_flag.resize(std::max<size_t>(2 * srv->done_flag.size(), t + 1), 0);
-    Request r{t, set_id, lwe, acc, result, Clock::now()};
+    srv->mem_in_use += bytes;
+    Request r{t, set_id, bytes, lwe, acc, result, Clock::now()};
     if (srv->completed == 0 && srv->queued == 0 && srv->launches == 0) srv->t_first = r.t_submit;
     srv->sets[set_id].pending.push_back(r);
     srv->queued++;
@@ -341,6 +386,7 @@ tp_status tp_server_reset_stats(tp_server* srv) {
     std::lock_guard<std::mutex> lk(srv->mu);
     srv->latency_ms.clear();
     srv->completed = srv->rejected = srv->launches = 0;
+    srv->rejected_memory = 0;
     return TP_OK;
 }
 

@@ -29,6 +29,15 @@ class BootstrapServer:
         self.sets.append(rotator)
         return sid.value
 
+    def set_memory_budget(self, nbytes: int) -> None:
+        """Device bytes admitted requests may reserve (default: free device memory at start)."""
+        _check(nat.lib().tp_server_set_memory_budget(self._h, nbytes))
+
+    def memory(self) -> dict:
+        b, u, r = nat.U64(), nat.U64(), nat.U64()
+        _check(nat.lib().tp_server_memory(self._h, ctypes.byref(b), ctypes.byref(u), ctypes.byref(r)))
+        return {"budget_bytes": b.value, "in_use_bytes": u.value, "rejected_for_memory": r.value}
+
     def start(self) -> None:
         _check(nat.lib().tp_server_start(self._h))
 

@@ -340,13 +340,25 @@ tp_status tp_server_create(int device, uint64_t max_queue, tp_server** out);
 tp_status tp_server_add_set(tp_server* srv, tp_br_ctx* ctx, uint32_t ring_dim, uint32_t lwe_dim, uint32_t max_batch,
                             uint32_t buffers, int out_coef, uint32_t* set_id);
 
+/* Device-memory admission. Every admitted request reserves its device bytes
+ * ((n+1) + 4N words: its LWE, test polynomial and result in a launch buffer)
+ * from the server's budget until its result is back in host memory; a submit
+ * that would exceed the budget is rejected with TP_ERR_OOM (and counted). The
+ * budget defaults to the device memory still free at tp_server_start (keys and
+ * launch buffers resident); tp_server_set_memory_budget sets it explicitly, at
+ * any time. tp_server_memory reads the budget, the bytes reserved now and the
+ * number of requests refused for memory (any output may be NULL). */
+tp_status tp_server_set_memory_budget(tp_server* srv, uint64_t bytes);
+tp_status tp_server_memory(tp_server* srv, uint64_t* budget, uint64_t* in_use, uint64_t* rejected_memory);
+
 /* Starts the scheduler thread (after every tp_server_add_set). */
 tp_status tp_server_start(tp_server* srv);
 
 /* Queues one rotation of set `set_id`: lwe (n+1 words) and acc (2N words) are
  * read and result (2N words) written by the scheduler, so the host buffers
  * must stay valid until tp_server_wait returns for the ticket. Returns
- * TP_ERR_STATE when the queue is full (the request is not admitted). */
+ * TP_ERR_STATE when the queue is full and TP_ERR_OOM when the device-memory
+ * budget is (the request is not admitted either way). */
 tp_status tp_server_submit(tp_server* srv, uint32_t set_id, const uint64_t* lwe, const uint64_t* acc,
                            uint64_t* result, uint64_t* ticket);
 tp_status tp_server_wait(tp_server* srv, uint64_t ticket, uint32_t timeout_ms);

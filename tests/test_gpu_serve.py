@@ -1,6 +1,7 @@
 """Serving loop: mixed parameter sets under continuous batching give, for every
 request, exactly the words the same request gives alone (integer results: the
-tolerance is zero), and admission control rejects beyond the queue bound."""
+tolerance is zero), and admission control rejects beyond the queue bound and beyond the
+device-memory budget, admitting again as launches complete."""
 import threading
 
 import numpy as np
@@ -88,6 +89,52 @@ def test_admission_control_bounds_the_queue(rotators):
     for t in tickets:
         srv.wait(t)
     assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_memory_budget_refuses_then_readmits(rotators, oracle):
+    from fhetoothpaste_b200 import BootstrapServer, TpError, _native
+    rots, keys = rotators
+    v, N, n, bl, dg = SETS[1]
+    req_bytes = ((n + 1) + 4 * N) * 8  # LWE, test polynomial and result of one request
+    srv = BootstrapServer(max_queue=1000)
+    sid = srv.add_set(rots[1], max_batch=4, buffers=1, out_coef=True)
+    srv.set_memory_budget(3 * req_bytes)
+    bufs = [(lwe_inputs(N, n, 1, 300 + k)[0], random_acc(N, 1, 400 + k)[0], np.zeros(2 * N, np.uint64))
+            for k in range(6)]
+    # not started: the first three fill the budget, the next two are refused for memory
+    tickets = [srv.submit(sid, *bufs[k]) for k in range(3)]
+    assert srv.memory()["in_use_bytes"] == 3 * req_bytes
+    for k in (3, 4):
+        with pytest.raises(TpError) as e:
+            srv.submit(sid, *bufs[k])
+        assert e.value.status == _native.TP_ERR_OOM
+    srv.start()
+    for t in tickets:
+        srv.wait(t)
+    srv.drain()
+    m = srv.memory()
+    assert m["in_use_bytes"] == 0 and m["rejected_for_memory"] == 2 and m["budget_bytes"] == 3 * req_bytes
+    # the completed launches returned their bytes: refused requests are admitted now
+    for k in (3, 4, 5):
+        srv.wait(srv.submit(sid, *bufs[k]))
+    for k in (0, 3, 5):
+        lwe, acc, res = bufs[k]
+        np.testing.assert_array_equal(res, oracle.blind_rotate(v, N, n, bl, dg, keys[1], lwe, acc, 1))
+    assert srv.stats()["rejected"] == 2
+    srv.close()
+
+
+def test_default_memory_budget_is_free_device_memory(rotators):
+    from fhetoothpaste_b200 import BootstrapServer
+    import torch
+    rots, _ = rotators
+    srv = BootstrapServer(max_queue=16)
+    srv.add_set(rots[0], max_batch=8, buffers=2)
+    srv.start()
+    free, _ = torch.cuda.mem_get_info()
+    budget = srv.memory()["budget_bytes"]
+    assert 0.5 * free < budget < 1.5 * free + (1 << 30)
     srv.close()
 
 
