@@ -8,6 +8,13 @@
 // OperatorContext<BlindRotator>) and once over toothpaste_b200::GpuRotationContext.
 // The Python test compares the two outputs word for word.
 //
+// NegacyclicFunctionEvaluator is not driven: its constructor
+// (negacyclic_function_evaluator.cpp:64-66) casts the rotation context's input container,
+// a tuple (LWE, RLWE) for CGGI and BMMP contexts, to an RLWE container and dereferences
+// the null result, so the reference cannot construct it over any rotation context (its
+// own negacyclic_func_test included). Its EvalFunc body is BlindRotate with coefficient
+// output followed by SampleExtract, which adp_rotate_in_place covers.
+//
 // The adapter needs read access to the generated key (m_brk); a reference tree adds
 // an accessor for it, here the access specifiers are opened instead.
 
@@ -20,7 +27,6 @@
 #include "operators/cggi_blind_rotation.h"
 #include "operators/endo_glwe_conversion.h"
 #include "operators/lwe_to_rgsw_conversion.h"
-#include "operators/negacyclic_function_evaluator.h"
 #include "operators/sap_decomposition.h"
 #include "operators/trace_evaluation.h"
 #undef private
@@ -82,29 +88,6 @@ int guarded(F&& f) {
 extern "C" {
 
 const char* adp_last_error(void) { return g_err.c_str(); }
-
-// NegacyclicFunctionEvaluator::EvalFunc(result, lwe, lut_rlwe) (negacyclic_function_evaluator.cpp:92-101)
-// of `count` LWEs (n+1 words each) with their LUT RLWEs (2N words each): results N+1 words each.
-int adp_eval_func(int variant, uint64_t N, uint64_t n, uint64_t basis_log2, uint64_t digits, double std_dev,
-                  const uint64_t* lwe_key, const uint64_t* rlwe_key, uint64_t seed, uint64_t count,
-                  const uint64_t* lwes, const uint64_t* luts, uint64_t* out_cpu, uint64_t* out_gpu) {
-    return guarded([&]() {
-        Contexts c = make_contexts(variant, N, n, basis_log2, digits, std_dev);
-        std::vector<GenericKey> keys = {{"LWE", lwe_key, n}, {"RLWE", rlwe_key, N}};
-        for (int side = 0; side < 2; ++side) {
-            auto ctx = std::make_shared<NegacyclicFunctionEvaluationContext>(side ? c.gpu : c.cpu);
-            ref_seed(seed);
-            auto op = ctx->ConstructOperator(keys);
-            uint64_t* out = side ? out_gpu : out_cpu;
-            std::vector<uint64_t> lut(2 * N);
-            for (uint64_t b = 0; b < count; ++b) {
-                std::copy(luts + b * 2 * N, luts + (b + 1) * 2 * N, lut.begin());
-                std::fill(out + b * (N + 1), out + (b + 1) * (N + 1), 0);
-                op->EvalFunc(out + b * (N + 1), lwes + b * (n + 1), lut.data());
-            }
-        }
-    });
-}
 
 // LWEtoRGSWConverter::Convert(output, input) (lwe_to_rgsw_conversion.cpp:168-225) with its
 // rotation, trace and squaring gadgets: outputs 4 N out_digits words each, zeroed first.
