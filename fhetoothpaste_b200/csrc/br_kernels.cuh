@@ -22,6 +22,9 @@
 // are contiguous across the warp.
 #pragma once
 
+#include <cooperative_groups.h>
+
+#include "cluster_ntt.cuh"
 #include "gl_arith.cuh"
 #include "ntt_block.cuh"
 
@@ -94,16 +97,24 @@ __host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int bl
 // slower (ternary N = 4096: 1856 vs 1977 rotations/s; the spills cost more), and
 // so did staging part of each row there (two components, the rest read from L2
 // at use: ternary 1918 vs 1978; BMMP 2939 vs 2889, within run-to-run spread).
-__host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge) {
-    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge, br_fused_radix4(loge, variant, 1)) : 0) +
-           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
+// Ring sizes above 4096 rotate on a cluster of 2^logs CTAs, each holding
+// 2^(logn - logs) = 2048 coefficients and slots (cluster_ntt.cuh); every plan
+// below is per CTA, in words of its local size, plus two receive areas of the
+// distributed transform's exchange.
+__host__ __device__ constexpr int br_cluster_logs(int logn) { return logn > 12 ? logn - 11 : 0; }
+
+__host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge, int logs = 0) {
+    return (size_t)(br_smem_twiddles(logn - logs)
+                        ? 2 * br_twiddle_words(logn - logs, loge, br_fused_radix4(loge, variant, 1))
+                        : 0) +
+           (size_t)(1 << (logn - logs)) * (2 * br_ntt_width(logn, variant) + 2 + (logs ? 2 : 0)) +
            1024;  // LWE area budget for the plan; the host adds the real size
 }
-__host__ __device__ constexpr size_t br_stage_words(int logn, int variant) {
-    return (size_t)(1 << logn) * 2 * br_rgsw_per_group(variant);
+__host__ __device__ constexpr size_t br_stage_words(int logn, int variant, int logs = 0) {
+    return (size_t)(1 << (logn - logs)) * 2 * br_rgsw_per_group(variant);
 }
-__host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int loge) {
-    return (br_base_words(logn, variant, loge) + br_stage_words(logn, variant)) * 8 <= 227u * 1024u;
+__host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int loge, int logs = 0) {
+    return (br_base_words(logn, variant, loge, logs) + br_stage_words(logn, variant, logs)) * 8 <= 227u * 1024u;
 }
 
 // Digit-staged multiply-accumulate (template parameter DL = the digit count l,
@@ -124,15 +135,19 @@ __host__ __device__ constexpr size_t br_digit_stage_words(int logn, int dl) {
     return dl > 0 ? (size_t)(2 * dl - 1) << logn : 0;
 }
 
-// Shared memory of one block, in words: twiddles (both directions, if kept
-// there), two exchange areas of width*N words, the accumulator (2N), the key
-// row stage (C*N, if used) or the digit stage (DL > 0), the LWE vector (n+1,
-// rounded up to an even count).
-__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge, int dl = 0) {
-    return (size_t)(br_smem_twiddles(logn) ? 2 * br_twiddle_words(logn, loge, br_fused_radix4(loge, variant, 1)) : 0) +
-           (size_t)(1 << logn) * (2 * br_ntt_width(logn, variant) + 2) +
-           (dl > 0 ? br_digit_stage_words(logn, dl)
-                   : (br_key_prefetch(logn, variant, loge) ? br_stage_words(logn, variant) : 0)) +
+// Shared memory of one block, in words (local size NL = 2^(logn - logs)):
+// twiddles (both directions, if kept there), two exchange areas of width*NL words,
+// the accumulator (2 NL), the key row stage (C NL, if used) or the digit stage
+// (DL > 0), two receive areas (2 NL, clusters only), the LWE vector (n+1, rounded
+// up to an even count).
+__host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge, int dl = 0,
+                                                   int logs = 0) {
+    return (size_t)(br_smem_twiddles(logn - logs)
+                        ? 2 * br_twiddle_words(logn - logs, loge, br_fused_radix4(loge, variant, 1))
+                        : 0) +
+           (size_t)(1 << (logn - logs)) * (2 * br_ntt_width(logn, variant) + 2 + (logs ? 2 : 0)) +
+           (dl > 0 ? br_digit_stage_words(logn - logs, dl)
+                   : (br_key_prefetch(logn, variant, loge, logs) ? br_stage_words(logn, variant, logs) : 0)) +
            ((n + 2) & ~1u);
 }
 
@@ -175,30 +190,37 @@ __host__ __device__ constexpr int br_min_blocks(int logn, int variant, int loge)
     return loge == 2 ? (logn <= 10 ? 2 : 1) : ((logn >= 11 || variant == kBmmpBinary) ? 1 : 2);
 }
 
-template <int LOGN, int VARIANT, int LOGE, int DL = 0>
-__global__ void __launch_bounds__((1 << LOGN) >> LOGE, br_min_blocks(LOGN, VARIANT, LOGE))
+// LOGS > 0: one rotation per cluster of 2^LOGS CTAs (launched with that cluster
+// size), each CTA holding the coefficients i = i' 2^LOGS + r and the slots
+// r NL .. r NL + NL - 1 of the cluster's rank r (cluster_ntt.cuh); the
+// multiply-accumulate, the update and the key words of a slot are local to its CTA.
+template <int LOGN, int VARIANT, int LOGE, int DL = 0, int LOGS = 0>
+__global__ void __launch_bounds__((1 << (LOGN - LOGS)) >> LOGE, br_min_blocks(LOGN - LOGS, VARIANT, LOGE))
 br_kernel(const BrKernelParams prm) {
-    using SH = NttShape<LOGN, LOGE>;
-    constexpr int N = SH::N;
+    constexpr int LOGL = LOGN - LOGS;        // log2 of the coefficients / slots per CTA
+    using SH = NttShape<LOGL, LOGE>;
+    constexpr int N = 1 << LOGN;             // ring dimension
+    constexpr int NL = SH::N;
     constexpr int T = SH::T;
     constexpr int E = SH::E;
     constexpr int G = br_rgsw_per_group(VARIANT);
     constexpr int C = 2 * G;                 // key components per slot
     constexpr int K = br_ntt_width(LOGN, VARIANT);  // polynomials per transform
-    constexpr bool TW_SMEM = br_smem_twiddles(LOGN);
+    constexpr bool TW_SMEM = br_smem_twiddles(LOGL);
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
     constexpr bool R4 = br_fused_radix4(LOGE, VARIANT, 1);
     constexpr bool DS = DL > 0;              // digit-staged multiply-accumulate (prm.digits == DL)
-    constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE);
+    constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE, LOGS);
     static_assert(!DS || (LOGE == 2 && K == 1), "the digit stage runs with 4 coefficients per thread");
+    static_assert(LOGS == 0 || (LOGE == 2 && K == 1 && !R4), "clusters run radix-2 with 4 coefficients per thread");
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
     const uint64_t* tw_f = prm.tw_fwd;
     const uint64_t* tw_i = prm.tw_inv;
     if constexpr (TW_SMEM) {
-        constexpr int TWW = br_twiddle_words(LOGN, LOGE, R4);
+        constexpr int TWW = br_twiddle_words(LOGL, LOGE, R4);  // the first NL words of the N-point tables
         for (int i = threadIdx.x; i < TWW; i += T) {
             base[i] = prm.tw_fwd[i];
             base[TWW + i] = prm.tw_inv[i];
@@ -208,12 +230,20 @@ br_kernel(const BrKernelParams prm) {
         base += 2 * TWW;
     }
     uint64_t* xbuf0 = base;
-    uint64_t* xbuf1 = base + K * N;
-    uint64_t* acc = base + 2 * K * N;        // [(h*E + j)*T + t], canonical, NTT domain
-    uint64_t* kst = acc + 2 * N;             // key row stage, device layout of one row (C*N words)
-    // digit stage (DS): row r < 2L-1 of this thread's slot pair jp at xs + r*N + (jp*T + t)*2
-    uint64_t* xs = acc + 2 * N;
-    uint64_t* lwe_s = kst + (PF ? C * N : (DS ? (2 * DL - 1) * N : 0));
+    uint64_t* xbuf1 = base + K * NL;
+    uint64_t* acc = base + 2 * K * NL;       // [(h*E + j)*T + t], canonical, NTT domain
+    uint64_t* kst = acc + 2 * NL;            // key row stage, this CTA's part of one row (C*NL words)
+    // digit stage (DS): row r < 2L-1 of this thread's slot pair jp at xs + r*NL + (jp*T + t)*2
+    uint64_t* xs = acc + 2 * NL;
+    uint64_t* recv0 = kst + (PF ? C * NL : (DS ? (2 * DL - 1) * NL : 0));  // cluster exchange areas
+    uint64_t* recv1 = recv0 + NL;
+    uint64_t* lwe_s = recv0 + (LOGS ? 2 * NL : 0);
+    int cr = 0;                              // rank in the cluster
+    if constexpr (LOGS > 0) {
+        cr = (int)cooperative_groups::this_cluster().block_rank();
+        cooperative_groups::this_cluster().sync();  // every CTA of the cluster running before remote stores
+    }
+    const uint32_t sbase = (uint32_t)cr << LOGL;  // first slot of this CTA
 
     const int t = threadIdx.x;
     const uint32_t n = prm.n;
@@ -228,8 +258,25 @@ br_kernel(const BrKernelParams prm) {
         sel ^= 1;
         return b;
     };
+    int rsel = 0;
+    auto recv_next = [&]() -> uint64_t* {
+        uint64_t* b = rsel ? recv1 : recv0;
+        rsel ^= 1;
+        return b;
+    };
+    // the cluster halves of a forward / backward transform (nothing for one CTA)
+    auto fwd_tail = [&](uint64_t (&v)[E]) {
+        if constexpr (LOGS > 0)
+            cluster_fwd_tail<LOGN, LOGS, true>(reinterpret_cast<uint64_t(&)[4]>(v), t, cr, recv_next(),
+                                               (1 << LOGS) > 4 ? xb() : nullptr, prm.tw_fwd);
+    };
+    auto inv_head = [&](uint64_t (&v)[E]) {
+        if constexpr (LOGS > 0)
+            cluster_inv_head<LOGN, LOGS>(reinterpret_cast<uint64_t(&)[4]>(v), t, cr, recv_next(),
+                                         (1 << LOGS) > 4 ? xb() : nullptr, prm.tw_inv);
+    };
 
-    for (uint64_t b = blockIdx.x; b < prm.batch; b += gridDim.x) {
+    for (uint64_t b = blockIdx.x >> LOGS; b < prm.batch; b += gridDim.x >> LOGS) {
         __syncthreads();  // previous ciphertext done with lwe_s / acc (and twiddles written)
         const uint64_t* lwe = prm.lwes + b * prm.lwe_stride;
         bool bad = false;
@@ -238,7 +285,7 @@ br_kernel(const BrKernelParams prm) {
             bad |= v > MASK2N;
             lwe_s[i] = v & MASK2N;
         }
-        if (bad) atomicOr(prm.err, 1u);
+        if (bad && cr == 0) atomicOr(prm.err, 1u);
         __syncthreads();
 
         // Prologue: acc = NTT(acc_in) * X^b   (cggi_blind_rotation.cpp:242,333-358)
@@ -251,13 +298,15 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + t + j * T];
-                ntt_forward_k<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                    for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + ((uint32_t)(t + j * T) << LOGS) + cr];
+                ntt_forward_k<LOGL, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                fwd_tail(x[0]);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int j = 0; j < E; ++j)
-                        acc_st(h0 + p, j, gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j), bb)));
+                        acc_st(h0 + p, j,
+                               gl_mul(x[p][j], mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(sbase + E * t + j), bb)));
             }
         }
 
@@ -272,7 +321,8 @@ br_kernel(const BrKernelParams prm) {
             } else {
                 if (a0 == 0) continue;                               // cggi_blind_rotation.cpp:369-370
             }
-            const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C);
+            // this CTA's part of the group's key rows (row stride C*N, part offset C*NL*cr)
+            const uint64_t* kit = prm.key + (uint64_t)(i / step) * (2ull * L * N * C) + (uint64_t)cr * (C * NL);
 
             // MAC accumulators (canonical: every update is a gl_fma); the digit-staged
             // form sums per slot pair after the digit loop instead
@@ -293,7 +343,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int j = 0; j < E; ++j) {
                     dst[j] = acc_ld(h, j);
                     if constexpr (VARIANT == kCggiBinary)
-                        dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(E * t + j),
+                        dst[j] = gl_mul(dst[j], gl_sub(mono<LOGN>(prm.psi_pow, slot_exponent<LOGN>(sbase + E * t + j),
                                                                   2u * N - a0), 1));
                 }
             };
@@ -306,7 +356,7 @@ br_kernel(const BrKernelParams prm) {
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
                 load_half(cx[1], 1);
-                ntt_backward_unscaled_k<LOGN, 2, LOGE, R4>(cx, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGL, 2, LOGE, R4>(cx, t, xb(), tw_i);
                 finish_half(cx[0]);
                 finish_half(cx[1]);
             }
@@ -329,7 +379,8 @@ br_kernel(const BrKernelParams prm) {
                     if (r == 0 || r == L) {
                         uint64_t (&c1)[1][E] = reinterpret_cast<uint64_t(&)[1][E]>(cx[0]);
                         load_half(cx[0], r == 0 ? 0 : 1);
-                        ntt_backward_unscaled_k<LOGN, 1, LOGE, R4>(c1, t, xb(), tw_i);
+                        inv_head(cx[0]);
+                        ntt_backward_unscaled_k<LOGL, 1, LOGE, R4>(c1, t, xb(), tw_i);
                         finish_half(cx[0]);
                     }
                 }
@@ -364,15 +415,16 @@ br_kernel(const BrKernelParams prm) {
                             x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
                         }
                     }
-                    fwd_pass_math<LOGN, 0, K, LOGE, R4, true>(x, t, tw_f);
+                    fwd_pass_math<LOGL, 0, K, LOGE, R4, true>(x, t, tw_f);
                 }
-                ntt_forward_after_pass0<LOGN, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                ntt_forward_after_pass0<LOGL, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                fwd_tail(x[0]);
                 if constexpr (DS) {
                     // rows before the last wait in the stage (this thread's own slots: no barrier)
                     if (r + 1 < 2 * L) {
 #pragma unroll
                         for (int jp = 0; jp < E / 2; ++jp)
-                            *reinterpret_cast<ulonglong2*>(xs + r * N + (jp * T + t) * 2) =
+                            *reinterpret_cast<ulonglong2*>(xs + r * NL + (jp * T + t) * 2) =
                                 make_ulonglong2(x[0][2 * jp], x[0][2 * jp + 1]);
                     }
                 } else {
@@ -398,7 +450,7 @@ br_kernel(const BrKernelParams prm) {
 
             // Accumulator update of slot j from its C key-component sums oj[c].
             auto update = [&](int j, const uint64_t* oj) {
-                const uint32_t ek = slot_exponent<LOGN>(E * t + j);
+                const uint32_t ek = slot_exponent<LOGN>(sbase + E * t + j);
                 uint64_t ua = acc_ld(0, j);
                 uint64_t ub = acc_ld(1, j);
                 if constexpr (VARIANT == kCggiBinary) {
@@ -439,7 +491,7 @@ br_kernel(const BrKernelParams prm) {
                                                                ((c * (E / 2) + jp) * T + t) * 2);
                 };
                 auto row_x = [&](int jp, int r) -> ulonglong2 {
-                    return r < R2 - 1 ? *reinterpret_cast<const ulonglong2*>(xs + r * N + (jp * T + t) * 2)
+                    return r < R2 - 1 ? *reinterpret_cast<const ulonglong2*>(xs + r * NL + (jp * T + t) * 2)
                                       : make_ulonglong2(x[0][2 * jp], x[0][2 * jp + 1]);
                 };
                 if constexpr (AH > 0) {
@@ -530,17 +582,19 @@ br_kernel(const BrKernelParams prm) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) x[p][j] = acc_ld(h0 + p, j);
             if (prm.out_coef) {
-                ntt_backward_unscaled_k<LOGN, K, LOGE, R4>(x, t, xb(), tw_i);
+                inv_head(x[0]);
+                ntt_backward_unscaled_k<LOGL, K, LOGE, R4>(x, t, xb(), tw_i);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
-                    for (int j = 0; j < E; ++j) res[(h0 + p) * N + t + j * T] = gl_div_pow2<LOGN>(x[p][j]);
+                    for (int j = 0; j < E; ++j)
+                        res[(h0 + p) * N + ((uint32_t)(t + j * T) << LOGS) + cr] = gl_div_pow2<LOGN>(x[p][j]);
             } else {
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int c = 0; c < E / 2; ++c)
-                        *reinterpret_cast<ulonglong2*>(res + (h0 + p) * N + E * t + 2 * c) =
+                        *reinterpret_cast<ulonglong2*>(res + (h0 + p) * N + sbase + E * t + 2 * c) =
                             make_ulonglong2(x[p][2 * c], x[p][2 * c + 1]);
             }
         }

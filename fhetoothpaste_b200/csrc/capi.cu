@@ -214,6 +214,7 @@ struct tp_br_ctx {
     const void* kernels[4] = {};  // by loge (2, 3)
     int grid_caps[4] = {};        // resident blocks on the device, by loge
     size_t smem[4] = {};          // dynamic shared memory bytes, by loge
+    int logs = 0;                 // log2 of the CTAs of one rotation's cluster (N > 4096), else 0
     int split = 1;                // thread blocks per rotation (2, 4: cluster kernels, tile 4 only)
     int mac = 0;                  // multiply-accumulate form of the one-block kernel at tile 4 (TP_MAC_*)
     const void* ds_kernel = nullptr;  // digit-staged one-block kernel (digits 3 or 4, N <= 2048)
@@ -231,6 +232,63 @@ struct tp_br_ctx {
     std::mutex mu;                // serializes host-pointer calls on one context
 };
 
+// Ring sizes above 4096: one rotation per cluster of 2^logs CTAs. Sets up the
+// row-by-row kernel and, for 3 or 4 digits where it fits, the digit-staged one
+// (the default then); 4 coefficients per thread, no split kernels.
+static tp_status br_setup_cluster(tp_br_ctx* c) {
+    const int S = 1 << c->logs;
+    const uint32_t T = c->prm.ring_dim >> (c->logs + 2);
+    auto probe = [&](const void* k, size_t smem, int* cap) -> bool {
+        if (!k || smem > 227u * 1024u) return false;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess && S > 8) e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        int clusters = 0;
+        if (e == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr = {};
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = (unsigned)S;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.gridDim = dim3((unsigned)S * (unsigned)sm_count(c->device));
+            cfg.blockDim = dim3(T);
+            cfg.dynamicSmemBytes = smem;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            e = cudaOccupancyMaxActiveClusters(&clusters, k, &cfg);
+        }
+        if (e != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            return false;
+        }
+        *cap = clusters;
+        return true;
+    };
+    const void* k = tp::br_kernel_lookup(c->logn, c->prm.variant, 2, 0);
+    const size_t smem = tp::br_smem_words(c->logn, c->prm.variant, c->prm.lwe_dim, 2, 0, c->logs) * 8;
+    int cap = 0;
+    if (!probe(k, smem, &cap))
+        return fail(TP_ERR_PARAM, "the %d-CTA cluster rotation kernel does not fit (N=%u, n=%u, smem=%zu) on device %d",
+                    S, c->prm.ring_dim, c->prm.lwe_dim, smem, c->device);
+    c->kernels[2] = k;
+    c->smem[2] = smem;
+    c->grid_caps[2] = cap;
+    c->loge = 2;
+    if (c->prm.digits == 3 || c->prm.digits == 4) {
+        const void* kd = tp::br_kernel_lookup(c->logn, c->prm.variant, 2, (int)c->prm.digits);
+        const size_t sd =
+            tp::br_smem_words(c->logn, c->prm.variant, c->prm.lwe_dim, 2, (int)c->prm.digits, c->logs) * 8;
+        int capd = 0;
+        if (probe(kd, sd, &capd)) {
+            c->ds_kernel = kd;
+            c->ds_smem = sd;
+            c->ds_cap = capd;
+            c->mac = TP_MAC_DIGIT_STAGED;
+        }
+    }
+    return TP_OK;
+}
+
 extern "C" {
 
 const char* tp_last_error(void) { return g_err.c_str(); }
@@ -243,7 +301,8 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
     if (p->modulus != kP) return fail(TP_ERR_PARAM, "modulus must be the Goldilocks prime 2^64-2^32+1");
     if (p->variant < 0 || p->variant > 2) return fail(TP_ERR_PARAM, "unknown variant %d", p->variant);
     const uint64_t N = p->ring_dim;
-    if (N < 128 || N > 4096 || (N & (N - 1))) return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (N < 128 || N > 32768 || (N & (N - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
     if (p->lwe_dim == 0) return fail(TP_ERR_PARAM, "lwe_dim must be positive");
     if (p->variant == TP_BR_BMMP_BINARY && (p->lwe_dim % 2)) return fail(TP_ERR_PARAM, "BMMP needs an even lwe_dim");
     if (p->basis < 2 || (p->basis & (p->basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
@@ -257,6 +316,7 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
     c->prm = *p;
     c->device = device;
     c->logn = ilog2(N);
+    c->logs = tp::br_cluster_logs(c->logn);
     c->G = tp::br_rgsw_per_group(p->variant);
     c->groups = p->variant == TP_BR_BMMP_BINARY ? p->lwe_dim / 2 : p->lwe_dim;
     c->key_words = c->groups * (uint64_t)c->G * 4 * N * p->digits;
@@ -326,6 +386,16 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
     // Digits small enough for the integer pass 0 of the digit transforms: signed digits lie in
     // [-2^(beta-1), 2^(beta-1)), unsigned in [0, 2^beta); the pass is exact up to 2^14.
     kp.small_digits = (p->variant == TP_BR_CGGI_BINARY ? beta <= 14 : beta <= 15) ? 1u : 0u;
+    if (c->logs > 0) {
+        tp_status cs = br_setup_cluster(c);
+        if (cs != TP_OK) {
+            cudaFree(c->err);
+            delete c;
+            return cs;
+        }
+        *out = c;
+        return TP_OK;
+    }
     for (int lg = 2; lg <= 3; ++lg) {
         const void* k = tp::br_kernel_lookup(c->logn, p->variant, lg);
         const size_t smem = tp::br_smem_words(c->logn, p->variant, p->lwe_dim, lg) * 8;
@@ -426,7 +496,7 @@ tp_status tp_br_upload_key(tp_br_ctx* c, const uint64_t* brk, uint64_t words) {
             const int threads = 256;
             const uint64_t blocks = std::min<uint64_t>((total + threads - 1) / threads, 65535);
             tp::key_relayout_kernel<<<(unsigned)blocks, threads>>>(c->key + g0 * per_group, stage, ng, c->G,
-                                                                    2 * c->prm.digits, c->logn, c->loge);
+                                                                    2 * c->prm.digits, c->logn, c->loge, c->logs);
             tp::note_launch();
             e = cudaGetLastError();
         }
@@ -447,6 +517,7 @@ tp_status tp_br_blind_rotate_batch(tp_br_ctx* c, uint64_t batch, uint64_t* resul
 // Moves the resident key to the layout of another tile (2x key memory while it runs).
 static tp_status br_retile(tp_br_ctx* c, int loge) {
     if (loge == c->loge) return TP_OK;
+    if (c->logs > 0) return fail(TP_ERR_PARAM, "cluster rotations run with 4 coefficients per thread only");
     if (c->key_ready) {
         uint64_t* nk = nullptr;
         TP_CUDA(cudaMalloc(&nk, c->key_words * 8));
@@ -474,6 +545,9 @@ tp_status tp_br_set_tile(tp_br_ctx* c, uint32_t coef_per_thread) {
     if (coef_per_thread == 8 && c->split > 1)
         return fail(TP_ERR_STATE, "the %d-block kernel runs with 4 coefficients per thread; set the split to 1 first",
                     c->split);
+    if (coef_per_thread == 8 && c->logs > 0)
+        return fail(TP_ERR_PARAM, "ring dimension %u rotates on a CTA cluster with 4 coefficients per thread only",
+                    c->prm.ring_dim);
     TP_CUDA(cudaSetDevice(c->device));
     return br_retile(c, coef_per_thread == 4 ? 2 : 3);
 }
@@ -565,6 +639,7 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     for (const Cand& cd : cands) {
         if ((cd.split == 2 && c->pair_cap == 0) || (cd.split == 4 && c->quad_cap == 0)) continue;
         if (cd.mac == TP_MAC_DIGIT_STAGED && !c->ds_kernel) continue;
+        if (cd.loge != 2 && c->logs > 0) continue;  // clusters: 4 coefficients per thread
         s = br_retile(c, cd.loge);
         if (s != TP_OK) break;
         c->split = cd.split;
@@ -2208,6 +2283,24 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
     }
     const bool ds = br_uses_ds(c);
     const unsigned grid = (unsigned)std::min<uint64_t>(batch, br_concurrency(c, 1));
+    if (c->logs > 0) {
+        // one rotation per cluster of 2^logs CTAs
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr = {};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = 1u << c->logs;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(grid << c->logs);
+        cfg.blockDim = dim3(c->prm.ring_dim >> (c->logs + 2));
+        cfg.dynamicSmemBytes = ds ? c->ds_smem : c->smem[2];
+        cfg.stream = (cudaStream_t)stream;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        TP_CUDA(cudaLaunchKernelExC(&cfg, ds ? c->ds_kernel : c->kernels[2], args));
+        tp::note_launch();
+        return TP_OK;
+    }
     TP_CUDA(cudaLaunchKernel(ds ? c->ds_kernel : c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge),
                              args, ds ? c->ds_smem : c->smem[c->loge], (cudaStream_t)stream));
     tp::note_launch();

@@ -14,6 +14,9 @@ const void* ntt_kernel_ptr_10(bool forward);
 const void* br_kernel_ptr_11(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_11(bool forward);
 const void* br_kernel_ptr_12(int variant, int loge, int dl);
+const void* br_kernel_ptr_13(int variant, int loge, int dl);
+const void* br_kernel_ptr_14(int variant, int loge, int dl);
+const void* br_kernel_ptr_15(int variant, int loge, int dl);
 const void* ntt_kernel_ptr_12(bool forward);
 const void* br_pair_kernel_ptr_7(int variant, int split);
 const void* br_pair_kernel_ptr_8(int variant, int split);
@@ -28,8 +31,9 @@ const void* ks_kernel_ptr_10(int mode, int loge);
 const void* ks_kernel_ptr_11(int mode, int loge);
 const void* ks_kernel_ptr_12(int mode, int loge);
 
-// One-block rotation kernel; dl = 0: multiply-accumulate row by row, dl = 3 or
-// 4: the digit-staged form for that digit count (nullptr where not built).
+// One-block rotation kernel (one cluster of CTAs per rotation above N = 4096);
+// dl = 0: multiply-accumulate row by row, dl = 3 or 4: the digit-staged form for
+// that digit count (nullptr where not built).
 inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0) {
     switch (logn) {
         case 7: return br_kernel_ptr_7(variant, loge, dl);
@@ -38,6 +42,9 @@ inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0)
         case 10: return br_kernel_ptr_10(variant, loge, dl);
         case 11: return br_kernel_ptr_11(variant, loge, dl);
         case 12: return br_kernel_ptr_12(variant, loge, dl);
+        case 13: return br_kernel_ptr_13(variant, loge, dl);
+        case 14: return br_kernel_ptr_14(variant, loge, dl);
+        case 15: return br_kernel_ptr_15(variant, loge, dl);
         default: return nullptr;
     }
 }

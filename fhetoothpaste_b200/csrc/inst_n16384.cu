@@ -1,0 +1,27 @@
+// Kernel instantiations for N = 16384: one rotation per cluster of 8 CTAs
+// (cluster_ntt.cuh), 4 coefficients per thread; compiled as a separate unit so
+// the ring sizes build in parallel.
+#include "br_kernels.cuh"
+#include "dispatch.h"
+
+namespace tp {
+
+const void* br_kernel_ptr_14(int variant, int loge, int dl) {
+    if (loge != 2 || (dl != 0 && dl != 3 && dl != 4)) return nullptr;
+    switch (variant) {
+        case kCggiBinary:
+            return dl == 0 ? (const void*)br_kernel<14, kCggiBinary, 2, 0, 3>
+                           : (dl == 3 ? (const void*)br_kernel<14, kCggiBinary, 2, 3, 3>
+                                      : (const void*)br_kernel<14, kCggiBinary, 2, 4, 3>);
+        case kCggiTernary:
+            return dl == 0 ? (const void*)br_kernel<14, kCggiTernary, 2, 0, 3>
+                           : (dl == 3 ? (const void*)br_kernel<14, kCggiTernary, 2, 3, 3>
+                                      : (const void*)br_kernel<14, kCggiTernary, 2, 4, 3>);
+        default:
+            return dl == 0 ? (const void*)br_kernel<14, kBmmpBinary, 2, 0, 3>
+                           : (dl == 3 ? (const void*)br_kernel<14, kBmmpBinary, 2, 3, 3>
+                                      : (const void*)br_kernel<14, kBmmpBinary, 2, 4, 3>);
+    }
+}
+
+}  // namespace tp

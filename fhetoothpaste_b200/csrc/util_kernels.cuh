@@ -9,18 +9,23 @@ namespace tp {
 // Device position of key word (group it, gadget row r, component c = 2g + h,
 // slot k) for a rotation kernel with 2^loge coefficients per thread: slot
 // k = E*t + 2jp + e sits at ((c*E/2 + jp)*T + t)*2 + e inside the (it, r) row.
+// A cluster of 2^logs CTAs (ring sizes above 4096) splits each row into 2^logs
+// parts of 2G * NL words, NL = N >> logs: slot k belongs to part k / NL and
+// takes the same position inside it as slot k mod NL of an NL-slot row.
 __device__ __forceinline__ uint64_t key_device_pos(uint64_t it, uint64_t r, uint64_t c, uint64_t k, uint32_t G,
-                                                   uint32_t rows, uint32_t logn, uint32_t loge) {
+                                                   uint32_t rows, uint32_t logn, uint32_t loge, uint32_t logs = 0) {
     const uint64_t N = 1ull << logn;
+    const uint64_t NL = N >> logs;
     const uint64_t E = 1ull << loge;
-    const uint64_t T = N >> loge;
-    const uint64_t t = k >> loge, jp = (k & (E - 1)) >> 1, e = k & 1;
-    return (it * rows + r) * 2 * G * N + ((c * (E / 2) + jp) * T + t) * 2 + e;
+    const uint64_t T = NL >> loge;
+    const uint64_t part = k / NL, kl = k % NL;
+    const uint64_t t = kl >> loge, jp = (kl & (E - 1)) >> 1, e = kl & 1;
+    return (it * rows + r) * 2 * G * N + part * (2 * G * NL) + ((c * (E / 2) + jp) * T + t) * 2 + e;
 }
 
 // Reference m_brk layout ((it*G + g)*rows + r)*2N + h*N + k  ->  device layout.
 __global__ void key_relayout_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
-                                    uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge) {
+                                    uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge, uint32_t logs = 0) {
     const uint64_t N = 1ull << logn;
     const uint64_t total = groups * G * rows * 2 * N;
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
@@ -30,7 +35,7 @@ __global__ void key_relayout_kernel(uint64_t* __restrict__ dst, const uint64_t* 
         const uint64_t r = (w / (2 * N)) % rows;
         const uint64_t ig = w / (2 * N * rows);
         const uint64_t g = ig % G, it = ig / G;
-        dst[key_device_pos(it, r, 2 * g + h, k, G, rows, logn, loge)] = src[w];
+        dst[key_device_pos(it, r, 2 * g + h, k, G, rows, logn, loge, logs)] = src[w];
     }
 }
 
