@@ -8,7 +8,8 @@
  *
  * Arithmetic is over the Goldilocks prime p = 2^64 - 2^32 + 1. All ciphertext
  * words are canonical residues in [0, p); polynomials have N coefficients with
- * N a power of two in [128, 4096]. "NTT domain" means the reference's
+ * N a power of two in [128, 4096] (blind rotation: up to 32768, on a cluster of
+ * 4, 8 or 16 CTAs per rotation above 4096). "NTT domain" means the reference's
  * evaluation order: slot k holds a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N)
  * (lib/src/backend/solinas.cpp:168-313 of the reference).
  *
@@ -127,8 +128,9 @@ uint32_t tp_br_get_split(const tp_br_ctx* ctx);
  * TP_MAC_ROWWISE keeps a canonical running sum per output word, one gadget row at
  * a time (the next key row staged in shared memory while the digit is transformed);
  * TP_MAC_DIGIT_STAGED transforms all 2l digits first and sums each output word over
- * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048; the default
- * where it is built). Both give the same words. Project-specific tuning (no
+ * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048 and on the
+ * CTA clusters of N = 8192..32768 where shared memory allows; the default up to
+ * N = 2048). Both give the same words. Project-specific tuning (no
  * reference counterpart); tp_br_autotune chooses between them. */
 enum { TP_MAC_ROWWISE = 0, TP_MAC_DIGIT_STAGED = 1 };
 tp_status tp_br_set_mac_form(tp_br_ctx* ctx, uint32_t form);

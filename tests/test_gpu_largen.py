@@ -35,9 +35,15 @@ def test_large_ring_matches_reference(native, oracle, name):
     brk = oracle.br_keygen(v, N, n, c["basis_log2"], c["digits"], c["std"], lk, rk, c["key_seed"])
     rot = GpuBlindRotator(BlindRotationContext(v, N, n, 1 << c["basis_log2"], c["digits"]), brk)
     lwes, accs, coefs = br_inputs(name, N, n, c["seed"])
-    forms = [0, 1] if c["digits"] in (3, 4) and rot.mac_form == 1 else [rot.mac_form]
-    for form in forms:
-        rot.set_mac_form(form)
+    assert rot.mac_form == 0  # row-by-row is the default on a cluster
+    for form in (0, 1):
+        if form == 1:
+            try:
+                rot.set_mac_form(1)   # the digit-staged form, where it fits
+            except Exception:
+                continue
+        else:
+            rot.set_mac_form(0)
         for i, oc in enumerate(coefs):
             res = np.zeros(2 * N, np.uint64)
             rot.BlindRotate(res, np.ascontiguousarray(lwes[i]), np.ascontiguousarray(accs[i]), bool(oc))
