@@ -63,6 +63,8 @@ def lib() -> ctypes.CDLL:
         "tp_br_get_split": (ctypes.c_uint32, [VP]),
         "tp_br_set_mac_form": (ctypes.c_int, [VP, ctypes.c_uint32]),
         "tp_br_get_mac_form": (ctypes.c_uint32, [VP]),
+        "tp_br_set_radix": (ctypes.c_int, [VP, ctypes.c_uint32]),
+        "tp_br_get_radix": (ctypes.c_uint32, [VP]),
         "tp_br_autotune": (ctypes.c_int, [VP, U64, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double)]),
         "tp_sample_extract_batch": (ctypes.c_int, [ctypes.c_uint32, U64, VP, VP, VP]),
         "tp_br_batch_graph_create": (ctypes.c_int, [VP, U64, VP, VP, U64, VP, U64, ctypes.c_int, VP,

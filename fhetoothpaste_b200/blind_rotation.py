@@ -137,6 +137,14 @@ class GpuBlindRotator:
     def set_mac_form(self, form: int) -> None:
         nat.check(nat.lib().tp_br_set_mac_form(self._h, form))
 
+    @property
+    def radix(self) -> int:
+        """NTT radix of the one-block kernel at tile 4 (2, or 4 for the fused radix-4 passes)."""
+        return int(nat.lib().tp_br_get_radix(self._h))
+
+    def set_radix(self, radix: int) -> None:
+        nat.check(nat.lib().tp_br_set_radix(self._h, radix))
+
     def autotune(self, batch: int) -> tuple[int, float]:
         """Times every tile (and the two- and four-block splits) on `batch` synthetic rotations and keeps
         the fastest."""

@@ -103,9 +103,9 @@ __host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int bl
 // distributed transform's exchange.
 __host__ __device__ constexpr int br_cluster_logs(int logn) { return logn > 12 ? logn - 11 : 0; }
 
-__host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge, int logs = 0) {
+__host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge, int logs = 0, bool r4 = false) {
     return (size_t)(br_smem_twiddles(logn - logs)
-                        ? 2 * br_twiddle_words(logn - logs, loge, br_fused_radix4(loge, variant, 1))
+                        ? 2 * br_twiddle_words(logn - logs, loge, r4 || br_fused_radix4(loge, variant, 1))
                         : 0) +
            (size_t)(1 << (logn - logs)) * (2 * br_ntt_width(logn, variant) + 2 + (logs ? 2 : 0)) +
            1024;  // LWE area budget for the plan; the host adds the real size
@@ -113,8 +113,8 @@ __host__ __device__ constexpr size_t br_base_words(int logn, int variant, int lo
 __host__ __device__ constexpr size_t br_stage_words(int logn, int variant, int logs = 0) {
     return (size_t)(1 << (logn - logs)) * 2 * br_rgsw_per_group(variant);
 }
-__host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int loge, int logs = 0) {
-    return (br_base_words(logn, variant, loge, logs) + br_stage_words(logn, variant, logs)) * 8 <= 227u * 1024u;
+__host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int loge, int logs = 0, bool r4 = false) {
+    return (br_base_words(logn, variant, loge, logs, r4) + br_stage_words(logn, variant, logs)) * 8 <= 227u * 1024u;
 }
 
 // Digit-staged multiply-accumulate (template parameter DL = the digit count l,
@@ -141,13 +141,13 @@ __host__ __device__ constexpr size_t br_digit_stage_words(int logn, int dl) {
 // (DL > 0), two receive areas (2 NL, clusters only), the LWE vector (n+1, rounded
 // up to an even count).
 __host__ __device__ constexpr size_t br_smem_words(int logn, int variant, uint32_t n, int loge, int dl = 0,
-                                                   int logs = 0) {
+                                                   int logs = 0, bool r4 = false) {
     return (size_t)(br_smem_twiddles(logn - logs)
-                        ? 2 * br_twiddle_words(logn - logs, loge, br_fused_radix4(loge, variant, 1))
+                        ? 2 * br_twiddle_words(logn - logs, loge, r4 || br_fused_radix4(loge, variant, 1))
                         : 0) +
            (size_t)(1 << (logn - logs)) * (2 * br_ntt_width(logn, variant) + 2 + (logs ? 2 : 0)) +
            (dl > 0 ? br_digit_stage_words(logn - logs, dl)
-                   : (br_key_prefetch(logn, variant, loge, logs) ? br_stage_words(logn, variant, logs) : 0)) +
+                   : (br_key_prefetch(logn, variant, loge, logs, r4) ? br_stage_words(logn, variant, logs) : 0)) +
            ((n + 2) & ~1u);
 }
 
@@ -194,7 +194,10 @@ __host__ __device__ constexpr int br_min_blocks(int logn, int variant, int loge)
 // size), each CTA holding the coefficients i = i' 2^LOGS + r and the slots
 // r NL .. r NL + NL - 1 of the cluster's rank r (cluster_ntt.cuh); the
 // multiply-accumulate, the update and the key words of a slot are local to its CTA.
-template <int LOGN, int VARIANT, int LOGE, int DL = 0, int LOGS = 0>
+// RADIX4: the transforms' radix-4 passes use the fused form (three products and a
+// shift per two levels, ntt_block.cuh) instead of radix-2 butterflies: a runtime
+// choice per context (tp_br_set_radix), built for one CTA per rotation.
+template <int LOGN, int VARIANT, int LOGE, int DL = 0, int LOGS = 0, bool RADIX4 = false>
 __global__ void __launch_bounds__((1 << (LOGN - LOGS)) >> LOGE, br_min_blocks(LOGN - LOGS, VARIANT, LOGE))
 br_kernel(const BrKernelParams prm) {
     constexpr int LOGL = LOGN - LOGS;        // log2 of the coefficients / slots per CTA
@@ -209,9 +212,10 @@ br_kernel(const BrKernelParams prm) {
     constexpr bool TW_SMEM = br_smem_twiddles(LOGL);
     constexpr uint32_t MASK2N = 2u * N - 1u;
     constexpr bool SIGNED = VARIANT != kCggiBinary;
-    constexpr bool R4 = br_fused_radix4(LOGE, VARIANT, 1);
+    constexpr bool R4 = RADIX4 || br_fused_radix4(LOGE, VARIANT, 1);
+    static_assert(!RADIX4 || LOGE == 2, "the fused radix-4 passes need 4 coefficients per thread");
     constexpr bool DS = DL > 0;              // digit-staged multiply-accumulate (prm.digits == DL)
-    constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE, LOGS);
+    constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE, LOGS, R4);
     static_assert(!DS || (LOGE == 2 && K == 1), "the digit stage runs with 4 coefficients per thread");
     static_assert(LOGS == 0 || (LOGE == 2 && K == 1 && !R4), "clusters run radix-2 with 4 coefficients per thread");
 

@@ -220,6 +220,13 @@ struct tp_br_ctx {
     const void* ds_kernel = nullptr;  // digit-staged one-block kernel (digits 3 or 4, N <= 2048)
     size_t ds_smem = 0;
     int ds_cap = 0;               // its resident blocks on the device (0: unavailable)
+    int radix = 2;                // NTT passes of the one-block kernel at tile 4: 2 or 4 (fused radix-4)
+    struct Form {
+        const void* k = nullptr;
+        size_t smem = 0;
+        int cap = 0;
+    };
+    Form r4_row, r4_ds;           // the fused radix-4 one-block kernels (row by row, digit-staged)
     const void* pair_kernel = nullptr;
     size_t pair_smem = 0;
     int pair_cap = 0;             // resident two-CTA clusters on the device (0: unavailable)
@@ -434,6 +441,25 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
             cudaGetLastError();  // clear the optional probe's error
         }
     }
+    // fused radix-4 forms at tile 4: optional (built for N = 1024 .. 4096, where they fit)
+    for (int dl : {0, (int)p->digits}) {
+        if (dl != 0 && dl != 3 && dl != 4) continue;
+        const void* k = tp::br_kernel_lookup(c->logn, p->variant, 2, dl, true);
+        const size_t smem = tp::br_smem_words(c->logn, p->variant, p->lwe_dim, 2, dl, 0, true) * 8;
+        int per_sm = 0;
+        cudaError_t re = k && smem <= 227u * 1024u
+                             ? cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                             : cudaErrorInvalidValue;
+        if (re == cudaSuccess) re = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(N >> 2), smem);
+        if (re == cudaSuccess && per_sm > 0) {
+            auto& f = dl == 0 ? c->r4_row : c->r4_ds;
+            f.k = k;
+            f.smem = smem;
+            f.cap = per_sm * sm_count(device);
+        } else if (k) {
+            cudaGetLastError();
+        }
+    }
     for (int split = 2; split <= 4; split += 2) {
         // two- and four-CTA cluster kernels; optional: a parameter set one does not fit keeps its cap 0
         const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant, split);
@@ -588,6 +614,19 @@ tp_status tp_br_set_mac_form(tp_br_ctx* c, uint32_t form) {
 
 uint32_t tp_br_get_mac_form(const tp_br_ctx* c) { return c ? (uint32_t)c->mac : 0u; }
 
+tp_status tp_br_set_radix(tp_br_ctx* c, uint32_t radix) {
+    if (!c) return fail(TP_ERR_PARAM, "null context");
+    if (radix != 2 && radix != 4) return fail(TP_ERR_PARAM, "radix must be 2 or 4");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (radix == 4 && !c->r4_row.k)
+        return fail(TP_ERR_PARAM, "fused radix-4 rotation kernels are not built for this parameter set "
+                                  "(N = 1024 .. 4096, shared memory permitting)");
+    c->radix = (int)radix;
+    return TP_OK;
+}
+
+uint32_t tp_br_get_radix(const tp_br_ctx* c) { return c ? (uint32_t)c->radix : 0u; }
+
 tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_thread, double* best_rotations_per_s) {
     if (!c) return fail(TP_ERR_PARAM, "null context");
     if (!c->key_ready) return fail(TP_ERR_STATE, "no key uploaded");
@@ -633,18 +672,22 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     std::lock_guard<std::mutex> lk(c->mu);
     int best_split = c->split;
     int best_mac = c->mac;
-    // tile (coefficients per thread), blocks per rotation, multiply-accumulate form
-    struct Cand { int loge, split, mac; };
-    const Cand cands[] = {{3, 1, TP_MAC_ROWWISE}, {2, 1, TP_MAC_ROWWISE}, {2, 1, TP_MAC_DIGIT_STAGED},
-                          {2, 2, TP_MAC_ROWWISE}, {2, 4, TP_MAC_ROWWISE}};
+    int best_radix = c->radix;
+    // tile (coefficients per thread), blocks per rotation, multiply-accumulate form, NTT radix
+    struct Cand { int loge, split, mac, radix; };
+    const Cand cands[] = {{3, 1, TP_MAC_ROWWISE, 2},      {2, 1, TP_MAC_ROWWISE, 2}, {2, 1, TP_MAC_DIGIT_STAGED, 2},
+                          {2, 1, TP_MAC_ROWWISE, 4},      {2, 1, TP_MAC_DIGIT_STAGED, 4},
+                          {2, 2, TP_MAC_ROWWISE, 2},      {2, 4, TP_MAC_ROWWISE, 2}};
     for (const Cand& cd : cands) {
         if ((cd.split == 2 && c->pair_cap == 0) || (cd.split == 4 && c->quad_cap == 0)) continue;
         if (cd.mac == TP_MAC_DIGIT_STAGED && !c->ds_kernel) continue;
+        if (cd.radix == 4 && !(cd.mac == TP_MAC_DIGIT_STAGED ? c->r4_ds.k : c->r4_row.k)) continue;
         if (cd.loge != 2 && c->logs > 0) continue;  // clusters: 4 coefficients per thread
         s = br_retile(c, cd.loge);
         if (s != TP_OK) break;
         c->split = cd.split;
         c->mac = cd.mac;
+        c->radix = cd.radix;
         for (int rep = 0; rep < 3 && s == TP_OK; ++rep) {  // one warm-up, two timed
             if (rep == 1) cudaEventRecord(e0, st);
             s = tp_br_blind_rotate_batch(c, tb, d_res, d_lwe, n + 1, d_acc, 0, 0, st);
@@ -664,6 +707,7 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
             best = cd.loge;
             best_split = cd.split;
             best_mac = cd.mac;
+            best_radix = cd.radix;
         }
     }
     c->split = 1;
@@ -671,6 +715,7 @@ tp_status tp_br_autotune(tp_br_ctx* c, uint64_t batch, uint32_t* best_coef_per_t
     if (s == TP_OK) {
         c->split = best_split;
         c->mac = best_mac;
+        c->radix = best_radix;
     }
     cleanup();
     if (s != TP_OK) return s;
@@ -2242,11 +2287,26 @@ static bool br_uses_ds(const tp_br_ctx* c) {
     return c->loge == 2 && c->mac == TP_MAC_DIGIT_STAGED && c->ds_kernel;
 }
 
+// The one-block kernel of the context's settings: tile, multiply-accumulate form
+// and radix (each form falls back to what is built).
+static tp_br_ctx::Form br_one_block(const tp_br_ctx* c) {
+    const bool ds = br_uses_ds(c);
+    if (c->loge == 2 && c->radix == 4) {
+        if (ds && c->r4_ds.k) return c->r4_ds;
+        if (!ds && c->r4_row.k) return c->r4_row;
+    }
+    tp_br_ctx::Form f;
+    f.k = ds ? c->ds_kernel : c->kernels[c->loge];
+    f.smem = ds ? c->ds_smem : c->smem[c->loge];
+    f.cap = ds ? c->ds_cap : c->grid_caps[c->loge];
+    return f;
+}
+
 uint64_t br_concurrency(const tp_br_ctx* c, int split) {
     if (!c) return 0;
     if (split == 2) return c->loge == 2 ? (uint64_t)c->pair_cap : 0;
     if (split == 4) return c->loge == 2 ? (uint64_t)c->quad_cap : 0;
-    return br_uses_ds(c) ? (uint64_t)c->ds_cap : (uint64_t)c->grid_caps[c->loge];
+    return (uint64_t)br_one_block(c).cap;
 }
 
 tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const uint64_t* lwes,
@@ -2302,8 +2362,8 @@ tp_status br_batch_launch(tp_br_ctx* c, uint64_t batch, uint64_t* results, const
         tp::note_launch();
         return TP_OK;
     }
-    TP_CUDA(cudaLaunchKernel(ds ? c->ds_kernel : c->kernels[c->loge], dim3(grid), dim3(c->prm.ring_dim >> c->loge),
-                             args, ds ? c->ds_smem : c->smem[c->loge], (cudaStream_t)stream));
+    const tp_br_ctx::Form f = br_one_block(c);
+    TP_CUDA(cudaLaunchKernel(f.k, dim3(grid), dim3(c->prm.ring_dim >> c->loge), args, f.smem, (cudaStream_t)stream));
     tp::note_launch();
     return TP_OK;
 }

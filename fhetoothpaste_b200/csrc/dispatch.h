@@ -3,20 +3,20 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_7(int variant, int loge, int dl);
+const void* br_kernel_ptr_7(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_7(bool forward);
-const void* br_kernel_ptr_8(int variant, int loge, int dl);
+const void* br_kernel_ptr_8(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_8(bool forward);
-const void* br_kernel_ptr_9(int variant, int loge, int dl);
+const void* br_kernel_ptr_9(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_9(bool forward);
-const void* br_kernel_ptr_10(int variant, int loge, int dl);
+const void* br_kernel_ptr_10(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_10(bool forward);
-const void* br_kernel_ptr_11(int variant, int loge, int dl);
+const void* br_kernel_ptr_11(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_11(bool forward);
-const void* br_kernel_ptr_12(int variant, int loge, int dl);
-const void* br_kernel_ptr_13(int variant, int loge, int dl);
-const void* br_kernel_ptr_14(int variant, int loge, int dl);
-const void* br_kernel_ptr_15(int variant, int loge, int dl);
+const void* br_kernel_ptr_12(int variant, int loge, int dl, bool r4);
+const void* br_kernel_ptr_13(int variant, int loge, int dl, bool r4);
+const void* br_kernel_ptr_14(int variant, int loge, int dl, bool r4);
+const void* br_kernel_ptr_15(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_12(bool forward);
 const void* br_pair_kernel_ptr_7(int variant, int split);
 const void* br_pair_kernel_ptr_8(int variant, int split);
@@ -33,18 +33,19 @@ const void* ks_kernel_ptr_12(int mode, int loge);
 
 // One-block rotation kernel (one cluster of CTAs per rotation above N = 4096);
 // dl = 0: multiply-accumulate row by row, dl = 3 or 4: the digit-staged form for
-// that digit count (nullptr where not built).
-inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0) {
+// that digit count; r4: the fused radix-4 passes (N = 1024 .. 4096, 4 coefficients
+// per thread) (nullptr where not built).
+inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0, bool r4 = false) {
     switch (logn) {
-        case 7: return br_kernel_ptr_7(variant, loge, dl);
-        case 8: return br_kernel_ptr_8(variant, loge, dl);
-        case 9: return br_kernel_ptr_9(variant, loge, dl);
-        case 10: return br_kernel_ptr_10(variant, loge, dl);
-        case 11: return br_kernel_ptr_11(variant, loge, dl);
-        case 12: return br_kernel_ptr_12(variant, loge, dl);
-        case 13: return br_kernel_ptr_13(variant, loge, dl);
-        case 14: return br_kernel_ptr_14(variant, loge, dl);
-        case 15: return br_kernel_ptr_15(variant, loge, dl);
+        case 7: return br_kernel_ptr_7(variant, loge, dl, r4);
+        case 8: return br_kernel_ptr_8(variant, loge, dl, r4);
+        case 9: return br_kernel_ptr_9(variant, loge, dl, r4);
+        case 10: return br_kernel_ptr_10(variant, loge, dl, r4);
+        case 11: return br_kernel_ptr_11(variant, loge, dl, r4);
+        case 12: return br_kernel_ptr_12(variant, loge, dl, r4);
+        case 13: return br_kernel_ptr_13(variant, loge, dl, r4);
+        case 14: return br_kernel_ptr_14(variant, loge, dl, r4);
+        case 15: return br_kernel_ptr_15(variant, loge, dl, r4);
         default: return nullptr;
     }
 }

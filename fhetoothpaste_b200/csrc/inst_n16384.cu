@@ -6,7 +6,8 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_14(int variant, int loge, int dl) {
+const void* br_kernel_ptr_14(int variant, int loge, int dl, bool r4) {
+    if (r4) return nullptr;  // fused radix-4 rotation kernels are built for N = 1024 .. 4096
     if (loge != 2 || (dl != 0 && dl != 3 && dl != 4)) return nullptr;
     switch (variant) {
         case kCggiBinary:

@@ -8,7 +8,23 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_11(int variant, int loge, int dl) {
+const void* br_kernel_ptr_11(int variant, int loge, int dl, bool r4) {
+    if (r4) {  // fused radix-4 passes, 4 coefficients per thread
+        if (loge != 2 || !(dl == 0 || dl == 3 || dl == 4)) return nullptr;
+        if (variant == kCggiBinary)
+            return dl == 0 ? (const void*)br_kernel<11, kCggiBinary, 2, 0, 0, true>
+                           : (dl == 3 ? (const void*)br_kernel<11, kCggiBinary, 2, 3, 0, true>
+                                      : (const void*)br_kernel<11, kCggiBinary, 2, 4, 0, true>);
+        if (variant == kCggiTernary)
+            return dl == 0 ? (const void*)br_kernel<11, kCggiTernary, 2, 0, 0, true>
+                           : (dl == 3 ? (const void*)br_kernel<11, kCggiTernary, 2, 3, 0, true>
+                                      : (const void*)br_kernel<11, kCggiTernary, 2, 4, 0, true>);
+        if (variant == kBmmpBinary)
+            return dl == 0 ? (const void*)br_kernel<11, kBmmpBinary, 2, 0, 0, true>
+                           : (dl == 3 ? (const void*)br_kernel<11, kBmmpBinary, 2, 3, 0, true>
+                                      : (const void*)br_kernel<11, kBmmpBinary, 2, 4, 0, true>);
+        return nullptr;
+    }
     if (dl == 3 || dl == 4) {  // digit-staged multiply-accumulate, 4 coefficients per thread
         if (loge != 2) return nullptr;
         switch (variant) {

@@ -8,7 +8,8 @@
 
 namespace tp {
 
-const void* br_kernel_ptr_9(int variant, int loge, int dl) {
+const void* br_kernel_ptr_9(int variant, int loge, int dl, bool r4) {
+    if (r4) return nullptr;  // fused radix-4 rotation kernels are built for N = 1024 .. 4096
     if (dl == 3 || dl == 4) {  // digit-staged multiply-accumulate, 4 coefficients per thread
         if (loge != 2) return nullptr;
         switch (variant) {

@@ -319,6 +319,14 @@ uint32_t GpuBlindRotator::Tile() const { return tp_br_get_tile(m_ctx); }
 
 uint32_t GpuBlindRotator::Split() const { return tp_br_get_split(m_ctx); }
 
+void GpuBlindRotator::SetMacForm(uint32_t form) { check(tp_br_set_mac_form(m_ctx, form)); }
+
+void GpuBlindRotator::SetRadix(uint32_t radix) { check(tp_br_set_radix(m_ctx, radix)); }
+
+uint32_t GpuBlindRotator::MacForm() const { return tp_br_get_mac_form(m_ctx); }
+
+uint32_t GpuBlindRotator::Radix() const { return tp_br_get_radix(m_ctx); }
+
 uint32_t GpuBlindRotator::Autotune(uint64_t batch, double* rotations_per_s) {
     uint32_t coef = 0;
     check(tp_br_autotune(m_ctx, batch, &coef, rotations_per_s));

@@ -118,6 +118,11 @@ public:
     // need 4 per thread), or both chosen by timing `batch` synthetic rotations.
     void SetTile(uint32_t coef_per_thread);
     void SetSplit(uint32_t blocks_per_rotation);
+    // multiply-accumulate form (TP_MAC_ROWWISE / TP_MAC_DIGIT_STAGED) and NTT radix (2 or 4)
+    void SetMacForm(uint32_t form);
+    void SetRadix(uint32_t radix);
+    uint32_t MacForm() const;
+    uint32_t Radix() const;
     uint32_t Tile() const;
     uint32_t Split() const;
     // returns the chosen coefficients per thread (the split is read back with Split())

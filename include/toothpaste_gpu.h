@@ -136,12 +136,20 @@ enum { TP_MAC_ROWWISE = 0, TP_MAC_DIGIT_STAGED = 1 };
 tp_status tp_br_set_mac_form(tp_br_ctx* ctx, uint32_t form);
 uint32_t tp_br_get_mac_form(const tp_br_ctx* ctx);
 
+/* NTT passes of the one-block kernel at 4 coefficients per thread: radix 2
+ * (butterflies, the default) or 4 (fused radix-4 passes: three products and a
+ * power-of-two shift per two levels). Built for N = 1024 .. 4096; same words
+ * either way. Project-specific tuning (no reference counterpart); tp_br_autotune
+ * chooses it with the other launch settings. */
+tp_status tp_br_set_radix(tp_br_ctx* ctx, uint32_t radix);
+uint32_t tp_br_get_radix(const tp_br_ctx* ctx);
+
 /* Times every launch form (8 or 4 coefficients per thread; at 4 also the
- * digit-staged multiply-accumulate and two or four blocks per rotation) on up to
- * two waves of `batch` synthetic rotations with the uploaded key, keeps the
- * fastest and reports it (either output may be NULL; the split and form are read
- * back with tp_br_get_split / tp_br_get_mac_form). Blocks until done; the context
- * must be idle. */
+ * digit-staged multiply-accumulate, the fused radix-4 passes and two or four
+ * blocks per rotation) on up to two waves of `batch` synthetic rotations with the
+ * uploaded key, keeps the fastest and reports it (either output may be NULL; the
+ * split, form and radix are read back with tp_br_get_split / tp_br_get_mac_form /
+ * tp_br_get_radix). Blocks until done; the context must be idle. */
 tp_status tp_br_autotune(tp_br_ctx* ctx, uint64_t batch, uint32_t* best_coef_per_thread,
                          double* best_rotations_per_s);
 

@@ -261,6 +261,32 @@ def test_both_accumulation_forms_match_reference(native, oracle, golden, name):
             np.testing.assert_array_equal(got, expect[idx], err_msg=f"form {form}")
 
 
+@pytest.mark.parametrize("name", ALL_CASES)
+def test_radix4_passes_match_reference(native, oracle, golden, name):
+    """The fused radix-4 passes (N = 1024 .. 4096) give the radix-2 words, with either
+    multiply-accumulate form that fits."""
+    from fhetoothpaste_b200 import _native
+    case, rot = rotator(oracle, golden, name)
+    rot.set_tile(4)
+    if not 1024 <= case["N"] <= 4096:
+        with pytest.raises(_native.TpError):
+            rot.set_radix(4)
+        return
+    rot.set_radix(4)
+    assert rot.radix == 4
+    lwes, accs, coefs = case_inputs(name, case)
+    expect = golden[1][f"br_{name}"]
+    for form in (0, 1):
+        try:
+            rot.set_mac_form(form)
+        except _native.TpError:
+            continue
+        for oc in (0, 1):
+            idx = [i for i, c in enumerate(coefs) if c == oc]
+            got = rot.blind_rotate_batch_host(lwes[idx], accs[idx], out_coef=bool(oc))
+            np.testing.assert_array_equal(got, expect[idx], err_msg=f"radix 4, form {form}")
+
+
 def test_autotune_picks_a_tile_and_keeps_results(native, oracle, golden):
     name = "small_bmmp_n512"
     case, rot = rotator(oracle, golden, name)
