@@ -940,6 +940,8 @@ struct tp_ks_ctx {
     size_t smem = 0;
     int loge = 2;                 // log2 coefficients per thread: 2 (4) or 3 (8)
     int per_sm[2][tp::kKsModes] = {};
+    int logs = 0;                 // log2 CTAs per item's cluster (N > 4096), else 0
+    int cluster_cap[tp::kKsModes] = {};  // resident clusters per mode (logs > 0)
     uint64_t* work = nullptr;     // packing tree nodes
     uint64_t work_words = 0;
     // PackConsecutively plan for consec_len inputs: leaf inputs, then each level's node pairs
@@ -955,8 +957,8 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
                            tp_ks_ctx** out) {
     if (!out) return fail(TP_ERR_PARAM, "null argument");
     *out = nullptr;
-    if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
-        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (ring_dim < 128 || ring_dim > 32768 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
     if (basis < 2 || (basis & (basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
     const int beta = ilog2(basis);
     if (beta > 30) return fail(TP_ERR_PARAM, "basis above 2^30 is not supported");
@@ -975,6 +977,7 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     c->index = index;
     c->nkeys = kind == 2 ? c->logn : 1;
     c->loge = 2;  // 4 per thread: faster than 8 in every mode and ring size measured
+    c->logs = tp::br_cluster_logs(c->logn);
     c->key_words = (uint64_t)c->nkeys * digits * 2 * ring_dim;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
@@ -992,7 +995,40 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
     kp.digits = digits;
     kp.n_inv = c->tab->n_inv;
     signed_digit_consts(beta, digits, kp.corr, kp.dshift, kp.dmask, kp.ddelta);
-    c->smem = tp::ks_smem_words(ring_dim) * 8;
+    c->smem = tp::ks_smem_words((int)ring_dim, 1 << c->logs) * 8;
+    if (c->logs > 0) {
+        // one item per cluster of 2^logs CTAs, 4 coefficients per thread
+        const int S = 1 << c->logs;
+        for (int mode = 0; mode < tp::kKsModes; ++mode) {
+            const void* k = tp::ks_kernel_lookup(c->logn, mode, 2);
+            e = k ? cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem)
+                  : cudaErrorInvalidValue;
+            if (e == cudaSuccess && S > 8) e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            int clusters = 0;
+            if (e == cudaSuccess) {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute attr = {};
+                attr.id = cudaLaunchAttributeClusterDimension;
+                attr.val.clusterDim.x = (unsigned)S;
+                attr.val.clusterDim.y = 1;
+                attr.val.clusterDim.z = 1;
+                cfg.gridDim = dim3((unsigned)S * (unsigned)sm_count(device));
+                cfg.blockDim = dim3(ring_dim >> (c->logs + 2));
+                cfg.dynamicSmemBytes = c->smem;
+                cfg.attrs = &attr;
+                cfg.numAttrs = 1;
+                e = cudaOccupancyMaxActiveClusters(&clusters, k, &cfg);
+            }
+            if (e != cudaSuccess || clusters < 1) {
+                delete c;
+                return fail(TP_ERR_CUDA, "key-switch cluster kernel set-up (N=%u): %s", ring_dim,
+                            e == cudaSuccess ? "no resident cluster" : cudaGetErrorString(e));
+            }
+            c->cluster_cap[mode] = clusters;
+        }
+        *out = c;
+        return TP_OK;
+    }
     for (int loge = 2; loge <= 3; ++loge) {
         for (int mode = 0; mode < tp::kKsModes; ++mode) {
             const void* k = tp::ks_kernel_lookup(c->logn, mode, loge);
@@ -1052,7 +1088,7 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
         const uint64_t total = c->key_words;
         const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 65535);
         tp::key_relayout_kernel<<<(unsigned)blocks, 256>>>(c->key, stage, c->nkeys, 1, c->digits, c->logn,
-                                                            c->loge);
+                                                            c->loge, c->logs);
         tp::note_launch();
         e = cudaGetLastError();
     }
@@ -1064,10 +1100,29 @@ tp_status tp_ks_upload_key(tp_ks_ctx* c, const uint64_t* ksk, uint64_t words) {
 }
 
 static tp_status ks_launch(tp_ks_ctx* c, int mode, const tp::KsKernelParams& kp, cudaStream_t st) {
-    const uint64_t grid =
-        std::min<uint64_t>(kp.items, (uint64_t)c->per_sm[c->loge - 2][mode] * sm_count(c->device));
     tp::KsKernelParams p = kp;
     void* args[] = {&p};
+    if (c->logs > 0) {
+        // one item per cluster of 2^logs CTAs
+        const uint64_t clusters = std::min<uint64_t>(kp.items, (uint64_t)c->cluster_cap[mode]);
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr = {};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = 1u << c->logs;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)(clusters << c->logs));
+        cfg.blockDim = dim3(c->N >> (c->logs + 2));
+        cfg.dynamicSmemBytes = c->smem;
+        cfg.stream = st;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        TP_CUDA(cudaLaunchKernelExC(&cfg, tp::ks_kernel_lookup(c->logn, mode, 2), args));
+        tp::note_launch();
+        return TP_OK;
+    }
+    const uint64_t grid =
+        std::min<uint64_t>(kp.items, (uint64_t)c->per_sm[c->loge - 2][mode] * sm_count(c->device));
     TP_CUDA(cudaLaunchKernel(tp::ks_kernel_lookup(c->logn, mode, c->loge), dim3((unsigned)grid),
                              dim3(c->N >> c->loge), args, c->smem, st));
     tp::note_launch();
@@ -1080,6 +1135,7 @@ tp_status tp_ks_set_tile(tp_ks_ctx* c, uint32_t coef_per_thread) {
     const int loge = coef_per_thread == 4 ? 2 : 3;
     std::lock_guard<std::mutex> lk(c->mu);
     if (loge == c->loge) return TP_OK;
+    if (c->logs > 0) return fail(TP_ERR_PARAM, "ring sizes above 4096 run on clusters with 4 coefficients per thread");
     TP_CUDA(cudaSetDevice(c->device));
     if (c->key_ready) {
         uint64_t* nk = nullptr;
@@ -1644,8 +1700,8 @@ tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* c, const char* path) {
 
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd, uint64_t in_stride = 0, uint64_t out_stride = 0) {
-    if (ring_dim < 128 || ring_dim > 4096 || (ring_dim & (ring_dim - 1)))
-        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 4096]");
+    if (ring_dim < 128 || ring_dim > 32768 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
     if (count == 0) return TP_OK;
     if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
     if (((uintptr_t)out & 15) || ((uintptr_t)in & 15)) return fail(TP_ERR_PARAM, "buffers must be 16-byte aligned");
@@ -1656,6 +1712,39 @@ static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, co
     tp_status s = get_tables(device, logn, &tab);
     if (s != TP_OK) return s;
     const void* k = tp::ntt_kernel_lookup(logn, fwd);
+    if (!in_stride) in_stride = ring_dim;
+    if (!out_stride) out_stride = ring_dim;
+    const int logs = tp::br_cluster_logs(logn);
+    if (logs > 0) {
+        // one polynomial per cluster of 2^logs CTAs of N / 2^(logs+2) threads; shared
+        // memory: 5 NL words (NL = N / 2^logs)
+        const unsigned S = 1u << logs;
+        const size_t smem = 5ull * (ring_dim >> logs) * 8;
+        TP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (S > 8) TP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr = {};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = S;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.gridDim = dim3(S * (unsigned)sm_count(device));
+        cfg.blockDim = dim3(ring_dim >> (logs + 2));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = (cudaStream_t)stream;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        TP_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k, &cfg));
+        if (clusters < 1) return fail(TP_ERR_CUDA, "NTT cluster kernel (N=%u): no resident cluster", ring_dim);
+        cfg.gridDim = dim3((unsigned)(std::min<uint64_t>(count, (uint64_t)clusters) << logs));
+        const uint64_t* tw = fwd ? tab->tw_fwd : tab->tw_inv;
+        uint64_t n_inv = tab->n_inv;
+        void* args[] = {&out, &in, &count, &tw, &n_inv, &in_stride, &out_stride};
+        TP_CUDA(cudaLaunchKernelExC(&cfg, k, args));
+        tp::note_launch();
+        return TP_OK;
+    }
     const size_t smem = 3ull * ring_dim * 8;
     TP_CUDA(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -1663,8 +1752,6 @@ static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, co
     const uint64_t grid = std::min<uint64_t>(count, (uint64_t)std::max(1, per_sm) * sm_count(device));
     const uint64_t* tw = fwd ? tab->tw_fwd : tab->tw_inv;
     uint64_t n_inv = tab->n_inv;
-    if (!in_stride) in_stride = ring_dim;
-    if (!out_stride) out_stride = ring_dim;
     void* args[] = {&out, &in, &count, &tw, &n_inv, &in_stride, &out_stride};
     TP_CUDA(cudaLaunchKernel(k, dim3((unsigned)grid), dim3(ring_dim / 8), args, smem, (cudaStream_t)stream));
     tp::note_launch();

@@ -18,6 +18,9 @@ const void* br_kernel_ptr_13(int variant, int loge, int dl, bool r4);
 const void* br_kernel_ptr_14(int variant, int loge, int dl, bool r4);
 const void* br_kernel_ptr_15(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_12(bool forward);
+const void* ntt_kernel_ptr_13(bool forward);  // cluster kernels (ntt_cluster_kernel)
+const void* ntt_kernel_ptr_14(bool forward);
+const void* ntt_kernel_ptr_15(bool forward);
 const void* br_pair_kernel_ptr_7(int variant, int split);
 const void* br_pair_kernel_ptr_8(int variant, int split);
 const void* br_pair_kernel_ptr_9(int variant, int split);
@@ -30,6 +33,9 @@ const void* ks_kernel_ptr_9(int mode, int loge);
 const void* ks_kernel_ptr_10(int mode, int loge);
 const void* ks_kernel_ptr_11(int mode, int loge);
 const void* ks_kernel_ptr_12(int mode, int loge);
+const void* ks_kernel_ptr_13(int mode, int loge);
+const void* ks_kernel_ptr_14(int mode, int loge);
+const void* ks_kernel_ptr_15(int mode, int loge);
 
 // One-block rotation kernel (one cluster of CTAs per rotation above N = 4096);
 // dl = 0: multiply-accumulate row by row, dl = 3 or 4: the digit-staged form for
@@ -72,6 +78,9 @@ inline const void* ntt_kernel_lookup(int logn, bool forward) {
         case 10: return ntt_kernel_ptr_10(forward);
         case 11: return ntt_kernel_ptr_11(forward);
         case 12: return ntt_kernel_ptr_12(forward);
+        case 13: return ntt_kernel_ptr_13(forward);
+        case 14: return ntt_kernel_ptr_14(forward);
+        case 15: return ntt_kernel_ptr_15(forward);
         default: return nullptr;
     }
 }
@@ -84,6 +93,9 @@ inline const void* ks_kernel_lookup(int logn, int mode, int loge) {
         case 10: return ks_kernel_ptr_10(mode, loge);
         case 11: return ks_kernel_ptr_11(mode, loge);
         case 12: return ks_kernel_ptr_12(mode, loge);
+        case 13: return ks_kernel_ptr_13(mode, loge);
+        case 14: return ks_kernel_ptr_14(mode, loge);
+        case 15: return ks_kernel_ptr_15(mode, loge);
         default: return nullptr;
     }
 }

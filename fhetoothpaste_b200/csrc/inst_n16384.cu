@@ -1,8 +1,11 @@
 // Kernel instantiations for N = 16384: one rotation per cluster of 8 CTAs
-// (cluster_ntt.cuh), 4 coefficients per thread; compiled as a separate unit so
+// (cluster_ntt.cuh), 4 coefficients per thread, for the rotation and the key-switching
+// modes; compiled as a separate unit so
 // the ring sizes build in parallel.
 #include "br_kernels.cuh"
 #include "dispatch.h"
+#include "ks_kernels.cuh"
+#include "misc_kernels.cuh"
 
 namespace tp {
 
@@ -23,6 +26,22 @@ const void* br_kernel_ptr_14(int variant, int loge, int dl, bool r4) {
                            : (dl == 3 ? (const void*)br_kernel<14, kBmmpBinary, 2, 3, 3>
                                       : (const void*)br_kernel<14, kBmmpBinary, 2, 4, 3>);
     }
+}
+
+const void* ks_kernel_ptr_14(int mode, int loge) {
+    if (loge != 2) return nullptr;  // clusters run with 4 coefficients per thread
+    switch (mode) {
+        case kKsRlwe: return (const void*)ks_kernel<14, kKsRlwe, 2, 3>;
+        case kKsAuto: return (const void*)ks_kernel<14, kKsAuto, 2, 3>;
+        case kKsMerge: return (const void*)ks_kernel<14, kKsMerge, 2, 3>;
+        case kKsTrace: return (const void*)ks_kernel<14, kKsTrace, 2, 3>;
+        default: return (const void*)ks_kernel<14, kKsSplit, 2, 3>;
+    }
+}
+
+const void* ntt_kernel_ptr_14(bool forward) {
+    return forward ? (const void*)ntt_cluster_kernel<14, true, 3>
+                   : (const void*)ntt_cluster_kernel<14, false, 3>;
 }
 
 }  // namespace tp

@@ -1,8 +1,11 @@
 // Kernel instantiations for N = 8192: one rotation per cluster of 4 CTAs
-// (cluster_ntt.cuh), 4 coefficients per thread; compiled as a separate unit so
+// (cluster_ntt.cuh), 4 coefficients per thread, for the rotation and the key-switching
+// modes; compiled as a separate unit so
 // the ring sizes build in parallel.
 #include "br_kernels.cuh"
 #include "dispatch.h"
+#include "ks_kernels.cuh"
+#include "misc_kernels.cuh"
 
 namespace tp {
 
@@ -23,6 +26,22 @@ const void* br_kernel_ptr_13(int variant, int loge, int dl, bool r4) {
                            : (dl == 3 ? (const void*)br_kernel<13, kBmmpBinary, 2, 3, 2>
                                       : (const void*)br_kernel<13, kBmmpBinary, 2, 4, 2>);
     }
+}
+
+const void* ks_kernel_ptr_13(int mode, int loge) {
+    if (loge != 2) return nullptr;  // clusters run with 4 coefficients per thread
+    switch (mode) {
+        case kKsRlwe: return (const void*)ks_kernel<13, kKsRlwe, 2, 2>;
+        case kKsAuto: return (const void*)ks_kernel<13, kKsAuto, 2, 2>;
+        case kKsMerge: return (const void*)ks_kernel<13, kKsMerge, 2, 2>;
+        case kKsTrace: return (const void*)ks_kernel<13, kKsTrace, 2, 2>;
+        default: return (const void*)ks_kernel<13, kKsSplit, 2, 2>;
+    }
+}
+
+const void* ntt_kernel_ptr_13(bool forward) {
+    return forward ? (const void*)ntt_cluster_kernel<13, true, 2>
+                   : (const void*)ntt_cluster_kernel<13, false, 2>;
 }
 
 }  // namespace tp

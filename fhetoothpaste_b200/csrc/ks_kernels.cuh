@@ -10,6 +10,9 @@
 // (C = 2 components, A and B, per slot).
 #pragma once
 
+#include <cooperative_groups.h>
+
+#include "cluster_ntt.cuh"
 #include "gl_arith.cuh"
 #include "ntt_block.cuh"
 
@@ -54,8 +57,9 @@ struct KsKernelParams {
     uint64_t ddelta[8];
 };
 
-// Shared memory of a key-switching block, in words: twiddles (2N) + two exchange buffers (2N).
-__host__ __device__ constexpr size_t ks_smem_words(int N) { return 4 * (size_t)N; }
+// Shared memory of a key-switching block, in words: twiddles (2N) + two exchange buffers (2N);
+// on a cluster of S CTAs (N > 4096) the same of the local size N/S plus two receive areas.
+__host__ __device__ constexpr size_t ks_smem_words(int N, int S = 1) { return (S > 1 ? 6 : 4) * (size_t)(N / S); }
 
 // Coefficient m of aut_t(x) for x in the coefficient domain: x_i moves to
 // i*t mod 2N with a sign flip past N (automorphism_evaluation.cpp:183-206), so
@@ -76,13 +80,18 @@ __device__ __forceinline__ uint64_t rot_coeff(const uint64_t* x, uint32_t m, uin
 }
 
 // sum_d NTT(digit_d(a)) * key_d for both components (canonical), a in the
-// coefficient layout and canonical.
-template <int LOGN, int LOGE>
+// coefficient layout and canonical. On a cluster (LOGS > 0, rank cr) a holds the
+// CTA's subsequence, o its slot block, and the key row part cr (2 NL words) is read.
+template <int LOGN, int LOGE, int LOGS = 0>
 __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelParams& prm, int t, uint64_t* buf0,
-                                       uint64_t* buf1, int& sel, const uint64_t* tw_f, uint64_t (&o)[2][1 << LOGE]) {
+                                       uint64_t* buf1, int& sel, const uint64_t* tw_f, uint64_t (&o)[2][1 << LOGE],
+                                       int cr = 0, uint64_t* recv0 = nullptr, uint64_t* recv1 = nullptr,
+                                       int* rsel = nullptr) {
     constexpr int N = 1 << LOGN;
+    constexpr int LOGL = LOGN - LOGS;
+    constexpr int NL = 1 << LOGL;
     constexpr int E = 1 << LOGE;
-    constexpr int T = N / E;
+    constexpr int T = NL / E;
 #pragma unroll
     for (int j = 0; j < E; ++j) {
         a[j] = gl_add(a[j], prm.corr);
@@ -97,7 +106,7 @@ __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelP
         uint64_t x[1][E];
 #pragma unroll
         for (int j = 0; j < E; ++j) x[0][j] = gl_sub((a[j] >> sh) & mk, dl);
-        const uint64_t* kr = prm.key + (uint64_t)d * (2 * N);
+        const uint64_t* kr = prm.key + (uint64_t)d * (2 * N) + (uint64_t)cr * (2 * NL);
         // with 4 coefficients per thread the digit's key words (8 registers) are
         // requested before its NTT, which hides their L2 latency; with 8 they
         // would not fit next to the NTT's registers and are read after it
@@ -109,8 +118,15 @@ __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelP
                 for (int jp = 0; jp < E / 2; ++jp)
                     kv[c][jp] = __ldg(reinterpret_cast<const ulonglong2*>(kr + ((c * (E / 2) + jp) * T + t) * 2));
         }
-        ntt_forward_k<LOGN, 1, LOGE, false, true>(x, t, sel ? buf1 : buf0, tw_f);
+        ntt_forward_k<LOGL, 1, LOGE, false, true>(x, t, sel ? buf1 : buf0, tw_f);
         sel ^= 1;
+        if constexpr (LOGS > 0) {
+            uint64_t* rv = *rsel ? recv1 : recv0;
+            *rsel ^= 1;
+            uint64_t* fb = sel ? buf1 : buf0;
+            if constexpr ((1 << LOGS) > 4) sel ^= 1;
+            cluster_fwd_tail<LOGN, LOGS, true>(reinterpret_cast<uint64_t(&)[4]>(x[0]), t, cr, rv, fb, prm.tw_fwd);
+        }
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
 #pragma unroll
@@ -129,18 +145,37 @@ __device__ __forceinline__ void ks_mac(uint64_t (&a)[1 << LOGE], const KsKernelP
 template <int LOGN, int LOGE>
 constexpr int ks_min_blocks() { return ((1 << LOGN) >> LOGE) <= 256 ? 2 : 1; }
 
-template <int LOGN, int MODE, int LOGE>
-__global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>()) ks_kernel(const KsKernelParams prm) {
+// LOGS > 0 (N > 4096): one item per cluster of 2^LOGS CTAs, launched with that
+// cluster size (cluster_ntt.cuh): CTA r holds the coefficients m = m' 2^LOGS + r and
+// the slots r NL .. r NL + NL - 1; inputs are read from global memory at their
+// global indices, so the automorphisms' gathers need no exchange.
+template <int LOGN, int MODE, int LOGE, int LOGS = 0>
+__global__ void __launch_bounds__((1 << (LOGN - LOGS)) >> LOGE, ks_min_blocks<LOGN - LOGS, LOGE>())
+ks_kernel(const KsKernelParams prm) {
     constexpr int N = 1 << LOGN;
+    constexpr int LOGL = LOGN - LOGS;
+    constexpr int NL = 1 << LOGL;
     constexpr int E = 1 << LOGE;
-    constexpr int T = N / E;
+    constexpr int T = NL / E;
+    static_assert(LOGS == 0 || LOGE == 2, "clusters run with 4 coefficients per thread");
     extern __shared__ __align__(16) uint64_t smem[];
-    uint64_t* tw_f = smem;
-    uint64_t* tw_i = smem + N;
-    uint64_t* buf0 = smem + 2 * N;
-    uint64_t* buf1 = smem + 3 * N;
+    uint64_t* tw_f = smem;          // the first NL words of the N-point tables (the NL-point tables)
+    uint64_t* tw_i = smem + NL;
+    uint64_t* buf0 = smem + 2 * NL;
+    uint64_t* buf1 = smem + 3 * NL;
+    uint64_t* recv0 = smem + 4 * NL;  // cluster exchange areas
+    uint64_t* recv1 = smem + 5 * NL;
     const int t = threadIdx.x;
-    for (int i = t; i < N; i += T) {
+    int cr = 0;
+    if constexpr (LOGS > 0) {
+        cr = (int)cooperative_groups::this_cluster().block_rank();
+        cooperative_groups::this_cluster().sync();  // every CTA of the cluster running before remote stores
+    }
+    const uint32_t sbase = (uint32_t)cr << LOGL;
+    // global index of this thread's local coefficient t + j T
+    auto gm = [&](int j) -> uint32_t { return ((uint32_t)(t + j * T) << LOGS) + (uint32_t)cr; };
+    int rsel = 0;
+    for (int i = t; i < NL; i += T) {
         tw_f[i] = prm.tw_fwd[i];
         tw_i[i] = prm.tw_inv[i];
     }
@@ -150,7 +185,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
     // writes them, so the early read is safe in place too). Measured +4-5% at
     // N = 1024 / 2048 with 4 coefficients per thread; at 1024 threads per block
     // (64 registers) it cost 6%, and with 8 per thread it would spill.
-    constexpr bool PF = MODE == kKsRlwe && LOGE == 2 && T <= 512;
+    constexpr bool PF = MODE == kKsRlwe && LOGE == 2 && T <= 512 && LOGS == 0;
     uint64_t a_next[E];
     if constexpr (PF) {
         if (blockIdx.x < prm.items) {
@@ -158,7 +193,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
             for (int j = 0; j < E; ++j) a_next[j] = prm.in[blockIdx.x * prm.in_stride + t + j * T];
         }
     }
-    for (uint64_t it = blockIdx.x; it < prm.items; it += gridDim.x) {
+    for (uint64_t it = blockIdx.x >> LOGS; it < prm.items; it += gridDim.x >> LOGS) {
         __syncthreads();
         const uint64_t* in = prm.in + it * prm.in_stride;
         uint64_t* out = prm.out + it * prm.out_stride;
@@ -175,12 +210,12 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
             }
         } else if constexpr (MODE == kKsRlwe) {
 #pragma unroll
-            for (int j = 0; j < E; ++j) a[j] = in[t + j * T];
+            for (int j = 0; j < E; ++j) a[j] = in[gm(j)];
         } else if constexpr (MODE == kKsAuto) {
 #pragma unroll
             for (int j = 0; j < E; ++j) {
-                a[j] = aut_coeff<LOGN>(in, t + j * T, prm.auto_index_inv);
-                bb[j] = aut_coeff<LOGN>(in + N, t + j * T, prm.auto_index_inv);
+                a[j] = aut_coeff<LOGN>(in, gm(j), prm.auto_index_inv);
+                bb[j] = aut_coeff<LOGN>(in + N, gm(j), prm.auto_index_inv);
             }
         } else {
             const uint64_t* left = in;
@@ -199,7 +234,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
             for (int h = 0; h < 2; ++h) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
-                    const uint32_t m = t + j * T;
+                    const uint32_t m = gm(j);
                     // diff = right - X^s left at the automorphism's source index
                     const uint32_t i = (m * prm.auto_index_inv) & (2 * N - 1);
                     const uint32_t src = i & (N - 1);
@@ -218,23 +253,30 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
         }
         // ---- key switch of the A part ----
         uint64_t o[2][E];
-        ks_mac<LOGN, LOGE>(a, prm, t, buf0, buf1, sel, tw_f, o);
+        ks_mac<LOGN, LOGE, LOGS>(a, prm, t, buf0, buf1, sel, tw_f, o, cr, recv0, recv1, &rsel);
         if constexpr (MODE == kKsRlwe) {
             // out -= KS; out.B += in.B (rlwe_conversion.cpp:243-248); slots E t .. E t + E - 1
 #pragma unroll
             for (int j = 0; j < E; ++j) {
-                const int k = E * t + j;
+                const uint32_t k = sbase + E * t + j;
                 out[k] = gl_sub(out[k], o[0][j]);
                 out[N + k] = gl_add(gl_sub(out[N + k], o[1][j]), in[N + k]);
             }
         } else {
             // NTT of the automorphism's B part (automorphism_evaluation.cpp:156)
-            ntt_forward_k<LOGN, 1, LOGE>(reinterpret_cast<uint64_t(&)[1][E]>(bb), t, sel ? buf1 : buf0, tw_f);
+            ntt_forward_k<LOGL, 1, LOGE>(reinterpret_cast<uint64_t(&)[1][E]>(bb), t, sel ? buf1 : buf0, tw_f);
             sel ^= 1;
+            if constexpr (LOGS > 0) {
+                uint64_t* rv = rsel ? recv1 : recv0;
+                rsel ^= 1;
+                uint64_t* fb = sel ? buf1 : buf0;
+                if constexpr ((1 << LOGS) > 4) sel ^= 1;
+                cluster_fwd_tail<LOGN, LOGS, false>(reinterpret_cast<uint64_t(&)[4]>(bb), t, cr, rv, fb, prm.tw_fwd);
+            }
             if constexpr (MODE == kKsAuto) {
 #pragma unroll
                 for (int j = 0; j < E; ++j) {
-                    const int k = E * t + j;
+                    const uint32_t k = sbase + E * t + j;
                     out[k] = gl_sub(out[k], o[0][j]);
                     out[N + k] = gl_add(gl_sub(out[N + k], o[1][j]), bb[j]);
                 }
@@ -247,7 +289,15 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
 #pragma unroll
                     for (int j = 0; j < E; ++j) r[0][j] = h == 0 ? gl_neg(o[0][j])
                                                                  : gl_sub(bb[j], o[1][j]);
-                    ntt_backward_unscaled_k<LOGN, 1, LOGE>(r, t, sel ? buf1 : buf0, tw_i);
+                    if constexpr (LOGS > 0) {
+                        uint64_t* rv = rsel ? recv1 : recv0;
+                        rsel ^= 1;
+                        uint64_t* fb = sel ? buf1 : buf0;
+                        if constexpr ((1 << LOGS) > 4) sel ^= 1;
+                        cluster_inv_head<LOGN, LOGS>(reinterpret_cast<uint64_t(&)[4]>(r[0]), t, cr, rv, fb,
+                                                     prm.tw_inv);
+                    }
+                    ntt_backward_unscaled_k<LOGL, 1, LOGE>(r, t, sel ? buf1 : buf0, tw_i);
                     sel ^= 1;
                     if constexpr (MODE == kKsSplit) {
                         // children of a truncation-tree node (sap_decomposer.cpp:266-284, in the
@@ -256,7 +306,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
                         const uint32_t s = prm.shift;
 #pragma unroll
                         for (int j = 0; j < E; ++j) {
-                            const uint32_t m = t + j * T;
+                            const uint32_t m = gm(j);
                             const uint64_t y = gl_div_pow2<LOGN>(r[0][j]);
                             out[h * N + m] = gl_add(base[h][j], y);
                             const uint64_t z = gl_sub(base[h][j], y);
@@ -266,7 +316,7 @@ __global__ void __launch_bounds__((1 << LOGN) >> LOGE, ks_min_blocks<LOGN, LOGE>
                     } else {
 #pragma unroll
                         for (int j = 0; j < E; ++j)
-                            out[h * N + t + j * T] = gl_add(base[h][j], gl_div_pow2<LOGN>(r[0][j]));
+                            out[h * N + gm(j)] = gl_add(base[h][j], gl_div_pow2<LOGN>(r[0][j]));
                     }
                 }
             }

@@ -8,8 +8,9 @@
  *
  * Arithmetic is over the Goldilocks prime p = 2^64 - 2^32 + 1. All ciphertext
  * words are canonical residues in [0, p); polynomials have N coefficients with
- * N a power of two in [128, 4096] (blind rotation: up to 32768, on a cluster of
- * 4, 8 or 16 CTAs per rotation above 4096). "NTT domain" means the reference's
+ * N a power of two in [128, 32768]; above 4096 one rotation, key switch or
+ * transform runs on a cluster of 4, 8 or 16 CTAs (N = 8192, 16384, 32768) that
+ * exchange through distributed shared memory. "NTT domain" means the reference's
  * evaluation order: slot k holds a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N)
  * (lib/src/backend/solinas.cpp:168-313 of the reference).
  *

@@ -90,3 +90,88 @@ def test_cluster_sizes_refuse_other_tiles(native, oracle):
     with pytest.raises(_native.TpError):
         rot.set_split(2)
     rot.close()
+
+
+KS_CASES = json.loads(GOLDEN.read_text())["ks"]
+
+
+@pytest.mark.parametrize("name", sorted(KS_CASES))
+def test_large_ring_key_switching_matches_reference(native, oracle, name):
+    """RLWEtoRLWEConverter::Convert, AutomorphismEvaluator::Eval and LWEtoRLWEPacker::Pack at
+    N = 8192 .. 32768 (one item per cluster of 4, 8 or 16 CTAs) against the reference's outputs."""
+    from kscases import ks_inputs, ks_key
+    from fhetoothpaste_b200 import GpuAutomorphismEvaluator, GpuLWEtoRLWEPacker, GpuRLWEtoRLWEConverter
+    c = KS_CASES[name]
+    N, base, dg = c["N"], 1 << c["basis_log2"], c["digits"]
+    key, x = ks_key(oracle, name, c), ks_inputs(c)
+    if c["kind"] == "pack":
+        op = GpuLWEtoRLWEPacker(N, base, dg, key)
+        got = [op.Pack(x, c["len"])[0]]
+    else:
+        op = (GpuRLWEtoRLWEConverter(N, base, dg, key) if c["kind"] == "rlwe_ks"
+              else GpuAutomorphismEvaluator(N, base, dg, c["index"], key))
+        assert op.tile == 4
+        out = np.zeros((2, 2 * N), np.uint64)
+        (op.Convert if c["kind"] == "rlwe_ks" else op.Eval)(out, x)
+        got = list(out)
+    assert [sha256(np.ascontiguousarray(g)) for g in got] == c["out_sha256"], name
+    op.close()
+
+
+def test_large_ring_key_switch_batch_larger_than_the_grid(native, oracle):
+    """More key switches than resident clusters, accumulated into a non-zero output."""
+    from kscases import ks_key
+    from fhetoothpaste_b200 import GpuRLWEtoRLWEConverter
+    name = "rks_n8192"
+    c = KS_CASES[name]
+    N, bl, dg = c["N"], c["basis_log2"], c["digits"]
+    k = ks_key(oracle, name, c)
+    conv = GpuRLWEtoRLWEConverter(N, 1 << bl, dg, k)
+    with pytest.raises(Exception):
+        conv.set_tile(8)
+    batch = 3 * (148 // 4) + 7
+    x = random_acc(N, batch, 530)
+    base = random_acc(N, batch, 531)
+    out = base.copy()
+    conv.Convert(out, x)
+    for b in (0, 36, 37, 111, batch - 1):
+        np.testing.assert_array_equal(out[b], oracle.rlwe_ks(N, bl, dg, k, x[b], out=base[b]), err_msg=f"item {b}")
+    conv.close()
+
+
+@pytest.mark.parametrize("N", [8192, 16384, 32768])
+def test_large_ring_ntt_matches_oracle(native, oracle, N):
+    """The standalone transforms on a cluster: forward against the oracle, backward inverts it
+    (out of place and in place, several polynomials)."""
+    import torch
+    from fhetoothpaste_b200 import ntt_backward, ntt_forward
+    count = 5
+    x = random_acc(N // 2, count, 540 + N)  # count x N words below p
+    d_in = torch.from_numpy(x.view(np.int64)).cuda()
+    d_out = torch.empty_like(d_in)
+    ntt_forward(N, count, d_out.data_ptr(), d_in.data_ptr())
+    got = d_out.cpu().numpy().view(np.uint64)
+    for b in (0, count - 1):
+        np.testing.assert_array_equal(got[b], oracle.ntt_forward(x[b]), err_msg=f"forward {b}")
+    ntt_backward(N, count, d_out.data_ptr(), d_out.data_ptr())
+    np.testing.assert_array_equal(d_out.cpu().numpy().view(np.uint64), x)
+
+
+def test_large_ring_trace_and_consecutive_packing_match_oracle(native, oracle):
+    """TraceEvaluator::Eval and PackConsecutively (a non-power-of-two length) at N = 8192."""
+    from fhetoothpaste_b200 import GpuLWEtoRLWEPacker, GpuTraceEvaluator
+    from oracle.oracle import P, uniform_mod
+    N, bl, dg = 8192, 16, 4
+    keys = oracle.pack_keygen(N, bl, dg, 3.2, rlwe_secret(N, 550), 551)
+    x = random_acc(N, 2, 552)
+    tr = GpuTraceEvaluator(N, 1 << bl, dg, keys)
+    got = tr.Eval(x)
+    for b in range(2):
+        np.testing.assert_array_equal(got[b], oracle.trace_eval(N, bl, dg, keys, x[b]), err_msg=f"trace {b}")
+    tr.close()
+    length = 11
+    lwes = uniform_mod(553, length * (N + 1), P).reshape(length, N + 1)
+    pk = GpuLWEtoRLWEPacker(N, 1 << bl, dg, keys)
+    np.testing.assert_array_equal(pk.PackConsecutively(lwes, length)[0],
+                                  oracle.pack_consecutive(N, bl, dg, keys, lwes, length))
+    pk.close()

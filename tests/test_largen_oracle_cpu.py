@@ -29,3 +29,24 @@ def test_oracle_matches_reference_at_large_ring_sizes(oracle, name):
     for i, oc in enumerate(coefs):
         out = oracle.blind_rotate(v, N, n, c["basis_log2"], c["digits"], brk, lwes[i], accs[i], oc)
         assert sha256(np.ascontiguousarray(out)) == c["out_sha256"][i], (name, i)
+
+
+KS_CASES = json.loads(GOLDEN.read_text())["ks"]
+
+
+@pytest.mark.parametrize("name", sorted(KS_CASES))
+def test_oracle_key_switching_matches_reference_at_large_ring_sizes(oracle, name):
+    """RLWE key switches, automorphisms and packings at N = 8192 .. 32768: the oracle's keys
+    and results hash to the reference's."""
+    from kscases import ks_inputs, ks_key
+    c = KS_CASES[name]
+    N, bl, dg = c["N"], c["basis_log2"], c["digits"]
+    key = ks_key(oracle, name, c)
+    x = ks_inputs(c)
+    if c["kind"] == "rlwe_ks":
+        got = [oracle.rlwe_ks(N, bl, dg, key, x[i]) for i in range(2)]
+    elif c["kind"] == "auto":
+        got = [oracle.auto_eval(N, bl, dg, c["index"], key, x[i]) for i in range(2)]
+    else:
+        got = [oracle.pack(N, bl, dg, key, x, c["len"])]
+    assert [sha256(np.ascontiguousarray(g)) for g in got] == c["out_sha256"], name
