@@ -89,6 +89,18 @@ __host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int bl
     return loge == 2 && variant == kBmmpBinary && blocks == 4;
 }
 
+// Power-of-two levels of the later transform passes as shifts (ntt_block.cuh,
+// pow2_block_pass) in every rotation kernel but the digit-staged CGGI ternary one
+// at 2048 coefficients per CTA, where the same change measured slower although it
+// spills no more (rotations/s, 4096 rotations, n = 630: 8695 on table twiddles,
+// 8523 with both directions shifted, 8355 forward only, 7449 backward only). In
+// the others it measured faster: CGGI binary N = 1024 digit-staged 20.58k ->
+// 21.58k, row by row 19.38k -> 20.00k; CGGI ternary N = 2048 row by row 7861 ->
+// 8014; BMMP N = 2048 9487 -> 9541; CGGI ternary N = 4096 2358 -> 2431.
+__host__ __device__ constexpr bool br_table_passes(int variant, bool digit_staged, int logl) {
+    return variant == kCggiTernary && digit_staged && logl == 11;
+}
+
 // Key rows staged in shared memory: each thread copies its own slots of the
 // next gadget row with cp.async before the digit's transforms and reads them
 // after, so the L2 latency of the key stream hides behind the NTTs. The stage
@@ -218,6 +230,7 @@ br_kernel(const BrKernelParams prm) {
     constexpr bool PF = !DS && br_key_prefetch(LOGN, VARIANT, LOGE, LOGS, R4);
     static_assert(!DS || (LOGE == 2 && K == 1), "the digit stage runs with 4 coefficients per thread");
     static_assert(LOGS == 0 || (LOGE == 2 && K == 1 && !R4), "clusters run radix-2 with 4 coefficients per thread");
+    constexpr int NF = (R4 ? kNttRadix4 : 0) | (br_table_passes(VARIANT, DS, LOGL) ? kNttTablePasses : 0);
 
     extern __shared__ __align__(16) uint64_t smem[];
     uint64_t* base = smem;
@@ -303,7 +316,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int p = 0; p < K; ++p)
 #pragma unroll
                     for (int j = 0; j < E; ++j) x[p][j] = ain[(h0 + p) * N + ((uint32_t)(t + j * T) << LOGS) + cr];
-                ntt_forward_k<LOGL, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                ntt_forward_k<LOGL, K, LOGE, NF, true>(x, t, xb(), tw_f);
                 fwd_tail(x[0]);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
@@ -360,7 +373,7 @@ br_kernel(const BrKernelParams prm) {
             if constexpr (K == 2) {
                 load_half(cx[0], 0);
                 load_half(cx[1], 1);
-                ntt_backward_unscaled_k<LOGL, 2, LOGE, R4>(cx, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGL, 2, LOGE, NF>(cx, t, xb(), tw_i);
                 finish_half(cx[0]);
                 finish_half(cx[1]);
             }
@@ -384,7 +397,7 @@ br_kernel(const BrKernelParams prm) {
                         uint64_t (&c1)[1][E] = reinterpret_cast<uint64_t(&)[1][E]>(cx[0]);
                         load_half(cx[0], r == 0 ? 0 : 1);
                         inv_head(cx[0]);
-                        ntt_backward_unscaled_k<LOGL, 1, LOGE, R4>(c1, t, xb(), tw_i);
+                        ntt_backward_unscaled_k<LOGL, 1, LOGE, NF>(c1, t, xb(), tw_i);
                         finish_half(cx[0]);
                     }
                 }
@@ -419,9 +432,9 @@ br_kernel(const BrKernelParams prm) {
                             x[p][j] = SIGNED ? gl_sub(raw, dl) : raw;
                         }
                     }
-                    fwd_pass_math<LOGL, 0, K, LOGE, R4, true>(x, t, tw_f);
+                    fwd_pass_math<LOGL, 0, K, LOGE, NF, true>(x, t, tw_f);
                 }
-                ntt_forward_after_pass0<LOGL, K, LOGE, R4, true>(x, t, xb(), tw_f);
+                ntt_forward_after_pass0<LOGL, K, LOGE, NF, true>(x, t, xb(), tw_f);
                 fwd_tail(x[0]);
                 if constexpr (DS) {
                     // rows before the last wait in the stage (this thread's own slots: no barrier)
@@ -587,7 +600,7 @@ br_kernel(const BrKernelParams prm) {
                 for (int j = 0; j < E; ++j) x[p][j] = acc_ld(h0 + p, j);
             if (prm.out_coef) {
                 inv_head(x[0]);
-                ntt_backward_unscaled_k<LOGL, K, LOGE, R4>(x, t, xb(), tw_i);
+                ntt_backward_unscaled_k<LOGL, K, LOGE, NF>(x, t, xb(), tw_i);
 #pragma unroll
                 for (int p = 0; p < K; ++p)
 #pragma unroll

@@ -29,6 +29,8 @@
 // to the same buffer.
 #pragma once
 
+#include <type_traits>
+
 #include "gl_arith.cuh"
 
 namespace tp {
@@ -181,75 +183,148 @@ __host__ __device__ constexpr int pow2_twiddle_exp(int level, int block, bool in
     return inverse ? (192 - e) % 192 : e;
 }
 
-// Pass 0 (levels 0 .. S-1, block 0 only) with its power-of-two twiddles as
+// The butterflies of one pass whose first level L0 has its block B known at
+// compile time (pass 0: B = 0; later passes: one instantiation per block, picked
+// by a warp-uniform switch, below). Level L0 + LV pairs registers J and
+// J + G/2^(LV+1) with twiddle block (B << LV) + (J >> (S - LV)), as the table
+// path of fwd_pass_math does. Levels below 5 take their power-of-two twiddles as
 // shifts (gl_pow2_mag): a sign of the twiddle swaps the butterfly's add and
-// subtract. Level LV pairs registers J and J + G/2^(LV+1) with twiddle block
-// J >> (S - LV), as the table path below does.
-template <int S, int LV, int J, int K, bool LAZY>
-__device__ __forceinline__ void fwd_pow2_level(uint64_t (&x)[K][1 << S]) {
+// subtract. Deeper levels read the table.
+template <int S, int L0, int B, int LV, int J, int K, bool LAZY>
+__device__ __forceinline__ void fwd_blk_level(uint64_t (&x)[K][1 << S], const uint64_t* __restrict__ tw) {
     constexpr int G = 1 << S;
     if constexpr (J < G) {
         constexpr int half = G >> (LV + 1);
         if constexpr ((J & half) == 0) {
-            constexpr int EX = pow2_twiddle_exp(LV, J >> (S - LV), false);
+            constexpr int LVL = L0 + LV;
+            constexpr int BI = (B << LV) + (J >> (S - LV));
+            if constexpr (LVL < 5) {
+                constexpr int EX = pow2_twiddle_exp(LVL, BI, false);
 #pragma unroll
-            for (int p = 0; p < K; ++p) {
-                const uint64_t u = x[p][J];
-                const uint64_t t = gl_pow2_mag<EX>(x[p][J + half]);
-                const uint64_t sum = LAZY ? gl_add_lazy(u, t) : gl_add(u, t);
-                const uint64_t dif = gl_sub(u, t);
-                x[p][J] = Pow2<EX>::NEG ? dif : sum;
-                x[p][J + half] = Pow2<EX>::NEG ? sum : dif;
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][J];
+                    const uint64_t t = gl_pow2_mag<EX>(x[p][J + half]);
+                    const uint64_t sum = LAZY ? gl_add_lazy(u, t) : gl_add(u, t);
+                    const uint64_t dif = gl_sub(u, t);
+                    x[p][J] = Pow2<EX>::NEG ? dif : sum;
+                    x[p][J + half] = Pow2<EX>::NEG ? sum : dif;
+                }
+            } else {
+                const uint64_t w = tw[(1 << LVL) + BI];
+#pragma unroll
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][J];
+                    const uint64_t v = gl_mul(x[p][J + half], w);
+                    x[p][J] = LAZY ? gl_add_lazy(u, v) : gl_add(u, v);
+                    x[p][J + half] = gl_sub(u, v);
+                }
             }
         }
-        fwd_pow2_level<S, LV, J + 1, K, LAZY>(x);
+        fwd_blk_level<S, L0, B, LV, J + 1, K, LAZY>(x, tw);
     }
 }
-template <int S, int LV, int K, bool LAZY>
-__device__ __forceinline__ void fwd_pow2_pass(uint64_t (&x)[K][1 << S]) {
+template <int S, int L0, int B, int LV, int K, bool LAZY>
+__device__ __forceinline__ void fwd_blk_pass(uint64_t (&x)[K][1 << S], const uint64_t* __restrict__ tw) {
     if constexpr (LV < S) {
-        fwd_pow2_level<S, LV, 0, K, LAZY>(x);
-        fwd_pow2_pass<S, LV + 1, K, LAZY>(x);
+        fwd_blk_level<S, L0, B, LV, 0, K, LAZY>(x, tw);
+        fwd_blk_pass<S, L0, B, LV + 1, K, LAZY>(x, tw);
     }
 }
-// Inverse (Gentleman-Sande): (u, v) -> (u + v, (u - v) 2^e); a negative
-// twiddle multiplies v - u instead.
-template <int S, int LV, int J, int K>
-__device__ __forceinline__ void inv_pow2_level(uint64_t (&x)[K][1 << S]) {
+// Inverse (Gentleman-Sande): (u, v) -> (u + v, (u - v) w); a negative
+// power-of-two twiddle multiplies v - u by its magnitude instead.
+template <int S, int L0, int B, int LV, int J, int K>
+__device__ __forceinline__ void inv_blk_level(uint64_t (&x)[K][1 << S], const uint64_t* __restrict__ tw) {
     constexpr int G = 1 << S;
     if constexpr (J < G) {
         constexpr int half = G >> (LV + 1);
         if constexpr ((J & half) == 0) {
-            constexpr int EX = pow2_twiddle_exp(LV, J >> (S - LV), true);
+            constexpr int LVL = L0 + LV;
+            constexpr int BI = (B << LV) + (J >> (S - LV));
+            if constexpr (LVL < 5) {
+                constexpr int EX = pow2_twiddle_exp(LVL, BI, true);
 #pragma unroll
-            for (int p = 0; p < K; ++p) {
-                const uint64_t u = x[p][J];
-                const uint64_t v = x[p][J + half];
-                x[p][J] = gl_add(u, v);
-                x[p][J + half] = gl_pow2_mag<EX>(Pow2<EX>::NEG ? gl_sub(v, u) : gl_sub(u, v));
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][J];
+                    const uint64_t v = x[p][J + half];
+                    x[p][J] = gl_add(u, v);
+                    x[p][J + half] = gl_pow2_mag<EX>(Pow2<EX>::NEG ? gl_sub(v, u) : gl_sub(u, v));
+                }
+            } else {
+                const uint64_t w = tw[(1 << LVL) + BI];
+#pragma unroll
+                for (int p = 0; p < K; ++p) {
+                    const uint64_t u = x[p][J];
+                    const uint64_t v = x[p][J + half];
+                    x[p][J] = gl_add(u, v);
+                    x[p][J + half] = gl_mul(gl_sub(u, v), w);
+                }
             }
         }
-        inv_pow2_level<S, LV, J + 1, K>(x);
+        inv_blk_level<S, L0, B, LV, J + 1, K>(x, tw);
     }
 }
-template <int S, int LV, int K>
-__device__ __forceinline__ void inv_pow2_pass(uint64_t (&x)[K][1 << S]) {
+template <int S, int L0, int B, int LV, int K>
+__device__ __forceinline__ void inv_blk_pass(uint64_t (&x)[K][1 << S], const uint64_t* __restrict__ tw) {
     if constexpr (LV >= 0) {
-        inv_pow2_level<S, LV, 0, K>(x);
-        inv_pow2_pass<S, LV - 1, K>(x);
+        inv_blk_level<S, L0, B, LV, 0, K>(x, tw);
+        inv_blk_pass<S, L0, B, LV - 1, K>(x, tw);
     }
 }
 
-// Forward butterflies of pass P on the thread's registers (R4: use the fused
-// radix-4 form for radix-4 passes; LAZY: see ntt_forward_k).
-template <int LOGN, int P, int K, int LOGE, bool R4, bool LAZY>
+// f(std::integral_constant<int, b>{}) for a runtime b in [0, NB), NB <= 16: one
+// instantiation per block, entered through a switch. Callers pass a b that is the
+// same across the warp, so the jump does not diverge.
+template <int NB, class F>
+__device__ __forceinline__ void block_switch(int b, F&& f) {
+    static_assert(NB >= 1 && NB <= 16, "up to 16 blocks");
+#define TP_BLOCK_CASE(i)                                              \
+    case i:                                                           \
+        if constexpr (i < NB) f(std::integral_constant<int, i>{});    \
+        break;
+    switch (b) {
+        TP_BLOCK_CASE(0) TP_BLOCK_CASE(1) TP_BLOCK_CASE(2) TP_BLOCK_CASE(3)
+        TP_BLOCK_CASE(4) TP_BLOCK_CASE(5) TP_BLOCK_CASE(6) TP_BLOCK_CASE(7)
+        TP_BLOCK_CASE(8) TP_BLOCK_CASE(9) TP_BLOCK_CASE(10) TP_BLOCK_CASE(11)
+        TP_BLOCK_CASE(12) TP_BLOCK_CASE(13) TP_BLOCK_CASE(14) TP_BLOCK_CASE(15)
+        default: break;
+    }
+#undef TP_BLOCK_CASE
+}
+
+// Transform forms: template flags of the pass functions below.
+constexpr int kNttRadix4 = 1;       // fused radix-4 passes (4 coefficients per thread)
+constexpr int kNttTablePasses = 2;  // later passes read table twiddles even on power-of-two levels
+
+// A later pass (P > 0) takes its power-of-two levels as shifts when its twiddle
+// block is the same for a whole warp: one radix-G group per thread (G = E) and
+// at least 32 threads per block (TMIN >= 32), so blk = t / TMIN is warp-uniform
+// and selects a compile-time instantiation. Only passes that start with at most
+// 4 blocks (first level 2 with 4 per thread, levels 2-3; level 3 with 8, levels
+// 3-5 of which 3-4 shift): the 16-way form that also takes level 4 with 4 per
+// thread made the rotation kernels spill and measured slower.
+template <int LOGN, int LOGE, int P>
+__host__ __device__ constexpr bool pow2_block_pass() {
+    using SH = NttShape<LOGN, LOGE>;
+    return P > 0 && SH::S(P) == LOGE && SH::L0(P) < 5 && (SH::N >> (SH::L0(P) + SH::S(P))) >= 32 &&
+           (1 << SH::L0(P)) <= 4;
+}
+
+// Forward butterflies of pass P on the thread's registers (FORM: kNttRadix4 uses
+// the fused radix-4 form for radix-4 passes, kNttTablePasses keeps the later
+// passes on table twiddles; LAZY: see ntt_forward_k).
+template <int LOGN, int P, int K, int LOGE, int FORM, bool LAZY>
 __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
-    if constexpr (R4 && LOGE == 2 && S == 2) {
+    if constexpr ((FORM & kNttRadix4) && LOGE == 2 && S == 2) {
         fwd_radix4<LOGN, P, K, LAZY>(x, t, tw);
     } else if constexpr (P == 0 && S == LOGE) {
-        fwd_pow2_pass<LOGE, 0, K, LAZY>(x);
+        fwd_blk_pass<LOGE, 0, 0, 0, K, LAZY>(x, tw);
+    } else if constexpr (!(FORM & kNttTablePasses) && pow2_block_pass<LOGN, LOGE, P>()) {
+        constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+        block_switch<(1 << SH::L0(P))>(t / TMIN, [&](auto blk) {
+            fwd_blk_pass<LOGE, SH::L0(P), decltype(blk)::value, 0, K, LAZY>(x, tw);
+        });
     } else {
         constexpr int G = 1 << S;
         constexpr int PER = SH::E / G;
@@ -279,14 +354,19 @@ __device__ __forceinline__ void fwd_pass_math(uint64_t (&x)[K][1 << LOGE], int t
 }
 
 // Inverse butterflies of pass P (levels in reverse order).
-template <int LOGN, int P, int K, int LOGE, bool R4>
+template <int LOGN, int P, int K, int LOGE, int FORM>
 __device__ __forceinline__ void inv_pass_math(uint64_t (&x)[K][1 << LOGE], int t, const uint64_t* __restrict__ tw) {
     using SH = NttShape<LOGN, LOGE>;
     constexpr int S = SH::S(P);
-    if constexpr (R4 && LOGE == 2 && S == 2) {
+    if constexpr ((FORM & kNttRadix4) && LOGE == 2 && S == 2) {
         inv_radix4<LOGN, P, K>(x, t, tw);
     } else if constexpr (P == 0 && S == LOGE) {
-        inv_pow2_pass<LOGE, LOGE - 1, K>(x);
+        inv_blk_pass<LOGE, 0, 0, LOGE - 1, K>(x, tw);
+    } else if constexpr (!(FORM & kNttTablePasses) && pow2_block_pass<LOGN, LOGE, P>()) {
+        constexpr int TMIN = SH::N >> (SH::L0(P) + S);
+        block_switch<(1 << SH::L0(P))>(t / TMIN, [&](auto blk) {
+            inv_blk_pass<LOGE, SH::L0(P), decltype(blk)::value, LOGE - 1, K>(x, tw);
+        });
     } else {
         constexpr int G = 1 << S;
         constexpr int PER = SH::E / G;
@@ -356,50 +436,51 @@ __device__ __forceinline__ void xload(const uint64_t* buf, uint64_t (&x)[K][1 <<
     }
 }
 
-template <int LOGN, int P, int K, int LOGE, bool R4, bool LAZY>
+template <int LOGN, int P, int K, int LOGE, int FORM, bool LAZY>
 __device__ __forceinline__ void fwd_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                 const uint64_t* tw) {
     using SH = NttShape<LOGN, LOGE>;
-    fwd_pass_math<LOGN, P, K, LOGE, R4, LAZY>(x, t, tw);
+    fwd_pass_math<LOGN, P, K, LOGE, FORM, LAZY>(x, t, tw);
     if constexpr (P + 1 < SH::NPASS) {
         xstore<LOGN, P, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P));
         xload<LOGN, P + 1, K, LOGE>(buf, x, t);
-        fwd_passes_from<LOGN, P + 1, K, LOGE, R4, LAZY>(x, t, buf, tw);
+        fwd_passes_from<LOGN, P + 1, K, LOGE, FORM, LAZY>(x, t, buf, tw);
     }
 }
 
-template <int LOGN, int P, int K, int LOGE, bool R4>
+template <int LOGN, int P, int K, int LOGE, int FORM>
 __device__ __forceinline__ void inv_passes_from(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                 const uint64_t* tw) {
     using SH = NttShape<LOGN, LOGE>;
-    inv_pass_math<LOGN, P, K, LOGE, R4>(x, t, tw);
+    inv_pass_math<LOGN, P, K, LOGE, FORM>(x, t, tw);
     if constexpr (P > 0) {
         xstore<LOGN, P, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(P - 1));
         xload<LOGN, P - 1, K, LOGE>(buf, x, t);
-        inv_passes_from<LOGN, P - 1, K, LOGE, R4>(x, t, buf, tw);
+        inv_passes_from<LOGN, P - 1, K, LOGE, FORM>(x, t, buf, tw);
     }
 }
 
 // Forward NTT of K polynomials: coefficient layout -> slot layout. buf holds K*N words.
-// R4 (4 coefficients per thread only) selects the fused radix-4 butterflies,
-// whose twiddle products sit at tw_fwd + N.
+// FORM: kNttRadix4 (4 coefficients per thread only) selects the fused radix-4
+// butterflies, whose twiddle products sit at tw_fwd + N; kNttTablePasses keeps
+// the power-of-two levels of passes after the first on table twiddles.
 // LAZY: the outputs are 64-bit values congruent to the evaluations but not
 // necessarily below p, for callers that only multiply them (gl_mul,
 // gl_fma take any 64-bit operand). Each butterfly's sum then skips the
 // canonical step (gl_add_lazy: its right operand, the twiddle product, is
 // canonical; the left may be any 64-bit value, and gl_sub takes that too). The
 // inputs must be canonical (the radix-4 form's first pass shifts them).
-template <int LOGN, int K, int LOGE = 3, bool R4 = false, bool LAZY = false>
+template <int LOGN, int K, int LOGE = 3, int FORM = 0, bool LAZY = false>
 __device__ __forceinline__ void ntt_forward_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                               const uint64_t* tw_fwd) {
-    fwd_passes_from<LOGN, 0, K, LOGE, R4, LAZY>(x, t, buf, tw_fwd);
+    fwd_passes_from<LOGN, 0, K, LOGE, FORM, LAZY>(x, t, buf, tw_fwd);
 }
 
 // The rest of a forward transform whose pass 0 the caller has already applied to x
 // (same layouts and LAZY rule as ntt_forward_k).
-template <int LOGN, int K, int LOGE, bool R4 = false, bool LAZY = false>
+template <int LOGN, int K, int LOGE, int FORM = 0, bool LAZY = false>
 __device__ __forceinline__ void ntt_forward_after_pass0(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                         const uint64_t* tw_fwd) {
     using SH = NttShape<LOGN, LOGE>;
@@ -407,7 +488,7 @@ __device__ __forceinline__ void ntt_forward_after_pass0(uint64_t (&x)[K][1 << LO
         xstore<LOGN, 0, K, LOGE>(buf, x, t);
         ntt_sync<LOGN, LOGE>(!SH::WarpLocal(0));
         xload<LOGN, 1, K, LOGE>(buf, x, t);
-        fwd_passes_from<LOGN, 1, K, LOGE, R4, LAZY>(x, t, buf, tw_fwd);
+        fwd_passes_from<LOGN, 1, K, LOGE, FORM, LAZY>(x, t, buf, tw_fwd);
     }
 }
 
@@ -433,10 +514,10 @@ __device__ __forceinline__ void ntt_pass0_small(const int64_t (&d)[4], uint64_t 
 }
 
 // Backward NTT of K polynomials without the 1/N factor: slot -> coefficient layout.
-template <int LOGN, int K, int LOGE = 3, bool R4 = false>
+template <int LOGN, int K, int LOGE = 3, int FORM = 0>
 __device__ __forceinline__ void ntt_backward_unscaled_k(uint64_t (&x)[K][1 << LOGE], int t, uint64_t* buf,
                                                         const uint64_t* tw_inv) {
-    inv_passes_from<LOGN, NttShape<LOGN, LOGE>::NPASS - 1, K, LOGE, R4>(x, t, buf, tw_inv);
+    inv_passes_from<LOGN, NttShape<LOGN, LOGE>::NPASS - 1, K, LOGE, FORM>(x, t, buf, tw_inv);
 }
 
 // One polynomial, 8 coefficients per thread.
