@@ -86,6 +86,8 @@ def lib() -> ctypes.CDLL:
         "tp_auto_eval_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
         "tp_pack_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
         "tp_pack_batch_noalloc": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
+        "tp_pack_subtree_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
+        "tp_pack_merge_batch": (ctypes.c_int, [VP, U64, U64, ctypes.c_uint32, ctypes.c_int, VP, VP, VP]),
         "tp_pack_consecutive_batch": (ctypes.c_int, [VP, U64, U64, VP, VP, VP]),
         "tp_trace_eval_batch": (ctypes.c_int, [VP, U64, VP, VP, VP]),
         "tp_trace_eval_auto_batch": (ctypes.c_int, [VP, U64, VP, VP, ctypes.c_uint32, VP]),

@@ -1369,6 +1369,48 @@ tp_status tp_pack_consecutive_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, 
     return TP_OK;
 }
 
+// Merges of the packing tree (lwe_to_rlwe_packing.cpp:170-224) over `packs` regions
+// of `count` nodes each (2N coefficient words per node, in tree position order, in
+// place at `work`): relative level k = 1 .. log2(count) merges nodes 2^k q and
+// 2^k q + 2^(k-1) of a region at absolute tree level L = level0 + k (automorphism
+// key 2^L + 1, shift N >> L), leaving each region's root at its first node. The
+// merge at a level depends on that level only, never on the node's place in the
+// whole tree, so a subtree runs exactly like the bottom of a smaller tree.
+static tp_status pack_merge_levels(tp_ks_ctx* c, uint64_t packs, uint64_t count, int level0, uint64_t* work,
+                                   cudaStream_t st) {
+    const uint64_t N = c->N;
+    const uint64_t kw = (uint64_t)c->digits * 2 * N;
+    tp::KsKernelParams kp = c->kp;
+    const int levels = ilog2(count);
+    for (int k = 1; k <= levels; ++k) {
+        const int L = level0 + k;
+        kp.key = c->key + (uint64_t)(L - 1) * kw;
+        kp.in = work;
+        kp.out = work;
+        kp.items = packs * (count >> k);
+        kp.in_stride = kp.out_stride = (1ull << k) * 2 * N;
+        kp.right_offset = (1ull << (k - 1)) * 2 * N;
+        kp.auto_index = (1u << L) + 1;
+        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
+        kp.shift = (uint32_t)(N >> L);
+        tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
+        if (s != TP_OK) return s;
+    }
+    return TP_OK;
+}
+
+// The context's work area holds at least `words` words.
+static tp_status pack_work(tp_ks_ctx* c, uint64_t words) {
+    if (c->work_words < words) {
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_words = 0;
+        TP_CUDA(cudaMalloc(&c->work, words * 8));
+        c->work_words = words;
+    }
+    return TP_OK;
+}
+
 tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out, const uint64_t* in, void* stream) {
     if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
     if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
@@ -1382,12 +1424,9 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
     std::lock_guard<std::mutex> lk(c->mu);
     TP_CUDA(cudaSetDevice(c->device));
     const uint64_t need = packs * len * 2 * N;
-    if (c->work_words < need) {
-        cudaFree(c->work);
-        c->work = nullptr;
-        c->work_words = 0;
-        TP_CUDA(cudaMalloc(&c->work, need * 8));
-        c->work_words = need;
+    {
+        tp_status s = pack_work(c, need);
+        if (s != TP_OK) return s;
     }
     cudaStream_t st = (cudaStream_t)stream;
     const int log_len = ilog2(len);
@@ -1398,20 +1437,8 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
         tp::note_launch();
         TP_CUDA(cudaGetLastError());
     }
-    const uint64_t kw = (uint64_t)c->digits * 2 * N;
-    tp::KsKernelParams kp = c->kp;
-    // tree merges, level by level (lwe_to_rlwe_packing.cpp:170-224)
-    for (int L = 1; L <= log_len; ++L) {
-        kp.key = c->key + (uint64_t)(L - 1) * kw;
-        kp.in = c->work;
-        kp.out = c->work;
-        kp.items = packs * (len >> L);
-        kp.in_stride = kp.out_stride = (1ull << L) * 2 * N;
-        kp.right_offset = (1ull << (L - 1)) * 2 * N;
-        kp.auto_index = (1u << L) + 1;
-        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
-        kp.shift = (uint32_t)(N >> L);
-        tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
+    {
+        tp_status s = pack_merge_levels(c, packs, len, 0, c->work, st);
         if (s != TP_OK) return s;
     }
     // trailing traces when len < N (lwe_to_rlwe_packing.cpp:228-234)
@@ -1420,6 +1447,70 @@ tp_status tp_pack_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* ou
         if (s != TP_OK) return s;
     }
     TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, c->work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
+    return TP_OK;
+}
+
+// One shard of a packing split over several devices: the subtree of `len` inputs
+// (L0 set-up and merges of levels 1 .. log2 len, no traces), its root left in the
+// coefficient domain for tp_pack_merge_batch.
+tp_status tp_pack_subtree_batch(tp_ks_ctx* c, uint64_t packs, uint64_t len, uint64_t* out, const uint64_t* in,
+                                void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (packs == 0) return TP_OK;
+    if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->N;
+    if (len < 1 || len > N || (len & (len - 1))) return fail(TP_ERR_PARAM, "len must be a power of two in [1, N]");
+    if (packs > (UINT64_MAX / 8) / (len * 2 * N))
+        return fail(TP_ERR_PARAM, "packs * len * 2N words overflow (%llu packs of length %llu)",
+                    (unsigned long long)packs, (unsigned long long)len);
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    const uint64_t need = packs * len * 2 * N;
+    tp_status s = pack_work(c, need);
+    if (s != TP_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    tp::pack_l0_kernel<<<(unsigned)std::min<uint64_t>((need + 255) / 256, 65535), 256, 0, st>>>(
+        c->work, in, packs, (uint32_t)len, (uint32_t)ilog2(len), (uint32_t)c->logn, c->tab->n_inv);
+    tp::note_launch();
+    TP_CUDA(cudaGetLastError());
+    s = pack_merge_levels(c, packs, len, 0, c->work, st);
+    if (s != TP_OK) return s;
+    TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, c->work, len * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice, st));
+    return TP_OK;
+}
+
+// The tree above `count` subtree roots of level `level0` (position order), then, with
+// `finish`, the trailing traces of levels level0 + log2(count) + 1 .. log2 N.
+tp_status tp_pack_merge_batch(tp_ks_ctx* c, uint64_t packs, uint64_t count, uint32_t level0, int finish,
+                              uint64_t* out, const uint64_t* nodes, void* stream) {
+    if (!c || c->kind != 2) return fail(TP_ERR_PARAM, "not a packing context");
+    if (!c->key_ready) return fail(TP_ERR_STATE, "no keys uploaded");
+    if (packs == 0) return TP_OK;
+    if (!out || !nodes) return fail(TP_ERR_PARAM, "null buffer");
+    const uint64_t N = c->N;
+    if (count < 1 || count > N || (count & (count - 1)))
+        return fail(TP_ERR_PARAM, "count must be a power of two in [1, N]");
+    const int top = (int)level0 + ilog2(count);
+    if (top > c->logn) return fail(TP_ERR_PARAM, "level0 + log2(count) must not exceed log2 N");
+    if (packs > (UINT64_MAX / 8) / (count * 2 * N))
+        return fail(TP_ERR_PARAM, "packs * count * 2N words overflow (%llu packs of %llu nodes)",
+                    (unsigned long long)packs, (unsigned long long)count);
+    std::lock_guard<std::mutex> lk(c->mu);
+    TP_CUDA(cudaSetDevice(c->device));
+    const uint64_t need = packs * count * 2 * N;
+    tp_status s = pack_work(c, need);
+    if (s != TP_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    TP_CUDA(cudaMemcpyAsync(c->work, nodes, need * 8, cudaMemcpyDeviceToDevice, st));
+    s = pack_merge_levels(c, packs, count, (int)level0, c->work, st);
+    if (s != TP_OK) return s;
+    if (finish) {
+        s = ks_trace_steps(c, packs, c->work, count * 2 * N, c->logn, top + 1, st);
+        if (s != TP_OK) return s;
+    }
+    TP_CUDA(cudaMemcpy2DAsync(out, 2 * N * 8, c->work, count * 2 * N * 8, 2 * N * 8, packs, cudaMemcpyDeviceToDevice,
+                              st));
     return TP_OK;
 }
 

@@ -98,6 +98,18 @@ class GpuLWEtoRLWEPacker(_KsBase):
     def pack_consecutive_batch(self, packs: int, length: int, out_ptr: int, in_ptr: int, stream=None) -> None:
         nat.check(nat.lib().tp_pack_consecutive_batch(self._h, packs, length, out_ptr, in_ptr, stream))
 
+    def pack_subtree_batch(self, packs: int, length: int, out_ptr: int, in_ptr: int, stream=None) -> None:
+        """Subtrees of `length` inputs: L0 set-up and merges, roots in the coefficient domain
+        (one shard of a packing split over devices; see sharded_pack)."""
+        nat.check(nat.lib().tp_pack_subtree_batch(self._h, packs, length, out_ptr, in_ptr, stream))
+
+    def pack_merge_batch(self, packs: int, count: int, level0: int, finish: bool, out_ptr: int, nodes_ptr: int,
+                         stream=None) -> None:
+        """The tree above `count` roots of level `level0` per pack; with `finish` the
+        trailing traces too, giving what pack_batch gives for the whole tree."""
+        nat.check(nat.lib().tp_pack_merge_batch(self._h, packs, count, level0, int(bool(finish)), out_ptr,
+                                                nodes_ptr, stream))
+
     def PackConsecutively(self, lwes: np.ndarray, length: int) -> np.ndarray:
         """PackConsecutively of `lwes` (packs*length rows of N+1 words); packs x 2N coefficients."""
         import torch

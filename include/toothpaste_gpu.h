@@ -242,6 +242,24 @@ tp_status tp_auto_eval_batch(tp_ks_ctx* ctx, uint64_t batch, uint64_t* out_dev, 
  * per level, in a context-owned work area of packs*len*2N words. Asynchronous. */
 tp_status tp_pack_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev, const uint64_t* in_dev,
                         void* stream);
+/* The packing tree split into shards, for a packing spread over several devices (no
+ * counterpart call in the reference: Pack (lwe_to_rlwe_packing.cpp:129-236) runs the
+ * whole tree in one call). A level-L merge depends only on L, so the subtree of leaf
+ * positions [r m, (r + 1) m) (m = len / W, W shards) is a pack of m inputs taken with
+ * stride W: input j W + s of pack p, s = (W - 1) ^ brv_{log2 W}(r), becomes that
+ * subtree's input j. tp_pack_subtree_batch runs the L0 set-up and merges of levels
+ * 1 .. log2 len of `packs` such subtrees (len = m inputs each, laid out as for
+ * tp_pack_batch, 1 <= len <= N) and writes each root (2N coefficient words, no
+ * traces) to out + p*2N. tp_pack_merge_batch continues a tree: nodes holds `packs`
+ * groups of `count` roots of level `level0` in position order (count a power of two,
+ * level0 + log2 count <= log2 N); it merges each group at levels level0 + 1 ..
+ * level0 + log2 count and, with `finish` != 0, applies the trailing traces, so
+ * out + p*2N gets what tp_pack_batch gives for the whole tree. Scratch: the
+ * context's work area (packs x len or count x 2N words). Asynchronous. */
+tp_status tp_pack_subtree_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t len, uint64_t* out_dev,
+                                const uint64_t* in_dev, void* stream);
+tp_status tp_pack_merge_batch(tp_ks_ctx* ctx, uint64_t packs, uint64_t count, uint32_t level0, int finish,
+                              uint64_t* out_dev, const uint64_t* nodes_dev, void* stream);
 /* LWEtoRLWEPacker::PackConsecutively(out, in, len) (lwe_to_rlwe_packing.cpp:260-393)
  * for `packs` packings of len inputs each (2 <= len <= N, any length): the inputs
  * land on the first len coefficients. Runs the reference's full N-leaf tree with

@@ -7,6 +7,8 @@ import subprocess
 import sys
 from pathlib import Path
 
+import numpy as np
+
 from oracle.oracle import sha256
 
 ROOT = Path(__file__).resolve().parents[1]
@@ -47,3 +49,39 @@ def test_single_process_needs_no_group():
         assert aggregate_rate(4096, 1, 0.5) == 8192
     finally:
         os.environ.update(env)
+
+
+def _run_sharded_pack(tmp_path, world: int, length: int):
+    out = tmp_path / f"pack{world}.json"
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", CUDA_VISIBLE_DEVICES="")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={world}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", str(ROOT / "tests" / "sharded_pack_worker.py"),
+           "--out", str(out), "--length", str(length)]
+    res = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    return json.loads(out.read_text())
+
+
+def test_sharded_packing_exchange_on_two_and_four_ranks(tmp_path):
+    """Pack split over W ranks (fhetoothpaste_b200/sharded_pack.py): each rank's shard rows, the
+    log2 W pairwise exchanges and the merge levels give the reference tree's leaf order on every
+    rank, with the traces applied once, on the last merge."""
+    for world, length in ((2, 16), (4, 16), (4, 4)):
+        reps = _run_sharded_pack(tmp_path, world, length)
+        assert [r["rank"] for r in reps] == list(range(world))
+        m = length // world
+        for r in reps:
+            assert r["ok"], (world, length, r)
+            lm = m.bit_length() - 1
+            w = world.bit_length() - 1
+            assert r["calls"] == [[2, lm + k, k == w - 1] for k in range(w)]
+
+
+def test_shard_rows_cover_every_input_once():
+    from fhetoothpaste_b200.sharded_pack import shard_rows
+    for length in (2, 8, 64, 2048):
+        for world in (1, 2, 4, 8):
+            if world > length:
+                continue
+            rows = np.concatenate([shard_rows(length, world, r) for r in range(world)])
+            assert sorted(rows.tolist()) == list(range(length))
