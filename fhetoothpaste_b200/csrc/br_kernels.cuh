@@ -110,10 +110,11 @@ __host__ __device__ constexpr bool br_table_passes(int variant, bool digit_stage
 // so did staging part of each row there (two components, the rest read from L2
 // at use: ternary 1918 vs 1978; BMMP 2939 vs 2889, within run-to-run spread).
 // Ring sizes above 4096 rotate on a cluster of 2^logs CTAs, each holding
-// 2^(logn - logs) = 2048 coefficients and slots (cluster_ntt.cuh); every plan
-// below is per CTA, in words of its local size, plus two receive areas of the
-// distributed transform's exchange.
-__host__ __device__ constexpr int br_cluster_logs(int logn) { return logn > 12 ? logn - 11 : 0; }
+// 2^(logn - logs) coefficients and slots (cluster_ntt.cuh): 2048 for N = 8192,
+// 16384 and 32768 (4, 8 and 16 CTAs), 4096 for N = 65536 (16 CTAs, the largest
+// cluster B200 runs); every plan below is per CTA, in words of its local size,
+// plus two receive areas of the distributed transform's exchange.
+__host__ __device__ constexpr int br_cluster_logs(int logn) { return logn > 12 ? (logn - 11 < 4 ? logn - 11 : 4) : 0; }
 
 __host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge, int logs = 0, bool r4 = false) {
     return (size_t)(br_smem_twiddles(logn - logs)

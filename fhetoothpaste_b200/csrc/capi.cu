@@ -309,8 +309,8 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
     if (p->modulus != kP) return fail(TP_ERR_PARAM, "modulus must be the Goldilocks prime 2^64-2^32+1");
     if (p->variant < 0 || p->variant > 2) return fail(TP_ERR_PARAM, "unknown variant %d", p->variant);
     const uint64_t N = p->ring_dim;
-    if (N < 128 || N > 32768 || (N & (N - 1)))
-        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
+    if (N < 128 || N > 65536 || (N & (N - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 65536]");
     if (p->lwe_dim == 0) return fail(TP_ERR_PARAM, "lwe_dim must be positive");
     if (p->variant == TP_BR_BMMP_BINARY && (p->lwe_dim % 2)) return fail(TP_ERR_PARAM, "BMMP needs an even lwe_dim");
     if (p->basis < 2 || (p->basis & (p->basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
@@ -957,8 +957,8 @@ static tp_status ks_create(int kind, uint32_t ring_dim, uint64_t basis, uint32_t
                            tp_ks_ctx** out) {
     if (!out) return fail(TP_ERR_PARAM, "null argument");
     *out = nullptr;
-    if (ring_dim < 128 || ring_dim > 32768 || (ring_dim & (ring_dim - 1)))
-        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
+    if (ring_dim < 128 || ring_dim > 65536 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 65536]");
     if (basis < 2 || (basis & (basis - 1))) return fail(TP_ERR_PARAM, "basis must be a power of two");
     const int beta = ilog2(basis);
     if (beta > 30) return fail(TP_ERR_PARAM, "basis above 2^30 is not supported");
@@ -1791,8 +1791,8 @@ tp_status tp_lwe_ks_upload_key_file(tp_lwe_ks_ctx* c, const char* path) {
 
 static tp_status ntt_launch(uint32_t ring_dim, uint64_t count, uint64_t* out, const uint64_t* in, void* stream,
                             bool fwd, uint64_t in_stride = 0, uint64_t out_stride = 0) {
-    if (ring_dim < 128 || ring_dim > 32768 || (ring_dim & (ring_dim - 1)))
-        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 32768]");
+    if (ring_dim < 128 || ring_dim > 65536 || (ring_dim & (ring_dim - 1)))
+        return fail(TP_ERR_PARAM, "ring_dim must be a power of two in [128, 65536]");
     if (count == 0) return TP_OK;
     if (!out || !in) return fail(TP_ERR_PARAM, "null buffer");
     if (((uintptr_t)out & 15) || ((uintptr_t)in & 15)) return fail(TP_ERR_PARAM, "buffers must be 16-byte aligned");

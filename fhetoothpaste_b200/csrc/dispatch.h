@@ -17,10 +17,12 @@ const void* br_kernel_ptr_12(int variant, int loge, int dl, bool r4);
 const void* br_kernel_ptr_13(int variant, int loge, int dl, bool r4);
 const void* br_kernel_ptr_14(int variant, int loge, int dl, bool r4);
 const void* br_kernel_ptr_15(int variant, int loge, int dl, bool r4);
+const void* br_kernel_ptr_16(int variant, int loge, int dl, bool r4);
 const void* ntt_kernel_ptr_12(bool forward);
 const void* ntt_kernel_ptr_13(bool forward);  // cluster kernels (ntt_cluster_kernel)
 const void* ntt_kernel_ptr_14(bool forward);
 const void* ntt_kernel_ptr_15(bool forward);
+const void* ntt_kernel_ptr_16(bool forward);
 const void* br_pair_kernel_ptr_7(int variant, int split);
 const void* br_pair_kernel_ptr_8(int variant, int split);
 const void* br_pair_kernel_ptr_9(int variant, int split);
@@ -36,8 +38,9 @@ const void* ks_kernel_ptr_12(int mode, int loge);
 const void* ks_kernel_ptr_13(int mode, int loge);
 const void* ks_kernel_ptr_14(int mode, int loge);
 const void* ks_kernel_ptr_15(int mode, int loge);
+const void* ks_kernel_ptr_16(int mode, int loge);
 
-// One-block rotation kernel (one cluster of CTAs per rotation above N = 4096);
+// One-block rotation kernel (one cluster of CTAs per rotation above N = 4096, N up to 65536);
 // dl = 0: multiply-accumulate row by row, dl = 3 or 4: the digit-staged form for
 // that digit count; r4: the fused radix-4 passes (N = 1024 .. 4096, 4 coefficients
 // per thread) (nullptr where not built).
@@ -52,6 +55,7 @@ inline const void* br_kernel_lookup(int logn, int variant, int loge, int dl = 0,
         case 13: return br_kernel_ptr_13(variant, loge, dl, r4);
         case 14: return br_kernel_ptr_14(variant, loge, dl, r4);
         case 15: return br_kernel_ptr_15(variant, loge, dl, r4);
+        case 16: return br_kernel_ptr_16(variant, loge, dl, r4);
         default: return nullptr;
     }
 }
@@ -81,6 +85,7 @@ inline const void* ntt_kernel_lookup(int logn, bool forward) {
         case 13: return ntt_kernel_ptr_13(forward);
         case 14: return ntt_kernel_ptr_14(forward);
         case 15: return ntt_kernel_ptr_15(forward);
+        case 16: return ntt_kernel_ptr_16(forward);
         default: return nullptr;
     }
 }
@@ -96,6 +101,7 @@ inline const void* ks_kernel_lookup(int logn, int mode, int loge) {
         case 13: return ks_kernel_ptr_13(mode, loge);
         case 14: return ks_kernel_ptr_14(mode, loge);
         case 15: return ks_kernel_ptr_15(mode, loge);
+        case 16: return ks_kernel_ptr_16(mode, loge);
         default: return nullptr;
     }
 }

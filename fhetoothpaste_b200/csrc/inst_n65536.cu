@@ -1,0 +1,38 @@
+// Kernel instantiations for N = 65536: one rotation per cluster of 16 CTAs of 4096
+// coefficients each (cluster_ntt.cuh; 1024 threads per CTA, 4 coefficients per
+// thread), for the rotation (row-by-row multiply-accumulate: the digit stage does not
+// fit beside 4096 coefficients) and the key-switching modes; compiled as a separate
+// unit so the ring sizes build in parallel.
+#include "br_kernels.cuh"
+#include "dispatch.h"
+#include "ks_kernels.cuh"
+#include "misc_kernels.cuh"
+
+namespace tp {
+
+const void* br_kernel_ptr_16(int variant, int loge, int dl, bool r4) {
+    if (r4 || loge != 2 || dl != 0) return nullptr;
+    switch (variant) {
+        case kCggiBinary: return (const void*)br_kernel<16, kCggiBinary, 2, 0, 4>;
+        case kCggiTernary: return (const void*)br_kernel<16, kCggiTernary, 2, 0, 4>;
+        default: return (const void*)br_kernel<16, kBmmpBinary, 2, 0, 4>;
+    }
+}
+
+const void* ks_kernel_ptr_16(int mode, int loge) {
+    if (loge != 2) return nullptr;  // clusters run with 4 coefficients per thread
+    switch (mode) {
+        case kKsRlwe: return (const void*)ks_kernel<16, kKsRlwe, 2, 4>;
+        case kKsAuto: return (const void*)ks_kernel<16, kKsAuto, 2, 4>;
+        case kKsMerge: return (const void*)ks_kernel<16, kKsMerge, 2, 4>;
+        case kKsTrace: return (const void*)ks_kernel<16, kKsTrace, 2, 4>;
+        default: return (const void*)ks_kernel<16, kKsSplit, 2, 4>;
+    }
+}
+
+const void* ntt_kernel_ptr_16(bool forward) {
+    return forward ? (const void*)ntt_cluster_kernel<16, true, 4>
+                   : (const void*)ntt_cluster_kernel<16, false, 4>;
+}
+
+}  // namespace tp

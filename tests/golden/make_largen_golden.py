@@ -5,8 +5,9 @@ Run here, where the reference sources exist: `python tests/golden/make_largen_go
 [br] [ks]` (default both; needs oracle/_ref/libtpref.so, see oracle/Makefile). The
 reference's SolinasWorker accepts N up to 2^16; its rotators build a monomial table of
 N (N + 2) words, so the rotation cases stop at N = 16384 (2.1 GB); the key-switching
-cases go to 32768. Inputs and keys are regenerated in the tests from the recorded seeds
-(same generators as make_golden.py); outputs are recorded as SHA-256 of each result
+cases go to 65536, the largest ring the worker accepts. Inputs and keys are
+regenerated in the tests from the recorded seeds (same generators as make_golden.py);
+outputs are recorded as SHA-256 of each result
 (rotations: NTT-domain output, then coefficient output), with the key's SHA-256.
 """
 from __future__ import annotations
@@ -48,6 +49,9 @@ KS_CASES = [
     ("pack16_n8192", "pack", 8192, 16, 4, 16),
     ("pack2_n16384", "pack", 16384, 16, 4, 2),
     ("pack4_n32768", "pack", 32768, 16, 4, 4),
+    ("rks_n65536", "rlwe_ks", 65536, 16, 4, None),
+    ("auto5_n65536", "auto", 65536, 16, 4, 5),
+    ("pack2_n65536", "pack", 65536, 16, 4, 2),
 ]
 
 

@@ -17,7 +17,7 @@ def test_library_exports_every_declared_symbol(native):
     assert not missing, f"declared but not exported: {missing}"
 
 
-@pytest.mark.parametrize("field,value", [("modulus", 36028797018972161), ("ring_dim", 1000), ("ring_dim", 65536),
+@pytest.mark.parametrize("field,value", [("modulus", 36028797018972161), ("ring_dim", 1000), ("ring_dim", 131072),
                                          ("ring_dim", 64), ("lwe_dim", 0), ("basis", 3), ("basis", 1 << 31),
                                          ("digits", 0), ("digits", 9), ("variant", 7)])
 def test_bad_parameters_are_rejected(native, field, value):

@@ -2,7 +2,8 @@
 CTAs with the transforms distributed over distributed shared memory (csrc/cluster_ntt.cuh).
 Bit-exact against the reference library's outputs (tests/golden/largen.json, N = 8192 and
 16384: SHA-256 of every output word) and against the C oracle (pinned to those outputs by
-tests/test_largen_oracle_cpu.py) at N = 32768 and on batches larger than the resident grid."""
+tests/test_largen_oracle_cpu.py) at N = 32768 and 65536 and on batches larger than the resident
+grid; key switching, automorphisms, packing and transforms up to N = 65536."""
 import json
 from pathlib import Path
 
@@ -51,9 +52,13 @@ def test_large_ring_matches_reference(native, oracle, name):
     rot.close()
 
 
+@pytest.mark.parametrize("N", [32768, 65536])
 @pytest.mark.parametrize("v,bl,dg", [(CGGI_TERNARY, 12, 3), (CGGI_BINARY, 16, 4), (BMMP_BINARY, 16, 4)])
-def test_n32768_matches_oracle(native, oracle, v, bl, dg):
-    N, n = 32768, 4
+def test_largest_rings_match_oracle(native, oracle, v, bl, dg, N):
+    """N = 32768 (16 CTAs of 2048 coefficients) and 65536 (16 CTAs of 4096), where the
+    reference's rotators cannot build their N (N + 2)-word monomial table: the oracle,
+    pinned to the reference at 8192 and 16384."""
+    n = 4 if N == 32768 else 2
     brk, rot = _rotator(oracle, v, N, n, bl, dg, 500 + v)
     lwes = lwe_inputs(N, n, 2, 510)
     accs = random_acc(N, 2, 511)
@@ -139,7 +144,7 @@ def test_large_ring_key_switch_batch_larger_than_the_grid(native, oracle):
     conv.close()
 
 
-@pytest.mark.parametrize("N", [8192, 16384, 32768])
+@pytest.mark.parametrize("N", [8192, 16384, 32768, 65536])
 def test_large_ring_ntt_matches_oracle(native, oracle, N):
     """The standalone transforms on a cluster: forward against the oracle, backward inverts it
     (out of place and in place, several polynomials)."""
