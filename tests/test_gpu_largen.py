@@ -180,3 +180,32 @@ def test_large_ring_trace_and_consecutive_packing_match_oracle(native, oracle):
     np.testing.assert_array_equal(pk.PackConsecutively(lwes, length)[0],
                                   oracle.pack_consecutive(N, bl, dg, keys, lwes, length))
     pk.close()
+
+
+def test_large_ring_scheme_switching_and_sap_match_oracle(native, oracle, cuda):
+    """The composite operators on the cluster kernels at N = 8192: LWEtoRGSWConverter::Convert
+    (rotation, trace, squaring key switch) and SAPDecomposer::Decompose (rotations, truncation
+    tree, LWE key switch), against the oracle restatement."""
+    from fhetoothpaste_b200 import GpuLWEtoRGSWConverter, GpuSAPDecomposer
+    N, n = 8192, 4
+    sk = lwe_secret(CGGI_BINARY, n, N, 560)
+    z = rlwe_secret(N, 561)
+    g = (16, 4)
+    keys = oracle.ss_keygen(CGGI_BINARY, N, n, g, g, g, 3.2, sk, z, 562)
+    conv = GpuLWEtoRGSWConverter((CGGI_BINARY, N, n, 1 << 16, 4), (1 << 16, 4), (1 << 16, 4), 4, 1 << 16, *keys)
+    lwes = lwe_inputs(N, n, 2, 563)
+    got = conv.Convert(lwes)
+    for j in range(2):
+        want = oracle.lwe_to_rgsw(CGGI_BINARY, N, n, g, keys[0], g, keys[1], g, keys[2], 4, 16, lwes[j])
+        np.testing.assert_array_equal(got[j], want, err_msg=f"LWE->RGSW input {j}")
+    skeys = oracle.sap_keygen(CGGI_BINARY, N, n, g, g, g, 3.2, sk, z, 564)
+    beta = int(np.count_nonzero(sk))
+    dec = GpuSAPDecomposer((CGGI_BINARY, N, n, 1 << 16, 4), (1 << 16, 4), (1 << 16, 4), *skeys,
+                           hamming_weight=beta, restart_period=4)
+    small = np.random.default_rng(565).integers(0, 1 << 12, (2, n + 1), dtype=np.uint64)
+    digits, outs = dec.Decompose(small, 16, 4)
+    for j in range(1):  # the oracle takes about 17 s per input at this size
+        d, want = oracle.sap_decompose(CGGI_BINARY, N, n, g, skeys[0], g, skeys[1], g, skeys[2], 16, beta, 4,
+                                       small[j], 4)
+        assert digits[j] == d
+        np.testing.assert_array_equal(outs[j], want, err_msg=f"SAP input {j}")
