@@ -2424,19 +2424,8 @@ extern "C" tp_status tp_pack_batch_noalloc(tp_ks_ctx* c, uint64_t packs, uint64_
         tp::note_launch();
         TP_CUDA(cudaGetLastError());
     }
-    const uint64_t kw = (uint64_t)c->digits * 2 * N;
-    tp::KsKernelParams kp = c->kp;
-    for (int L = 1; L <= log_len; ++L) {
-        kp.key = c->key + (uint64_t)(L - 1) * kw;
-        kp.in = work;
-        kp.out = work;
-        kp.items = packs * (len >> L);
-        kp.in_stride = kp.out_stride = (1ull << L) * 2 * N;
-        kp.right_offset = (1ull << (L - 1)) * 2 * N;
-        kp.auto_index = (1u << L) + 1;
-        kp.auto_index_inv = inv_mod_2n(kp.auto_index, 2 * (uint32_t)N);
-        kp.shift = (uint32_t)(N >> L);
-        tp_status s = ks_launch(c, tp::kKsMerge, kp, st);
+    {
+        tp_status s = pack_merge_levels(c, packs, len, 0, work, st);  // the merges of tp_pack_batch
         if (s != TP_OK) return s;
     }
     {

@@ -513,6 +513,25 @@ void GpuLWEtoRLWEPacker::PackConsecutively(uint64_t* output, const uint64_t* inp
         throw std::runtime_error("toothpaste_b200: copy back failed");
 }
 
+void GpuLWEtoRLWEPacker::PackSubtree(uint64_t* root, const uint64_t* input, uint64_t len) {
+    DevBuf din(len * (m_N + 1ull)), dout(2ull * m_N);
+    if (cudaMemcpy(din.p, input, len * (m_N + 1ull) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_pack_subtree_batch(m_ctx, 1, len, dout.p, din.p, nullptr));
+    if (cudaMemcpy(root, dout.p, 16ull * m_N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
+void GpuLWEtoRLWEPacker::PackMerge(uint64_t* output, const uint64_t* roots, uint64_t count, uint32_t level0,
+                                   bool finish) {
+    DevBuf din(count * 2ull * m_N), dout(2ull * m_N);
+    if (cudaMemcpy(din.p, roots, count * 16ull * m_N, cudaMemcpyHostToDevice) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy in failed");
+    check(tp_pack_merge_batch(m_ctx, 1, count, level0, finish ? 1 : 0, dout.p, din.p, nullptr));
+    if (cudaMemcpy(output, dout.p, 16ull * m_N, cudaMemcpyDeviceToHost) != cudaSuccess)
+        throw std::runtime_error("toothpaste_b200: copy back failed");
+}
+
 GpuLWEtoLWEConverter::GpuLWEtoLWEConverter(uint32_t n_in, uint32_t n_out, uint64_t basis, uint32_t digits,
                                            const std::vector<uint64_t>& ksk, int device)
     : m_n_in(n_in), m_n_out(n_out) {

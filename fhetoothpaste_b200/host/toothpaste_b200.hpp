@@ -238,6 +238,14 @@ public:
     void Pack(uint64_t* output, const uint64_t* input, uint64_t len);
     // lwe_to_rlwe_packing.cpp:260-393: the inputs on the first len coefficients, any 2 <= len <= N
     void PackConsecutively(uint64_t* output, const uint64_t* input, uint64_t len);
+    // One shard of a Pack split over devices (no reference counterpart): the subtree of len inputs
+    // (L0 set-up and merges, no traces), its root (2N coefficient words) to `root`
+    // (tp_pack_subtree_batch).
+    void PackSubtree(uint64_t* root, const uint64_t* input, uint64_t len);
+    // The tree above `count` roots of tree level `level0` (position order); with `finish` the
+    // trailing traces as well, so `output` is what Pack gives for the whole tree
+    // (tp_pack_merge_batch).
+    void PackMerge(uint64_t* output, const uint64_t* roots, uint64_t count, uint32_t level0, bool finish);
 
 private:
     tp_ks_ctx* m_ctx = nullptr;

@@ -7,6 +7,7 @@
 //   keygen-pack N beta digits std seed rlwe_key out
 //   rotate      variant N n beta digits std seed lwe_key rlwe_key lwes count accs out
 //   pack        N beta digits std seed rlwe_key lwes len out
+//   pack-shards N beta digits std seed rlwe_key lwes len shards out   (PackSubtree per shard, PackMerge)
 //   evalfunc    N n beta digits seed lwe_key rlwe_key lwes(3 rows) lut out
 //   keygen-ss   variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed lwe_key rlwe_key out
 //   ss          variant N n br_beta br_digits tr_beta tr_digits sq_beta sq_digits std seed out_digits out_beta
@@ -142,6 +143,30 @@ static int run(int argc, char** argv) {
         std::vector<uint64_t> out(2ull * N);
         packer.Pack(out.data(), lwes.data(), u(argv[9]));
         save(argv[10], out.data(), out.size());
+        return 0;
+    }
+    if (mode == "pack-shards" && argc == 12) {
+        // shard r packs the inputs j W + s_r, s_r = (W - 1) ^ brv(r) over log2 W bits
+        const uint32_t N = (uint32_t)u(argv[2]), beta = (uint32_t)u(argv[3]), digits = (uint32_t)u(argv[4]);
+        Sampler rng(u(argv[6]));
+        const auto keys = keygen::PackingKeys(rng, N, beta, digits, std::atof(argv[5]), load(argv[7]));
+        GpuLWEtoRLWEPacker packer(N, 1ull << beta, digits, keys, 0);
+        const auto lwes = load(argv[8]);
+        const uint64_t len = u(argv[9]), W = u(argv[10]), m = len / W;
+        int w = 0, lm = 0;
+        while ((1ull << w) < W) ++w;
+        while ((1ull << lm) < m) ++lm;
+        std::vector<uint64_t> roots(W * 2ull * N), sub(m * (N + 1ull)), out(2ull * N);
+        for (uint64_t r = 0; r < W; ++r) {
+            uint64_t br = 0;
+            for (int b = 0; b < w; ++b) br |= ((r >> b) & 1) << (w - 1 - b);
+            const uint64_t s = (W - 1) ^ br;
+            for (uint64_t j = 0; j < m; ++j)
+                std::copy_n(lwes.data() + (j * W + s) * (N + 1ull), N + 1, sub.data() + j * (N + 1ull));
+            packer.PackSubtree(roots.data() + r * 2ull * N, sub.data(), m);
+        }
+        packer.PackMerge(out.data(), roots.data(), W, (uint32_t)lm, true);
+        save(argv[11], out.data(), out.size());
         return 0;
     }
     if (mode == "keygen-ss" && argc == 16) {

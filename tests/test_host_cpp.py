@@ -103,6 +103,19 @@ def test_cpp_packer_like_oracle(driver, oracle, cuda, tmp_path):
 
 
 @pytest.mark.gpu
+def test_cpp_sharded_pack_like_oracle(driver, oracle, cuda, tmp_path):
+    """PackSubtree on each of W shards, then PackMerge over their roots: the words of one Pack."""
+    N, beta, digits, std, length = 128, 16, 4, 3.2, 8
+    z = rlwe_secret(N, seed=63)
+    lwes = (sm64(64, length * (N + 1)) % np.uint64(0xFFFFFFFF00000001)).reshape(length, N + 1)
+    keys = oracle.pack_keygen(N, beta, digits, std, z, seed=19)
+    want = oracle.pack(N, beta, digits, keys, lwes, length)
+    for shards in (2, 4):
+        got = run(driver, tmp_path, "pack-shards", N, beta, digits, std, 19, z, lwes, length, shards)
+        assert np.array_equal(got, want), shards
+
+
+@pytest.mark.gpu
 def test_cpp_function_evaluator_like_oracle(driver, oracle, cuda, tmp_path):
     """GpuNegacyclicFunctionEvaluator: BlindRotate (coefficient output) + SampleExtract into a
     caller buffer whose words stay where the rotated A coefficient is 0, as in the reference."""
