@@ -5,26 +5,35 @@
 
 namespace tp {
 
-// L0Setup of every packing input (lwe_to_rlwe_packing.cpp:238-251), written in
-// the packing tree's element order: node c of pack p takes input
-// (len-1) ^ brv_{log len}(c) (lwe_to_rlwe_packing.cpp:143).
+// The two consecutive words k, k + 1 (k even) of a packing leaf, L0Setup
+// (lwe_to_rlwe_packing.cpp:238-251) of the LWE at `lwe`: A = (a0, -a_{N-1}, ..,
+// -a_1) and B = (b, 0, .., 0), times N^-1.
+__device__ __forceinline__ ulonglong2 pack_l0_pair(const uint64_t* __restrict__ lwe, uint64_t k, uint64_t N,
+                                                   uint64_t n_inv) {
+    uint64_t v0 = 0, v1 = 0;
+    if (k == 0) v0 = lwe[0];
+    else if (k < N) v0 = gl_neg(lwe[N - k]);
+    else if (k == N) v0 = lwe[N];
+    if (k + 1 < N) v1 = gl_neg(lwe[N - k - 1]);
+    return make_ulonglong2(gl_mul(v0, n_inv), gl_mul(v1, n_inv));
+}
+
+// L0Setup of every packing input, written in the packing tree's element order:
+// node c of pack p takes input (len-1) ^ brv_{log len}(c) (lwe_to_rlwe_packing.cpp:143).
+// Each thread writes 16-byte word pairs; N and len are powers of two, so the
+// indices are shifts and masks.
 __global__ void pack_l0_kernel(uint64_t* __restrict__ nodes, const uint64_t* __restrict__ in, uint64_t packs,
                                uint32_t len, uint32_t log_len, uint32_t logn, uint64_t n_inv) {
     const uint64_t N = 1ull << logn;
-    const uint64_t total = packs * len * 2 * N;
-    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
-         w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = w % (2 * N);
-        const uint64_t c = (w / (2 * N)) % len;
-        const uint64_t p = w / (2 * N * len);
-        const uint32_t src = (len - 1) ^ (log_len ? (__brev((uint32_t)c) >> (32 - log_len)) : 0u);
-        const uint64_t* lwe = in + (p * len + src) * (N + 1);
-        uint64_t v;
-        if (k == 0) v = lwe[0];
-        else if (k < N) v = gl_neg(lwe[N - k]);
-        else if (k == N) v = lwe[N];
-        else v = 0;
-        nodes[w] = gl_mul(v, n_inv);
+    const uint64_t pairs = (packs * len) << logn;  // 2N words per node
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < pairs;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = (q << 1) & (2 * N - 1);
+        const uint64_t node = q >> logn;
+        const uint32_t c = (uint32_t)(node & (len - 1));
+        const uint64_t p = node >> log_len;
+        const uint32_t src = (len - 1) ^ (log_len ? (__brev(c) >> (32 - log_len)) : 0u);
+        reinterpret_cast<ulonglong2*>(nodes)[q] = pack_l0_pair(in + (p * len + src) * (N + 1), k, N, n_inv);
     }
 }
 
@@ -34,19 +43,13 @@ __global__ void pack_l0_idx_kernel(uint64_t* __restrict__ nodes, const uint64_t*
                                    const uint32_t* __restrict__ src, uint64_t packs, uint32_t count, uint32_t len,
                                    uint32_t logn, uint64_t n_inv) {
     const uint64_t N = 1ull << logn;
-    const uint64_t total = (packs * count) << (logn + 1);
-    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
-         w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = w & (2 * N - 1);
-        const uint64_t node = w >> (logn + 1);
+    const uint64_t pairs = (packs * count) << logn;
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < pairs;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = (q << 1) & (2 * N - 1);
+        const uint64_t node = q >> logn;
         const uint64_t p = node / count, c = node - p * count;
-        const uint64_t* lwe = in + (p * len + src[c]) * (N + 1);
-        uint64_t v;
-        if (k == 0) v = lwe[0];
-        else if (k < N) v = gl_neg(lwe[N - k]);
-        else if (k == N) v = lwe[N];
-        else v = 0;
-        nodes[w] = gl_mul(v, n_inv);
+        reinterpret_cast<ulonglong2*>(nodes)[q] = pack_l0_pair(in + (p * len + src[c]) * (N + 1), k, N, n_inv);
     }
 }
 
