@@ -24,34 +24,42 @@ __device__ __forceinline__ uint64_t key_device_pos(uint64_t it, uint64_t r, uint
 }
 
 // Reference m_brk layout ((it*G + g)*rows + r)*2N + h*N + k  ->  device layout.
+// Words k, k + 1 (k even) stay neighbours in the device layout, so each thread
+// moves 16-byte pairs; the polynomial index is a shift, the small row and group
+// counts 32-bit divisions.
 __global__ void key_relayout_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
                                     uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge, uint32_t logs = 0) {
     const uint64_t N = 1ull << logn;
-    const uint64_t total = groups * G * rows * 2 * N;
-    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
-         w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = w % N;
-        const uint64_t h = (w / N) & 1;
-        const uint64_t r = (w / (2 * N)) % rows;
-        const uint64_t ig = w / (2 * N * rows);
-        const uint64_t g = ig % G, it = ig / G;
-        dst[key_device_pos(it, r, 2 * g + h, k, G, rows, logn, loge, logs)] = src[w];
+    const uint64_t pairs = (groups * G * rows) << logn;  // 2N words per (it, g, r)
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < pairs;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t w = q << 1;
+        const uint64_t k = w & (N - 1);
+        const uint64_t poly = w >> logn;                 // (ig * rows + r) * 2 + h
+        const uint32_t h = (uint32_t)(poly & 1);
+        const uint32_t rig = (uint32_t)(poly >> 1);      // ig * rows + r
+        const uint32_t r = rig % rows, ig = rig / rows;
+        const uint32_t g = ig % G, it = ig / G;
+        reinterpret_cast<ulonglong2*>(dst)[key_device_pos(it, r, 2 * g + h, k, G, rows, logn, loge, logs) >> 1] =
+            reinterpret_cast<const ulonglong2*>(src)[q];
     }
 }
 
-// Device layout for one coefficients-per-thread count -> another (same key).
+// Device layout for one coefficients-per-thread count -> another (same key),
+// 16-byte pairs as above.
 __global__ void key_retile_kernel(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t groups,
                                   uint32_t G, uint32_t rows, uint32_t logn, uint32_t loge_src, uint32_t loge_dst) {
     const uint64_t N = 1ull << logn;
-    const uint64_t total = groups * G * rows * 2 * N;
-    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total;
-         w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = w % N;
-        const uint64_t c = (w / N) % (2 * G);
-        const uint64_t r = (w / (2 * G * N)) % rows;
-        const uint64_t it = w / (2 * G * N * rows);
-        dst[key_device_pos(it, r, c, k, G, rows, logn, loge_dst)] =
-            src[key_device_pos(it, r, c, k, G, rows, logn, loge_src)];
+    const uint64_t pairs = (groups * G * rows) << logn;
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < pairs;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t w = q << 1;
+        const uint64_t k = w & (N - 1);
+        const uint32_t poly = (uint32_t)(w >> logn);     // (it * rows + r) * 2G + c
+        const uint32_t c = poly % (2 * G), rit = poly / (2 * G);
+        const uint32_t r = rit % rows, it = rit / rows;
+        reinterpret_cast<ulonglong2*>(dst)[key_device_pos(it, r, c, k, G, rows, logn, loge_dst) >> 1] =
+            reinterpret_cast<const ulonglong2*>(src)[key_device_pos(it, r, c, k, G, rows, logn, loge_src) >> 1];
     }
 }
 
