@@ -22,4 +22,8 @@ tp_status set_error(tp_status s, const char* fmt, ...);
 // (split 1, 2, 4); 0 when that kernel is not available for the context.
 uint64_t br_concurrency(const tp_br_ctx* c, int split);
 
+// CTAs (SMs) one rotation occupies with one block per rotation: 1, or the cluster
+// size of a ring above 4096.
+int br_cluster_ctas(const tp_br_ctx* c);
+
 }  // namespace tp

@@ -2469,6 +2469,8 @@ static tp_br_ctx::Form br_one_block(const tp_br_ctx* c) {
     return f;
 }
 
+int br_cluster_ctas(const tp_br_ctx* c) { return c ? 1 << c->logs : 1; }
+
 uint64_t br_concurrency(const tp_br_ctx* c, int split) {
     if (!c) return 0;
     if (split == 2) return c->loge == 2 ? (uint64_t)c->pair_cap : 0;

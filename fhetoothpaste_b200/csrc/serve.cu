@@ -156,7 +156,9 @@ void launch_pending(tp_server* srv, uint32_t si) {
         // other launches, so it is not used.
         const int split = tp::serve_split(take, busy, srv->sm_count, tp::br_concurrency(s.ctx, 4),
                                           tp::br_concurrency(s.ctx, 2));
-        b.blocks = (uint32_t)tp::serve_blocks(split, take, tp::br_concurrency(s.ctx, split));
+        // thread blocks (SMs) the launch keeps busy; a ring above 4096 takes a cluster per rotation
+        b.blocks = (uint32_t)(tp::serve_blocks(split, take, tp::br_concurrency(s.ctx, split)) *
+                              (split == 1 ? (uint64_t)tp::br_cluster_ctas(s.ctx) : 1u));
         tp_status st = e == cudaSuccess ? tp::br_batch_launch(s.ctx, take, b.d_res, b.d_lwe, lw, b.d_acc, aw,
                                                                s.out_coef, b.stream, split)
                                         : TP_ERR_CUDA;

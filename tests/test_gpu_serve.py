@@ -150,3 +150,33 @@ def test_poisson_load_generator_reports_latency(rotators):
     assert st["completed"] > 1000
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["p999_ms"] <= st["max_ms"]
     srv.close()
+
+
+def test_cluster_ring_set_in_the_mix(native, oracle):
+    """A set of ring size 8192 (one rotation per cluster of four CTAs) served beside a small set:
+    every request equals the oracle."""
+    from fhetoothpaste_b200 import BlindRotationContext, BootstrapServer, GpuBlindRotator
+    sets = [(1, 8192, 4, 12, 3), (0, 512, 20, 16, 4)]
+    rots, keys = [], []
+    for i, (v, N, n, bl, dg) in enumerate(sets):
+        brk = oracle.br_keygen(v, N, n, bl, dg, 3.2, lwe_secret(v, n, N, 70 + i), rlwe_secret(N, 80 + i), 90 + i)
+        rots.append(GpuBlindRotator(BlindRotationContext(v, N, n, 1 << bl, dg), brk))
+        keys.append(brk)
+    srv = BootstrapServer(max_queue=1000)
+    sids = [srv.add_set(r, max_batch=8, buffers=2, out_coef=True) for r in rots]
+    srv.start()
+    reqs = []
+    for k in range(24):
+        s = k % 2
+        v, N, n, bl, dg = sets[s]
+        req = (s, lwe_inputs(N, n, 1, 3000 + k)[0], random_acc(N, 1, 4000 + k)[0], np.zeros(2 * N, np.uint64))
+        reqs.append((req, srv.submit(sids[s], req[1], req[2], req[3])))
+    for _, t in reqs:
+        srv.wait(t)
+    for (s, lwe, acc, res), _ in reqs[:6]:
+        v, N, n, bl, dg = sets[s]
+        np.testing.assert_array_equal(res, oracle.blind_rotate(v, N, n, bl, dg, keys[s], lwe, acc, 1))
+    srv.drain()
+    srv.close()
+    for r in rots:
+        r.close()
