@@ -303,6 +303,36 @@ def bmmp_batch_sweep(device: int) -> dict:
     return out
 
 
+LARGE_RINGS = ((8192, 4), (16384, 8), (32768, 16), (65536, 16))  # (N, CTAs per rotation)
+
+
+def large_ring_run(device: int) -> dict:
+    """CGGI ternary rotations (base 2^12, l = 3, n = 64) at the ring sizes that run one rotation
+    per cluster of CTAs, two waves of the resident clusters each (uniform key words; the
+    parity of these sizes is in tests/test_gpu_largen.py)."""
+    import torch
+    from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
+    from oracle.oracle import lwe_inputs
+    n = 64
+    out = {"workload": "CGGI ternary, base 2^12 l=3, n=64, one rotation per cluster", "unit": "BR/s"}
+    stream = torch.cuda.current_stream().cuda_stream
+    for N, ctas in LARGE_RINGS:
+        ctx = BlindRotationContext(1, N, n, 1 << 12, 3)
+        rot = GpuBlindRotator(ctx, _uniform_key(ctx.key_words(), 41), device=device)
+        batch = 2 * (torch.cuda.get_device_properties(device).multi_processor_count // ctas)
+        lw = torch.from_numpy(lwe_inputs(N, n, batch, 43).view(np.int64)).cuda()
+        ac = torch.from_numpy(lut_polys(N, batch, 44).view(np.int64)).cuda()
+        res = torch.empty((batch, 2 * N), dtype=torch.int64, device="cuda")
+        ms = _timed(torch, lambda: rot.blind_rotate_batch(res.data_ptr(), lw.data_ptr(), n + 1, ac.data_ptr(),
+                                                          2 * N, batch, stream=stream), 1, 3, stream)
+        rot.check(stream)
+        out[str(N)] = {"BR_per_s": round(batch / (ms * 1e-3), 1), "batch": batch, "ms_per_launch": round(ms, 3),
+                       "ctas_per_rotation": ctas}
+        rot.close()
+        del lw, ac, res
+    return out
+
+
 def packing_run(device: int) -> dict:
     """Config-4 key switching: 2048 LWEs (n = N = 2048) packed into one RLWE with the
     11 automorphism keys (base 2^16, l = 4), 64 packings per launch; then RLWE->RLWE
@@ -651,6 +681,7 @@ def main():
         line["bootstrap"] = bootstrap_run(local)
         line["scheme_switch"] = scheme_switch_run(local)
         line["sap"] = sap_run(local)
+        line["large_rings"] = large_ring_run(local)
     line["gpu_launches_detail"] = {"timed_region": int(timed_launches), "e2e_timed_region": int(e2e_launches),
                                    "counted_by": "tp_kernel_launches() deltas (graph replays count their kernels)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
