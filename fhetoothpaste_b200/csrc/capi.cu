@@ -288,7 +288,7 @@ static tp_status br_setup_cluster(tp_br_ctx* c) {
         int capd = 0;
         if (probe(kd, sd, &capd)) {
             // selectable, not the default: on a cluster the row-by-row form measured faster at
-            // N = 8192 (ternary n = 1024: 670 vs 600 rotations/s; N = 32768: 185 vs 193)
+            // N = 8192 (ternary n = 1024: 670 vs 600 rotations/s)
             c->ds_kernel = kd;
             c->ds_smem = sd;
             c->ds_cap = capd;

@@ -10,6 +10,8 @@
 
 namespace tp {
 
+static_assert(br_cluster_logs(16) == 4, "cluster size of this unit");
+
 const void* br_kernel_ptr_16(int variant, int loge, int dl, bool r4) {
     if (r4 || loge != 2 || dl != 0) return nullptr;
     switch (variant) {

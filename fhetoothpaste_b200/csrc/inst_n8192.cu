@@ -9,6 +9,8 @@
 
 namespace tp {
 
+static_assert(br_cluster_logs(13) == 2, "cluster size of this unit");
+
 const void* br_kernel_ptr_13(int variant, int loge, int dl, bool r4) {
     if (r4) return nullptr;  // fused radix-4 rotation kernels are built for N = 1024 .. 4096
     if (loge != 2 || (dl != 0 && dl != 3 && dl != 4)) return nullptr;

@@ -9,9 +9,9 @@
  * Arithmetic is over the Goldilocks prime p = 2^64 - 2^32 + 1. All ciphertext
  * words are canonical residues in [0, p); polynomials have N coefficients with
  * N a power of two in [128, 65536]; above 4096 one rotation, key switch or
- * transform runs on a cluster of 4, 8 or 16 CTAs (N = 8192, 16384, 32768 and
- * 65536; 4096 coefficients per CTA at 65536) that exchange through distributed
- * shared memory. "NTT domain" means the reference's
+ * transform runs on a cluster of CTAs that exchange through distributed shared
+ * memory: 4 CTAs of 2048 coefficients at N = 8192, 4, 8 and 16 CTAs of 4096 at
+ * N = 16384, 32768 and 65536. "NTT domain" means the reference's
  * evaluation order: slot k holds a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N)
  * (lib/src/backend/solinas.cpp:168-313 of the reference).
  *
@@ -131,7 +131,7 @@ uint32_t tp_br_get_split(const tp_br_ctx* ctx);
  * a time (the next key row staged in shared memory while the digit is transformed);
  * TP_MAC_DIGIT_STAGED transforms all 2l digits first and sums each output word over
  * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048 and on the
- * CTA clusters of N = 8192..32768 where shared memory allows (not at 65536); the default up to
+ * CTA clusters of N = 8192 where shared memory allows; the default up to
  * N = 2048). Both give the same words. Project-specific tuning (no
  * reference counterpart); tp_br_autotune chooses between them. */
 enum { TP_MAC_ROWWISE = 0, TP_MAC_DIGIT_STAGED = 1 };

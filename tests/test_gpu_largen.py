@@ -55,7 +55,7 @@ def test_large_ring_matches_reference(native, oracle, name):
 @pytest.mark.parametrize("N", [32768, 65536])
 @pytest.mark.parametrize("v,bl,dg", [(CGGI_TERNARY, 12, 3), (CGGI_BINARY, 16, 4), (BMMP_BINARY, 16, 4)])
 def test_largest_rings_match_oracle(native, oracle, v, bl, dg, N):
-    """N = 32768 (16 CTAs of 2048 coefficients) and 65536 (16 CTAs of 4096), where the
+    """N = 32768 (8 CTAs of 4096 coefficients) and 65536 (16 CTAs of 4096), where the
     reference's rotators cannot build their N (N + 2)-word monomial table: the oracle,
     pinned to the reference at 8192 and 16384."""
     n = 4 if N == 32768 else 2
@@ -103,7 +103,7 @@ KS_CASES = json.loads(GOLDEN.read_text())["ks"]
 @pytest.mark.parametrize("name", sorted(KS_CASES))
 def test_large_ring_key_switching_matches_reference(native, oracle, name):
     """RLWEtoRLWEConverter::Convert, AutomorphismEvaluator::Eval and LWEtoRLWEPacker::Pack at
-    N = 8192 .. 32768 (one item per cluster of 4, 8 or 16 CTAs) against the reference's outputs."""
+    N = 8192 .. 65536 (one item per cluster of 4, 8 or 16 CTAs) against the reference's outputs."""
     from kscases import ks_inputs, ks_key
     from fhetoothpaste_b200 import GpuAutomorphismEvaluator, GpuLWEtoRLWEPacker, GpuRLWEtoRLWEConverter
     c = KS_CASES[name]
