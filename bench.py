@@ -303,7 +303,7 @@ def bmmp_batch_sweep(device: int) -> dict:
     return out
 
 
-LARGE_RINGS = ((8192, 4), (16384, 4), (32768, 8), (65536, 16))  # (N, CTAs per rotation)
+LARGE_RINGS = ((8192, 2), (16384, 4), (32768, 8), (65536, 16))  # (N, CTAs per rotation)
 
 
 def large_ring_run(device: int) -> dict:

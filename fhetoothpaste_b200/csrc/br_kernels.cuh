@@ -109,18 +109,15 @@ __host__ __device__ constexpr bool br_table_passes(int variant, bool digit_stage
 // slower (ternary N = 4096: 1856 vs 1977 rotations/s; the spills cost more), and
 // so did staging part of each row there (two components, the rest read from L2
 // at use: ternary 1918 vs 1978; BMMP 2939 vs 2889, within run-to-run spread).
-// Ring sizes above 4096 rotate on a cluster of 2^logs CTAs, each holding
-// 2^(logn - logs) coefficients and slots (cluster_ntt.cuh): 2048 for N = 8192 (4 CTAs),
-// 4096 for N = 16384, 32768 and 65536 (4, 8 and 16 CTAs). Fewer, larger CTAs measured
-// faster than 2048 per CTA (rotations/s, n = 64: ternary N = 16384 5201 vs 4918 on 8 CTAs,
-// N = 32768 2167 vs 1823 on 16, binary N = 16384 4819 vs 4315): the GPU keeps more SMs busy
-// with small clusters (32 of 4 CTAs, 15 of 8, 7 of 16 resident) and a transform exchanges
-// with fewer CTAs, which outweighs the 4096-coefficient plan's register spills. Every plan
-// below is per CTA, in words of its local size, plus two receive areas of the distributed
-// transform's exchange.
-__host__ __device__ constexpr int br_cluster_logs(int logn) {
-    return logn > 12 ? (logn - 12 < 2 ? 2 : logn - 12) : 0;
-}
+// Ring sizes above 4096 rotate on a cluster of 2^logs CTAs of 4096 coefficients and
+// slots each (cluster_ntt.cuh): 2, 4, 8 and 16 CTAs for N = 8192 .. 65536. Fewer, larger
+// CTAs measured faster than 2048 per CTA (rotations/s, n = 64: ternary N = 16384 5201 vs
+// 4918 on 8 CTAs, N = 32768 2167 vs 1823 on 16, binary N = 16384 4819 vs 4315): the GPU
+// keeps more SMs busy with small clusters (32 of 4 CTAs, 15 of 8, 7 of 16 resident) and a
+// transform exchanges with fewer CTAs, which outweighs the 4096-coefficient plan's register
+// spills. Every plan below is per CTA, in words of its local size, plus two receive areas
+// of the distributed transform's exchange.
+__host__ __device__ constexpr int br_cluster_logs(int logn) { return logn > 12 ? logn - 12 : 0; }
 
 __host__ __device__ constexpr size_t br_base_words(int logn, int variant, int loge, int logs = 0, bool r4 = false) {
     return (size_t)(br_smem_twiddles(logn - logs)

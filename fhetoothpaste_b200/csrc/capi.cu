@@ -287,8 +287,9 @@ static tp_status br_setup_cluster(tp_br_ctx* c) {
             tp::br_smem_words(c->logn, c->prm.variant, c->prm.lwe_dim, 2, (int)c->prm.digits, c->logs) * 8;
         int capd = 0;
         if (probe(kd, sd, &capd)) {
-            // selectable, not the default: on a cluster the row-by-row form measured faster at
-            // N = 8192 (ternary n = 1024: 670 vs 600 rotations/s)
+            // selectable, not the default (with 2048 coefficients per CTA the row-by-row form
+            // measured faster on a cluster: N = 8192, ternary n = 1024, 670 vs 600 rotations/s);
+            // the clusters of 4096 coefficients per CTA built now have no digit-staged kernel
             c->ds_kernel = kd;
             c->ds_smem = sd;
             c->ds_cap = capd;

@@ -1,7 +1,7 @@
 // Negacyclic NTT of one polynomial of N = 2^LOGN coefficients spread over a
-// cluster of S = 2^LOGS CTAs (N > 4096: one CTA's shared memory cannot hold a
-// rotation at that size). 4 coefficients per thread, T = N / (4 S) threads per
-// CTA; the local size NL = N / S.
+// cluster of S = 2^LOGS CTAs, S = 2 .. 16 (N > 4096: one CTA's shared memory
+// cannot hold a rotation at that size). 4 coefficients per thread, T = N / (4 S)
+// threads per CTA; the local size NL = N / S.
 //
 // Layouts (CTA rank r of the cluster):
 //   coefficient layout: CTA r holds the coefficients i = i' S + r (the
@@ -45,8 +45,9 @@ struct ClusterShape {
     static constexpr int NL = 1 << LOGL;
     static constexpr int T = NL / 4;
     static constexpr int G = NL / S;  // slot groups owned per CTA
-    static_assert(LOGS >= 2 && LOGS <= 4, "clusters of 4, 8 or 16 CTAs");
-    static_assert(G % 4 == 0 && G <= T, "a thread's four local slots belong to one group owner");
+    static_assert(LOGS >= 1 && LOGS <= 4, "clusters of 2, 4, 8 or 16 CTAs");
+    static_assert(LOGS == 1 ? G == 2 * T : (G % 4 == 0 && G <= T),
+                  "a thread's four local slots belong to one group owner");
 };
 
 // Group levels of the forward transform on the S positions of group g (global
@@ -107,7 +108,19 @@ __device__ __forceinline__ void cluster_fwd_tail(uint64_t (&x)[4], int t, int r,
     reinterpret_cast<ulonglong2*>(dst)[0] = make_ulonglong2(x[0], x[1]);
     reinterpret_cast<ulonglong2*>(dst)[1] = make_ulonglong2(x[2], x[3]);
     cluster.sync();
-    if constexpr (CS::S == 4) {
+    if constexpr (CS::S == 2) {
+        // G = 2T: thread t owns groups g = r G + 2t and g + 1, whose two positions each
+        // are its four slots (one butterfly per group, twiddle tw[NL + g])
+        const ulonglong2 p0 = *reinterpret_cast<const ulonglong2*>(recv + 2 * t);          // position 0
+        const ulonglong2 p1 = *reinterpret_cast<const ulonglong2*>(recv + CS::G + 2 * t);  // position 1
+        const uint32_t g = (uint32_t)(r * CS::G + 2 * t);
+        const uint64_t v0 = gl_mul(p1.x, __ldg(tw + CS::NL + g));
+        const uint64_t v1 = gl_mul(p1.y, __ldg(tw + CS::NL + g + 1));
+        x[0] = LAZY ? gl_add_lazy(p0.x, v0) : gl_add(p0.x, v0);
+        x[1] = gl_sub(p0.x, v0);
+        x[2] = LAZY ? gl_add_lazy(p0.y, v1) : gl_add(p0.y, v1);
+        x[3] = gl_sub(p0.y, v1);
+    } else if constexpr (CS::S == 4) {
         // G = T: thread t owns group r G + t, whose slots are its own four
 #pragma unroll
         for (int c = 0; c < 4; ++c) x[c] = recv[c * CS::G + t];
@@ -143,7 +156,15 @@ __device__ __forceinline__ void cluster_inv_head(uint64_t (&x)[4], int t, int r,
     using CS = ClusterShape<LOGN, LOGS>;
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    if constexpr (CS::S == 4) {
+    if constexpr (CS::S == 2) {
+        // groups g = r G + 2t (slots x0, x1) and g + 1 (x2, x3); position c of each goes
+        // to CTA c as its local slot g, g + 1
+        const uint32_t g = (uint32_t)(r * CS::G + 2 * t);
+        const uint64_t a0 = gl_add(x[0], x[1]), b0 = gl_mul(gl_sub(x[0], x[1]), __ldg(tw + CS::NL + g));
+        const uint64_t a1 = gl_add(x[2], x[3]), b1 = gl_mul(gl_sub(x[2], x[3]), __ldg(tw + CS::NL + g + 1));
+        *reinterpret_cast<ulonglong2*>(cluster.map_shared_rank(recv, 0) + g) = make_ulonglong2(a0, a1);
+        *reinterpret_cast<ulonglong2*>(cluster.map_shared_rank(recv, 1) + g) = make_ulonglong2(b0, b1);
+    } else if constexpr (CS::S == 4) {
         const uint32_t g = (uint32_t)(r * CS::G + t);
         cluster_group_inv<LOGN, LOGS>(reinterpret_cast<uint64_t(&)[4]>(x), g, tw);
         // position g S + c goes to CTA c as its local slot g

@@ -10,8 +10,8 @@
  * words are canonical residues in [0, p); polynomials have N coefficients with
  * N a power of two in [128, 65536]; above 4096 one rotation, key switch or
  * transform runs on a cluster of CTAs that exchange through distributed shared
- * memory: 4 CTAs of 2048 coefficients at N = 8192, 4, 8 and 16 CTAs of 4096 at
- * N = 16384, 32768 and 65536. "NTT domain" means the reference's
+ * memory: 2, 4, 8 and 16 CTAs of 4096 coefficients at N = 8192, 16384, 32768 and
+ * 65536. "NTT domain" means the reference's
  * evaluation order: slot k holds a(psi^(2*brv(k)+1)), psi = 7^((p-1)/2N)
  * (lib/src/backend/solinas.cpp:168-313 of the reference).
  *
@@ -130,9 +130,8 @@ uint32_t tp_br_get_split(const tp_br_ctx* ctx);
  * TP_MAC_ROWWISE keeps a canonical running sum per output word, one gadget row at
  * a time (the next key row staged in shared memory while the digit is transformed);
  * TP_MAC_DIGIT_STAGED transforms all 2l digits first and sums each output word over
- * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048 and on the
- * CTA clusters of N = 8192 where shared memory allows; the default up to
- * N = 2048). Both give the same words. Project-specific tuning (no
+ * the 2l rows exactly before one reduction (digits 3 or 4, N <= 2048, one CTA per
+ * rotation, where shared memory allows; the default there). Both give the same words. Project-specific tuning (no
  * reference counterpart); tp_br_autotune chooses between them. */
 enum { TP_MAC_ROWWISE = 0, TP_MAC_DIGIT_STAGED = 1 };
 tp_status tp_br_set_mac_form(tp_br_ctx* ctx, uint32_t form);

@@ -1,4 +1,4 @@
-"""Blind rotation at ring sizes above 4096 on the GPU: one rotation per cluster of 4, 8 or 16
+"""Blind rotation at ring sizes above 4096 on the GPU: one rotation per cluster of 2, 4, 8 or 16
 CTAs with the transforms distributed over distributed shared memory (csrc/cluster_ntt.cuh).
 Bit-exact against the reference library's outputs (tests/golden/largen.json, N = 8192 and
 16384: SHA-256 of every output word) and against the C oracle (pinned to those outputs by
@@ -103,7 +103,7 @@ KS_CASES = json.loads(GOLDEN.read_text())["ks"]
 @pytest.mark.parametrize("name", sorted(KS_CASES))
 def test_large_ring_key_switching_matches_reference(native, oracle, name):
     """RLWEtoRLWEConverter::Convert, AutomorphismEvaluator::Eval and LWEtoRLWEPacker::Pack at
-    N = 8192 .. 65536 (one item per cluster of 4, 8 or 16 CTAs) against the reference's outputs."""
+    N = 8192 .. 65536 (one item per cluster of 2, 4, 8 or 16 CTAs) against the reference's outputs."""
     from kscases import ks_inputs, ks_key
     from fhetoothpaste_b200 import GpuAutomorphismEvaluator, GpuLWEtoRLWEPacker, GpuRLWEtoRLWEConverter
     c = KS_CASES[name]
