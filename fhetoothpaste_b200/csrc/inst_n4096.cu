@@ -10,7 +10,7 @@ namespace tp {
 
 const void* br_kernel_ptr_12(int variant, int loge, int dl, bool r4) {
     if (r4) {  // fused radix-4 passes, 4 coefficients per thread
-        if (loge != 2 || !dl == 0) return nullptr;
+        if (loge != 2 || dl != 0) return nullptr;
         if (variant == kCggiBinary) return (const void*)br_kernel<12, kCggiBinary, 2, 0, 0, true>;
         if (variant == kCggiTernary) return (const void*)br_kernel<12, kCggiTernary, 2, 0, 0, true>;
         if (variant == kBmmpBinary) return (const void*)br_kernel<12, kBmmpBinary, 2, 0, 0, true>;
