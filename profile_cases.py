@@ -62,6 +62,11 @@ def case_br_ternary_n4096(torch):
     _rotation(torch, 1, 4096, 32, 12, 3, 148)
 
 
+def case_br_ternary_n8192(torch):
+    """br_kernel on two-CTA clusters, CGGI ternary N=8192 base 2^12 l=3, n reduced to 32, one wave (74)."""
+    _rotation(torch, 1, 8192, 32, 12, 3, 74)
+
+
 def case_br_pair_ternary_n2048(torch):
     """br_pair_kernel (two blocks per rotation), CGGI ternary N=2048 l=3, n reduced to 64, batch 37."""
     from fhetoothpaste_b200 import BlindRotationContext, GpuBlindRotator
