@@ -13,7 +13,7 @@ LIMIT_WORDS = 227 * 1024 // 8
 
 
 @pytest.fixture(scope="module")
-def plans():
+def driver_output():
     if shutil.which("nvcc") is None:
         pytest.skip("nvcc not on PATH")
     out_dir = ROOT / "tests" / "_build"  # git-ignored build folder
@@ -22,12 +22,29 @@ def plans():
     subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O1",
                     f"-I{ROOT / 'include'}", f"-I{ROOT / 'fhetoothpaste_b200' / 'csrc'}",
                     str(ROOT / "tests" / "cpp" / "smem_plan_driver.cu"), "-o", str(exe)], check=True)
-    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    return subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+
+
+@pytest.fixture(scope="module")
+def plans(driver_output):
     rows = {}
-    for line in out.splitlines():
+    for line in driver_output:
+        if line.startswith("C "):
+            continue
         logn, v, one, pair, qfits, quad, qxb, ppf, qpf = map(int, line.split())
         rows[(logn, v)] = dict(one=one, pair=pair, quad_fits=qfits, quad=quad, quad_xbufs=qxb)
     assert len(rows) == 18
+    return rows
+
+
+@pytest.fixture(scope="module")
+def cluster_plans(driver_output):
+    rows = {}
+    for line in driver_output:
+        if line.startswith("C "):
+            logn, v, logs, one, ks = map(int, line.split()[1:])
+            rows[(logn, v)] = dict(logs=logs, one=one, ks=ks)
+    assert len(rows) == 12
     return rows
 
 
@@ -44,3 +61,12 @@ def test_four_block_kernel_sets(plans):
     assert refused == {(12, 2)}
     single = {k for k, r in plans.items() if r["quad_fits"] and r["quad_xbufs"] == 1}
     assert single == {(12, 1)}
+
+
+def test_cluster_plans(cluster_plans):
+    """Rings above 4096: 2, 4, 8, 16 CTAs of 4096 coefficients for N = 8192 .. 65536, and every
+    per-CTA plan (rotation with a 1023-word LWE, key switching) fits one SM."""
+    for (logn, v), r in cluster_plans.items():
+        assert r["logs"] == logn - 12, (logn, v)
+        assert r["one"] <= LIMIT_WORDS, (logn, v)
+        assert r["ks"] <= LIMIT_WORDS, (logn, v)
