@@ -670,7 +670,7 @@ def main():
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "clocks": clk.summary(),
         "launch": {"form": "CUDA graph, one kernel per step", "coef_per_thread": rot.tile,
-                   "blocks_per_rotation": rot.split, "mac_form": rot.mac_form,
+                   "blocks_per_rotation": rot.split, "mac_form": rot.mac_form, "radix": rot.radix,
                    "key": "uniform random key words (timing does not depend on key values)"},
     }
     if rank == 0 and world == 1 and not args.no_serving:
