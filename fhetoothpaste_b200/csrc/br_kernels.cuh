@@ -145,19 +145,14 @@ __host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int lo
 // Measured (rotations/s, full waves, N = 2048): CGGI ternary 8185 (ring, 5 ahead),
 // 7850 (8), 7274 (11), 7911 (groups); BMMP 9212 (groups) against 6204 and 6020
 // for rings of 5 and 8; CGGI binary N = 1024 about equal (20.35k to 20.55k).
-// Re-measured on the current kernel: CGGI ternary 8695 (5 ahead), 7799 (4), 8817 (6),
-// 8340 (7), 8236 (8), with the fused radix-4 passes 8884 at 6; binary N = 1024
-// 21.59k (5), 21.53k (6).
-__host__ __device__ constexpr int br_ds_ahead(int variant) {
-    return variant == kBmmpBinary ? 0 : (variant == kCggiTernary ? 6 : 5);
-}
-
-// The NTT radix a context starts with for the digit-staged one-block kernel: the fused
-// radix-4 passes where they measured faster (CGGI ternary N = 2048, l = 3: 8884 against
-// 8817 rotations/s), radix 2 elsewhere (binary N = 1024: 18.2k against 21.6k).
-__host__ __device__ constexpr bool br_ds_radix4_default(int logn, int variant, int dl) {
-    return variant == kCggiTernary && logn == 11 && dl == 3;
-}
+// Re-measured on the current kernel: CGGI ternary 9089 (groups), 8695 (ring, 5 ahead),
+// 7799 (4), 8817 (6), 8340 (7), 8236 (8), with the fused radix-4 passes 8858 (groups),
+// 8884 (6); binary N = 1024 21.55k (5), 21.50k (4), 21.49k (6), 21.39k (groups); BMMP
+// 9546 (groups), 6174 (4), 6313 (6).
+__host__ __device__ constexpr int br_ds_ahead(int variant) { return variant == kCggiBinary ? 5 : 0; }
+// Contexts start with radix-2 passes: with the digit-staged sums the fused radix-4 form
+// measured slower (CGGI ternary N = 2048, l = 3: 8858 against 9089 rotations/s; binary
+// N = 1024: 18.2k against 21.6k); tp_br_set_radix and the autotuner still offer it.
 
 __host__ __device__ constexpr size_t br_digit_stage_words(int logn, int dl) {
     return dl > 0 ? (size_t)(2 * dl - 1) << logn : 0;

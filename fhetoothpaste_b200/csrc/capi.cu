@@ -461,8 +461,6 @@ tp_status tp_br_create(const tp_br_params* p, int device, tp_br_ctx** out) {
             cudaGetLastError();
         }
     }
-    if (c->mac == TP_MAC_DIGIT_STAGED && c->r4_ds.k && tp::br_ds_radix4_default(c->logn, p->variant, (int)p->digits))
-        c->radix = 4;
     for (int split = 2; split <= 4; split += 2) {
         // two- and four-CTA cluster kernels; optional: a parameter set one does not fit keeps its cap 0
         const void* k = tp::br_pair_kernel_lookup(c->logn, p->variant, split);
