@@ -93,7 +93,8 @@ __host__ __device__ constexpr bool br_fused_radix4(int loge, int variant, int bl
 // pow2_block_pass) in every rotation kernel but the digit-staged CGGI ternary one
 // at 2048 coefficients per CTA, where the same change measured slower although it
 // spills no more (rotations/s, 4096 rotations, n = 630: 8695 on table twiddles,
-// 8523 with both directions shifted, 8355 forward only, 7449 backward only). In
+// 8523 with both directions shifted, 8355 forward only, 7449 backward only; with its
+// key loads grouped, 9085 on table twiddles against 8780 shifted). In
 // the others it measured faster: CGGI binary N = 1024 digit-staged 20.58k ->
 // 21.58k, row by row 19.38k -> 20.00k; CGGI ternary N = 2048 row by row 7861 ->
 // 8014; BMMP N = 2048 9487 -> 9541; CGGI ternary N = 4096 2358 -> 2431.
