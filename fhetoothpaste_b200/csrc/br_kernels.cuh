@@ -149,8 +149,11 @@ __host__ __device__ constexpr bool br_key_prefetch(int logn, int variant, int lo
 // Re-measured on the current kernel: CGGI ternary 9089 (groups), 8695 (ring, 5 ahead),
 // 7799 (4), 8817 (6), 8340 (7), 8236 (8), with the fused radix-4 passes 8858 (groups),
 // 8884 (6); binary N = 1024 21.55k (5), 21.50k (4), 21.49k (6), 21.39k (groups); BMMP
-// 9546 (groups), 6174 (4), 6313 (6).
-__host__ __device__ constexpr int br_ds_ahead(int variant) { return variant == kCggiBinary ? 5 : 0; }
+// 9546 (groups), 6174 (4), 6313 (6); CGGI ternary N = 1024 24.76k (5) against 24.63k
+// (groups), N = 512 49.87k either way.
+__host__ __device__ constexpr int br_ds_ahead(int variant, int logl) {
+    return variant == kBmmpBinary ? 0 : (variant == kCggiTernary && logl >= 11 ? 0 : 5);
+}
 // Contexts start with radix-2 passes: with the digit-staged sums the fused radix-4 form
 // measured slower (CGGI ternary N = 2048, l = 3: 8858 against 9089 rotations/s; binary
 // N = 1024: 18.2k against 21.6k); tp_br_set_radix and the autotuner still offer it.
@@ -514,7 +517,7 @@ br_kernel(const BrKernelParams prm) {
                 // ((c*E/2 + jp)*T + t)*2 of that row. The loads run ahead of their use in one
                 // of two schedules (br_ds_ahead).
                 constexpr int R2 = 2 * (DL > 0 ? DL : 1);
-                constexpr int AH = br_ds_ahead(VARIANT);
+                constexpr int AH = br_ds_ahead(VARIANT, LOGL);
                 auto kaddr = [&](int jp, int c, int r) {
                     return reinterpret_cast<const ulonglong2*>(kit + (uint64_t)r * (N * C) +
                                                                ((c * (E / 2) + jp) * T + t) * 2);
