@@ -202,7 +202,9 @@ __device__ __forceinline__ uint64_t mono(const uint64_t* __restrict__ psi_pow, u
 // variant and ring size (rotations/s, full waves: ternary N = 2048 7286 vs
 // 6798, BMMP N = 2048 7658 vs 7099, binary N = 1024 18786 vs 17168, ternary
 // N = 4096 2188 vs 1874): twice the warps per SM hide the integer pipes'
-// dependency latency that 8 per thread left exposed.
+// dependency latency that 8 per thread left exposed. Re-measured on the current
+// kernels at N = 4096 (rotations/s): ternary 2432 vs 1789, binary 4132 vs 4033,
+// BMMP 2818 vs 2091.
 __host__ __device__ constexpr int br_default_loge(int logn, int variant) {
     return (void)logn, (void)variant, 2;
 }
